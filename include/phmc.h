@@ -1,0 +1,234 @@
+/*
+ * phmc.h — C ABI of the B200-native constant-pH Monte Carlo energy engine.
+ *
+ * The engine replaces the energy and move layer of the ph_brush MC program
+ * (reference: MC/include/energy.hpp, MC/include/pme.hpp, MC/include/neighbor.hpp,
+ * MC/include/mc.hpp).  Every entry point returns an int status (PHMC_OK == 0),
+ * never throws, and records a message retrievable with phmc_last_error().
+ * The engine owns all device memory; callers own host buffers.  One engine is
+ * driven by one host thread; engines are independent of each other.
+ *
+ * Units follow the reference: Coulomb prefactor ke/epsilon_r with
+ * ke = 138.935458 (MC/src/pme.cu:305).  Reduced units are obtained with
+ * beta = 1 and epsilon_r = 138.935458 / l_B.
+ *
+ * An engine holds R >= 1 independent replicas (same kernels; one replica is
+ * the plain engine, many replicas are the batched titration sweep).
+ */
+#ifndef PHMC_H
+#define PHMC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHMC_ABI_VERSION 1
+
+/* ---- status codes ---- */
+enum {
+    PHMC_OK = 0,
+    PHMC_ERR_ARG = 1,         /* invalid argument / inconsistent input */
+    PHMC_ERR_CUDA = 2,        /* CUDA runtime error (message has details) */
+    PHMC_ERR_CAPACITY = 3,    /* a fixed capacity (cell, slot, pending) was exceeded */
+    PHMC_ERR_BUDGET = 4,      /* a bounded device loop gave up (iteration budget) */
+    PHMC_ERR_STATE = 5,       /* engine in a state that forbids the call */
+    PHMC_ERR_UNSUPPORTED = 6, /* feature combination not implemented */
+    PHMC_ERR_IO = 7           /* file could not be read / parsed */
+};
+
+/* ---- Coulomb kinds (reference: Params::coulombtype, MC/include/types.hpp:42) ---- */
+enum { PHMC_COUL_NONE = 0, PHMC_COUL_CUT = 1, PHMC_COUL_EWALD = 2 };
+
+/* ---- particle flags ---- */
+#define PHMC_F_MOBILE     0x01 /* may be displaced */
+#define PHMC_F_TITRATABLE 0x02 /* protonation site (weak base) */
+#define PHMC_F_GHOST      0x04 /* empty slot: not present, interacts with nothing */
+#define PHMC_F_CATION     0x08 /* mobile salt cation (reservoir swaps) */
+#define PHMC_F_ANION      0x10 /* mobile anion (counterion / salt anion) */
+
+/* ---- move kinds ---- */
+enum { PHMC_MOVE_DISP = 0, PHMC_MOVE_TITR = 1, PHMC_MOVE_SWAP = 2, PHMC_MOVE_NONE = 3 };
+
+/*
+ * One replica's particle system, host arrays.  Slots [0, n_particles) hold
+ * the initial particles; slots [n_particles, capacity) are empty (ghost) and
+ * receive inserted ions.  Bonds are 1-2 pairs of 0-based slot indices
+ * (reference: System::bonds, MC/include/types.hpp:18-28).
+ */
+typedef struct phmc_system {
+    int n_particles;
+    int capacity;
+    const float* x;
+    const float* y;
+    const float* z;
+    const float* q;
+    const int* type;   /* 0-based type ids */
+    const int* flags;  /* PHMC_F_* */
+    int n_bonds;
+    const int* bond_i;
+    const int* bond_j;
+    double box[3];     /* Lx, Ly, Lz (Lz already padded when the slab correction is on) */
+} phmc_system;
+
+/*
+ * Interaction model, move set and engine tuning for one replica.
+ * Reference-compatible energies: lj_rc = NULL and rc_lj = rc_coul (single
+ * shared cutoff, MC/src/neighbor.cu:97), excl_bonded_lj = excl_bonded_coul = 1
+ * (MC/src/neighbor.cu:17-19), order 4, ref_moduli = 1.
+ */
+typedef struct phmc_params {
+    int n_types;
+    const double* lj_eps;  /* n_types*n_types, row-major, symmetric */
+    const double* lj_sig;  /* n_types*n_types */
+    const double* lj_rc;   /* n_types*n_types per-pair cutoff, or NULL: rc_lj for all */
+    double rc_lj;
+    int lj_shift;          /* shift LJ to zero at its cutoff (MC/src/io.cpp:270-281) */
+    int coulomb;           /* PHMC_COUL_* */
+    double rc_coul;
+    double epsilon_r;
+    double ewald_alpha;    /* > 0 for PHMC_COUL_EWALD */
+    int mesh[3];           /* SPME mesh nx, ny, nz */
+    int order;             /* B-spline order p (points per dimension), 4..8 */
+    int ref_moduli;        /* 1: reference moduli exactly (MC/src/pme.cu:77-113); 0: zero-modulus interpolation */
+    int slab;              /* Yeh-Berkowitz + net-charge slab term (MC/src/pme.cu:434-447) */
+    int excl_bonded_lj;    /* exclude 1-2 pairs from LJ */
+    int excl_bonded_coul;  /* exclude 1-2 pairs from real-space Coulomb */
+    double fene_k, fene_r0;  /* FENE bonds; fene_k == 0 disables */
+    double wall_lo, wall_hi; /* hard walls in z; wall_hi <= wall_lo disables (z periodic) */
+    double beta;
+    /* titration (weak base: neutral <-> +1 with counterion insert/delete) */
+    double pH, pKa;
+    int type_site_neutral, type_site_charged;
+    float q_site_charged;
+    int type_counterion;
+    float q_counterion;
+    /* reservoir salt swaps (cation/anion pair insert/delete) */
+    double salt_conc;      /* reservoir pair concentration, sigma^-3 (ideal activity) */
+    int type_cation;
+    float q_cation;
+    /* move mix (probabilities; their sum must be <= 1, remainder is a no-op) */
+    double p_disp, p_titr, p_swap;
+    double disp_max;
+    uint64_t seed;
+    /* engine tuning (0 = default) */
+    int cell_cap;          /* particles per cell capacity */
+    int pending_max;       /* stencils buffered before the potential mesh is rebuilt */
+    int threads;           /* threads per replica block in the MC kernel */
+} phmc_params;
+
+typedef struct phmc_energy_components {
+    double lj;         /* LJ / WCA pair energy */
+    double fene;       /* bonded FENE energy */
+    double coul_real;  /* real-space Coulomb (erfc) or plain cutoff Coulomb */
+    double coul_recip; /* SPME reciprocal */
+    double self;       /* Ewald self term */
+    double qcorr;      /* net-charge term */
+    double slab;       /* Yeh-Berkowitz slab term */
+    double total;
+} phmc_energy_components;
+
+/* A trial = up to two particle changes, evaluated against the current state. */
+typedef struct phmc_change {
+    int index;      /* slot */
+    int present;    /* 1: present after the change; 0: removed */
+    float x, y, z, q;
+    int type;
+} phmc_change;
+
+typedef struct phmc_trial {
+    int n_changes;  /* 1 or 2 */
+    phmc_change c[2];
+} phmc_trial;
+
+typedef struct phmc_run_stats {
+    int64_t attempted[3];  /* per move kind */
+    int64_t accepted[3];
+    int64_t flushes;       /* potential-mesh rebuilds */
+    int n_titratable;
+    int n_charged_sites;   /* currently protonated sites */
+    int n_cations, n_anions;
+    double energy;         /* tracked total energy (FP64) */
+    double energy_drift;   /* |tracked - recomputed| at the last flush */
+} phmc_run_stats;
+
+typedef struct phmc_engine phmc_engine;
+
+/* ---- library ---- */
+int phmc_abi_version(void);
+const char* phmc_last_error(void);
+
+/* ---- lifecycle ----
+ * Replaces the reference set-up: upload_atoms_to_device + copy_csr_to_device +
+ * build_half_neighbors_gpu + pmeCreate (MC/src/main.cu:18-41,127-141,
+ * MC/src/neighbor.cu:65-125, MC/src/pme.cu:291-335). */
+int phmc_create(int n_replicas, const phmc_system* systems, const phmc_params* params,
+                int device, phmc_engine** out);
+int phmc_destroy(phmc_engine* e);
+
+/* ---- energies ----
+ * Full recompute on the device (replaces total_energy, MC/src/mc.cu:43-60:
+ * compute_lj_sr_energy_gpu + pmeEnergy).  out has n_replicas entries. */
+int phmc_energy(phmc_engine* e, phmc_energy_components* out);
+
+/* dE of n independent trials of replica r, each against the current state.
+ * No counterpart in the reference (it recomputes the total per trial). */
+int phmc_delta_energy(phmc_engine* e, int replica, const phmc_trial* trials, int n, double* dE);
+
+/* Apply one trial to replica r (state, cell list, pending mesh changes). */
+int phmc_commit(phmc_engine* e, int replica, const phmc_trial* trial);
+
+/* Identity change of one particle (reference: set_atom_identity, MC/src/mc.cu:33-41;
+ * type is 0-based as on the reference's device side). */
+int phmc_set_identity(phmc_engine* e, int replica, int i, int type, float q);
+
+/* ---- Monte Carlo ----
+ * Run n_trials Metropolis trials per replica on the device (persistent
+ * kernel, potential-mesh rebuilds in between).  Replaces the host trial
+ * loops (MC/src/mc.cu:159-318,320-550).  stats has n_replicas entries. */
+int phmc_run(phmc_engine* e, int64_t n_trials, phmc_run_stats* stats);
+
+/* Record per-trial (move, dE, accept) of the next phmc_run into host arrays of
+ * length >= n_trials (replica 0 only; NULL disables).  For replay checks. */
+int phmc_set_trial_log(phmc_engine* e, int64_t capacity, int* move, double* dE, int* accepted);
+
+/* Replay mode: the next phmc_run takes accept decisions from `decisions`
+ * (replica 0, one int per trial) instead of the Metropolis test. NULL disables. */
+int phmc_set_replay(phmc_engine* e, int64_t n, const int* decisions);
+
+/* ---- state ---- */
+int phmc_get_state(phmc_engine* e, int replica, float* x, float* y, float* z, float* q,
+                   int* type, int* flags);
+/* cell index of every slot (-1 for ghosts) and the cell grid dimensions */
+int phmc_get_cells(phmc_engine* e, int replica, int* cell_of, int dims[3]);
+int phmc_capacity(phmc_engine* e, int replica);
+
+/* ---- synthetic input (no counterpart in the reference, whose inputs are
+ * LAMMPS data files, MC/src/io.cpp:79-146) ----
+ * Grafted brush: chains on a square lattice at z = 0, self-avoiding random
+ * walks, random initial ionisation, counterions and salt pairs in the slab.
+ * Types: 0 neutral site, 1 charged site (+1), 2 anion (-1), 3 cation (+1),
+ * 4 permanently charged bead (+1). */
+typedef struct phmc_brush_spec {
+    int chains_x, chains_y;
+    double graft_spacing;
+    int len_min, len_max;      /* beads per chain, drawn uniformly */
+    int n_permanent;           /* inner beads with a permanent +1 charge (diblock) */
+    int graft_titratable;      /* grafted (immobile) bead is a titratable site */
+    double height;             /* slab height: particles in [0, height) */
+    double lz;                 /* box Lz (padded for the slab correction) */
+    double ion_frac;           /* initial fraction of titratable sites charged */
+    double salt_conc;          /* salt pairs per sigma^3 of the slab */
+    double bond_len, min_dist;
+    uint64_t seed;
+} phmc_brush_spec;
+
+/* counts[0] = particles, counts[1] = bonds; box_out = {Lx, Ly, Lz}. */
+int phmc_build_brush(const phmc_brush_spec* spec, int capacity, float* x, float* y, float* z, float* q, int* type,
+                     int* flags, int max_bonds, int* bond_i, int* bond_j, int* counts, double* box_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHMC_H */

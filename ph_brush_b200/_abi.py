@@ -1,0 +1,158 @@
+"""ctypes mirror of include/phmc.h and the loader of the in-tree libphmc.so.
+
+The library is the only compute path: importing this module on a machine
+without the built library raises immediately (there is no CPU fallback).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libphmc.so")
+
+PHMC_OK = 0
+ERRORS = {1: "ARG", 2: "CUDA", 3: "CAPACITY", 4: "BUDGET", 5: "STATE", 6: "UNSUPPORTED", 7: "IO"}
+COUL_NONE, COUL_CUT, COUL_EWALD = 0, 1, 2
+F_MOBILE, F_TITRATABLE, F_GHOST, F_CATION, F_ANION = 0x01, 0x02, 0x04, 0x08, 0x10
+MOVE_DISP, MOVE_TITR, MOVE_SWAP, MOVE_NONE = 0, 1, 2, 3
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+
+
+class System(C.Structure):
+    _fields_ = [("n_particles", C.c_int), ("capacity", C.c_int),
+                ("x", _fp), ("y", _fp), ("z", _fp), ("q", _fp),
+                ("type", _ip), ("flags", _ip),
+                ("n_bonds", C.c_int), ("bond_i", _ip), ("bond_j", _ip),
+                ("box", C.c_double * 3)]
+
+
+class Params(C.Structure):
+    _fields_ = [("n_types", C.c_int), ("lj_eps", _dp), ("lj_sig", _dp), ("lj_rc", _dp),
+                ("rc_lj", C.c_double), ("lj_shift", C.c_int), ("coulomb", C.c_int),
+                ("rc_coul", C.c_double), ("epsilon_r", C.c_double), ("ewald_alpha", C.c_double),
+                ("mesh", C.c_int * 3), ("order", C.c_int), ("ref_moduli", C.c_int), ("slab", C.c_int),
+                ("excl_bonded_lj", C.c_int), ("excl_bonded_coul", C.c_int),
+                ("fene_k", C.c_double), ("fene_r0", C.c_double),
+                ("wall_lo", C.c_double), ("wall_hi", C.c_double), ("beta", C.c_double),
+                ("pH", C.c_double), ("pKa", C.c_double),
+                ("type_site_neutral", C.c_int), ("type_site_charged", C.c_int), ("q_site_charged", C.c_float),
+                ("type_counterion", C.c_int), ("q_counterion", C.c_float),
+                ("salt_conc", C.c_double), ("type_cation", C.c_int), ("q_cation", C.c_float),
+                ("p_disp", C.c_double), ("p_titr", C.c_double), ("p_swap", C.c_double), ("disp_max", C.c_double),
+                ("seed", C.c_uint64),
+                ("cell_cap", C.c_int), ("pending_max", C.c_int), ("threads", C.c_int)]
+
+
+class EnergyComponents(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("lj", "fene", "coul_real", "coul_recip", "self", "qcorr", "slab", "total")]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Change(C.Structure):
+    _fields_ = [("index", C.c_int), ("present", C.c_int), ("x", C.c_float), ("y", C.c_float),
+                ("z", C.c_float), ("q", C.c_float), ("type", C.c_int)]
+
+
+class Trial(C.Structure):
+    _fields_ = [("n_changes", C.c_int), ("c", Change * 2)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("attempted", C.c_int64 * 3), ("accepted", C.c_int64 * 3), ("flushes", C.c_int64),
+                ("n_titratable", C.c_int), ("n_charged_sites", C.c_int), ("n_cations", C.c_int),
+                ("n_anions", C.c_int), ("energy", C.c_double), ("energy_drift", C.c_double)]
+
+
+class BrushSpec(C.Structure):
+    _fields_ = [("chains_x", C.c_int), ("chains_y", C.c_int), ("graft_spacing", C.c_double),
+                ("len_min", C.c_int), ("len_max", C.c_int), ("n_permanent", C.c_int),
+                ("graft_titratable", C.c_int), ("height", C.c_double), ("lz", C.c_double),
+                ("ion_frac", C.c_double), ("salt_conc", C.c_double), ("bond_len", C.c_double),
+                ("min_dist", C.c_double), ("seed", C.c_uint64)]
+
+
+EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
+           "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
+           "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush"]
+
+
+def load_library(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise ImportError(f"libphmc.so not built at {path}: run `make -C ph_brush_b200` "
+                          "(the engine has no CPU fallback)")
+    lib = C.CDLL(path)
+    lib.phmc_last_error.restype = C.c_char_p
+    eng = C.c_void_p
+    sig = {
+        "phmc_abi_version": ([], C.c_int),
+        "phmc_create": ([C.c_int, C.POINTER(System), C.POINTER(Params), C.c_int, C.POINTER(eng)], C.c_int),
+        "phmc_destroy": ([eng], C.c_int),
+        "phmc_energy": ([eng, C.POINTER(EnergyComponents)], C.c_int),
+        "phmc_delta_energy": ([eng, C.c_int, C.POINTER(Trial), C.c_int, _dp], C.c_int),
+        "phmc_commit": ([eng, C.c_int, C.POINTER(Trial)], C.c_int),
+        "phmc_set_identity": ([eng, C.c_int, C.c_int, C.c_int, C.c_float], C.c_int),
+        "phmc_run": ([eng, C.c_int64, C.POINTER(RunStats)], C.c_int),
+        "phmc_set_trial_log": ([eng, C.c_int64, _ip, _dp, _ip], C.c_int),
+        "phmc_set_replay": ([eng, C.c_int64, _ip], C.c_int),
+        "phmc_get_state": ([eng, C.c_int, _fp, _fp, _fp, _fp, _ip, _ip], C.c_int),
+        "phmc_get_cells": ([eng, C.c_int, _ip, _ip], C.c_int),
+        "phmc_capacity": ([eng, C.c_int], C.c_int),
+        "phmc_build_brush": ([C.POINTER(BrushSpec), C.c_int, _fp, _fp, _fp, _fp, _ip, _ip, C.c_int, _ip, _ip, _ip, _dp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = load_library()
+    return _LIB
+
+
+class PhmcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"phmc error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def check(status):
+    if status != PHMC_OK:
+        raise PhmcError(status, lib().phmc_last_error().decode())
+    return status
+
+
+def fptr(a):
+    return a.ctypes.data_as(_fp)
+
+
+def iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+def dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def as_f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def as_i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def as_f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)

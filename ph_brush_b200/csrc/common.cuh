@@ -1,0 +1,217 @@
+// Shared device-side definitions of the phmc engine (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/phmc.h"
+
+#define PHMC_MAX_TYPES 8
+#define PHMC_MAX_ORDER 6
+#define PHMC_MAX_PEND 64
+#define PHMC_FIX_SCALE 1099511627776.0   /* 2^40: fixed-point scale of the charge mesh */
+#define PHMC_FIX_INV (1.0 / 1099511627776.0)
+
+// Per-replica constant description (the ragged descriptor table).
+struct RepDesc {
+    // particles
+    int cap, slot_off;
+    float L[3];
+    double V;
+    // cells
+    int ncell[3], cell_off, cell_cap;
+    float cell_scale[3];  // ncell / L (float), cell = (int)(x * scale)
+    // mesh
+    int mesh[3];
+    long long mesh_off;   // offset (elements) into real / complex mesh arrays
+    int oct[3];           // G octant dims (n/2+1)
+    long long oct_off;
+    int mod_off[3];       // offsets of the B-spline moduli per axis
+    int tw_off[3];        // offsets of the twiddle tables per axis
+    int order;
+    int coulomb;
+    int ref_corner;
+    int slab;
+    float alpha, elf, rc_coul2;
+    float ewald_factor;   // (pi/alpha)^2
+    // walls, bonds
+    int walls;
+    float wall_lo, wall_hi;
+    float fene_k, fene_r02;
+    int excl_lj, excl_coul;
+    // LJ tables (T <= 8)
+    int T;
+    float lj_eps[PHMC_MAX_TYPES * PHMC_MAX_TYPES];
+    float lj_sig2[PHMC_MAX_TYPES * PHMC_MAX_TYPES];
+    float lj_rc2[PHMC_MAX_TYPES * PHMC_MAX_TYPES];
+    float lj_shift[PHMC_MAX_TYPES * PHMC_MAX_TYPES];
+    // moves
+    double beta, titr_log;   // titr_log = ln10 * (pKa - pH)
+    double salt_c2V2;        // c_s^2 * V_slab^2
+    float p_disp, p_titr, p_swap, disp_max;
+    int type_site_neutral, type_site_charged, type_counterion, type_cation;
+    float q_site_charged, q_counterion, q_cation;
+    uint32_t key[2];
+    int n_titr;
+    int pend_max;
+    // Ewald scalar coefficients
+    double self_coef;   // -elf * alpha / sqrt(pi)
+    double qcorr_coef;  // -pi * elf / (2 V alpha^2)
+    double slab_coef;   // 2 pi elf / V
+    double Lz2_12;      // Lz^2 / 12
+};
+
+// Per-replica mutable state (device-resident between launches).
+struct RepState {
+    int n_mobile, n_anion, n_cation, n_free;
+    int error;          // PHMC_ERR_* raised inside a kernel (0 = none)
+    int stop_reason;    // 0 target reached, 1 pending full
+    long long trial;    // next trial index (Philox counter)
+    long long target;   // run until trial == target
+    long long run_start; // trial index at the start of the current phmc_run (log / replay origin)
+    long long att[3], acc[3];
+    long long flushes;
+    double E;           // tracked total energy
+    double E_pair_lj, E_pair_c, E_fene, E_rec, E_self, E_qcorr, E_slab;  // tracked components
+    double Q, Q2, Mz, S2;  // charge moments
+    double drift;       // |tracked E_rec - recomputed| at the last flush
+    double E_rec_flush; // E_rec computed at the last flush
+};
+
+// Device pointers of the whole engine (all replicas concatenated).
+struct DevPtrs {
+    float4* posq;       // x, y, z, q
+    int* type;
+    int* flags;
+    int4* bonds;        // up to 4 partners (local slot index), -1 = none
+    int* cell_of;       // -1 for ghosts
+    int* cell_pos;
+    int* cell_count;
+    int* cell_list;     // cell_off*cell_cap + c*cell_cap + k (local slot)
+    int* mobile; int* mobile_pos;
+    int* anions; int* anion_pos;
+    int* cations; int* cation_pos;
+    int* freel;
+    int* titr;
+    unsigned long long* qfix;  // fixed-point charge mesh
+    float2* cmesh;             // complex work mesh
+    float* phi;                // potential mesh (real)
+    float* goct;               // influence kernel octant
+    float* moduli;
+    float2* twiddle;
+    RepDesc* desc;
+    RepState* state;
+    double* partials;          // reduction scratch
+    int* dirty;                // per replica: potential mesh stale
+    // trial log / replay (replica 0)
+    int* log_move; double* log_dE; int* log_acc; long long log_cap;
+    const int* replay; long long replay_n;
+};
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11), written from the paper's definition.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline void philox4x32_10(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
+                                              uint32_t c2, uint32_t c3, uint32_t out[4]) {
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__host__ __device__ inline float u24(uint32_t v) { return (float)(v >> 8) * (1.0f / 16777216.0f); }
+__host__ __device__ inline double u53(uint32_t a, uint32_t b) {
+    uint64_t v = ((uint64_t)a << 21) ^ (uint64_t)(b >> 11);
+    return (double)(v & ((1ull << 53) - 1)) * (1.0 / 9007199254740992.0);
+}
+__host__ __device__ inline int pick_index(uint32_t v, int n) { return (int)(((uint64_t)v * (uint64_t)n) >> 32); }
+
+// Cardinal B-spline weights of order P at fractional offset t (see the
+// spreading convention: point base + j gets M_P(t + P-1-j)).
+template <int P>
+__device__ __forceinline__ void bspline_weights(float t, float* w) {
+    float c[P];
+    c[0] = t; c[1] = 1.0f - t;
+#pragma unroll
+    for (int n = 3; n <= P; ++n) {
+        const float inv = 1.0f / (float)(n - 1);
+        float nc[P];
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            float a = (i < n - 1) ? c[i] : 0.0f;
+            float b = (i >= 1) ? c[i - 1] : 0.0f;
+            nc[i] = ((t + (float)i) * a + ((float)n - t - (float)i) * b) * inv;
+        }
+#pragma unroll
+        for (int i = 0; i < n; ++i) c[i] = nc[i];
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) w[j] = c[P - 1 - j];
+}
+
+__device__ __forceinline__ float min_image(float d, float L) { return d - L * rintf(d / L); }
+
+__device__ __forceinline__ int wrap_idx(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// Pair energy between two present particles (FP32), split into LJ and Coulomb.
+// `bonded` applies the 1-2 exclusion policy.
+__device__ __forceinline__ void pair_energy(const RepDesc& D, float dx, float dy, float dz, int ti, int tj,
+                                            float qi, float qj, bool bonded, float& elj, float& ec) {
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const int p = ti * D.T + tj;
+    elj = 0.0f; ec = 0.0f;
+    if (!(bonded && D.excl_lj) && r2 <= D.lj_rc2[p] && D.lj_eps[p] > 0.0f) {
+        float s2 = D.lj_sig2[p] / r2;
+        float s6 = s2 * s2 * s2;
+        elj = 4.0f * D.lj_eps[p] * (s6 * s6 - s6) - D.lj_shift[p];
+    }
+    if (D.coulomb != PHMC_COUL_NONE && !(bonded && D.excl_coul) && r2 <= D.rc_coul2) {
+        float qq = qi * qj;
+        if (qq != 0.0f) {
+            float r = sqrtf(r2);
+            ec = (D.coulomb == PHMC_COUL_EWALD) ? D.elf * qq * erfcf(D.alpha * r) / r : D.elf * qq / r;
+        }
+    }
+}
+
+__device__ __forceinline__ bool in_bonds(int4 b, int j) { return b.x == j || b.y == j || b.z == j || b.w == j; }
+
+__device__ __forceinline__ int cell_index(const RepDesc& D, float x, float y, float z) {
+    int a = min(D.ncell[0] - 1, max(0, (int)(x * D.cell_scale[0])));
+    int b = min(D.ncell[1] - 1, max(0, (int)(y * D.cell_scale[1])));
+    int c = min(D.ncell[2] - 1, max(0, (int)(z * D.cell_scale[2])));
+    return (c * D.ncell[1] + b) * D.ncell[0] + a;
+}
+
+// FENE bond energy (FP32 term); returns +inf beyond R0.
+__device__ __forceinline__ float fene_energy(const RepDesc& D, float r2) {
+    if (r2 >= D.fene_r02) return __int_as_float(0x7f800000);
+    return -0.5f * D.fene_k * D.fene_r02 * logf(1.0f - r2 / D.fene_r02);
+}
+
+// Block-wide FP64 sum (all threads get the result).  `red` holds >= 32 doubles.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = (l < NT / 32) ? red[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (l == 0) red[32] = s;
+    }
+    __syncthreads();
+    return red[32];
+}

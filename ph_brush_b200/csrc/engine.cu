@@ -1,0 +1,683 @@
+// C-ABI implementation of the phmc engine (include/phmc.h): replica layout,
+// uploads, influence-kernel construction, the trial/rebuild loop and state
+// readback.  All entry points return a status code and never throw.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+#include "engine.h"
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+#define CU(x)                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" int phmc_abi_version(void) { return PHMC_ABI_VERSION; }
+extern "C" const char* phmc_last_error(void) { return g_err.c_str(); }
+
+struct phmc_engine {
+    Engine E;
+    // trial log (host destinations)
+    int* h_log_move = nullptr; double* h_log_dE = nullptr; int* h_log_acc = nullptr; long long log_cap = 0;
+    int* d_replay = nullptr; long long replay_n = 0;
+    long long replay_cap = 0;
+    phmc_trial* d_trials = nullptr; double* d_dE = nullptr; int trials_cap = 0;
+    std::vector<int> caps;
+};
+
+template <typename T>
+static int dalloc(Engine& E, T** p, size_t n) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * n);
+    if (e != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    E.allocs.push_back((void*)*p);
+    return PHMC_OK;
+}
+#define DALLOC(p, n) do { int s_ = dalloc(E, &(p), (n)); if (s_) return s_; } while (0)
+
+static bool smooth235(int n) {
+    if (n < 1) return false;
+    for (int p : {2, 3, 5}) while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+// |DFT(M_p)|^2 on a length-n grid from the cardinal B-spline values at the
+// integer points (de Boor recursion, restating MC/src/pme.cu:77-113).
+// ref_style 1: the reference's clamp (exact zero -> 1e-30) and Nyquist patch;
+// ref_style 0: a modulus below 1e-7 (odd orders at Nyquist) is replaced by the
+// mean of its neighbours.
+static std::vector<double> bspline_moduli(int n, int order, int ref_style) {
+    const int s = order - 1;
+    std::vector<double> d((size_t)s, 0.0);
+    d[0] = 1.0;
+    for (int k = 2; k <= s; ++k) {
+        const double inv = 1.0 / k;
+        for (int m = k - 1; m > 0; --m) d[m] = inv * ((k - m) * d[m - 1] + (m + 1) * d[m]);
+        d[0] = inv * d[0];
+    }
+    std::vector<double> mod((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        double c = 0, sn = 0;
+        for (int j = 0; j < s; ++j) {
+            const double a = 2.0 * M_PI * i * (j + 1) / (double)n;
+            c += d[j] * std::cos(a);
+            sn += d[j] * std::sin(a);
+        }
+        double v = c * c + sn * sn;
+        if (ref_style && !(v > 0.0)) v = 1e-30;
+        mod[i] = v;
+    }
+    if (ref_style) {
+        if (n % 2 == 0 && !(mod[n / 2] > 0.0)) mod[n / 2] = mod[n / 2 - 1];
+    } else {
+        std::vector<double> c = mod;
+        for (int i = 0; i < n; ++i)
+            if (c[i] < 1e-7) mod[i] = 0.5 * (c[(i - 1 + n) % n] + c[(i + 1) % n]);
+    }
+    return mod;
+}
+
+static int validate(int R, const phmc_system* sys, const phmc_params* prm) {
+    if (R < 1 || !sys || !prm) return fail(PHMC_ERR_ARG, "phmc_create: need n_replicas >= 1 and non-null systems/params");
+    for (int r = 0; r < R; ++r) {
+        const phmc_system& S = sys[r];
+        const phmc_params& P = prm[r];
+        char b[256];
+        if (S.n_particles < 0 || S.capacity < S.n_particles || S.capacity < 1) {
+            snprintf(b, sizeof b, "replica %d: invalid n_particles/capacity (%d/%d)", r, S.n_particles, S.capacity);
+            return fail(PHMC_ERR_ARG, b);
+        }
+        if (S.n_particles > 0 && (!S.x || !S.y || !S.z || !S.q || !S.type || !S.flags)) return fail(PHMC_ERR_ARG, "null particle array");
+        if (!(S.box[0] > 0 && S.box[1] > 0 && S.box[2] > 0)) return fail(PHMC_ERR_ARG, "box lengths must be > 0");
+        if (P.n_types < 1 || P.n_types > PHMC_MAX_TYPES || !P.lj_eps || !P.lj_sig)
+            return fail(PHMC_ERR_ARG, "n_types must be 1..8 with LJ tables");
+        for (int i = 0; i < S.n_particles; ++i) {
+            if (S.type[i] < 0 || S.type[i] >= P.n_types) { snprintf(b, sizeof b, "replica %d: particle %d type %d out of range", r, i, S.type[i]); return fail(PHMC_ERR_ARG, b); }
+            if (!(S.flags[i] & PHMC_F_GHOST)) {
+                if (!(S.x[i] >= 0 && S.x[i] < S.box[0] && S.y[i] >= 0 && S.y[i] < S.box[1] && S.z[i] >= 0 && S.z[i] < S.box[2])) {
+                    snprintf(b, sizeof b, "replica %d: particle %d outside [0,L) (wrap positions first)", r, i);
+                    return fail(PHMC_ERR_ARG, b);
+                }
+            }
+        }
+        for (int k = 0; k < S.n_bonds; ++k)
+            if (S.bond_i[k] < 0 || S.bond_i[k] >= S.n_particles || S.bond_j[k] < 0 || S.bond_j[k] >= S.n_particles || S.bond_i[k] == S.bond_j[k])
+                return fail(PHMC_ERR_ARG, "bond index out of range");
+        if (P.coulomb < 0 || P.coulomb > 2) return fail(PHMC_ERR_ARG, "coulomb kind");
+        if (P.coulomb != PHMC_COUL_NONE && !(P.epsilon_r > 0)) return fail(PHMC_ERR_ARG, "epsilon_r must be > 0");
+        if (P.coulomb == PHMC_COUL_EWALD) {
+            if (!(P.ewald_alpha > 0)) return fail(PHMC_ERR_ARG, "ewald_alpha must be > 0");
+            if (P.order < 4 || P.order > 6) return fail(PHMC_ERR_UNSUPPORTED, "SPME order must be 4, 5 or 6");
+            if (P.order != prm[0].order) return fail(PHMC_ERR_UNSUPPORTED, "all replicas must share the SPME order");
+            for (int k = 0; k < 3; ++k)
+                if (!smooth235(P.mesh[k]) || P.mesh[k] < P.order) return fail(PHMC_ERR_UNSUPPORTED, "mesh sizes must be 2^a 3^b 5^c and >= order");
+            if ((size_t)P.mesh[0] * P.mesh[1] * 16 > 227 * 1024) return fail(PHMC_ERR_UNSUPPORTED, "mesh plane nx*ny too large for one block");
+            if ((size_t)P.mesh[2] * ZPASS_TX * 16 > 227 * 1024) return fail(PHMC_ERR_UNSUPPORTED, "mesh nz too large for one block");
+        }
+        if (!(P.beta > 0)) return fail(PHMC_ERR_ARG, "beta must be > 0");
+        if (P.p_disp < 0 || P.p_titr < 0 || P.p_swap < 0 || P.p_disp + P.p_titr + P.p_swap > 1.0 + 1e-12)
+            return fail(PHMC_ERR_ARG, "move probabilities must be >= 0 with sum <= 1");
+        if (P.p_swap > 0 && !(P.salt_conc > 0)) return fail(PHMC_ERR_ARG, "swap moves need salt_conc > 0");
+    }
+    return PHMC_OK;
+}
+
+static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_params* prm, int device) {
+    Engine& E = h->E;
+    E.R = R;
+    E.device = device;
+    CU(cudaSetDevice(device));
+    CU(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
+    E.order = prm[0].order;
+    E.coulomb = prm[0].coulomb;
+    E.threads = prm[0].threads == 128 ? 128 : 256;
+    E.pend_max = prm[0].pending_max > 0 ? std::min(std::max(prm[0].pending_max, 4), PHMC_MAX_PEND) : 16;
+    E.cell_cap = prm[0].cell_cap > 0 ? prm[0].cell_cap : 64;
+    for (int r = 1; r < R; ++r)
+        if (prm[r].coulomb != E.coulomb) return fail(PHMC_ERR_UNSUPPORTED, "all replicas must share the Coulomb kind");
+    const bool ewald = E.coulomb == PHMC_COUL_EWALD;
+
+    // ---- descriptors ----
+    E.desc.resize(R);
+    std::vector<double> h_mod;
+    std::vector<float2> h_tw;
+    std::map<int, int> tw_off;
+    int slot_off = 0, cell_off = 0;
+    long long mesh_off = 0, oct_off = 0;
+    for (int r = 0; r < R; ++r) {
+        const phmc_system& S = sys[r];
+        const phmc_params& P = prm[r];
+        RepDesc& D = E.desc[r];
+        std::memset(&D, 0, sizeof(D));
+        D.cap = S.capacity; D.slot_off = slot_off; slot_off += S.capacity;
+        for (int k = 0; k < 3; ++k) D.L[k] = (float)S.box[k];
+        D.V = S.box[0] * S.box[1] * S.box[2];
+        D.T = P.n_types;
+        double rmax = 0.0;
+        for (int a = 0; a < D.T; ++a)
+            for (int b = 0; b < D.T; ++b) {
+                const int k = a * D.T + b;
+                const double eps = P.lj_eps[k], sig = P.lj_sig[k];
+                const double rc = P.lj_rc ? P.lj_rc[k] : P.rc_lj;
+                D.lj_eps[k] = (eps > 0 && sig > 0) ? (float)eps : 0.0f;
+                D.lj_sig2[k] = (float)(sig * sig);
+                D.lj_rc2[k] = (float)(rc * rc);
+                double sh = 0.0;
+                if (P.lj_shift && eps > 0 && sig > 0) {
+                    const double sr6 = std::pow(sig / rc, 6);
+                    sh = 4.0 * eps * (sr6 * sr6 - sr6);
+                }
+                D.lj_shift[k] = (float)sh;
+                if (eps > 0 && sig > 0) rmax = std::max(rmax, rc);
+            }
+        D.coulomb = P.coulomb;
+        if (P.coulomb != PHMC_COUL_NONE) rmax = std::max(rmax, P.rc_coul);
+        if (!(rmax > 0)) rmax = 1.0;
+        for (int k = 0; k < 3; ++k) {
+            D.ncell[k] = (int)std::floor(S.box[k] / rmax);
+            if (D.ncell[k] < 3) return fail(PHMC_ERR_UNSUPPORTED, "box must hold at least 3 cells of the largest cutoff per axis");
+            D.cell_scale[k] = (float)D.ncell[k] / D.L[k];
+        }
+        D.cell_off = cell_off; cell_off += D.ncell[0] * D.ncell[1] * D.ncell[2];
+        D.cell_cap = E.cell_cap;
+        const double elf = 138.935458 / (P.epsilon_r > 0 ? P.epsilon_r : 1.0);
+        D.elf = (float)elf;
+        D.alpha = (float)P.ewald_alpha;
+        D.rc_coul2 = (float)(P.rc_coul * P.rc_coul);
+        D.ewald_factor = ewald ? (float)((M_PI / P.ewald_alpha) * (M_PI / P.ewald_alpha)) : 0.0f;
+        D.slab = P.slab;
+        D.ref_corner = P.ref_moduli;
+        D.order = E.order;
+        D.walls = P.wall_hi > P.wall_lo;
+        D.wall_lo = (float)P.wall_lo; D.wall_hi = (float)P.wall_hi;
+        D.fene_k = (float)P.fene_k; D.fene_r02 = (float)(P.fene_r0 * P.fene_r0);
+        D.excl_lj = P.excl_bonded_lj; D.excl_coul = P.excl_bonded_coul;
+        D.beta = P.beta;
+        D.titr_log = std::log(10.0) * (P.pKa - P.pH);
+        const double Vs = (double)D.L[0] * (double)D.L[1] * (D.walls ? (double)(D.wall_hi - D.wall_lo) : (double)D.L[2]);
+        D.salt_c2V2 = P.salt_conc * P.salt_conc * Vs * Vs;
+        D.p_disp = (float)P.p_disp; D.p_titr = (float)P.p_titr; D.p_swap = (float)P.p_swap; D.disp_max = (float)P.disp_max;
+        D.type_site_neutral = P.type_site_neutral; D.type_site_charged = P.type_site_charged;
+        D.type_counterion = P.type_counterion; D.type_cation = P.type_cation;
+        D.q_site_charged = P.q_site_charged; D.q_counterion = P.q_counterion; D.q_cation = P.q_cation;
+        D.key[0] = (uint32_t)(P.seed & 0xffffffffu); D.key[1] = (uint32_t)(P.seed >> 32);
+        D.pend_max = E.pend_max;
+        if (ewald) {
+            D.self_coef = -elf * P.ewald_alpha / std::sqrt(M_PI);
+            D.qcorr_coef = -(M_PI * elf) / (2.0 * D.V * P.ewald_alpha * P.ewald_alpha);
+            D.slab_coef = (2.0 * M_PI / D.V) * elf;
+            D.Lz2_12 = S.box[2] * S.box[2] / 12.0;
+            for (int k = 0; k < 3; ++k) {
+                D.mesh[k] = P.mesh[k];
+                D.oct[k] = P.mesh[k] / 2 + 1;
+                std::vector<double> m = bspline_moduli(P.mesh[k], P.order, P.ref_moduli);
+                D.mod_off[k] = (int)h_mod.size();
+                h_mod.insert(h_mod.end(), m.begin(), m.end());
+                auto it = tw_off.find(P.mesh[k]);
+                if (it == tw_off.end()) {
+                    const int n = P.mesh[k];
+                    tw_off[n] = (int)h_tw.size();
+                    for (int j = 0; j < n; ++j) h_tw.push_back(make_float2((float)std::cos(-2.0 * M_PI * j / n), (float)std::sin(-2.0 * M_PI * j / n)));
+                }
+                D.tw_off[k] = tw_off[P.mesh[k]];
+            }
+            D.mesh_off = mesh_off; mesh_off += (long long)D.mesh[0] * D.mesh[1] * D.mesh[2];
+            D.oct_off = oct_off; oct_off += (long long)D.oct[0] * D.oct[1] * D.oct[2];
+        }
+    }
+    E.total_slots = slot_off;
+    E.total_cells = cell_off;
+    E.total_mesh = mesh_off;
+    E.total_oct = oct_off;
+
+    // ---- host particle arrays + lists ----
+    const int N = E.total_slots;
+    std::vector<float4> h_posq((size_t)N, make_float4(0, 0, 0, 0));
+    std::vector<int> h_type((size_t)N, 0), h_flags((size_t)N, PHMC_F_GHOST), h_rep((size_t)N);
+    std::vector<int4> h_bonds((size_t)N, make_int4(-1, -1, -1, -1));
+    std::vector<int> h_mobile((size_t)N, -1), h_mpos((size_t)N, -1), h_an((size_t)N, -1), h_apos((size_t)N, -1);
+    std::vector<int> h_cat((size_t)N, -1), h_cpos((size_t)N, -1), h_free((size_t)N, -1), h_titr((size_t)N, -1);
+    std::vector<RepState> h_state((size_t)R);
+    for (int r = 0; r < R; ++r) {
+        const phmc_system& S = sys[r];
+        RepDesc& D = E.desc[r];
+        RepState& st = h_state[r];
+        std::memset(&st, 0, sizeof(st));
+        const int so = D.slot_off;
+        for (int i = 0; i < D.cap; ++i) h_rep[so + i] = r;
+        for (int i = 0; i < S.n_particles; ++i) {
+            h_posq[so + i] = make_float4(S.x[i], S.y[i], S.z[i], S.q[i]);
+            h_type[so + i] = S.type[i];
+            h_flags[so + i] = S.flags[i];
+        }
+        for (int k = 0; k < S.n_bonds; ++k) {
+            int ends[2] = {S.bond_i[k], S.bond_j[k]};
+            for (int e = 0; e < 2; ++e) {
+                int4& b = h_bonds[so + ends[e]];
+                const int other = ends[1 - e];
+                if (b.x == other || b.y == other || b.z == other || b.w == other) continue;
+                if (b.x < 0) b.x = other; else if (b.y < 0) b.y = other; else if (b.z < 0) b.z = other; else if (b.w < 0) b.w = other;
+                else return fail(PHMC_ERR_UNSUPPORTED, "more than 4 bonds on one particle");
+            }
+        }
+        int nt = 0;
+        for (int i = 0; i < D.cap; ++i) {
+            const int f = h_flags[so + i];
+            if (f & PHMC_F_GHOST) continue;
+            if (f & PHMC_F_MOBILE) { h_mpos[so + i] = st.n_mobile; h_mobile[so + st.n_mobile++] = i; }
+            if (f & PHMC_F_TITRATABLE) h_titr[so + nt++] = i;
+            if (f & PHMC_F_ANION) { h_apos[so + i] = st.n_anion; h_an[so + st.n_anion++] = i; }
+            if (f & PHMC_F_CATION) { h_cpos[so + i] = st.n_cation; h_cat[so + st.n_cation++] = i; }
+        }
+        D.n_titr = nt;
+        for (int i = D.cap - 1; i >= 0; --i)
+            if (h_flags[so + i] & PHMC_F_GHOST) h_free[so + st.n_free++] = i;
+    }
+
+    // ---- device allocations ----
+    DevPtrs& d = E.d;
+    DALLOC(d.posq, N); DALLOC(d.type, N); DALLOC(d.flags, N); DALLOC(d.bonds, N);
+    DALLOC(d.cell_of, N); DALLOC(d.cell_pos, N);
+    DALLOC(d.cell_count, E.total_cells); DALLOC(d.cell_list, (size_t)E.total_cells * E.cell_cap);
+    DALLOC(d.mobile, N); DALLOC(d.mobile_pos, N); DALLOC(d.anions, N); DALLOC(d.anion_pos, N);
+    DALLOC(d.cations, N); DALLOC(d.cation_pos, N); DALLOC(d.freel, N); DALLOC(d.titr, N);
+    DALLOC(d.desc, R); DALLOC(d.state, R); DALLOC(d.dirty, R);
+    DALLOC(E.d_rep_of, N);
+    DALLOC(E.d_cell_rep, E.total_cells);
+    int maxcap = 0;
+    for (int r = 0; r < R; ++r) maxcap = std::max(maxcap, E.desc[r].cap);
+    E.energy_blocks = std::max(1, std::min(64, (maxcap + 127) / 128));
+    DALLOC(d.partials, (size_t)R * E.energy_blocks * 8);
+    DALLOC(E.d_active, 1);
+    CU(cudaMallocHost((void**)&E.h_active, sizeof(int)));
+
+    CU(cudaMemcpy(d.posq, h_posq.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.type, h_type.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.flags, h_flags.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.bonds, h_bonds.data(), sizeof(int4) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.mobile, h_mobile.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.mobile_pos, h_mpos.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.anions, h_an.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.anion_pos, h_apos.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.cations, h_cat.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.cation_pos, h_cpos.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.freel, h_free.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.titr, h_titr.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d_rep_of, h_rep.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.desc, E.desc.data(), sizeof(RepDesc) * R, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.state, h_state.data(), sizeof(RepState) * R, cudaMemcpyHostToDevice));
+    CU(cudaMemset(d.dirty, 0, sizeof(int) * R));
+    {
+        std::vector<int> hc((size_t)E.total_cells);
+        for (int r = 0; r < R; ++r) {
+            const RepDesc& D = E.desc[r];
+            for (int c = 0; c < D.ncell[0] * D.ncell[1] * D.ncell[2]; ++c) hc[(size_t)D.cell_off + c] = r;
+        }
+        CU(cudaMemcpy(E.d_cell_rep, hc.data(), sizeof(int) * hc.size(), cudaMemcpyHostToDevice));
+    }
+    h->caps.resize(R);
+    for (int r = 0; r < R; ++r) h->caps[r] = E.desc[r].cap;
+
+    // ---- mesh ----
+    if (ewald) {
+        DALLOC(d.qfix, E.total_mesh); DALLOC(d.cmesh, E.total_mesh); DALLOC(d.phi, E.total_mesh);
+        DALLOC(d.goct, E.total_oct);
+        DALLOC(d.moduli, h_mod.size()); DALLOC(d.twiddle, h_tw.size());
+        std::vector<float> hm(h_mod.begin(), h_mod.end());
+        CU(cudaMemcpy(d.moduli, hm.data(), sizeof(float) * hm.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(d.twiddle, h_tw.data(), sizeof(float2) * h_tw.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemset(d.qfix, 0, sizeof(unsigned long long) * E.total_mesh));
+        std::vector<int2> pj;
+        std::vector<int4> zj;
+        std::vector<int> zoff;
+        for (int r = 0; r < R; ++r) {
+            const RepDesc& D = E.desc[r];
+            for (int z = 0; z < D.mesh[2]; ++z) pj.push_back(make_int2(r, z));
+            zoff.push_back((int)zj.size());
+            for (int y = 0; y < D.mesh[1]; ++y)
+                for (int x0 = 0; x0 < D.mesh[0]; x0 += ZPASS_TX) zj.push_back(make_int4(r, y, x0, 0));
+            E.plane_smem = std::max(E.plane_smem, (size_t)2 * D.mesh[0] * D.mesh[1] * sizeof(float2));
+            E.zpass_smem = std::max(E.zpass_smem, (size_t)2 * ZPASS_TX * D.mesh[2] * sizeof(float2));
+        }
+        zoff.push_back((int)zj.size());
+        E.n_plane_jobs = (int)pj.size(); E.n_zjobs = (int)zj.size();
+        DALLOC(E.d_plane_jobs, pj.size()); DALLOC(E.d_zjobs, zj.size()); DALLOC(E.d_zjob_off, zoff.size());
+        DALLOC(E.d_epart, zj.size());
+        CU(cudaMemcpy(E.d_plane_jobs, pj.data(), sizeof(int2) * pj.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(E.d_zjobs, zj.data(), sizeof(int4) * zj.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(E.d_zjob_off, zoff.data(), sizeof(int) * zoff.size(), cudaMemcpyHostToDevice));
+        CU(mesh_set_smem_limits(E));
+    }
+    return PHMC_OK;
+}
+
+static int check_kernel_errors(phmc_engine* h) {
+    Engine& E = h->E;
+    CU(cudaStreamSynchronize(E.stream));
+    CU(cudaGetLastError());
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    for (int r = 0; r < E.R; ++r)
+        if (st[r].error) {
+            char b[160];
+            snprintf(b, sizeof b, "replica %d: device error %d (%s)", r, st[r].error,
+                     st[r].error == PHMC_ERR_CAPACITY ? "cell or slot capacity exceeded; raise cell_cap/capacity" : "kernel error");
+            return fail(st[r].error, b);
+        }
+    return PHMC_OK;
+}
+
+// Rebuild the potential mesh of all replicas (mode 1) and recompute every energy component.
+static int full_recompute(phmc_engine* h) {
+    Engine& E = h->E;
+    if (E.coulomb == PHMC_COUL_EWALD) {
+        launch_spread(E, nullptr, E.stream);
+        launch_fft_pipeline(E, nullptr, 1, E.stream);
+        CU(cudaGetLastError());
+    }
+    launch_full_energy(E, E.stream);
+    CU(cudaGetLastError());
+    return check_kernel_errors(h);
+}
+
+extern "C" int phmc_create(int n_replicas, const phmc_system* systems, const phmc_params* params, int device,
+                           phmc_engine** out) {
+    if (!out) return fail(PHMC_ERR_ARG, "out is null");
+    *out = nullptr;
+    int s = validate(n_replicas, systems, params);
+    if (s) return s;
+    phmc_engine* h = new (std::nothrow) phmc_engine;
+    if (!h) return fail(PHMC_ERR_ARG, "out of host memory");
+    s = build(h, n_replicas, systems, params, device);
+    if (s) { phmc_destroy(h); return s; }
+    Engine& E = h->E;
+    launch_cell_build(E, E.stream);
+    if (E.coulomb == PHMC_COUL_EWALD) {
+        // influence kernel G = potential of a unit charge on mesh point 0
+        launch_unit_charge(E, E.stream);
+        launch_fft_pipeline(E, nullptr, 1, E.stream);
+        for (int r = 0; r < E.R; ++r) launch_extract_octant(E, r, E.stream);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { phmc_destroy(h); return fail(PHMC_ERR_CUDA, std::string("G build: ") + cudaGetErrorString(e)); }
+    }
+    s = full_recompute(h);
+    if (s) { std::string m = g_err; phmc_destroy(h); g_err = m; return s; }
+    *out = h;
+    return PHMC_OK;
+}
+
+extern "C" int phmc_destroy(phmc_engine* h) {
+    if (!h) return PHMC_OK;
+    Engine& E = h->E;
+    if (E.stream) cudaStreamSynchronize(E.stream);
+    for (void* p : E.allocs) cudaFree(p);
+    E.allocs.clear();
+    if (E.h_active) cudaFreeHost(E.h_active);
+    if (h->d_replay) cudaFree(h->d_replay);
+    if (h->d_trials) cudaFree(h->d_trials);
+    if (h->d_dE) cudaFree(h->d_dE);
+    if (E.d.log_move) { cudaFree(E.d.log_move); cudaFree(E.d.log_dE); cudaFree(E.d.log_acc); }
+    if (E.stream) cudaStreamDestroy(E.stream);
+    delete h;
+    return PHMC_OK;
+}
+
+static void fill_components(const RepState& s, phmc_energy_components* c) {
+    c->lj = s.E_pair_lj; c->fene = s.E_fene; c->coul_real = s.E_pair_c; c->coul_recip = s.E_rec;
+    c->self = s.E_self; c->qcorr = s.E_qcorr; c->slab = s.E_slab; c->total = s.E;
+}
+
+extern "C" int phmc_energy(phmc_engine* h, phmc_energy_components* out) {
+    if (!h || !out) return fail(PHMC_ERR_ARG, "null argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    int s = full_recompute(h);
+    if (s) return s;
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    for (int r = 0; r < E.R; ++r) fill_components(st[r], &out[r]);
+    return PHMC_OK;
+}
+
+static int check_trials(phmc_engine* h, int rep, const phmc_trial* t, int n) {
+    if (rep < 0 || rep >= h->E.R) return fail(PHMC_ERR_ARG, "replica index out of range");
+    for (int k = 0; k < n; ++k) {
+        if (t[k].n_changes < 1 || t[k].n_changes > 2) return fail(PHMC_ERR_ARG, "trial must have 1 or 2 changes");
+        for (int c = 0; c < t[k].n_changes; ++c) {
+            const phmc_change& ch = t[k].c[c];
+            if (ch.index < 0 || ch.index >= h->caps[rep]) return fail(PHMC_ERR_ARG, "change index out of range");
+            if (ch.type < 0 || ch.type >= h->E.desc[rep].T) return fail(PHMC_ERR_ARG, "change type out of range");
+            const RepDesc& D = h->E.desc[rep];
+            if (ch.present && !(ch.x >= 0 && ch.x < D.L[0] && ch.y >= 0 && ch.y < D.L[1] && ch.z >= 0 && ch.z < D.L[2]))
+                return fail(PHMC_ERR_ARG, "change position outside [0,L)");
+        }
+        if (t[k].n_changes == 2 && t[k].c[0].index == t[k].c[1].index) return fail(PHMC_ERR_ARG, "changes must touch distinct slots");
+    }
+    return PHMC_OK;
+}
+
+static int ensure_trial_buffers(phmc_engine* h, int n) {
+    if (n <= h->trials_cap) return PHMC_OK;
+    if (h->d_trials) { cudaFree(h->d_trials); cudaFree(h->d_dE); h->d_trials = nullptr; h->d_dE = nullptr; }
+    CU(cudaMalloc((void**)&h->d_trials, sizeof(phmc_trial) * n));
+    CU(cudaMalloc((void**)&h->d_dE, sizeof(double) * n));
+    h->trials_cap = n;
+    return PHMC_OK;
+}
+
+static int flush_dirty(phmc_engine* h) {
+    Engine& E = h->E;
+    if (E.coulomb != PHMC_COUL_EWALD) return PHMC_OK;
+    launch_spread(E, E.d.dirty, E.stream);
+    launch_fft_pipeline(E, E.d.dirty, 0, E.stream);
+    CU(cudaGetLastError());
+    return PHMC_OK;
+}
+
+extern "C" int phmc_delta_energy(phmc_engine* h, int rep, const phmc_trial* trials, int n, double* dE) {
+    if (!h || (n > 0 && (!trials || !dE))) return fail(PHMC_ERR_ARG, "null argument");
+    if (n == 0) return PHMC_OK;
+    int s = check_trials(h, rep, trials, n);
+    if (s) return s;
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    s = ensure_trial_buffers(h, n);
+    if (s) return s;
+    CU(cudaMemcpyAsync(h->d_trials, trials, sizeof(phmc_trial) * n, cudaMemcpyHostToDevice, E.stream));
+    CU(launch_mc(E, MC_EVAL, rep, h->d_trials, n, h->d_dE, E.stream));
+    CU(cudaMemcpyAsync(dE, h->d_dE, sizeof(double) * n, cudaMemcpyDeviceToHost, E.stream));
+    return check_kernel_errors(h);
+}
+
+extern "C" int phmc_commit(phmc_engine* h, int rep, const phmc_trial* trial) {
+    if (!h || !trial) return fail(PHMC_ERR_ARG, "null argument");
+    int s = check_trials(h, rep, trial, 1);
+    if (s) return s;
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    s = ensure_trial_buffers(h, 1);
+    if (s) return s;
+    CU(cudaMemcpyAsync(h->d_trials, trial, sizeof(phmc_trial), cudaMemcpyHostToDevice, E.stream));
+    CU(launch_mc(E, MC_APPLY, rep, h->d_trials, 1, h->d_dE, E.stream));
+    s = flush_dirty(h);
+    if (s) return s;
+    return check_kernel_errors(h);
+}
+
+extern "C" int phmc_set_identity(phmc_engine* h, int rep, int i, int type, float q) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    if (rep < 0 || rep >= h->E.R || i < 0 || i >= h->caps[rep]) return fail(PHMC_ERR_ARG, "index out of range");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    float4 p; int f;
+    CU(cudaMemcpy(&p, E.d.posq + E.desc[rep].slot_off + i, sizeof(float4), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&f, E.d.flags + E.desc[rep].slot_off + i, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f & PHMC_F_GHOST) return fail(PHMC_ERR_STATE, "set_identity on an empty slot");
+    phmc_trial t;
+    std::memset(&t, 0, sizeof t);
+    t.n_changes = 1;
+    t.c[0].index = i; t.c[0].present = 1; t.c[0].x = p.x; t.c[0].y = p.y; t.c[0].z = p.z; t.c[0].q = q; t.c[0].type = type;
+    return phmc_commit(h, rep, &t);
+}
+
+__global__ void k_set_target(RepState* st, int R, long long n) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    st[r].target = st[r].trial + n;
+    st[r].run_start = st[r].trial;
+    st[r].att[0] = st[r].att[1] = st[r].att[2] = 0;
+    st[r].acc[0] = st[r].acc[1] = st[r].acc[2] = 0;
+}
+
+__global__ void k_count_active(const RepState* st, int R, int* active) {
+    __shared__ int c;
+    if (threadIdx.x == 0) c = 0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < R; r += blockDim.x)
+        if (st[r].trial < st[r].target && st[r].error == 0) atomicAdd(&c, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) *active = c;
+}
+
+extern "C" int phmc_set_trial_log(phmc_engine* h, int64_t cap, int* move, double* dE, int* acc) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    Engine& E = h->E;
+    if (E.d.log_move) { cudaFree(E.d.log_move); cudaFree(E.d.log_dE); cudaFree(E.d.log_acc); }
+    E.d.log_move = nullptr; E.d.log_dE = nullptr; E.d.log_acc = nullptr; E.d.log_cap = 0;
+    h->h_log_move = move; h->h_log_dE = dE; h->h_log_acc = acc; h->log_cap = 0;
+    if (!move || !dE || !acc || cap <= 0) return PHMC_OK;
+    CU(cudaMalloc((void**)&E.d.log_move, sizeof(int) * cap));
+    CU(cudaMalloc((void**)&E.d.log_dE, sizeof(double) * cap));
+    CU(cudaMalloc((void**)&E.d.log_acc, sizeof(int) * cap));
+    E.d.log_cap = cap; h->log_cap = cap;
+    return PHMC_OK;
+}
+
+extern "C" int phmc_set_replay(phmc_engine* h, int64_t n, const int* decisions) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    Engine& E = h->E;
+    if (h->d_replay) { cudaFree(h->d_replay); h->d_replay = nullptr; }
+    E.d.replay = nullptr; E.d.replay_n = 0;
+    if (!decisions || n <= 0) return PHMC_OK;
+    CU(cudaMalloc((void**)&h->d_replay, sizeof(int) * n));
+    CU(cudaMemcpy(h->d_replay, decisions, sizeof(int) * n, cudaMemcpyHostToDevice));
+    E.d.replay = h->d_replay; E.d.replay_n = n;
+    return PHMC_OK;
+}
+
+static int collect_stats(phmc_engine* h, phmc_run_stats* stats) {
+    Engine& E = h->E;
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    for (int r = 0; r < E.R; ++r) {
+        phmc_run_stats& o = stats[r];
+        std::memset(&o, 0, sizeof o);
+        for (int k = 0; k < 3; ++k) { o.attempted[k] = st[r].att[k]; o.accepted[k] = st[r].acc[k]; }
+        o.flushes = st[r].flushes;
+        o.n_titratable = E.desc[r].n_titr;
+        o.n_cations = st[r].n_cation; o.n_anions = st[r].n_anion;
+        o.energy = st[r].E; o.energy_drift = st[r].drift;
+    }
+    // protonated sites: count titratable sites with q != 0 (host side, small)
+    for (int r = 0; r < E.R; ++r) {
+        const RepDesc& D = E.desc[r];
+        if (D.n_titr == 0) continue;
+        std::vector<int> titr((size_t)D.n_titr);
+        std::vector<float4> pq((size_t)D.cap);
+        CU(cudaMemcpy(titr.data(), E.d.titr + D.slot_off, sizeof(int) * D.n_titr, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(pq.data(), E.d.posq + D.slot_off, sizeof(float4) * D.cap, cudaMemcpyDeviceToHost));
+        int c = 0;
+        for (int i : titr) if (pq[i].w != 0.0f) ++c;
+        stats[r].n_charged_sites = c;
+    }
+    return PHMC_OK;
+}
+
+// Run the trial/rebuild loop (internal; also used by the timed entry points).
+int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
+    Engine& E = h->E;
+    k_set_target<<<(E.R + 127) / 128, 128, 0, E.stream>>>(E.d.state, E.R, n_trials);
+    if (E.d.log_move) {
+        CU(cudaMemsetAsync(E.d.log_move, 0xff, sizeof(int) * E.d.log_cap, E.stream));
+    }
+    long long iter = 0;
+    const long long max_iter = n_trials + 8;
+    for (;;) {
+        for (int k = 0; k < check_every; ++k) {
+            CU(launch_mc(E, MC_RUN, 0, nullptr, 0, nullptr, E.stream));
+            int s = flush_dirty(h);
+            if (s) return s;
+            ++iter;
+        }
+        k_count_active<<<1, 256, 0, E.stream>>>(E.d.state, E.R, E.d_active);
+        CU(cudaMemcpyAsync(E.h_active, E.d_active, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
+        CU(cudaStreamSynchronize(E.stream));
+        if (*E.h_active == 0) break;
+        if (iter > max_iter) return fail(PHMC_ERR_BUDGET, "trial loop made no progress");
+    }
+    return PHMC_OK;
+}
+
+extern "C" int phmc_run(phmc_engine* h, int64_t n_trials, phmc_run_stats* stats) {
+    if (!h || n_trials < 0) return fail(PHMC_ERR_ARG, "invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    int s = phmc_run_loop(h, n_trials, 1);
+    if (s) return s;
+    s = check_kernel_errors(h);
+    if (s) return s;
+    if (h->h_log_move && E.d.log_move) {
+        const long long n = std::min<long long>(n_trials, E.d.log_cap);
+        CU(cudaMemcpy(h->h_log_move, E.d.log_move, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(h->h_log_dE, E.d.log_dE, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(h->h_log_acc, E.d.log_acc, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    }
+    if (stats) return collect_stats(h, stats);
+    return PHMC_OK;
+}
+
+extern "C" int phmc_get_state(phmc_engine* h, int rep, float* x, float* y, float* z, float* q, int* type, int* flags) {
+    if (!h || rep < 0 || rep >= h->E.R) return fail(PHMC_ERR_ARG, "invalid replica");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    const RepDesc& D = E.desc[rep];
+    std::vector<float4> pq((size_t)D.cap);
+    CU(cudaMemcpy(pq.data(), E.d.posq + D.slot_off, sizeof(float4) * D.cap, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < D.cap; ++i) {
+        if (x) x[i] = pq[i].x;
+        if (y) y[i] = pq[i].y;
+        if (z) z[i] = pq[i].z;
+        if (q) q[i] = pq[i].w;
+    }
+    if (type) CU(cudaMemcpy(type, E.d.type + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
+    if (flags) CU(cudaMemcpy(flags, E.d.flags + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
+    return PHMC_OK;
+}
+
+extern "C" int phmc_get_cells(phmc_engine* h, int rep, int* cell_of, int dims[3]) {
+    if (!h || rep < 0 || rep >= h->E.R) return fail(PHMC_ERR_ARG, "invalid replica");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    const RepDesc& D = E.desc[rep];
+    if (dims) for (int k = 0; k < 3; ++k) dims[k] = D.ncell[k];
+    if (cell_of) CU(cudaMemcpy(cell_of, E.d.cell_of + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
+    return PHMC_OK;
+}
+
+extern "C" int phmc_capacity(phmc_engine* h, int rep) {
+    if (!h || rep < 0 || rep >= h->E.R) return -1;
+    return h->caps[rep];
+}

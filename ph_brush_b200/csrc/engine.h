@@ -1,0 +1,60 @@
+// Host-side engine object and kernel launchers (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "common.cuh"
+
+#define ZPASS_TX 16
+
+struct Engine {
+    int R = 0;
+    int device = 0;
+    int order = 4;
+    int coulomb = 0;
+    int total_slots = 0;
+    int total_cells = 0;
+    int cell_cap = 0;
+    long long total_mesh = 0;
+    long long total_oct = 0;
+    int threads = 256;
+    int pend_max = 16;
+    cudaStream_t stream = nullptr;
+    DevPtrs d{};
+    std::vector<RepDesc> desc;
+    // flush job tables
+    int n_plane_jobs = 0, n_zjobs = 0;
+    int2* d_plane_jobs = nullptr;
+    int4* d_zjobs = nullptr;
+    int* d_zjob_off = nullptr;
+    double* d_epart = nullptr;
+    size_t plane_smem = 0, zpass_smem = 0;
+    int* d_rep_of = nullptr;
+    int* d_cell_rep = nullptr;   // replica of every global cell
+    int* d_dirty = nullptr;      // per replica: mesh must be rebuilt
+    int* d_active = nullptr;     // device counter: replicas still running
+    int* h_active = nullptr;     // pinned mirror
+    // full-energy scratch
+    double* d_epair = nullptr;   // per (replica, block) partial components
+    int energy_blocks = 0;
+    // host copies for trial logs
+    std::vector<int> bonds_host;
+    std::vector<void*> allocs;
+    bool has_G = false;
+};
+
+// k_mesh.cu
+void launch_spread(Engine& E, const int* dirty, cudaStream_t st);
+void launch_fft_pipeline(Engine& E, const int* dirty, int mode, cudaStream_t st);
+void launch_unit_charge(Engine& E, cudaStream_t st);
+void launch_extract_octant(Engine& E, int r, cudaStream_t st);
+cudaError_t mesh_set_smem_limits(Engine& E);
+
+// k_pair.cu
+void launch_cell_build(Engine& E, cudaStream_t st);
+void launch_full_energy(Engine& E, cudaStream_t st);
+
+// k_mc.cu
+enum { MC_RUN = 0, MC_EVAL = 1, MC_APPLY = 2 };
+cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* d_trials, int n, double* d_dE, cudaStream_t st);
+size_t mc_smem_bytes(int order, int pend_max);

@@ -1,0 +1,613 @@
+// Persistent Monte Carlo kernel: one thread block per replica runs trials
+// back to back until its trial target is reached or its pending-stencil
+// buffer is full (the potential mesh is then rebuilt by the mesh kernels).
+//
+// Per trial (replaces total_energy per trial, MC/src/mc.cu:43-60,241,275,425):
+//  * proposal from a counter-based Philox stream (trial index = counter), so a
+//    trial is reproducible and replayable;
+//  * pair dE (LJ/WCA + real-space Coulomb) over the 27 neighbour cells of
+//    every changed particle's old and new state, FP32 terms, FP64 sums;
+//  * FENE dE of displaced bonded beads, wall test;
+//  * reciprocal dE = sum_t c_t [W_t . phi + sum_e c_e S(W_t, W_e)]
+//                    + 1/2 sum_{t,t'} c_t c_t' S(W_t, W_t'),
+//    phi the potential mesh of the last rebuild, W_e the stencils of changes
+//    accepted since then, S(W_a, W_b) = sum_delta G[D + delta] Kx Ky Kz with
+//    K the 1-D cross-correlations of the two stencils' weights and G the
+//    influence kernel (octant table);
+//  * self / net-charge / slab terms from FP64 charge moments;
+//  * Metropolis in FP64 with the move's log factor (MC/src/mc.cu:438-440).
+#include "common.cuh"
+#include "engine.h"
+
+#define NST_MAX 4    // stencils per trial
+#define NPROBE_MAX 4 // (old, new) states of up to two particles
+
+template <int P>
+struct Stencil {
+    int base[3];
+    int m[3][P];   // wrapped mesh coordinates
+    float w[3][P];
+    float coef;
+};
+
+template <int P>
+struct PairK {
+    float K[3][2 * P - 1];
+    int f[3][2 * P - 1];  // folded octant coordinate of D + delta
+    float coef;
+    int pad;
+};
+
+struct TrialS {
+    int stop, skip, move, nch, accept, nprobe, nst, ext_k;
+    double logf;
+    uint32_t ua, ub;
+    long long tnum;
+    int idx[2], pres_old[2], pres_new[2], to[2], tn[2];
+    float4 po[2], pn[2];
+    int4 bonds[2];
+    float4 probe_p[NPROBE_MAX];
+    int probe_t[NPROBE_MAX], probe_owner[NPROBE_MAX], probe_cell[NPROBE_MAX];
+    float probe_sign[NPROBE_MAX];
+    float4 st_pos[NST_MAX];
+    float st_coef[NST_MAX];
+    double d_direct_lj, d_direct_c, d_fene;
+    int total_cand, npairs;
+};
+
+__device__ __forceinline__ void probe_add(TrialS& T, float4 p, int type, int owner, float sign, const RepDesc& D) {
+    const int k = T.nprobe++;
+    T.probe_p[k] = p; T.probe_t[k] = type; T.probe_owner[k] = owner; T.probe_sign[k] = sign;
+    T.probe_cell[k] = cell_index(D, p.x, p.y, p.z);
+}
+
+__device__ __forceinline__ void stencil_add(TrialS& T, float4 p, float c) {
+    if (c == 0.0f) return;
+    T.st_pos[T.nst] = p; T.st_coef[T.nst] = c; T.nst++;
+}
+
+// Fill probes and stencils from the changes in T (old -> new states).
+__device__ void trial_setup(TrialS& T, const RepDesc& D) {
+    T.nprobe = 0; T.nst = 0;
+    for (int k = 0; k < T.nch; ++k) {
+        if (T.pres_old[k]) probe_add(T, T.po[k], T.to[k], k, -1.0f, D);
+        if (T.pres_new[k]) probe_add(T, T.pn[k], T.tn[k], k, 1.0f, D);
+        if (D.coulomb == PHMC_COUL_EWALD) {
+            const bool same_pos = T.pres_old[k] && T.pres_new[k] && T.po[k].x == T.pn[k].x && T.po[k].y == T.pn[k].y &&
+                                  T.po[k].z == T.pn[k].z;
+            if (same_pos) {
+                stencil_add(T, T.pn[k], T.pn[k].w - T.po[k].w);
+            } else {
+                if (T.pres_old[k]) stencil_add(T, T.po[k], -T.po[k].w);
+                if (T.pres_new[k]) stencil_add(T, T.pn[k], T.pn[k].w);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float4 rand_pos(const RepDesc& D, uint32_t a, uint32_t b, uint32_t c) {
+    float4 p;
+    p.x = __fmul_rn(D.L[0], u24(a));
+    p.y = __fmul_rn(D.L[1], u24(b));
+    p.z = D.walls ? __fadd_rn(D.wall_lo, __fmul_rn(__fsub_rn(D.wall_hi, D.wall_lo), u24(c))) : __fmul_rn(D.L[2], u24(c));
+    p.w = 0.0f;
+    return p;
+}
+
+// Proposal of trial T.tnum from the Philox stream (same rules as the oracle's MC).
+__device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const DevPtrs& d) {
+    const long long t = T.tnum;
+    uint32_t A[4], B[4], C[4];
+    philox4x32_10(D.key[0], D.key[1], (uint32_t)t, (uint32_t)((unsigned long long)t >> 32), 0u, 0u, A);
+    philox4x32_10(D.key[0], D.key[1], (uint32_t)t, (uint32_t)((unsigned long long)t >> 32), 1u, 0u, B);
+    philox4x32_10(D.key[0], D.key[1], (uint32_t)t, (uint32_t)((unsigned long long)t >> 32), 2u, 0u, C);
+    T.ua = B[2]; T.ub = B[3];
+    const float um = u24(A[0]);
+    int move = PHMC_MOVE_NONE;
+    if (um < D.p_disp) move = PHMC_MOVE_DISP;
+    else if (um < D.p_disp + D.p_titr) move = PHMC_MOVE_TITR;
+    else if (um < D.p_disp + D.p_titr + D.p_swap) move = PHMC_MOVE_SWAP;
+    T.move = move; T.skip = 0; T.nch = 0; T.logf = 0.0;
+    const int so = D.slot_off;
+    auto load_old = [&](int k, int i) {
+        T.idx[k] = i;
+        T.pres_old[k] = !(d.flags[so + i] & PHMC_F_GHOST);
+        T.po[k] = d.posq[so + i]; T.to[k] = d.type[so + i]; T.bonds[k] = d.bonds[so + i];
+    };
+    if (move == PHMC_MOVE_DISP) {
+        if (S.n_mobile == 0) { T.skip = 1; return; }
+        const int i = d.mobile[so + pick_index(A[1], S.n_mobile)];
+        load_old(0, i);
+        const float dm = D.disp_max;
+        const float dx = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[2])), 1.0f));
+        const float dy = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[3])), 1.0f));
+        const float dz = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(B[0])), 1.0f));
+        float nx = __fadd_rn(T.po[0].x, dx), ny = __fadd_rn(T.po[0].y, dy), nz = __fadd_rn(T.po[0].z, dz);
+        if (nx < 0.0f) nx = __fadd_rn(nx, D.L[0]); else if (nx >= D.L[0]) nx = __fsub_rn(nx, D.L[0]);
+        if (ny < 0.0f) ny = __fadd_rn(ny, D.L[1]); else if (ny >= D.L[1]) ny = __fsub_rn(ny, D.L[1]);
+        if (!D.walls) { if (nz < 0.0f) nz = __fadd_rn(nz, D.L[2]); else if (nz >= D.L[2]) nz = __fsub_rn(nz, D.L[2]); }
+        T.pres_new[0] = 1; T.pn[0] = make_float4(nx, ny, nz, T.po[0].w); T.tn[0] = T.to[0];
+        T.nch = 1;
+        if (D.walls && (nz < D.wall_lo || nz >= D.wall_hi)) T.skip = 2;  // hard wall: infinite energy
+    } else if (move == PHMC_MOVE_TITR) {
+        if (D.n_titr == 0) { T.skip = 1; return; }
+        const int site = d.titr[so + pick_index(A[1], D.n_titr)];
+        load_old(0, site);
+        T.pres_new[0] = 1;
+        if (T.po[0].w == 0.0f) {
+            if (S.n_free == 0) { T.skip = 1; return; }
+            const int g = d.freel[so + S.n_free - 1];
+            load_old(1, g);
+            T.pn[0] = make_float4(T.po[0].x, T.po[0].y, T.po[0].z, D.q_site_charged); T.tn[0] = D.type_site_charged;
+            float4 pg = rand_pos(D, A[2], A[3], B[0]); pg.w = D.q_counterion;
+            T.pres_new[1] = 1; T.pn[1] = pg; T.tn[1] = D.type_counterion;
+            T.logf = D.titr_log;
+        } else {
+            if (S.n_anion == 0) { T.skip = 1; return; }
+            const int g = d.anions[so + pick_index(B[1], S.n_anion)];
+            load_old(1, g);
+            T.pn[0] = make_float4(T.po[0].x, T.po[0].y, T.po[0].z, 0.0f); T.tn[0] = D.type_site_neutral;
+            T.pres_new[1] = 0; T.pn[1] = T.po[1]; T.tn[1] = T.to[1];
+            T.logf = -D.titr_log;
+        }
+        T.nch = 2;
+    } else if (move == PHMC_MOVE_SWAP) {
+        if (u24(A[1]) < 0.5f) {
+            if (S.n_free < 2) { T.skip = 1; return; }
+            const int g1 = d.freel[so + S.n_free - 1], g2 = d.freel[so + S.n_free - 2];
+            load_old(0, g1); load_old(1, g2);
+            float4 p1 = rand_pos(D, A[2], A[3], B[0]); p1.w = D.q_cation;
+            float4 p2 = rand_pos(D, C[0], C[1], C[2]); p2.w = D.q_counterion;
+            T.pres_new[0] = 1; T.pn[0] = p1; T.tn[0] = D.type_cation;
+            T.pres_new[1] = 1; T.pn[1] = p2; T.tn[1] = D.type_counterion;
+            T.logf = log(D.salt_c2V2 / ((double)(S.n_cation + 1) * (double)(S.n_anion + 1)));
+        } else {
+            if (S.n_cation == 0 || S.n_anion == 0) { T.skip = 1; return; }
+            const int g1 = d.cations[so + pick_index(B[1], S.n_cation)];
+            const int g2 = d.anions[so + pick_index(C[3], S.n_anion)];
+            load_old(0, g1); load_old(1, g2);
+            T.pres_new[0] = 0; T.pn[0] = T.po[0]; T.tn[0] = T.to[0];
+            T.pres_new[1] = 0; T.pn[1] = T.po[1]; T.tn[1] = T.to[1];
+            T.logf = log((double)S.n_cation * (double)S.n_anion / D.salt_c2V2);
+        }
+        T.nch = 2;
+    } else {
+        T.skip = 3;  // no-op draw
+    }
+}
+
+// External trial (phmc_delta_energy / phmc_commit / phmc_set_identity).
+__device__ void load_external(TrialS& T, const RepDesc& D, const DevPtrs& d, const phmc_trial& e) {
+    const int so = D.slot_off;
+    T.nch = e.n_changes; T.skip = 0; T.logf = 0.0; T.move = PHMC_MOVE_NONE;
+    for (int k = 0; k < e.n_changes; ++k) {
+        const int i = e.c[k].index;
+        T.idx[k] = i;
+        T.pres_old[k] = !(d.flags[so + i] & PHMC_F_GHOST);
+        T.po[k] = d.posq[so + i]; T.to[k] = d.type[so + i]; T.bonds[k] = d.bonds[so + i];
+        T.pres_new[k] = e.c[k].present;
+        T.pn[k] = make_float4(e.c[k].x, e.c[k].y, e.c[k].z, e.c[k].q);
+        T.tn[k] = e.c[k].type;
+    }
+    if (T.nch == 1) T.move = PHMC_MOVE_DISP;
+}
+
+template <int P>
+__device__ __forceinline__ void make_stencil(Stencil<P>& s, const RepDesc& D, float4 p, float coef) {
+    const float g[3] = {p.x / D.L[0] * (float)D.mesh[0], p.y / D.L[1] * (float)D.mesh[1], p.z / D.L[2] * (float)D.mesh[2]};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float fl = floorf(g[k]);
+        bspline_weights<P>(g[k] - fl, s.w[k]);
+        s.base[k] = (int)fl + P / 2 - P + 1;
+#pragma unroll
+        for (int j = 0; j < P; ++j) s.m[k][j] = wrap_idx(s.base[k] + j, D.mesh[k]);
+    }
+    s.coef = coef;
+}
+
+template <int P>
+__device__ __forceinline__ void make_pair(PairK<P>& q, const Stencil<P>& a, const Stencil<P>& b, float coef, const RepDesc& D) {
+    constexpr int W = 2 * P - 1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int n = D.mesh[k];
+        const int Dd = a.base[k] - b.base[k];
+#pragma unroll
+        for (int t = 0; t < W; ++t) {
+            const int delta = t - (P - 1);
+            float s = 0.0f;
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                const int j = i - delta;
+                if (j >= 0 && j < P) s += a.w[k][i] * b.w[k][j];
+            }
+            q.K[k][t] = s;
+            int m = wrap_idx(Dd + delta, n);
+            q.f[k][t] = min(m, n - m);
+        }
+    }
+    q.coef = coef;
+}
+
+__device__ __forceinline__ void list_remove(int* list, int* pos, int& n, int so, int i) {
+    const int k = pos[so + i];
+    const int last = list[so + n - 1];
+    list[so + k] = last; pos[so + last] = k;
+    --n;
+    pos[so + i] = -1;
+}
+__device__ __forceinline__ void list_append(int* list, int* pos, int& n, int so, int i) {
+    list[so + n] = i; pos[so + i] = n; ++n;
+}
+
+__device__ bool cell_remove(const DevPtrs& d, const RepDesc& D, int i) {
+    const int gi = D.slot_off + i;
+    const int c = d.cell_of[gi], k = d.cell_pos[gi];
+    int* cnt = d.cell_count + D.cell_off + c;
+    int* l = d.cell_list + ((size_t)D.cell_off + c) * D.cell_cap;
+    const int n = *cnt;
+    const int last = l[n - 1];
+    l[k] = last; d.cell_pos[D.slot_off + last] = k;
+    *cnt = n - 1;
+    d.cell_of[gi] = -1; d.cell_pos[gi] = -1;
+    return true;
+}
+__device__ bool cell_insert(const DevPtrs& d, const RepDesc& D, int i, int c) {
+    const int gi = D.slot_off + i;
+    int* cnt = d.cell_count + D.cell_off + c;
+    const int n = *cnt;
+    if (n >= D.cell_cap) return false;
+    d.cell_list[((size_t)D.cell_off + c) * D.cell_cap + n] = i;
+    *cnt = n + 1;
+    d.cell_of[gi] = c; d.cell_pos[gi] = n;
+    return true;
+}
+
+__device__ __forceinline__ double slab_energy(const RepDesc& D, double Q, double Mz, double S2) {
+    if (!D.slab) return 0.0;
+    double e = D.slab_coef * Mz * Mz;
+    if (fabs(Q) > 1e-4) e -= D.slab_coef * Q * (S2 + Q * D.Lz2_12);
+    return e;
+}
+
+template <int NT>
+__device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[w * 3] = a; red[w * 3 + 1] = b; red[w * 3 + 2] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0, y = 0, z = 0;
+        for (int k = 0; k < NT / 32; ++k) { x += red[k * 3]; y += red[k * 3 + 1]; z += red[k * 3 + 2]; }
+        red[96] = x; red[97] = y; red[98] = z;
+    }
+    __syncthreads();
+    a = red[96]; b = red[97]; c = red[98];
+}
+
+template <int P, int NT>
+__global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
+                                           double* __restrict__ ext_dE, int pend_max) {
+    constexpr int W = 2 * P - 1;
+    constexpr int W3 = W * W * W;
+    constexpr int P3 = P * P * P;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    Stencil<P>* s_pend = reinterpret_cast<Stencil<P>*>(dsm);
+    Stencil<P>* s_tst = s_pend + pend_max;
+    PairK<P>* s_pair = reinterpret_cast<PairK<P>*>(s_tst + NST_MAX);
+    __shared__ TrialS T;
+    __shared__ RepState S;
+    __shared__ int s_cnt[NPROBE_MAX * 27], s_off[NPROBE_MAX * 27 + 1], s_cell[NPROBE_MAX * 27];
+    __shared__ double red[100];
+    __shared__ int s_npend;
+
+    const int r = (mode == MC_RUN) ? blockIdx.x : ext_rep;
+    const RepDesc& D = d.desc[r];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        S = d.state[r];
+        s_npend = 0;
+        T.ext_k = 0;
+        T.stop = 0;
+    }
+    __syncthreads();
+
+    for (;;) {
+        // ---------------- proposal ----------------
+        if (tid == 0) {
+            T.stop = 0;
+            if (S.error) T.stop = 1;
+            else if (mode == MC_RUN) {
+                if (S.trial >= S.target) { T.stop = 1; S.stop_reason = 0; }
+                else if (s_npend + 2 > pend_max) { T.stop = 1; S.stop_reason = 1; }
+                else { T.tnum = S.trial; propose(T, D, S, d); S.trial++; }
+            } else {
+                if (T.ext_k >= n_ext) T.stop = 1;
+                else { load_external(T, D, d, ext[T.ext_k]); T.tnum = T.ext_k; }
+            }
+            if (!T.stop && T.skip == 0) trial_setup(T, D);
+        }
+        __syncthreads();
+        if (T.stop) break;
+        if (T.skip) {
+            if (tid == 0) {
+                if (T.move < 3) S.att[T.move]++;
+                const long long li = T.tnum - S.run_start;
+                if (mode == MC_RUN && r == 0 && d.log_move && li < d.log_cap) {
+                    d.log_move[li] = T.move;
+                    d.log_dE[li] = (T.skip == 2) ? __longlong_as_double(0x7ff0000000000000ll) : __longlong_as_double(0x7ff8000000000000ll);
+                    d.log_acc[li] = 0;
+                }
+                if (mode != MC_RUN) {
+                    if (ext_dE) ext_dE[T.ext_k] = __longlong_as_double(0x7ff0000000000000ll);
+                    T.ext_k++;
+                }
+            }
+            __syncthreads();
+            continue;
+        }
+        // ---------------- phase 2: cell counts, stencils, direct & bonded terms ----------------
+        const int nent = T.nprobe * 27;
+        if (tid < nent) {
+            const int p = tid / 27, nb = tid % 27;
+            const int c = T.probe_cell[p];
+            const int cx = c % D.ncell[0], cy = (c / D.ncell[0]) % D.ncell[1], cz = c / (D.ncell[0] * D.ncell[1]);
+            const int nc = (wrap_idx(cz + nb / 9 - 1, D.ncell[2]) * D.ncell[1] + wrap_idx(cy + (nb / 3) % 3 - 1, D.ncell[1])) *
+                               D.ncell[0] + wrap_idx(cx + nb % 3 - 1, D.ncell[0]);
+            s_cell[tid] = nc;
+            s_cnt[tid] = min(d.cell_count[D.cell_off + nc], D.cell_cap);
+        }
+        if (tid >= 108 && tid < 108 + T.nst) {
+            const int k = tid - 108;
+            make_stencil<P>(s_tst[k], D, T.st_pos[k], T.st_coef[k]);
+        }
+        if (tid == 112) {
+            double dl = 0.0, dc = 0.0;
+            if (T.nch == 2) {
+                const bool bonded = in_bonds(T.bonds[0], T.idx[1]);
+                float elj, ec;
+                if (T.pres_new[0] && T.pres_new[1]) {
+                    pair_energy(D, min_image(T.pn[0].x - T.pn[1].x, D.L[0]), min_image(T.pn[0].y - T.pn[1].y, D.L[1]),
+                                min_image(T.pn[0].z - T.pn[1].z, D.L[2]), T.tn[0], T.tn[1], T.pn[0].w, T.pn[1].w, bonded, elj, ec);
+                    dl += elj; dc += ec;
+                }
+                if (T.pres_old[0] && T.pres_old[1]) {
+                    pair_energy(D, min_image(T.po[0].x - T.po[1].x, D.L[0]), min_image(T.po[0].y - T.po[1].y, D.L[1]),
+                                min_image(T.po[0].z - T.po[1].z, D.L[2]), T.to[0], T.to[1], T.po[0].w, T.po[1].w, bonded, elj, ec);
+                    dl -= elj; dc -= ec;
+                }
+            }
+            T.d_direct_lj = dl; T.d_direct_c = dc;
+        }
+        if (tid == 113) {
+            double df = 0.0;
+            if (D.fene_k > 0.0f) {
+                for (int k = 0; k < T.nch; ++k) {
+                    if (!(T.pres_old[k] && T.pres_new[k])) continue;
+                    const int bl[4] = {T.bonds[k].x, T.bonds[k].y, T.bonds[k].z, T.bonds[k].w};
+                    for (int b = 0; b < 4; ++b) {
+                        const int j = bl[b];
+                        if (j < 0 || (T.nch == 2 && (j == T.idx[0] || j == T.idx[1]))) continue;
+                        const float4 pj = d.posq[D.slot_off + j];
+                        float dx = min_image(T.pn[k].x - pj.x, D.L[0]), dy = min_image(T.pn[k].y - pj.y, D.L[1]),
+                              dz = min_image(T.pn[k].z - pj.z, D.L[2]);
+                        const float en = fene_energy(D, dx * dx + dy * dy + dz * dz);
+                        dx = min_image(T.po[k].x - pj.x, D.L[0]); dy = min_image(T.po[k].y - pj.y, D.L[1]);
+                        dz = min_image(T.po[k].z - pj.z, D.L[2]);
+                        const float eo = fene_energy(D, dx * dx + dy * dy + dz * dz);
+                        df += (double)en - (double)eo;
+                    }
+                }
+            }
+            T.d_fene = df;
+        }
+        __syncthreads();
+        // ---------------- phase 3: candidate offsets, stencil pair kernels ----------------
+        if (tid < 32) {
+            int carry = 0;
+            for (int b0 = 0; b0 < nent; b0 += 32) {
+                const int e = b0 + tid;
+                const int v = (e < nent) ? s_cnt[e] : 0;
+                int x = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (tid >= o) x += y;
+                }
+                if (e < nent) s_off[e] = carry + x - v;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (tid == 0) { s_off[nent] = carry; T.total_cand = carry; }
+        } else {
+            const int nst = T.nst, np = s_npend;
+            const int npairs = nst * np + nst * (nst + 1) / 2;
+            for (int q = tid - 32; q < npairs; q += NT - 32) {
+                if (q < nst * np) {
+                    const int t = q / np, e = q % np;
+                    make_pair<P>(s_pair[q], s_tst[t], s_pend[e], s_tst[t].coef * s_pend[e].coef, D);
+                } else {
+                    int rem = q - nst * np, t = 0;
+                    while (rem >= nst - t) { rem -= nst - t; ++t; }
+                    const int t2 = t + rem;
+                    const float c = s_tst[t].coef * s_tst[t2].coef * (t == t2 ? 0.5f : 1.0f);
+                    make_pair<P>(s_pair[q], s_tst[t], s_tst[t2], c, D);
+                }
+            }
+            if (tid == 32) T.npairs = npairs;
+        }
+        __syncthreads();
+        // ---------------- phase 4: all pair / mesh work items ----------------
+        double acc_lj = 0.0, acc_c = 0.0, acc_rec = 0.0;
+        {
+            const int total = T.total_cand;
+            const int so = D.slot_off;
+            for (int it = tid; it < total; it += NT) {
+                int lo = 0, hi = nent - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+                }
+                const int p = lo / 27;
+                const int j = d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + (it - s_off[lo])];
+                if (j == T.idx[0] || (T.nch == 2 && j == T.idx[1])) continue;
+                const float4 pj = d.posq[so + j];
+                const int tj = d.type[so + j];
+                const float4 pp = T.probe_p[p];
+                float elj, ec;
+                pair_energy(D, min_image(pp.x - pj.x, D.L[0]), min_image(pp.y - pj.y, D.L[1]), min_image(pp.z - pj.z, D.L[2]),
+                            T.probe_t[p], tj, pp.w, pj.w, in_bonds(T.bonds[T.probe_owner[p]], j), elj, ec);
+                acc_lj += (double)(T.probe_sign[p] * elj);
+                acc_c += (double)(T.probe_sign[p] * ec);
+            }
+        }
+        if (D.coulomb == PHMC_COUL_EWALD) {
+            const float* phi = d.phi + D.mesh_off;
+            const int nx = D.mesh[0], ny = D.mesh[1];
+            const int nphi = T.nst * P3;
+            for (int it = tid; it < nphi; it += NT) {
+                const int st = it / P3, rem = it % P3;
+                const int c = rem / (P * P), b = (rem / P) % P, a = rem % P;
+                const Stencil<P>& s = s_tst[st];
+                const float v = phi[((size_t)s.m[2][c] * ny + s.m[1][b]) * nx + s.m[0][a]];
+                acc_rec += (double)(s.coef * s.w[0][a] * s.w[1][b] * s.w[2][c] * v);
+            }
+            const float* G = d.goct + D.oct_off;
+            const int ox = D.oct[0], oy = D.oct[1];
+            const int nit = T.npairs * W3;
+            for (int it = tid; it < nit; it += NT) {
+                const int q = it / W3, rem = it % W3;
+                const int dz = rem / (W * W), dy = (rem / W) % W, dx = rem % W;
+                const PairK<P>& pk = s_pair[q];
+                const float g = __ldg(&G[((size_t)pk.f[2][dz] * oy + pk.f[1][dy]) * ox + pk.f[0][dx]]);
+                acc_rec += (double)(pk.coef * pk.K[0][dx] * pk.K[1][dy] * pk.K[2][dz] * g);
+            }
+        }
+        block_sum3<NT>(acc_lj, acc_c, acc_rec, red);
+        // ---------------- phase 5: decision and update ----------------
+        if (tid == 0) {
+            double dQ = 0, dQ2 = 0, dMz = 0, dS2 = 0;
+            for (int k = 0; k < T.nch; ++k) {
+                if (T.pres_new[k]) {
+                    const double q = T.pn[k].w, z = T.pn[k].z;
+                    dQ += q; dQ2 += q * q; dMz += q * z; dS2 += q * z * z;
+                }
+                if (T.pres_old[k]) {
+                    const double q = T.po[k].w, z = T.po[k].z;
+                    dQ -= q; dQ2 -= q * q; dMz -= q * z; dS2 -= q * z * z;
+                }
+            }
+            double dself = 0, dqc = 0, dslab = 0;
+            if (D.coulomb == PHMC_COUL_EWALD) {
+                dself = D.self_coef * dQ2;
+                const double Qn = S.Q + dQ;
+                dqc = D.qcorr_coef * (Qn * Qn - S.Q * S.Q);
+                dslab = slab_energy(D, Qn, S.Mz + dMz, S.S2 + dS2) - slab_energy(D, S.Q, S.Mz, S.S2);
+            }
+            const double dlj = acc_lj + T.d_direct_lj, dc = acc_c + T.d_direct_c;
+            const double dE = dlj + dc + T.d_fene + acc_rec + dself + dqc + dslab;
+            int accept = 0;
+            if (mode == MC_RUN) {
+                const long long li = T.tnum - S.run_start;
+                if (r == 0 && d.replay && li < d.replay_n) accept = d.replay[li];
+                else {
+                    const double expo = -D.beta * dE + T.logf;
+                    accept = (expo >= 0.0) || (u53(T.ua, T.ub) < exp(expo));
+                }
+                if (r == 0 && d.log_move && li < d.log_cap) { d.log_move[li] = T.move; d.log_dE[li] = dE; d.log_acc[li] = accept; }
+                S.att[T.move]++;
+            } else if (mode == MC_EVAL) {
+                if (ext_dE) ext_dE[T.ext_k] = dE;
+            } else {
+                accept = 1;
+                if (ext_dE) ext_dE[T.ext_k] = dE;
+            }
+            if (mode != MC_RUN) T.ext_k++;
+            if (accept) {
+                if (mode == MC_RUN) S.acc[T.move]++;
+                const int so = D.slot_off;
+                for (int k = 0; k < T.nch; ++k) {
+                    const int i = T.idx[k];
+                    const int gi = so + i;
+                    if (T.pres_old[k] && T.pres_new[k]) {
+                        d.posq[gi] = T.pn[k];
+                        d.type[gi] = T.tn[k];
+                        const int nc = cell_index(D, T.pn[k].x, T.pn[k].y, T.pn[k].z);
+                        if (nc != d.cell_of[gi]) {
+                            cell_remove(d, D, i);
+                            if (!cell_insert(d, D, i, nc)) S.error = PHMC_ERR_CAPACITY;
+                        }
+                    } else if (!T.pres_old[k] && T.pres_new[k]) {  // insertion into a free slot
+                        int fk = -1;
+                        for (int f = S.n_free - 1; f >= 0; --f) if (d.freel[so + f] == i) { fk = f; break; }
+                        if (fk >= 0) { d.freel[so + fk] = d.freel[so + S.n_free - 1]; S.n_free--; }
+                        d.posq[gi] = T.pn[k];
+                        d.type[gi] = T.tn[k];
+                        int fl = PHMC_F_MOBILE;
+                        list_append(d.mobile, d.mobile_pos, S.n_mobile, so, i);
+                        if (T.pn[k].w > 0.0f) { fl |= PHMC_F_CATION; list_append(d.cations, d.cation_pos, S.n_cation, so, i); }
+                        else if (T.pn[k].w < 0.0f) { fl |= PHMC_F_ANION; list_append(d.anions, d.anion_pos, S.n_anion, so, i); }
+                        d.flags[gi] = fl;
+                        if (!cell_insert(d, D, i, cell_index(D, T.pn[k].x, T.pn[k].y, T.pn[k].z))) S.error = PHMC_ERR_CAPACITY;
+                    } else if (T.pres_old[k] && !T.pres_new[k]) {  // deletion
+                        const int fl = d.flags[gi];
+                        if (fl & PHMC_F_CATION) list_remove(d.cations, d.cation_pos, S.n_cation, so, i);
+                        if (fl & PHMC_F_ANION) list_remove(d.anions, d.anion_pos, S.n_anion, so, i);
+                        if (fl & PHMC_F_MOBILE) list_remove(d.mobile, d.mobile_pos, S.n_mobile, so, i);
+                        d.flags[gi] = PHMC_F_GHOST;
+                        d.freel[so + S.n_free] = i; S.n_free++;
+                        cell_remove(d, D, i);
+                    }
+                }
+                for (int k = 0; k < T.nst; ++k) {
+                    if (s_npend < pend_max) s_pend[s_npend++] = s_tst[k];
+                    else S.error = PHMC_ERR_CAPACITY;
+                }
+                S.Q += dQ; S.Q2 += dQ2; S.Mz += dMz; S.S2 += dS2;
+                S.E_pair_lj += dlj; S.E_pair_c += dc; S.E_fene += T.d_fene; S.E_rec += acc_rec;
+                S.E_self += dself; S.E_qcorr += dqc; S.E_slab += dslab;
+                S.E += dE;
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        d.state[r] = S;
+        if (s_npend > 0) d.dirty[r] = 1;  // potential mesh is stale: rebuild before the next MC launch
+    }
+}
+
+template <int P, int NT>
+static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
+    const size_t smem = mc_smem_bytes(P, E.pend_max);
+    cudaError_t e = cudaFuncSetAttribute(k_mc<P, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (mode == MC_RUN) ? E.R : 1;
+    k_mc<P, NT><<<grid, NT, smem, st>>>(E.d, mode, rep, t, n, dE, E.pend_max);
+    return cudaGetLastError();
+}
+
+size_t mc_smem_bytes(int order, int pend_max) {
+    size_t st = 0, pk = 0;
+    switch (order) {
+        case 4: st = sizeof(Stencil<4>); pk = sizeof(PairK<4>); break;
+        case 5: st = sizeof(Stencil<5>); pk = sizeof(PairK<5>); break;
+        default: st = sizeof(Stencil<6>); pk = sizeof(PairK<6>); break;
+    }
+    const size_t npairs = (size_t)NST_MAX * pend_max + NST_MAX * (NST_MAX + 1) / 2;
+    return st * (pend_max + NST_MAX) + pk * npairs;
+}
+
+cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
+    const int NTh = E.threads;
+    switch (E.order) {
+        case 4: return NTh == 128 ? launch_mc_t<4, 128>(E, mode, rep, t, n, dE, st) : launch_mc_t<4, 256>(E, mode, rep, t, n, dE, st);
+        case 5: return NTh == 128 ? launch_mc_t<5, 128>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256>(E, mode, rep, t, n, dE, st);
+        default: return NTh == 128 ? launch_mc_t<6, 128>(E, mode, rep, t, n, dE, st) : launch_mc_t<6, 256>(E, mode, rep, t, n, dE, st);
+    }
+}
