@@ -1,0 +1,302 @@
+#!/usr/bin/env python3
+"""Benchmark: Monte Carlo sweeps/s of the plain engine on the config-2 brush.
+
+Workload: 10x10 grafted chains x 50 titratable beads (pKa 7.5, pH 6.5), box
+40x40x100 sigma padded to 300 for the slab correction, 0.1 M salt (about 12k
+particles), SPME mesh 64x64x384 order 5, WCA + FENE + erfc Coulomb, moves 90 %
+displacement (0.3 sigma) / 10 % protonation with counterion insert/delete.
+One step = one sweep = N_particles trial moves of the replica.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank runs its own replica
+(replicas only, weak scaling); the timed region is bracketed by barriers and
+the max device time over ranks is reported.  `--impl reference` runs the
+reference's own CUDA build (compiled from its sources into oracle/_ref) on the
+same system in the reference's model and prints the same metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC sweeps/s on 1 B200: batched+surrogate vs plain, α(pH) within 0.005"
+UNIT = "sweeps/s"
+FALLBACK_HBM_GBS = 6650.0
+WORKLOAD = ("config 2: plain constant-pH MC, 10x10 chains x 50 titratable beads, 40x40x100 box padded to 300, "
+            "0.1 M salt, ~12k particles, SPME 64x64x384 order 5, rc 3, 90% displacement / 10% protonation")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.path = tempfile.mktemp(suffix=".csv")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(dev)], stdout=open(self.path, "w"),
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return float(json.load(open(path))["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    try:
+        return json.load(open(path)).get(kernel, {}).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def reduce_max(val, world, dev):
+    if world == 1:
+        return val
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([val], dtype=torch.float64, device=f"cuda:{dev}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(s, p, seconds):
+    """The FP64 oracle's Monte Carlo (same move set, energy from scratch per trial) on the host cores."""
+    from oracle import pyoracle as O
+    mc = O.MC(s, p)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        mc.step()
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds and n >= 2:
+            break
+    mc.close()
+    tps = n / el
+    cores = os.cpu_count()
+    return {"value": tps / s.n, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} trials of the config-2 system in {el:.1f} s (FP64, O(N^2) pairs + FP64 FFT per trial, "
+                      f"{cores} OpenMP threads); sweeps/s = trials/s / {s.n}",
+            "trials_per_s": tps}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from ph_brush_b200 import configs
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build missing: run `make -C oracle ref`"}))
+        return
+    sn, _ = configs.config2()
+    n_sites = int(((sn.flags & 2) != 0).sum())
+    n_charged = int(((sn.flags & 2) != 0).__and__(sn.q != 0).sum())
+    spacing = 0.7  # reference mesh rule: 60x60x432 (1.56 M points) for the 40x40x300 box
+    s, p = configs.to_reference_semantics(sn, n_w=n_sites, spacing=spacing, seed=5)
+    d = tempfile.mkdtemp()
+    configs.write_lammps_data(os.path.join(d, "in.data"), s)
+    pct = 100.0 * (n_charged + 0.5) / n_sites  # floor(pct/100 * sites) == current count (build_plan needs target >= current)
+    configs.write_params_in(os.path.join(d, "params.in"), p, spacing, extra={"target_pct": f"{pct:.8f}"})
+    per_step = 20
+    r = subprocess.run([harness, "time", os.path.join(d, "in.data"), os.path.join(d, "params.in"),
+                        str(per_step * args.steps), str(per_step * args.warmup)], capture_output=True, text=True)
+    if r.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": "reference harness failed: " + r.stderr.strip()[-200:]}))
+        return
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    sweeps = out["trials_per_s"] / sn.n
+    line = {"impl": "reference", "metric": METRIC, "value": sweeps, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * out["seconds"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brush generator)",
+            "config": {"workload": WORKLOAD + " (reference model: LJ cut at 3 sigma, 1-2 exclusions, cubic SPME, "
+                                  "mesh from pme_spacing 0.7 -> %s; moves: the reference's phase-2 identity swaps)"
+                                  % out["mesh"], "particles": sn.n, "reference_atoms": out["natoms"],
+                       "trials_per_step": per_step},
+            "cpu_baseline": {"value": sweeps, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{out['trials']} trials of phase2_swap_jitter (MC/src/mc.cu:159-318) in the "
+                                       f"reference's CUDA build on this B200 (one host thread), CUDA-event timed"},
+            "e2e": {"value": sweeps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "trials_per_s": out["trials_per_s"], "reference_seconds": out["seconds"]}
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import numpy as np
+    from ph_brush_b200 import Engine, configs
+
+    s, p = configs.config2(seed=2026 + rank)
+    N = s.n
+    eng = Engine(s, p, device=local)
+    for _ in range(args.warmup):
+        eng.run(N)
+    # ---- device-timed region: inputs resident, L2 flushed between steps ----
+    eng.set_profiling(True)
+    eng.profile(reset=True)
+    clocks = Clocks(local)
+    barrier(world)
+    dev_ms = 0.0
+    for _ in range(args.steps):
+        eng.flush_l2(256 << 20)
+        dev_ms += eng.run_timed(N)
+    barrier(world)
+    clk = clocks.stop()
+    prof = eng.profile(reset=True)
+    eng.set_profiling(False)
+    max_ms = reduce_max(dev_ms, world, local)
+    value = world * args.steps / (max_ms / 1e3)
+
+    # ---- end to end through the public API: pinned host state in, state + energy out ----
+    st = eng.state()
+    try:
+        import torch
+        pinned = {k: torch.from_numpy(v.copy()).pin_memory().numpy() for k, v in st.items()}
+    except Exception:
+        pinned = {k: v.copy() for k, v in st.items()}
+    cap = len(st["x"])
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.set_state(pinned)
+        res = eng.run(N)
+        out = eng.state()
+        energy = res[0]["energy"]
+    e2e_s = time.perf_counter() - t0
+    barrier(world)
+    e2e_s = reduce_max(e2e_s, world, local)
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": cap * (16 + 4 + 4), "d2h_bytes_per_step": cap * (16 + 4 + 4) + 8,
+           "timing": "host wall clock around phmc_set_state + phmc_run + phmc_get_state (synchronous calls)"}
+
+    # ---- roofline of the dominant kernel ----
+    peak, peak_kind = measured_peak()
+    kern = []
+    if prof["mc_launches"]:
+        ms = prof["mc_ms"] / prof["mc_launches"]
+        by = prof["mc_alg_bytes"] / prof["mc_launches"]
+        kern.append(("k_mc", prof["mc_ms"], ms, by))
+    if prof["flush_launches"]:
+        ms = prof["flush_ms"] / prof["flush_launches"]
+        by = prof["flush_alg_bytes"] / prof["flush_launches"]
+        kern.append(("mesh_rebuild", prof["flush_ms"], ms, by))
+    kern.sort(key=lambda k: -k[1])
+    rl = {}
+    for name, tot, ms, by in kern:
+        ach = by / (ms / 1e3) / 1e9
+        rl[name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "peak_source": peak_kind, "traffic": ncu_traffic(name), "alg_bytes_per_launch": by,
+                    "avg_launch_ms": ms, "launches": prof[("mc" if name == "k_mc" else "flush") + "_launches"],
+                    "share_of_timed": tot / dev_ms if dev_ms else None}
+    dominant = kern[0][0] if kern else None
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (f64 accumulation and Metropolis)",
+            "data": "synthetic (seeded brush generator, seed 2026 + rank)",
+            "config": {"workload": WORKLOAD, "particles": N, "trials_per_step": N, "mesh": list(p.mesh),
+                       "order": p.order, "pending_max": p.pending_max or 16,
+                       "l2": "flushed between steps (256 MiB write on the engine stream)",
+                       "parallelism": f"replicas only x{world}"},
+            "roofline": dict(rl[dominant], kernel=dominant) if dominant else None,
+            "roofline_other": {k: v for k, v in rl.items() if k != dominant},
+            "e2e": e2e, "gpu_launches": int(prof["kernel_launches"]),
+            "trials_per_s": world * prof["trials"] / (max_ms / 1e3) if prof["trials"] else None,
+            "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(s, p, args.cpu_seconds)
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

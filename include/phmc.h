@@ -200,6 +200,30 @@ int phmc_set_replay(phmc_engine* e, int64_t n, const int* decisions);
 /* ---- state ---- */
 int phmc_get_state(phmc_engine* e, int replica, float* x, float* y, float* z, float* q,
                    int* type, int* flags);
+/* Replace replica r's particle state from host arrays of capacity length (bonds
+ * unchanged); rebuilds lists, cells and the potential mesh.  The reference's
+ * counterpart is upload_atoms_to_device (MC/src/main.cu:18-41). */
+int phmc_set_state(phmc_engine* e, int replica, const float* x, const float* y, const float* z,
+                   const float* q, const int* type, const int* flags);
+
+/* ---- measurement (no counterpart in the reference) ---- */
+typedef struct phmc_profile {
+    double mc_ms;            /* summed device time of Monte Carlo kernel launches */
+    double flush_ms;         /* summed device time of potential-mesh rebuilds */
+    int64_t mc_launches;
+    int64_t flush_launches;  /* rebuild pipelines (each = spread + 3 FFT passes + reduce) */
+    int64_t kernel_launches; /* every kernel the engine launched */
+    double mc_alg_bytes;     /* algorithmic bytes of all trials (per-trial model in the docs) */
+    double flush_alg_bytes;  /* algorithmic bytes of all rebuilds: 16 N + 16 M + 16 Mc per replica */
+    int64_t trials;
+} phmc_profile;
+/* Profiling on: per-launch CUDA events around the MC kernel and the rebuilds. */
+int phmc_set_profiling(phmc_engine* e, int on);
+int phmc_get_profile(phmc_engine* e, phmc_profile* out, int reset);
+/* phmc_run with its device time (CUDA events on the engine stream) in *device_ms. */
+int phmc_run_timed(phmc_engine* e, int64_t n_trials, double* device_ms);
+/* Write `bytes` of scratch on the engine stream (evicts L2 between timed steps). */
+int phmc_flush_l2(phmc_engine* e, int64_t bytes);
 /* cell index of every slot (-1 for ghosts) and the cell grid dimensions */
 int phmc_get_cells(phmc_engine* e, int replica, int* cell_of, int dims[3]);
 int phmc_capacity(phmc_engine* e, int replica);

@@ -69,6 +69,15 @@ class RunStats(C.Structure):
                 ("n_anions", C.c_int), ("energy", C.c_double), ("energy_drift", C.c_double)]
 
 
+class Profile(C.Structure):
+    _fields_ = [("mc_ms", C.c_double), ("flush_ms", C.c_double), ("mc_launches", C.c_int64),
+                ("flush_launches", C.c_int64), ("kernel_launches", C.c_int64), ("mc_alg_bytes", C.c_double),
+                ("flush_alg_bytes", C.c_double), ("trials", C.c_int64)]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class BrushSpec(C.Structure):
     _fields_ = [("chains_x", C.c_int), ("chains_y", C.c_int), ("graft_spacing", C.c_double),
                 ("len_min", C.c_int), ("len_max", C.c_int), ("n_permanent", C.c_int),
@@ -79,7 +88,8 @@ class BrushSpec(C.Structure):
 
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
-           "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush"]
+           "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
+           "phmc_set_state", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2"]
 
 
 def load_library(path=LIB_PATH):
@@ -104,6 +114,11 @@ def load_library(path=LIB_PATH):
         "phmc_get_cells": ([eng, C.c_int, _ip, _ip], C.c_int),
         "phmc_capacity": ([eng, C.c_int], C.c_int),
         "phmc_build_brush": ([C.POINTER(BrushSpec), C.c_int, _fp, _fp, _fp, _fp, _ip, _ip, C.c_int, _ip, _ip, _ip, _dp], C.c_int),
+        "phmc_set_state": ([eng, C.c_int, _fp, _fp, _fp, _fp, _ip, _ip], C.c_int),
+        "phmc_set_profiling": ([eng, C.c_int], C.c_int),
+        "phmc_get_profile": ([eng, C.POINTER(Profile), C.c_int], C.c_int),
+        "phmc_run_timed": ([eng, C.c_int64, _dp], C.c_int),
+        "phmc_flush_l2": ([eng, C.c_int64], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -74,6 +74,8 @@ struct RepState {
     double Q, Q2, Mz, S2;  // charge moments
     double drift;       // |tracked E_rec - recomputed| at the last flush
     double E_rec_flush; // E_rec computed at the last flush
+    double alg_bytes;   // algorithmic bytes of the trials run so far
+    long long trials_run;
 };
 
 // Device pointers of the whole engine (all replicas concatenated).

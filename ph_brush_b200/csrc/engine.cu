@@ -34,7 +34,26 @@ struct phmc_engine {
     long long replay_cap = 0;
     phmc_trial* d_trials = nullptr; double* d_dE = nullptr; int trials_cap = 0;
     std::vector<int> caps;
+    // measurement
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<size_t, size_t>> ev_mc, ev_flush;  // (start, end) indices into ev_pool
+    phmc_profile prof{};
+    void* l2_scratch = nullptr;
+    int64_t l2_bytes = 0;
+    std::vector<int> n_present;  // present particles per replica (for the rebuild byte model)
 };
+
+static cudaEvent_t next_event(phmc_engine* h, size_t* idx) {
+    if (h->ev_used == h->ev_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->ev_pool.push_back(e);
+    }
+    *idx = h->ev_used;
+    return h->ev_pool[h->ev_used++];
+}
 
 template <typename T>
 static int dalloc(Engine& E, T** p, size_t n) {
@@ -328,6 +347,10 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     }
     h->caps.resize(R);
     for (int r = 0; r < R; ++r) h->caps[r] = E.desc[r].cap;
+    h->n_present.assign(R, 0);
+    for (int r = 0; r < R; ++r)
+        for (int i = 0; i < E.desc[r].cap; ++i)
+            if (!(h_flags[E.desc[r].slot_off + i] & PHMC_F_GHOST)) h->n_present[r]++;
 
     // ---- mesh ----
     if (ewald) {
@@ -424,6 +447,8 @@ extern "C" int phmc_destroy(phmc_engine* h) {
     for (void* p : E.allocs) cudaFree(p);
     E.allocs.clear();
     if (E.h_active) cudaFreeHost(E.h_active);
+    if (h->l2_scratch) cudaFree(h->l2_scratch);
+    for (cudaEvent_t ev : h->ev_pool) cudaEventDestroy(ev);
     if (h->d_replay) cudaFree(h->d_replay);
     if (h->d_trials) cudaFree(h->d_trials);
     if (h->d_dE) cudaFree(h->d_dE);
@@ -611,21 +636,112 @@ int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
     if (E.d.log_move) {
         CU(cudaMemsetAsync(E.d.log_move, 0xff, sizeof(int) * E.d.log_cap, E.stream));
     }
+    h->prof.kernel_launches += 1;
+    std::vector<RepState> st0;
+    if (h->profiling) {
+        st0.resize((size_t)E.R);
+        CU(cudaMemcpyAsync(st0.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost, E.stream));
+        CU(cudaStreamSynchronize(E.stream));
+        h->ev_used = 0;
+        h->ev_mc.clear();
+        h->ev_flush.clear();
+    }
+    const int flush_kernels = (E.coulomb == PHMC_COUL_EWALD) ? 5 : 0;
     long long iter = 0;
     const long long max_iter = n_trials + 8;
     for (;;) {
         for (int k = 0; k < check_every; ++k) {
+            size_t a = 0, b = 0, c = 0, e2 = 0;
+            if (h->profiling) CU(cudaEventRecord(next_event(h, &a), E.stream));
             CU(launch_mc(E, MC_RUN, 0, nullptr, 0, nullptr, E.stream));
-            int s = flush_dirty(h);
-            if (s) return s;
+            if (h->profiling) { CU(cudaEventRecord(next_event(h, &b), E.stream)); h->ev_mc.push_back({a, b}); }
+            if (flush_kernels) {
+                if (h->profiling) CU(cudaEventRecord(next_event(h, &c), E.stream));
+                int s = flush_dirty(h);
+                if (s) return s;
+                if (h->profiling) { CU(cudaEventRecord(next_event(h, &e2), E.stream)); h->ev_flush.push_back({c, e2}); }
+            }
+            h->prof.kernel_launches += 1 + flush_kernels;
             ++iter;
         }
         k_count_active<<<1, 256, 0, E.stream>>>(E.d.state, E.R, E.d_active);
+        h->prof.kernel_launches += 1;
         CU(cudaMemcpyAsync(E.h_active, E.d_active, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
         CU(cudaStreamSynchronize(E.stream));
         if (*E.h_active == 0) break;
         if (iter > max_iter) return fail(PHMC_ERR_BUDGET, "trial loop made no progress");
     }
+    if (h->profiling) {
+        for (auto& pr : h->ev_mc) {
+            float ms = 0.f;
+            CU(cudaEventElapsedTime(&ms, h->ev_pool[pr.first], h->ev_pool[pr.second]));
+            h->prof.mc_ms += ms;
+        }
+        for (auto& pr : h->ev_flush) {
+            float ms = 0.f;
+            CU(cudaEventElapsedTime(&ms, h->ev_pool[pr.first], h->ev_pool[pr.second]));
+            h->prof.flush_ms += ms;
+        }
+        h->prof.mc_launches += (int64_t)h->ev_mc.size();
+        h->prof.flush_launches += (int64_t)h->ev_flush.size();
+        std::vector<RepState> st1((size_t)E.R);
+        CU(cudaMemcpy(st1.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+        for (int r = 0; r < E.R; ++r) {
+            const RepDesc& D = E.desc[r];
+            h->prof.mc_alg_bytes += st1[r].alg_bytes - st0[r].alg_bytes;
+            h->prof.trials += st1[r].trials_run - st0[r].trials_run;
+            const double M = (double)D.mesh[0] * D.mesh[1] * D.mesh[2];
+            const double Mc = (double)(D.mesh[0] / 2 + 1) * D.mesh[1] * D.mesh[2];
+            h->prof.flush_alg_bytes += (double)(st1[r].flushes - st0[r].flushes) * (16.0 * h->n_present[r] + 16.0 * M + 16.0 * Mc);
+        }
+    }
+    return PHMC_OK;
+}
+
+extern "C" int phmc_set_profiling(phmc_engine* h, int on) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    h->profiling = on != 0;
+    return PHMC_OK;
+}
+
+extern "C" int phmc_get_profile(phmc_engine* h, phmc_profile* out, int reset) {
+    if (!h || !out) return fail(PHMC_ERR_ARG, "null argument");
+    *out = h->prof;
+    if (reset) std::memset(&h->prof, 0, sizeof(h->prof));
+    return PHMC_OK;
+}
+
+extern "C" int phmc_run_timed(phmc_engine* h, int64_t n_trials, double* device_ms) {
+    if (!h || n_trials < 0 || !device_ms) return fail(PHMC_ERR_ARG, "invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    CU(cudaEventRecord(a, E.stream));
+    int s = phmc_run_loop(h, n_trials, 1);
+    if (s) { cudaEventDestroy(a); cudaEventDestroy(b); return s; }
+    CU(cudaEventRecord(b, E.stream));
+    CU(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *device_ms = ms;
+    return check_kernel_errors(h);
+}
+
+extern "C" int phmc_flush_l2(phmc_engine* h, int64_t bytes) {
+    if (!h || bytes <= 0) return fail(PHMC_ERR_ARG, "invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    if (bytes > h->l2_bytes) {
+        if (h->l2_scratch) cudaFree(h->l2_scratch);
+        h->l2_scratch = nullptr;
+        CU(cudaMalloc(&h->l2_scratch, (size_t)bytes));
+        h->l2_bytes = bytes;
+    }
+    CU(cudaMemsetAsync(h->l2_scratch, 0x5a, (size_t)bytes, E.stream));
     return PHMC_OK;
 }
 
@@ -664,6 +780,57 @@ extern "C" int phmc_get_state(phmc_engine* h, int rep, float* x, float* y, float
     if (type) CU(cudaMemcpy(type, E.d.type + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
     if (flags) CU(cudaMemcpy(flags, E.d.flags + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
     return PHMC_OK;
+}
+
+extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const float* y, const float* z, const float* q,
+                              const int* type, const int* flags) {
+    if (!h || rep < 0 || rep >= h->E.R || !x || !y || !z || !q || !type || !flags) return fail(PHMC_ERR_ARG, "invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    RepDesc& D = E.desc[rep];
+    const int cap = D.cap, so = D.slot_off;
+    std::vector<float4> pq((size_t)cap);
+    std::vector<int> mob(cap, -1), mpos(cap, -1), an(cap, -1), apos(cap, -1), ca(cap, -1), cpos(cap, -1), fr(cap, -1), ti(cap, -1);
+    RepState st;
+    CU(cudaMemcpy(&st, E.d.state + rep, sizeof(RepState), cudaMemcpyDeviceToHost));
+    st.n_mobile = st.n_anion = st.n_cation = st.n_free = 0;
+    int nt = 0, npres = 0;
+    for (int i = 0; i < cap; ++i) {
+        if (type[i] < 0 || type[i] >= D.T) return fail(PHMC_ERR_ARG, "type out of range");
+        const int f = flags[i];
+        if (!(f & PHMC_F_GHOST) && !(x[i] >= 0 && x[i] < D.L[0] && y[i] >= 0 && y[i] < D.L[1] && z[i] >= 0 && z[i] < D.L[2]))
+            return fail(PHMC_ERR_ARG, "particle outside [0,L)");
+        pq[i] = make_float4(x[i], y[i], z[i], q[i]);
+        if (f & PHMC_F_GHOST) continue;
+        ++npres;
+        if (f & PHMC_F_MOBILE) { mpos[i] = st.n_mobile; mob[st.n_mobile++] = i; }
+        if (f & PHMC_F_TITRATABLE) ti[nt++] = i;
+        if (f & PHMC_F_ANION) { apos[i] = st.n_anion; an[st.n_anion++] = i; }
+        if (f & PHMC_F_CATION) { cpos[i] = st.n_cation; ca[st.n_cation++] = i; }
+    }
+    for (int i = cap - 1; i >= 0; --i)
+        if (flags[i] & PHMC_F_GHOST) fr[st.n_free++] = i;
+    D.n_titr = nt;
+    h->n_present[rep] = npres;
+    const cudaStream_t s = E.stream;
+    CU(cudaMemcpyAsync(E.d.posq + so, pq.data(), sizeof(float4) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.type + so, type, sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.flags + so, flags, sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.mobile + so, mob.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.mobile_pos + so, mpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.anions + so, an.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.anion_pos + so, apos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.cations + so, ca.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.cation_pos + so, cpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.freel + so, fr.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.titr + so, ti.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.state + rep, &st, sizeof(RepState), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(E.d.desc + rep, &D, sizeof(RepDesc), cudaMemcpyHostToDevice, s));
+    launch_cell_build(E, s);
+    h->prof.kernel_launches += 2;
+    int rc = full_recompute(h);
+    h->prof.kernel_launches += (E.coulomb == PHMC_COUL_EWALD ? 5 : 0) + 2;
+    return rc;
 }
 
 extern "C" int phmc_get_cells(phmc_engine* h, int rep, int* cell_of, int dims[3]) {

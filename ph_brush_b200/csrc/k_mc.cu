@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
         if (T.skip) {
             if (tid == 0) {
                 if (T.move < 3) S.att[T.move]++;
+                if (mode == MC_RUN) { S.alg_bytes += 16.0; S.trials_run++; }
                 const long long li = T.tnum - S.run_start;
                 if (mode == MC_RUN && r == 0 && d.log_move && li < d.log_cap) {
                     d.log_move[li] = T.move;
@@ -521,6 +522,10 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 }
                 if (r == 0 && d.log_move && li < d.log_cap) { d.log_move[li] = T.move; d.log_dE[li] = dE; d.log_acc[li] = accept; }
                 S.att[T.move]++;
+                // algorithmic bytes of this trial: float4+type of every candidate, the
+                // moved particle, the phi stencils and the pending-correction reads
+                S.alg_bytes += 20.0 * T.total_cand + 16.0 + 4.0 * P3 * T.nst + 16.0 * P3 * s_npend + (accept ? 32.0 : 0.0);
+                S.trials_run++;
             } else if (mode == MC_EVAL) {
                 if (ext_dE) ext_dE[T.ext_k] = dE;
             } else {

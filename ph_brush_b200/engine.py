@@ -108,6 +108,28 @@ class Engine:
                                             _abi.fptr(q), _abi.iptr(t), _abi.iptr(f)))
         return {"x": x, "y": y, "z": z, "q": q, "type": t, "flags": f}
 
+    def set_state(self, st, replica=0):
+        a = [_abi.as_f32(st[k]) for k in ("x", "y", "z", "q")] + [_abi.as_i32(st["type"]), _abi.as_i32(st["flags"])]
+        _abi.check(self._lib.phmc_set_state(self._h, replica, *(_abi.fptr(v) for v in a[:4]), _abi.iptr(a[4]),
+                                            _abi.iptr(a[5])))
+
+    # ---- measurement ----
+    def set_profiling(self, on=True):
+        _abi.check(self._lib.phmc_set_profiling(self._h, int(on)))
+
+    def profile(self, reset=False):
+        p = _abi.Profile()
+        _abi.check(self._lib.phmc_get_profile(self._h, C.byref(p), int(reset)))
+        return p.asdict()
+
+    def run_timed(self, n_trials):
+        ms = C.c_double()
+        _abi.check(self._lib.phmc_run_timed(self._h, int(n_trials), C.byref(ms)))
+        return ms.value
+
+    def flush_l2(self, nbytes=256 << 20):
+        _abi.check(self._lib.phmc_flush_l2(self._h, int(nbytes)))
+
     def cells(self, replica=0):
         n = self.caps[replica]
         c = np.zeros(n, np.int32)
