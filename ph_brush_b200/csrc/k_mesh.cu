@@ -303,8 +303,14 @@ void launch_unit_charge(Engine& E, cudaStream_t st) { k_unit_charge<<<(E.R + 127
 
 void launch_extract_octant(Engine& E, int r, cudaStream_t st) { k_extract_octant<<<148, 256, 0, st>>>(E.d, r); }
 
+// The cap is the device's opt-in maximum (not this engine's need), so that
+// engines with different meshes can coexist on one device.
 cudaError_t mesh_set_smem_limits(Engine& E) {
-    cudaError_t e = cudaFuncSetAttribute(k_plane<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, E.plane_smem);
+    int optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_zpass<256, ZPASS_TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, E.zpass_smem);
+    if ((size_t)optin < E.plane_smem || (size_t)optin < E.zpass_smem) return cudaErrorInvalidValue;
+    e = cudaFuncSetAttribute(k_plane<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_zpass<256, ZPASS_TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
 }
