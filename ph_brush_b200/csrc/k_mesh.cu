@@ -3,6 +3,9 @@
 // influence-function multiply fused between the forward and inverse z passes),
 // potential-mesh readout.  Replaces k_spread_cubic + cuFFT R2C +
 // k_recip_energy_and_apply of the reference (MC/src/pme.cu:140-249,384-422).
+#include <cmath>
+#include <cstring>
+#include <string>
 #include "common.cuh"
 #include "engine.h"
 
@@ -305,12 +308,21 @@ void launch_extract_octant(Engine& E, int r, cudaStream_t st) { k_extract_octant
 
 // The cap is the device's opt-in maximum (not this engine's need), so that
 // engines with different meshes can coexist on one device.
-cudaError_t mesh_set_smem_limits(Engine& E) {
+template <typename K>
+static cudaError_t raise_dynamic_smem_cap(K kernel, int device, size_t need) {
     int optin = 0;
-    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return e;
-    if ((size_t)optin < E.plane_smem || (size_t)optin < E.zpass_smem) return cudaErrorInvalidValue;
-    e = cudaFuncSetAttribute(k_plane<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, kernel);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_zpass<256, ZPASS_TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    const int cap = optin - (int)fa.sharedSizeBytes;  // static shared memory counts against the opt-in limit
+    if (cap < (int)need) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+}
+
+cudaError_t mesh_set_smem_limits(Engine& E) {
+    cudaError_t e = raise_dynamic_smem_cap(k_plane<256>, E.device, E.plane_smem);
+    if (e != cudaSuccess) return e;
+    return raise_dynamic_smem_cap(k_zpass<256, ZPASS_TX>, E.device, E.zpass_smem);
 }
