@@ -228,6 +228,24 @@ int phmc_flush_l2(phmc_engine* e, int64_t bytes);
 int phmc_get_cells(phmc_engine* e, int replica, int* cell_of, int dims[3]);
 int phmc_capacity(phmc_engine* e, int replica);
 
+/* ---- allocation-free reciprocal energy ----
+ * No counterpart in the reference.  SPME reciprocal-space energy of n point
+ * charges (host arrays), for callers that cannot call cudaMalloc: code running
+ * while a stream is being captured into a CUDA graph, hosts whose device memory
+ * is budgeted by another allocator, or per-trial loops that must not stall on an
+ * allocation's implicit synchronisation.  It uses one file-scope device array
+ * (about 3 MB, held by every GPU that loads the library until exit) and never
+ * allocates.  Limits: n <= PHMC_STATIC_MAX_PARTICLES, nx*ny*nz <=
+ * PHMC_STATIC_MAX_MESH, each side 2^a 3^b 5^c in [order, 512]; larger inputs
+ * return PHMC_ERR_CAPACITY.  Works on the current device; that device's first
+ * call looks up the array's device address (make it before any stream
+ * capture).  Calls share the array: calls that overlap on the GPU race. */
+#define PHMC_STATIC_MAX_PARTICLES 32768
+#define PHMC_STATIC_MAX_MESH 131072
+int phmc_recip_energy_static(const float* x, const float* y, const float* z, const float* q, int n,
+                             const double box[3], const int mesh[3], int order, double ewald_alpha,
+                             double epsilon_r, int ref_moduli, double* e_recip);
+
 /* ---- synthetic input (no counterpart in the reference, whose inputs are
  * LAMMPS data files, MC/src/io.cpp:79-146) ----
  * Grafted brush: chains on a square lattice at z = 0, self-avoiding random

@@ -89,7 +89,8 @@ class BrushSpec(C.Structure):
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
-           "phmc_set_state", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2"]
+           "phmc_set_state", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
+           "phmc_recip_energy_static"]
 
 
 def load_library(path=LIB_PATH):
@@ -119,6 +120,8 @@ def load_library(path=LIB_PATH):
         "phmc_get_profile": ([eng, C.POINTER(Profile), C.c_int], C.c_int),
         "phmc_run_timed": ([eng, C.c_int64, _dp], C.c_int),
         "phmc_flush_l2": ([eng, C.c_int64], C.c_int),
+        "phmc_recip_energy_static": ([_fp, _fp, _fp, _fp, C.c_int, _dp, _ip, C.c_int, C.c_double, C.c_double,
+                                      C.c_int, _dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

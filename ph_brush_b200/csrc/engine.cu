@@ -23,6 +23,8 @@ static int fail(int code, const std::string& msg) {
         if (e_ != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+void phmc_set_error(int code, const std::string& msg) { (void)fail(code, msg); }
+
 extern "C" int phmc_abi_version(void) { return PHMC_ABI_VERSION; }
 extern "C" const char* phmc_last_error(void) { return g_err.c_str(); }
 

@@ -43,6 +43,9 @@ struct Engine {
     bool has_G = false;
 };
 
+// engine.cu: records the thread's last error message
+void phmc_set_error(int code, const std::string& msg);
+
 // k_mesh.cu
 void launch_spread(Engine& E, const int* dirty, cudaStream_t st);
 void launch_fft_pipeline(Engine& E, const int* dirty, int mode, cudaStream_t st);

@@ -326,3 +326,226 @@ cudaError_t mesh_set_smem_limits(Engine& E) {
     if (e != cudaSuccess) return e;
     return raise_dynamic_smem_cap(k_zpass<256, ZPASS_TX>, E.device, E.zpass_smem);
 }
+
+// ---------------------------------------------------------------------------
+// Reciprocal-space energy with no device allocation.
+//
+// For callers that must not allocate device memory: code that evaluates the
+// SPME energy inside a region where cudaMalloc is forbidden or unwanted (a
+// stream being captured into a CUDA graph, a host with a fixed device-memory
+// budget handed out by another allocator, a per-trial loop where an
+// allocation's implicit device synchronisation would stall the pipeline).
+// The reference itself allocates a device scalar on every energy call
+// (MC/src/energy_gpu.cu:55, MC/src/pme.cu:363).
+//
+// All scratch lives in one file-scope __device__ array (every GPU that loads
+// the library holds it until the process exits): particle staging, the
+// fixed-point charge mesh, the complex work mesh, FFT job tables, moduli,
+// twiddles and the energy partials.  Limits: n <= PHMC_STATIC_MAX_PARTICLES,
+// nx*ny*nz <= PHMC_STATIC_MAX_MESH, each mesh side <= 512.
+// Every call shares the array and leaves its contents behind; the call clears
+// what must start at zero.  Calls that overlap on the GPU (other host threads,
+// other streams) race on the array.
+// ---------------------------------------------------------------------------
+#define ST_MAX_N PHMC_STATIC_MAX_PARTICLES
+#define ST_MAX_M PHMC_STATIC_MAX_MESH
+#define ST_MAX_SIDE 512
+#define ST_MAX_ZJOBS 4096
+namespace {
+constexpr size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t ST_OFF_QFIX = 0;
+constexpr size_t ST_OFF_CMESH = ST_OFF_QFIX + al256(sizeof(unsigned long long) * ST_MAX_M);
+constexpr size_t ST_OFF_POSQ = ST_OFF_CMESH + al256(sizeof(float2) * ST_MAX_M);
+constexpr size_t ST_OFF_FLAGS = ST_OFF_POSQ + al256(sizeof(float4) * ST_MAX_N);
+constexpr size_t ST_OFF_REP = ST_OFF_FLAGS + al256(sizeof(int) * ST_MAX_N);
+constexpr size_t ST_OFF_MOD = ST_OFF_REP + al256(sizeof(int) * ST_MAX_N);
+constexpr size_t ST_OFF_TW = ST_OFF_MOD + al256(sizeof(float) * 3 * ST_MAX_SIDE);
+constexpr size_t ST_OFF_PJOB = ST_OFF_TW + al256(sizeof(float2) * 3 * ST_MAX_SIDE);
+constexpr size_t ST_OFF_ZJOB = ST_OFF_PJOB + al256(sizeof(int2) * ST_MAX_SIDE);
+constexpr size_t ST_OFF_ZOFF = ST_OFF_ZJOB + al256(sizeof(int4) * ST_MAX_ZJOBS);
+constexpr size_t ST_OFF_EPART = ST_OFF_ZOFF + al256(sizeof(int) * 2);
+constexpr size_t ST_OFF_DESC = ST_OFF_EPART + al256(sizeof(double) * ST_MAX_ZJOBS);
+constexpr size_t ST_OFF_STATE = ST_OFF_DESC + al256(sizeof(RepDesc));
+constexpr size_t ST_BYTES = ST_OFF_STATE + al256(sizeof(RepState));
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_recip_scratch[ST_BYTES];
+
+// Device address of g_recip_scratch per device, looked up on the first call made
+// with that device current.
+static unsigned char* g_recip_scratch_addr[64];
+
+// Host staging of the small tables (the same process-wide sharing rules apply).
+static float4 h_st_posq[ST_MAX_N];
+static int h_st_flags[ST_MAX_N];
+static float h_st_mod[3 * ST_MAX_SIDE];
+static float2 h_st_tw[3 * ST_MAX_SIDE];
+static int2 h_st_pjob[ST_MAX_SIDE];
+static int4 h_st_zjob[ST_MAX_ZJOBS];
+
+static bool st_smooth(int n) {
+    if (n < 1) return false;
+    for (int p : {2, 3, 5}) while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+// |DFT(M_p)|^2 on a length-n grid (same rule as the engine's moduli, written
+// into a caller array).
+static void st_moduli(int n, int order, int ref_style, float* out) {
+    double d[16] = {0};
+    const int s = order - 1;
+    d[0] = 1.0;
+    for (int k = 2; k <= s; ++k) {
+        const double inv = 1.0 / k;
+        for (int m = k - 1; m > 0; --m) d[m] = inv * ((k - m) * d[m - 1] + (m + 1) * d[m]);
+        d[0] = inv * d[0];
+    }
+    double v[ST_MAX_SIDE];
+    for (int i = 0; i < n; ++i) {
+        double c = 0, sn = 0;
+        for (int j = 0; j < s; ++j) {
+            const double a = 2.0 * M_PI * i * (j + 1) / (double)n;
+            c += d[j] * cos(a);
+            sn += d[j] * sin(a);
+        }
+        v[i] = c * c + sn * sn;
+        if (ref_style && !(v[i] > 0.0)) v[i] = 1e-30;
+    }
+    for (int i = 0; i < n; ++i) {
+        double m = v[i];
+        if (ref_style) {
+            if (n % 2 == 0 && i == n / 2 && !(m > 0.0)) m = v[n / 2 - 1];
+        } else if (m < 1e-7) {
+            m = 0.5 * (v[(i - 1 + n) % n] + v[(i + 1) % n]);
+        }
+        out[i] = (float)m;
+    }
+}
+
+extern "C" int phmc_recip_energy_static(const float* x, const float* y, const float* z, const float* q, int n,
+                                        const double box[3], const int mesh[3], int order, double ewald_alpha,
+                                        double epsilon_r, int ref_moduli, double* e_recip) {
+    if (!x || !y || !z || !q || !box || !mesh || !e_recip || n < 0) {
+        phmc_set_error(PHMC_ERR_ARG, "phmc_recip_energy_static: null argument or negative n");
+        return PHMC_ERR_ARG;
+    }
+    if (n > ST_MAX_N) {
+        phmc_set_error(PHMC_ERR_CAPACITY, "phmc_recip_energy_static: more particles than PHMC_STATIC_MAX_PARTICLES");
+        return PHMC_ERR_CAPACITY;
+    }
+    if (order < 4 || order > 6 || !(ewald_alpha > 0) || !(epsilon_r > 0) || !(box[0] > 0 && box[1] > 0 && box[2] > 0)) {
+        phmc_set_error(PHMC_ERR_ARG, "phmc_recip_energy_static: order must be 4..6, alpha/epsilon_r/box > 0");
+        return PHMC_ERR_ARG;
+    }
+    const long long M = (long long)mesh[0] * mesh[1] * mesh[2];
+    int zj = 0;
+    for (int k = 0; k < 3; ++k)
+        if (mesh[k] > ST_MAX_SIDE || !st_smooth(mesh[k]) || mesh[k] < order) {
+            phmc_set_error(PHMC_ERR_CAPACITY, "phmc_recip_energy_static: each mesh side must be 2^a 3^b 5^c, >= order, <= 512");
+            return PHMC_ERR_CAPACITY;
+        }
+    zj = mesh[1] * ((mesh[0] + ZPASS_TX - 1) / ZPASS_TX);
+    const size_t plane_smem = (size_t)2 * mesh[0] * mesh[1] * sizeof(float2);
+    const size_t zpass_smem = (size_t)2 * ZPASS_TX * mesh[2] * sizeof(float2);
+    if (M > ST_MAX_M || zj > ST_MAX_ZJOBS || plane_smem > 227 * 1024 || zpass_smem > 227 * 1024) {
+        phmc_set_error(PHMC_ERR_CAPACITY, "phmc_recip_energy_static: mesh larger than PHMC_STATIC_MAX_MESH points");
+        return PHMC_ERR_CAPACITY;
+    }
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess || dev < 0 || dev >= 64) {
+        phmc_set_error(PHMC_ERR_CUDA, std::string("phmc_recip_energy_static: no current device: ") + cudaGetErrorString(ce));
+        return PHMC_ERR_CUDA;
+    }
+    if (!g_recip_scratch_addr[dev]) {  // set-up on this device's first call
+        void* p = nullptr;
+        ce = cudaGetSymbolAddress(&p, g_recip_scratch);
+        if (ce != cudaSuccess || !p) {
+            phmc_set_error(PHMC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
+            return PHMC_ERR_CUDA;
+        }
+        g_recip_scratch_addr[dev] = (unsigned char*)p;
+    }
+    unsigned char* base = g_recip_scratch_addr[dev];
+    // host tables
+    RepDesc D;
+    memset(&D, 0, sizeof D);
+    D.cap = n; D.slot_off = 0;
+    for (int k = 0; k < 3; ++k) { D.L[k] = (float)box[k]; D.mesh[k] = mesh[k]; D.oct[k] = mesh[k] / 2 + 1; }
+    D.V = box[0] * box[1] * box[2];
+    D.order = order; D.coulomb = PHMC_COUL_EWALD; D.ref_corner = ref_moduli;
+    D.alpha = (float)ewald_alpha; D.elf = (float)(138.935458 / epsilon_r);
+    D.ewald_factor = (float)((M_PI / ewald_alpha) * (M_PI / ewald_alpha));
+    for (int k = 0; k < 3; ++k) {
+        D.mod_off[k] = k * ST_MAX_SIDE;
+        st_moduli(mesh[k], order, ref_moduli, h_st_mod + k * ST_MAX_SIDE);
+        D.tw_off[k] = k * ST_MAX_SIDE;
+        for (int j = 0; j < mesh[k]; ++j)
+            h_st_tw[k * ST_MAX_SIDE + j] = make_float2((float)cos(-2.0 * M_PI * j / mesh[k]), (float)sin(-2.0 * M_PI * j / mesh[k]));
+    }
+    for (int i = 0; i < n; ++i) { h_st_posq[i] = make_float4(x[i], y[i], z[i], q[i]); h_st_flags[i] = 0; }
+    for (int zz = 0; zz < mesh[2]; ++zz) h_st_pjob[zz] = make_int2(0, zz);
+    int nzj = 0;
+    for (int yy = 0; yy < mesh[1]; ++yy)
+        for (int x0 = 0; x0 < mesh[0]; x0 += ZPASS_TX) h_st_zjob[nzj++] = make_int4(0, yy, x0, 0);
+    const int zoff[2] = {0, nzj};
+    // device pointers into the static array
+    DevPtrs d;
+    memset(&d, 0, sizeof d);
+    d.qfix = (unsigned long long*)(base + ST_OFF_QFIX);
+    d.cmesh = (float2*)(base + ST_OFF_CMESH);
+    d.posq = (float4*)(base + ST_OFF_POSQ);
+    d.flags = (int*)(base + ST_OFF_FLAGS);
+    d.moduli = (float*)(base + ST_OFF_MOD);
+    d.twiddle = (float2*)(base + ST_OFF_TW);
+    d.desc = (RepDesc*)(base + ST_OFF_DESC);
+    d.state = (RepState*)(base + ST_OFF_STATE);
+    int* rep_of = (int*)(base + ST_OFF_REP);
+    int2* pjob = (int2*)(base + ST_OFF_PJOB);
+    int4* zjob = (int4*)(base + ST_OFF_ZJOB);
+    int* zjob_off = (int*)(base + ST_OFF_ZOFF);
+    double* epart = (double*)(base + ST_OFF_EPART);
+    const cudaStream_t st = 0;
+#define ST_CU(call)                                                                                   \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) {                                                                      \
+            phmc_set_error(PHMC_ERR_CUDA, std::string("phmc_recip_energy_static: ") + #call + ": " + cudaGetErrorString(e_)); \
+            return PHMC_ERR_CUDA;                                                                     \
+        }                                                                                             \
+    } while (0)
+    // clear what must start at zero: the fixed-point mesh, replica ids, the state
+    ST_CU(cudaMemsetAsync(d.qfix, 0, sizeof(unsigned long long) * (size_t)M, st));
+    if (n > 0) ST_CU(cudaMemsetAsync(rep_of, 0, sizeof(int) * (size_t)n, st));
+    ST_CU(cudaMemsetAsync(d.state, 0, sizeof(RepState), st));
+    if (n > 0) {
+        ST_CU(cudaMemcpyAsync(d.posq, h_st_posq, sizeof(float4) * n, cudaMemcpyHostToDevice, st));
+        ST_CU(cudaMemcpyAsync(d.flags, h_st_flags, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    }
+    ST_CU(cudaMemcpyAsync(d.moduli, h_st_mod, sizeof(float) * 3 * ST_MAX_SIDE, cudaMemcpyHostToDevice, st));
+    ST_CU(cudaMemcpyAsync(d.twiddle, h_st_tw, sizeof(float2) * 3 * ST_MAX_SIDE, cudaMemcpyHostToDevice, st));
+    ST_CU(cudaMemcpyAsync(pjob, h_st_pjob, sizeof(int2) * mesh[2], cudaMemcpyHostToDevice, st));
+    ST_CU(cudaMemcpyAsync(zjob, h_st_zjob, sizeof(int4) * nzj, cudaMemcpyHostToDevice, st));
+    ST_CU(cudaMemcpyAsync(zjob_off, zoff, sizeof(zoff), cudaMemcpyHostToDevice, st));
+    ST_CU(cudaMemcpyAsync(d.desc, &D, sizeof(RepDesc), cudaMemcpyHostToDevice, st));
+    ST_CU(raise_dynamic_smem_cap(k_plane<256>, dev, plane_smem));
+    ST_CU(raise_dynamic_smem_cap(k_zpass<256, ZPASS_TX>, dev, zpass_smem));
+    if (n > 0) {
+        const int nb = (n + 255) / 256;
+        switch (order) {
+            case 4: k_spread<4><<<nb, 256, 0, st>>>(d, rep_of, n, nullptr); break;
+            case 5: k_spread<5><<<nb, 256, 0, st>>>(d, rep_of, n, nullptr); break;
+            default: k_spread<6><<<nb, 256, 0, st>>>(d, rep_of, n, nullptr); break;
+        }
+    }
+    k_plane<256><<<mesh[2], 256, plane_smem, st>>>(d, pjob, 1, nullptr);
+    k_zpass<256, ZPASS_TX><<<nzj, 256, zpass_smem, st>>>(d, zjob, epart, nullptr);
+    k_flush_reduce<<<1, 32, 0, st>>>(d, zjob_off, epart, 1, 1, nullptr);
+    ST_CU(cudaGetLastError());
+    RepState out;
+    ST_CU(cudaMemcpyAsync(&out, d.state, sizeof(RepState), cudaMemcpyDeviceToHost, st));
+    ST_CU(cudaStreamSynchronize(st));
+#undef ST_CU
+    *e_recip = out.E_rec;
+    return PHMC_OK;
+}
