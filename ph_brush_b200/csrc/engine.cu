@@ -163,7 +163,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     E.order = prm[0].order;
     E.coulomb = prm[0].coulomb;
     E.threads = prm[0].threads == 128 ? 128 : 256;
-    E.pend_max = prm[0].pending_max > 0 ? std::min(std::max(prm[0].pending_max, 4), PHMC_MAX_PEND) : 16;
+    E.pend_max = prm[0].pending_max > 0 ? std::min(std::max(prm[0].pending_max, 4), PHMC_MAX_PEND) : 48;
     E.cell_cap = prm[0].cell_cap > 0 ? prm[0].cell_cap : 64;
     for (int r = 1; r < R; ++r)
         if (prm[r].coulomb != E.coulomb) return fail(PHMC_ERR_UNSUPPORTED, "all replicas must share the Coulomb kind");
@@ -721,7 +721,7 @@ extern "C" int phmc_run_timed(phmc_engine* h, int64_t n_trials, double* device_m
     CU(cudaEventCreate(&a));
     CU(cudaEventCreate(&b));
     CU(cudaEventRecord(a, E.stream));
-    int s = phmc_run_loop(h, n_trials, 1);
+    int s = phmc_run_loop(h, n_trials, 4);
     if (s) { cudaEventDestroy(a); cudaEventDestroy(b); return s; }
     CU(cudaEventRecord(b, E.stream));
     CU(cudaEventSynchronize(b));
@@ -751,7 +751,7 @@ extern "C" int phmc_run(phmc_engine* h, int64_t n_trials, phmc_run_stats* stats)
     if (!h || n_trials < 0) return fail(PHMC_ERR_ARG, "invalid argument");
     Engine& E = h->E;
     CU(cudaSetDevice(E.device));
-    int s = phmc_run_loop(h, n_trials, 1);
+    int s = phmc_run_loop(h, n_trials, 4);
     if (s) return s;
     s = check_kernel_errors(h);
     if (s) return s;

@@ -16,6 +16,7 @@
 //    influence kernel (octant table);
 //  * self / net-charge / slab terms from FP64 charge moments;
 //  * Metropolis in FP64 with the move's log factor (MC/src/mc.cu:438-440).
+#include <algorithm>
 #include "common.cuh"
 #include "engine.h"
 
@@ -36,6 +37,9 @@ struct PairK {
     int f[3][2 * P - 1];  // folded octant coordinate of D + delta
     float coef;
     int pad;
+    // per (dz, dy) row: octant row offset and coef * Ky * Kz
+    int roff[(2 * P - 1) * (2 * P - 1)];
+    float kyz[(2 * P - 1) * (2 * P - 1)];
 };
 
 struct TrialS {
@@ -53,6 +57,17 @@ struct TrialS {
     float st_coef[NST_MAX];
     double d_direct_lj, d_direct_c, d_fene;
     int total_cand, npairs;
+    // cell bookkeeping of the old states, loaded off the critical path (phase 4)
+    int cell_old[2], cpos_old[2], cnt_old[2], last_old[2];
+};
+
+// Next trial's primary particle, loaded during the current trial's parallel
+// phase.  Valid while no accepted change touched it or the lists.
+struct Prefetch {
+    long long t;
+    int valid, move, idx, flags, type;
+    float4 pq;
+    int4 bonds;
 };
 
 __device__ __forceinline__ void probe_add(TrialS& T, float4 p, int type, int owner, float sign, const RepDesc& D) {
@@ -94,19 +109,45 @@ __device__ __forceinline__ float4 rand_pos(const RepDesc& D, uint32_t a, uint32_
     return p;
 }
 
-// Proposal of trial T.tnum from the Philox stream (same rules as the oracle's MC).
-__device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const DevPtrs& d) {
-    const long long t = T.tnum;
-    uint32_t A[4], B[4], C[4];
-    philox4x32_10(D.key[0], D.key[1], (uint32_t)t, (uint32_t)((unsigned long long)t >> 32), 0u, 0u, A);
-    philox4x32_10(D.key[0], D.key[1], (uint32_t)t, (uint32_t)((unsigned long long)t >> 32), 1u, 0u, B);
-    philox4x32_10(D.key[0], D.key[1], (uint32_t)t, (uint32_t)((unsigned long long)t >> 32), 2u, 0u, C);
+// The 12 Philox words of trial t: A = ctr (t, 0), B = ctr (t, 1), C = ctr (t, 2).
+__device__ __forceinline__ void trial_words(const RepDesc& D, long long t, uint32_t* w) {
+    const uint32_t lo = (uint32_t)t, hi = (uint32_t)((unsigned long long)t >> 32);
+    philox4x32_10(D.key[0], D.key[1], lo, hi, 0u, 0u, w);
+    philox4x32_10(D.key[0], D.key[1], lo, hi, 1u, 0u, w + 4);
+    philox4x32_10(D.key[0], D.key[1], lo, hi, 2u, 0u, w + 8);
+}
+
+__device__ __forceinline__ int move_of(const RepDesc& D, uint32_t a0) {
+    const float um = u24(a0);
+    if (um < D.p_disp) return PHMC_MOVE_DISP;
+    if (um < D.p_disp + D.p_titr) return PHMC_MOVE_TITR;
+    if (um < D.p_disp + D.p_titr + D.p_swap) return PHMC_MOVE_SWAP;
+    return PHMC_MOVE_NONE;
+}
+
+// Load the primary particle of trial t into pf (list index from the current sizes).
+__device__ void prefetch_primary(Prefetch& pf, long long t, const uint32_t* rw, const RepDesc& D, const RepState& S,
+                                 const DevPtrs& d) {
+    pf.valid = 0;
+    const int mv = move_of(D, rw[0]);
+    const int so = D.slot_off;
+    int i = -1;
+    if (mv == PHMC_MOVE_DISP && S.n_mobile > 0) i = d.mobile[so + pick_index(rw[1], S.n_mobile)];
+    else if (mv == PHMC_MOVE_TITR && D.n_titr > 0) i = d.titr[so + pick_index(rw[1], D.n_titr)];
+    if (i < 0) return;
+    pf.t = t; pf.move = mv; pf.idx = i;
+    pf.flags = d.flags[so + i]; pf.pq = d.posq[so + i]; pf.type = d.type[so + i]; pf.bonds = d.bonds[so + i];
+    pf.valid = 1;
+}
+
+// Proposal of trial T.tnum from its Philox words (same rules as the oracle's MC).
+__device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const DevPtrs& d, const uint32_t* rw,
+                        const Prefetch& pf) {
+    const uint32_t* A = rw;
+    const uint32_t* B = rw + 4;
+    const uint32_t* C = rw + 8;
     T.ua = B[2]; T.ub = B[3];
-    const float um = u24(A[0]);
-    int move = PHMC_MOVE_NONE;
-    if (um < D.p_disp) move = PHMC_MOVE_DISP;
-    else if (um < D.p_disp + D.p_titr) move = PHMC_MOVE_TITR;
-    else if (um < D.p_disp + D.p_titr + D.p_swap) move = PHMC_MOVE_SWAP;
+    const int move = move_of(D, A[0]);
     T.move = move; T.skip = 0; T.nch = 0; T.logf = 0.0;
     const int so = D.slot_off;
     auto load_old = [&](int k, int i) {
@@ -114,10 +155,19 @@ __device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const De
         T.pres_old[k] = !(d.flags[so + i] & PHMC_F_GHOST);
         T.po[k] = d.posq[so + i]; T.to[k] = d.type[so + i]; T.bonds[k] = d.bonds[so + i];
     };
+    // primary particle from the prefetch when it is still valid
+    const bool use_pf = pf.valid && pf.t == T.tnum && pf.move == move;
+    auto load_primary = [&](int i_from_list) {
+        if (use_pf) {
+            T.idx[0] = pf.idx; T.pres_old[0] = !(pf.flags & PHMC_F_GHOST);
+            T.po[0] = pf.pq; T.to[0] = pf.type; T.bonds[0] = pf.bonds;
+        } else {
+            load_old(0, i_from_list);
+        }
+    };
     if (move == PHMC_MOVE_DISP) {
         if (S.n_mobile == 0) { T.skip = 1; return; }
-        const int i = d.mobile[so + pick_index(A[1], S.n_mobile)];
-        load_old(0, i);
+        load_primary(use_pf ? -1 : d.mobile[so + pick_index(A[1], S.n_mobile)]);
         const float dm = D.disp_max;
         const float dx = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[2])), 1.0f));
         const float dy = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[3])), 1.0f));
@@ -131,8 +181,7 @@ __device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const De
         if (D.walls && (nz < D.wall_lo || nz >= D.wall_hi)) T.skip = 2;  // hard wall: infinite energy
     } else if (move == PHMC_MOVE_TITR) {
         if (D.n_titr == 0) { T.skip = 1; return; }
-        const int site = d.titr[so + pick_index(A[1], D.n_titr)];
-        load_old(0, site);
+        load_primary(use_pf ? -1 : d.titr[so + pick_index(A[1], D.n_titr)]);
         T.pres_new[0] = 1;
         if (T.po[0].w == 0.0f) {
             if (S.n_free == 0) { T.skip = 1; return; }
@@ -201,34 +250,17 @@ __device__ __forceinline__ void make_stencil(Stencil<P>& s, const RepDesc& D, fl
         bspline_weights<P>(g[k] - fl, s.w[k]);
         s.base[k] = (int)fl + P / 2 - P + 1;
 #pragma unroll
-        for (int j = 0; j < P; ++j) s.m[k][j] = wrap_idx(s.base[k] + j, D.mesh[k]);
+        for (int j = 0; j < P; ++j) {  // base + j lies in [-P, n + P): one correction wraps it
+            int m = s.base[k] + j;
+            m += (m < 0) ? D.mesh[k] : 0;
+            m -= (m >= D.mesh[k]) ? D.mesh[k] : 0;
+            s.m[k][j] = m;
+        }
     }
     s.coef = coef;
 }
 
-template <int P>
-__device__ __forceinline__ void make_pair(PairK<P>& q, const Stencil<P>& a, const Stencil<P>& b, float coef, const RepDesc& D) {
-    constexpr int W = 2 * P - 1;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int n = D.mesh[k];
-        const int Dd = a.base[k] - b.base[k];
-#pragma unroll
-        for (int t = 0; t < W; ++t) {
-            const int delta = t - (P - 1);
-            float s = 0.0f;
-#pragma unroll
-            for (int i = 0; i < P; ++i) {
-                const int j = i - delta;
-                if (j >= 0 && j < P) s += a.w[k][i] * b.w[k][j];
-            }
-            q.K[k][t] = s;
-            int m = wrap_idx(Dd + delta, n);
-            q.f[k][t] = min(m, n - m);
-        }
-    }
-    q.coef = coef;
-}
+__device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
 __device__ __forceinline__ void list_remove(int* list, int* pos, int& n, int so, int i) {
     const int k = pos[so + i];
@@ -295,43 +327,66 @@ template <int P, int NT>
 __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
     constexpr int W = 2 * P - 1;
-    constexpr int W3 = W * W * W;
     constexpr int P3 = P * P * P;
     extern __shared__ __align__(16) unsigned char dsm[];
+    // pending stencils [0, s_npend) followed by the current trial's stencils (a
+    // commit just advances s_npend); then the stencil-pair tables
     Stencil<P>* s_pend = reinterpret_cast<Stencil<P>*>(dsm);
-    Stencil<P>* s_tst = s_pend + pend_max;
-    PairK<P>* s_pair = reinterpret_cast<PairK<P>*>(s_tst + NST_MAX);
+    PairK<P>* s_pair = reinterpret_cast<PairK<P>*>(s_pend + pend_max + NST_MAX);
     __shared__ TrialS T;
     __shared__ RepState S;
     __shared__ int s_cnt[NPROBE_MAX * 27], s_off[NPROBE_MAX * 27 + 1], s_cell[NPROBE_MAX * 27];
     __shared__ double red[100];
     __shared__ int s_npend;
+    __shared__ uint32_t s_rng[32][12];  // Philox words of trials s_rng_base .. s_rng_base+31
+    __shared__ long long s_rng_base;
+    __shared__ Prefetch pf;
 
     const int r = (mode == MC_RUN) ? blockIdx.x : ext_rep;
-    const RepDesc& D = d.desc[r];
     const int tid = threadIdx.x;
+    // the replica's descriptor lives in shared memory for the whole launch
+    __shared__ __align__(16) RepDesc sD;
+    {
+        const int* src = reinterpret_cast<const int*>(d.desc + r);
+        int* dst = reinterpret_cast<int*>(&sD);
+        for (int k = tid; k < (int)(sizeof(RepDesc) / sizeof(int)); k += NT) dst[k] = src[k];
+    }
+    const RepDesc& D = sD;
     if (tid == 0) {
         S = d.state[r];
         s_npend = 0;
         T.ext_k = 0;
         T.stop = 0;
+        s_rng_base = -64;
+        pf.valid = 0;
     }
     __syncthreads();
 
     for (;;) {
         // ---------------- proposal ----------------
-        if (tid == 0) {
-            T.stop = 0;
-            if (S.error) T.stop = 1;
-            else if (mode == MC_RUN) {
-                if (S.trial >= S.target) { T.stop = 1; S.stop_reason = 0; }
-                else if (s_npend + 2 > pend_max) { T.stop = 1; S.stop_reason = 1; }
-                else { T.tnum = S.trial; propose(T, D, S, d); S.trial++; }
-            } else {
-                if (T.ext_k >= n_ext) T.stop = 1;
-                else { load_external(T, D, d, ext[T.ext_k]); T.tnum = T.ext_k; }
+        if (tid < 32) {
+            if (mode == MC_RUN) {  // warp 0 refills the Philox table every 32 trials
+                const long long t = S.trial;
+                if (t - s_rng_base >= 32 || t < s_rng_base) {
+                    trial_words(D, t + tid, s_rng[tid]);
+                    __syncwarp();
+                    if (tid == 0) s_rng_base = t;
+                    __syncwarp();
+                }
             }
-            if (!T.stop && T.skip == 0) trial_setup(T, D);
+            if (tid == 0) {
+                T.stop = 0;
+                if (S.error) T.stop = 1;
+                else if (mode == MC_RUN) {
+                    if (S.trial >= S.target) { T.stop = 1; S.stop_reason = 0; }
+                    else if (s_npend + 2 > pend_max) { T.stop = 1; S.stop_reason = 1; }
+                    else { T.tnum = S.trial; propose(T, D, S, d, s_rng[S.trial - s_rng_base], pf); S.trial++; }
+                } else {
+                    if (T.ext_k >= n_ext) T.stop = 1;
+                    else { load_external(T, D, d, ext[T.ext_k]); T.tnum = T.ext_k; }
+                }
+                if (!T.stop && T.skip == 0) trial_setup(T, D);
+            }
         }
         __syncthreads();
         if (T.stop) break;
@@ -355,12 +410,13 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
         }
         // ---------------- phase 2: cell counts, stencils, direct & bonded terms ----------------
         const int nent = T.nprobe * 27;
+        Stencil<P>* s_tst = s_pend + s_npend;  // this trial's stencils
         if (tid < nent) {
             const int p = tid / 27, nb = tid % 27;
             const int c = T.probe_cell[p];
             const int cx = c % D.ncell[0], cy = (c / D.ncell[0]) % D.ncell[1], cz = c / (D.ncell[0] * D.ncell[1]);
-            const int nc = (wrap_idx(cz + nb / 9 - 1, D.ncell[2]) * D.ncell[1] + wrap_idx(cy + (nb / 3) % 3 - 1, D.ncell[1])) *
-                               D.ncell[0] + wrap_idx(cx + nb % 3 - 1, D.ncell[0]);
+            const int nc = (wrap1(cz + nb / 9 - 1, D.ncell[2]) * D.ncell[1] + wrap1(cy + (nb / 3) % 3 - 1, D.ncell[1])) *
+                               D.ncell[0] + wrap1(cx + nb % 3 - 1, D.ncell[0]);
             s_cell[tid] = nc;
             s_cnt[tid] = min(d.cell_count[D.cell_off + nc], D.cell_cap);
         }
@@ -392,10 +448,15 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 for (int k = 0; k < T.nch; ++k) {
                     if (!(T.pres_old[k] && T.pres_new[k])) continue;
                     const int bl[4] = {T.bonds[k].x, T.bonds[k].y, T.bonds[k].z, T.bonds[k].w};
+                    float4 pjs[4];
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)  // independent loads, issued together
+                        pjs[b] = (bl[b] >= 0) ? d.posq[D.slot_off + bl[b]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
                     for (int b = 0; b < 4; ++b) {
                         const int j = bl[b];
                         if (j < 0 || (T.nch == 2 && (j == T.idx[0] || j == T.idx[1]))) continue;
-                        const float4 pj = d.posq[D.slot_off + j];
+                        const float4 pj = pjs[b];
                         float dx = min_image(T.pn[k].x - pj.x, D.L[0]), dy = min_image(T.pn[k].y - pj.y, D.L[1]),
                               dz = min_image(T.pn[k].z - pj.z, D.L[2]);
                         const float en = fene_energy(D, dx * dx + dy * dy + dz * dz);
@@ -425,25 +486,84 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 carry += __shfl_sync(0xffffffffu, x, 31);
             }
             if (tid == 0) { s_off[nent] = carry; T.total_cand = carry; }
-        } else {
+        } else if (D.coulomb == PHMC_COUL_EWALD) {
             const int nst = T.nst, np = s_npend;
             const int npairs = nst * np + nst * (nst + 1) / 2;
-            for (int q = tid - 32; q < npairs; q += NT - 32) {
+            constexpr int W = 2 * P - 1;
+            // one (pair, axis, offset) element per work item
+            for (int e = tid - 32; e < 3 * W * npairs; e += NT - 32) {
+                const int q = e / (3 * W), r3 = e - q * (3 * W);
+                const int k = r3 / W, t = r3 - k * W;
+                int ta, tb;
+                const Stencil<P>* sb;
+                float c;
                 if (q < nst * np) {
-                    const int t = q / np, e = q % np;
-                    make_pair<P>(s_pair[q], s_tst[t], s_pend[e], s_tst[t].coef * s_pend[e].coef, D);
+                    ta = q / np; tb = q - ta * np;
+                    sb = &s_pend[tb];
+                    c = s_tst[ta].coef * s_pend[tb].coef;
                 } else {
-                    int rem = q - nst * np, t = 0;
-                    while (rem >= nst - t) { rem -= nst - t; ++t; }
-                    const int t2 = t + rem;
-                    const float c = s_tst[t].coef * s_tst[t2].coef * (t == t2 ? 0.5f : 1.0f);
-                    make_pair<P>(s_pair[q], s_tst[t], s_tst[t2], c, D);
+                    int rem = q - nst * np;
+                    ta = 0;
+                    while (rem >= nst - ta) { rem -= nst - ta; ++ta; }
+                    tb = ta + rem;
+                    sb = &s_tst[tb];
+                    c = s_tst[ta].coef * s_tst[tb].coef * (ta == tb ? 0.5f : 1.0f);
                 }
+                const Stencil<P>& sa = s_tst[ta];
+                const int delta = t - (P - 1);
+                float s = 0.0f;
+#pragma unroll
+                for (int i = 0; i < P; ++i) {
+                    const int j = i - delta;
+                    if (j >= 0 && j < P) s += sa.w[k][i] * sb->w[k][j];
+                }
+                const int n = D.mesh[k];
+                int m = sa.base[k] - sb->base[k] + delta;
+                m += (m < 0) ? n : 0;
+                m += (m < 0) ? n : 0;
+                m -= (m >= n) ? n : 0;
+                m -= (m >= n) ? n : 0;
+                s_pair[q].K[k][t] = s;
+                s_pair[q].f[k][t] = min(m, n - m);
+                if (r3 == 0) s_pair[q].coef = c;
             }
             if (tid == 32) T.npairs = npairs;
         }
         __syncthreads();
+        if (D.coulomb == PHMC_COUL_EWALD) {
+            // phase 3b: per (pair, dz, dy) row, the octant row offset and coef * Ky * Kz
+            constexpr int W = 2 * P - 1;
+            const int ox = D.oct[0], oy = D.oct[1];
+            const int nrow = T.npairs * W * W;
+            for (int e = tid; e < nrow; e += NT) {
+                const int q = e / (W * W), rw = e - q * (W * W);
+                const int dz = rw / W, dy = rw - dz * W;
+                PairK<P>& pk = s_pair[q];
+                pk.roff[rw] = (pk.f[2][dz] * oy + pk.f[1][dy]) * ox;
+                pk.kyz[rw] = pk.coef * pk.K[1][dy] * pk.K[2][dz];
+            }
+            __syncthreads();
+        }
         // ---------------- phase 4: all pair / mesh work items ----------------
+        // helper loads off the critical path: the next trial's primary particle,
+        // and the cell bookkeeping a commit of this trial would need
+        if (tid == NT - 1 && mode == MC_RUN) {
+            const long long tn = T.tnum + 1;
+            if (tn - s_rng_base >= 0 && tn - s_rng_base < 32) prefetch_primary(pf, tn, s_rng[tn - s_rng_base], D, S, d);
+            else pf.valid = 0;
+        }
+        if (tid >= NT - 3 && tid < NT - 1) {
+            const int k = NT - 2 - tid;
+            if (k < T.nch && T.pres_old[k]) {
+                const int gi = D.slot_off + T.idx[k];
+                const int c = cell_index(D, T.po[k].x, T.po[k].y, T.po[k].z);
+                const int cnt = d.cell_count[D.cell_off + c];
+                T.cell_old[k] = c;
+                T.cpos_old[k] = d.cell_pos[gi];
+                T.cnt_old[k] = cnt;
+                T.last_old[k] = (cnt > 0) ? d.cell_list[((size_t)D.cell_off + c) * D.cell_cap + cnt - 1] : -1;
+            }
+        }
         double acc_lj = 0.0, acc_c = 0.0, acc_rec = 0.0;
         {
             const int total = T.total_cand;
@@ -468,25 +588,41 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
             }
         }
         if (D.coulomb == PHMC_COUL_EWALD) {
+            // W_t . phi: element (stencil, c, b, a), a fastest (lanes read consecutive x)
             const float* phi = d.phi + D.mesh_off;
             const int nx = D.mesh[0], ny = D.mesh[1];
+            constexpr int P3 = P * P * P;
             const int nphi = T.nst * P3;
             for (int it = tid; it < nphi; it += NT) {
-                const int st = it / P3, rem = it % P3;
-                const int c = rem / (P * P), b = (rem / P) % P, a = rem % P;
+                const int st = it / P3, rem = it - st * P3;
+                const int c = rem / (P * P), rb = rem - c * (P * P);
+                const int b = rb / P, a = rb - b * P;
                 const Stencil<P>& s = s_tst[st];
                 const float v = phi[((size_t)s.m[2][c] * ny + s.m[1][b]) * nx + s.m[0][a]];
                 acc_rec += (double)(s.coef * s.w[0][a] * s.w[1][b] * s.w[2][c] * v);
             }
+            // S(W_a, W_b) = sum_delta Kx Ky Kz G[fz, fy, fx]: element (pair, dz, dy, dx), dx fastest
+            // (lanes read consecutive x of a G row); each thread issues RB loads before using them
             const float* G = d.goct + D.oct_off;
             const int ox = D.oct[0], oy = D.oct[1];
+            constexpr int W3 = W * W * W;
             const int nit = T.npairs * W3;
-            for (int it = tid; it < nit; it += NT) {
-                const int q = it / W3, rem = it % W3;
-                const int dz = rem / (W * W), dy = (rem / W) % W, dx = rem % W;
-                const PairK<P>& pk = s_pair[q];
-                const float g = __ldg(&G[((size_t)pk.f[2][dz] * oy + pk.f[1][dy]) * ox + pk.f[0][dx]]);
-                acc_rec += (double)(pk.coef * pk.K[0][dx] * pk.K[1][dy] * pk.K[2][dz] * g);
+            constexpr int RB = 4;
+            (void)ox; (void)oy;
+            for (int it0 = tid; it0 < nit; it0 += RB * NT) {
+                float g[RB], kk[RB];
+#pragma unroll
+                for (int u = 0; u < RB; ++u) {
+                    const int it = it0 + u * NT;
+                    const int itc = it < nit ? it : nit - 1;
+                    const int rowg = itc / W, dx = itc - rowg * W;  // rowg = pair * W*W + row
+                    const int q = rowg / (W * W), rw = rowg - q * (W * W);
+                    const PairK<P>& pk = s_pair[q];
+                    g[u] = __ldg(&G[pk.roff[rw] + pk.f[0][dx]]);
+                    kk[u] = (it < nit) ? pk.kyz[rw] * pk.K[0][dx] : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < RB; ++u) acc_rec += (double)(kk[u] * g[u]);
             }
         }
         block_sum3<NT>(acc_lj, acc_c, acc_rec, red);
@@ -543,7 +679,25 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                         d.posq[gi] = T.pn[k];
                         d.type[gi] = T.tn[k];
                         const int nc = cell_index(D, T.pn[k].x, T.pn[k].y, T.pn[k].z);
-                        if (nc != d.cell_of[gi]) {
+                        if (k == 0 && T.nch == 1 && T.nprobe == 2) {
+                            // displacement: the old cell's tail and the new cell's count were
+                            // loaded during the parallel phase (probe 1 = new state, entry 13 = its cell)
+                            if (nc != T.cell_old[0]) {
+                                const int c = T.cell_old[0], kp = T.cpos_old[0], n = T.cnt_old[0], last = T.last_old[0];
+                                int* l = d.cell_list + ((size_t)D.cell_off + c) * D.cell_cap;
+                                l[kp] = last;
+                                d.cell_pos[so + last] = kp;
+                                d.cell_count[D.cell_off + c] = n - 1;
+                                const int nn = s_cnt[27 + 13];
+                                if (nn >= D.cell_cap) S.error = PHMC_ERR_CAPACITY;
+                                else {
+                                    d.cell_list[((size_t)D.cell_off + nc) * D.cell_cap + nn] = i;
+                                    d.cell_count[D.cell_off + nc] = nn + 1;
+                                    d.cell_of[gi] = nc;
+                                    d.cell_pos[gi] = nn;
+                                }
+                            }
+                        } else if (nc != d.cell_of[gi]) {
                             cell_remove(d, D, i);
                             if (!cell_insert(d, D, i, nc)) S.error = PHMC_ERR_CAPACITY;
                         }
@@ -569,10 +723,12 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                         cell_remove(d, D, i);
                     }
                 }
-                for (int k = 0; k < T.nst; ++k) {
-                    if (s_npend < pend_max) s_pend[s_npend++] = s_tst[k];
-                    else S.error = PHMC_ERR_CAPACITY;
-                }
+                // the trial's stencils already sit right after the pending ones
+                if (s_npend + T.nst <= pend_max + NST_MAX) s_npend += T.nst;
+                else S.error = PHMC_ERR_CAPACITY;
+                // the next trial's prefetched particle is stale if this commit touched it or the lists
+                for (int k = 0; k < T.nch; ++k)
+                    if (T.idx[k] == pf.idx || T.pres_old[k] != T.pres_new[k]) pf.valid = 0;
                 S.Q += dQ; S.Q2 += dQ2; S.Mz += dMz; S.S2 += dS2;
                 S.E_pair_lj += dlj; S.E_pair_c += dc; S.E_fene += T.d_fene; S.E_rec += acc_rec;
                 S.E_self += dself; S.E_qcorr += dqc; S.E_slab += dslab;
@@ -604,7 +760,9 @@ size_t mc_smem_bytes(int order, int pend_max) {
         case 5: st = sizeof(Stencil<5>); pk = sizeof(PairK<5>); break;
         default: st = sizeof(Stencil<6>); pk = sizeof(PairK<6>); break;
     }
-    const size_t npairs = (size_t)NST_MAX * pend_max + NST_MAX * (NST_MAX + 1) / 2;
+    // Monte Carlo trials carry <= 2 stencils against <= pend_max pending ones;
+    // external trials (<= NST_MAX stencils) always start with none pending
+    const size_t npairs = std::max((size_t)2 * pend_max + 3, (size_t)(NST_MAX * (NST_MAX + 1) / 2));
     return st * (pend_max + NST_MAX) + pk * npairs;
 }
 

@@ -253,11 +253,21 @@ __global__ void __launch_bounds__(NT) k_zpass(DevPtrs d, const int4* __restrict_
 // (update tracked energies, record drift); mode 1: plain recompute (set E_rec).
 __global__ void k_flush_reduce(DevPtrs d, const int* __restrict__ zjob_off, const double* __restrict__ epart, int R,
                                int mode, const int* __restrict__ dirty) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    // one block per replica; each thread sums a strided slice, then a fixed-order tree
+    __shared__ double red[128];
+    const int r = blockIdx.x;
     if (r >= R) return;
     if (dirty && !dirty[r]) return;
-    double s = 0.0;
-    for (int k = zjob_off[r]; k < zjob_off[r + 1]; ++k) s += epart[k];
+    double part = 0.0;
+    for (int k = zjob_off[r] + threadIdx.x; k < zjob_off[r + 1]; k += blockDim.x) part += epart[k];
+    red[threadIdx.x] = part;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const double s = red[0];
     RepState& S = d.state[r];
     S.E_rec_flush = s;
     if (mode == 0) {
@@ -299,7 +309,7 @@ void launch_fft_pipeline(Engine& E, const int* dirty, int mode, cudaStream_t st)
     k_plane<256><<<E.n_plane_jobs, 256, E.plane_smem, st>>>(E.d, E.d_plane_jobs, 1, dirty);
     k_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty);
     k_plane<256><<<E.n_plane_jobs, 256, E.plane_smem, st>>>(E.d, E.d_plane_jobs, 0, dirty);
-    k_flush_reduce<<<(E.R + 127) / 128, 128, 0, st>>>(E.d, E.d_zjob_off, E.d_epart, E.R, mode, dirty);
+    k_flush_reduce<<<E.R, 128, 0, st>>>(E.d, E.d_zjob_off, E.d_epart, E.R, mode, dirty);
 }
 
 void launch_unit_charge(Engine& E, cudaStream_t st) { k_unit_charge<<<(E.R + 127) / 128, 128, 0, st>>>(E.d, E.R); }
