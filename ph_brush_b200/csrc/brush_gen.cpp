@@ -8,6 +8,14 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+#include <string>
+
+void phmc_set_error(int code, const std::string& msg);  // engine.cu
+
+static int gen_fail(int code, const char* msg) {
+    phmc_set_error(code, msg);
+    return code;
+}
 #include "../../include/phmc.h"
 
 namespace {
@@ -78,12 +86,18 @@ struct Grid {
         px.push_back(x); py.push_back(y); pz.push_back(z);
         cells[idx(x, y, z)].push_back(id);
     }
+    // remove the most recently added point (it is the last entry of its cell)
+    void pop() {
+        const int id = (int)px.size() - 1;
+        cells[idx(px[id], py[id], pz[id])].pop_back();
+        px.pop_back(); py.pop_back(); pz.pop_back();
+    }
 };
 }  // namespace
 
 extern "C" int phmc_build_brush(const phmc_brush_spec* sp, int capacity, float* x, float* y, float* z, float* q, int* type,
                                 int* flags, int max_bonds, int* bond_i, int* bond_j, int* counts, double* box_out) {
-    if (!sp || !x || !y || !z || !q || !type || !flags || !counts || !box_out) return PHMC_ERR_ARG;
+    if (!sp || !x || !y || !z || !q || !type || !flags || !counts || !box_out) return gen_fail(PHMC_ERR_ARG, "phmc_build_brush: null argument");
     Rng rng(sp->seed);
     const double a = sp->graft_spacing;
     const double Lx = sp->chains_x * a, Ly = sp->chains_y * a, H = sp->height;
@@ -97,28 +111,44 @@ extern "C" int phmc_build_brush(const phmc_brush_spec* sp, int capacity, float* 
     const int nch = sp->chains_x * sp->chains_y;
     for (int c = 0; c < nch; ++c) {
         const int len = sp->len_min + (sp->len_max > sp->len_min ? rng.below(sp->len_max - sp->len_min + 1) : 0);
-        double cx = ((c % sp->chains_x) + 0.5) * a, cy = ((c / sp->chains_x) + 0.5) * a, cz = 0.0;
+        // grow the chain's coordinates; a walk that traps itself is discarded and regrown
+        const int first = (int)g.px.size();
+        bool grown = false;
+        for (int attempt = 0; attempt < 50 && !grown; ++attempt) {
+            double cx = ((c % sp->chains_x) + 0.5) * a, cy = ((c / sp->chains_x) + 0.5) * a, cz = 0.0;
+            int prev = -1;
+            grown = true;
+            for (int k = 0; k < len && grown; ++k) {
+                if (k > 0) {
+                    bool ok = false;
+                    // dense grafting (>= 0.08 sigma^-2) starts from stretched chains: steps
+                    // point away from the plane; regrowth of a trapped chain stretches more
+                    const double dense = 1.0 / (a * a) >= 0.08 ? 1.0 : 0.0;
+                    const double umin = attempt < 2 ? (dense > 0 ? 0.0 : -1.0) : (attempt < 10 ? 0.0 : 0.3);
+                    for (int tries = 0; tries < 2000 && !ok; ++tries) {
+                        const double dm = tries < 1000 ? dmin : 0.8 * dmin;
+                        const double u = umin + (1.0 - umin) * rng.uni(), ph = 2.0 * M_PI * rng.uni();
+                        const double s = std::sqrt(std::max(0.0, 1.0 - u * u));
+                        double nx = cx + b * s * std::cos(ph), ny = cy + b * s * std::sin(ph), nz = cz + b * u;
+                        if (nz < 0.0 || nz >= H) continue;
+                        nx -= Lx * std::floor(nx / Lx);
+                        ny -= Ly * std::floor(ny / Ly);
+                        if (nx >= Lx) nx = 0.0;
+                        if (ny >= Ly) ny = 0.0;
+                        if (!g.free_at(nx, ny, nz, dm, prev)) continue;
+                        cx = nx; cy = ny; cz = nz; ok = true;
+                    }
+                    if (!ok) { grown = false; break; }
+                }
+                prev = (int)g.px.size();
+                g.add(cx, cy, cz);
+            }
+            if (!grown) while ((int)g.px.size() > first) g.pop();
+        }
+        if (!grown) return gen_fail(PHMC_ERR_CAPACITY, "phmc_build_brush: a chain could not be grown without overlaps (grafting too dense)");
         int prev = -1;
         for (int k = 0; k < len; ++k) {
-            if (k > 0) {
-                bool ok = false;
-                for (int tries = 0; tries < 4000 && !ok; ++tries) {
-                    const double dm = tries < 2000 ? dmin : 0.8 * dmin;
-                    const double u = 2.0 * rng.uni() - 1.0, ph = 2.0 * M_PI * rng.uni();
-                    const double s = std::sqrt(std::max(0.0, 1.0 - u * u));
-                    double nx = cx + b * s * std::cos(ph), ny = cy + b * s * std::sin(ph), nz = cz + b * u;
-                    if (nz < 0.0 || nz >= H) continue;
-                    nx -= Lx * std::floor(nx / Lx);
-                    ny -= Ly * std::floor(ny / Ly);
-                    if (nx >= Lx) nx = 0.0;
-                    if (ny >= Ly) ny = 0.0;
-                    if (!g.free_at(nx, ny, nz, dm, prev)) continue;
-                    cx = nx; cy = ny; cz = nz; ok = true;
-                }
-                if (!ok) return PHMC_ERR_CAPACITY;
-            }
-            const int id = (int)g.px.size();
-            g.add(cx, cy, cz);
+            const int id = first + k;
             const bool perm = k < sp->n_permanent;
             const bool titr = !perm && (k > 0 || sp->graft_titratable);
             int t, f = (k == 0) ? 0 : PHMC_F_MOBILE;
@@ -145,15 +175,15 @@ extern "C" int phmc_build_brush(const phmc_brush_spec* sp, int capacity, float* 
         return false;
     };
     for (int k = 0; k < n_pos; ++k)
-        if (!place(2, -1.0f, PHMC_F_MOBILE | PHMC_F_ANION)) return PHMC_ERR_CAPACITY;
+        if (!place(2, -1.0f, PHMC_F_MOBILE | PHMC_F_ANION)) return gen_fail(PHMC_ERR_CAPACITY, "phmc_build_brush: no free spot for an ion (slab too dense)");
     const int n_salt = (int)std::lround(sp->salt_conc * Lx * Ly * H);
     for (int k = 0; k < n_salt; ++k) {
-        if (!place(3, 1.0f, PHMC_F_MOBILE | PHMC_F_CATION)) return PHMC_ERR_CAPACITY;
-        if (!place(2, -1.0f, PHMC_F_MOBILE | PHMC_F_ANION)) return PHMC_ERR_CAPACITY;
+        if (!place(3, 1.0f, PHMC_F_MOBILE | PHMC_F_CATION)) return gen_fail(PHMC_ERR_CAPACITY, "phmc_build_brush: no free spot for an ion (slab too dense)");
+        if (!place(2, -1.0f, PHMC_F_MOBILE | PHMC_F_ANION)) return gen_fail(PHMC_ERR_CAPACITY, "phmc_build_brush: no free spot for an ion (slab too dense)");
     }
     const int n = (int)g.px.size();
     counts[0] = n; counts[1] = (int)bi.size();
-    if (n > capacity || (int)bi.size() > max_bonds) return PHMC_ERR_CAPACITY;
+    if (n > capacity || (int)bi.size() > max_bonds) return gen_fail(PHMC_ERR_CAPACITY, "phmc_build_brush: output arrays too small");
     for (int i = 0; i < n; ++i) {
         x[i] = (float)g.px[i]; y[i] = (float)g.py[i]; z[i] = (float)g.pz[i];
         if (x[i] >= (float)Lx) x[i] = 0.0f;

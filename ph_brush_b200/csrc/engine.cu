@@ -45,17 +45,57 @@ struct phmc_engine {
     void* l2_scratch = nullptr;
     int64_t l2_bytes = 0;
     std::vector<int> n_present;  // present particles per replica (for the rebuild byte model)
+    // captured trial/rebuild chunks (re-captured when the launch set-up changes)
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_chunks = 0;
+    bool graph_prof = false;
+    std::vector<cudaEvent_t> gev;  // 4 per chunk when profiling
 };
 
-static cudaEvent_t next_event(phmc_engine* h, size_t* idx) {
-    if (h->ev_used == h->ev_pool.size()) {
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        h->ev_pool.push_back(e);
-    }
-    *idx = h->ev_used;
-    return h->ev_pool[h->ev_used++];
+static void drop_graph(phmc_engine* h) {
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+    h->graph_chunks = 0;
 }
+
+static int flush_dirty(phmc_engine* h);
+
+// Capture `chunks` x (MC launch + potential-mesh rebuild) on the engine stream.
+static int build_chunk_graph(phmc_engine* h, int chunks) {
+    Engine& E = h->E;
+    if (h->graph_exec && h->graph_chunks == chunks && h->graph_prof == h->profiling) return PHMC_OK;
+    drop_graph(h);
+    while ((int)h->gev.size() < 4 * chunks) {
+        cudaEvent_t ev;
+        CU(cudaEventCreate(&ev));
+        h->gev.push_back(ev);
+    }
+    CU(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t err = cudaSuccess;
+    int s = PHMC_OK;
+    for (int k = 0; k < chunks && err == cudaSuccess && s == PHMC_OK; ++k) {
+        if (h->profiling) err = cudaEventRecordWithFlags(h->gev[4 * k], E.stream, cudaEventRecordExternal);
+        if (err == cudaSuccess) err = launch_mc(E, MC_RUN, 0, nullptr, 0, nullptr, E.stream);
+        if (err == cudaSuccess && h->profiling) err = cudaEventRecordWithFlags(h->gev[4 * k + 1], E.stream, cudaEventRecordExternal);
+        if (err == cudaSuccess && E.coulomb == PHMC_COUL_EWALD) {
+            if (h->profiling) err = cudaEventRecordWithFlags(h->gev[4 * k + 2], E.stream, cudaEventRecordExternal);
+            if (err == cudaSuccess) s = flush_dirty(h);
+            if (err == cudaSuccess && s == PHMC_OK && h->profiling) err = cudaEventRecordWithFlags(h->gev[4 * k + 3], E.stream, cudaEventRecordExternal);
+        }
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(E.stream, &g);
+    if (err != cudaSuccess) { if (g) cudaGraphDestroy(g); return fail(PHMC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(err)); }
+    if (s != PHMC_OK) { if (g) cudaGraphDestroy(g); return s; }
+    if (e2 != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e2));
+    cudaError_t e3 = cudaGraphInstantiate(&h->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) { h->graph_exec = nullptr; return fail(PHMC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e3)); }
+    h->graph_chunks = chunks;
+    h->graph_prof = h->profiling;
+    return PHMC_OK;
+}
+
 
 template <typename T>
 static int dalloc(Engine& E, T** p, size_t n) {
@@ -384,6 +424,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         CU(cudaMemcpy(E.d_zjob_off, zoff.data(), sizeof(int) * zoff.size(), cudaMemcpyHostToDevice));
         CU(mesh_set_smem_limits(E));
     }
+    CU(prepare_mc(E));
     return PHMC_OK;
 }
 
@@ -451,6 +492,8 @@ extern "C" int phmc_destroy(phmc_engine* h) {
     if (E.h_active) cudaFreeHost(E.h_active);
     if (h->l2_scratch) cudaFree(h->l2_scratch);
     for (cudaEvent_t ev : h->ev_pool) cudaEventDestroy(ev);
+    drop_graph(h);
+    for (cudaEvent_t ev : h->gev) cudaEventDestroy(ev);
     if (h->d_replay) cudaFree(h->d_replay);
     if (h->d_trials) cudaFree(h->d_trials);
     if (h->d_dE) cudaFree(h->d_dE);
@@ -580,6 +623,7 @@ __global__ void k_count_active(const RepState* st, int R, int* active) {
 extern "C" int phmc_set_trial_log(phmc_engine* h, int64_t cap, int* move, double* dE, int* acc) {
     if (!h) return fail(PHMC_ERR_ARG, "null engine");
     Engine& E = h->E;
+    drop_graph(h);  // captured launches hold the old log pointers
     if (E.d.log_move) { cudaFree(E.d.log_move); cudaFree(E.d.log_dE); cudaFree(E.d.log_acc); }
     E.d.log_move = nullptr; E.d.log_dE = nullptr; E.d.log_acc = nullptr; E.d.log_cap = 0;
     h->h_log_move = move; h->h_log_dE = dE; h->h_log_acc = acc; h->log_cap = 0;
@@ -594,6 +638,7 @@ extern "C" int phmc_set_trial_log(phmc_engine* h, int64_t cap, int* move, double
 extern "C" int phmc_set_replay(phmc_engine* h, int64_t n, const int* decisions) {
     if (!h) return fail(PHMC_ERR_ARG, "null engine");
     Engine& E = h->E;
+    drop_graph(h);  // captured launches hold the old replay pointer
     if (h->d_replay) { cudaFree(h->d_replay); h->d_replay = nullptr; }
     E.d.replay = nullptr; E.d.replay_n = 0;
     if (!decisions || n <= 0) return PHMC_OK;
@@ -651,41 +696,35 @@ int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
     const int flush_kernels = (E.coulomb == PHMC_COUL_EWALD) ? 5 : 0;
     long long iter = 0;
     const long long max_iter = n_trials + 8;
+    int s = build_chunk_graph(h, check_every);
+    if (s) return s;
     for (;;) {
-        for (int k = 0; k < check_every; ++k) {
-            size_t a = 0, b = 0, c = 0, e2 = 0;
-            if (h->profiling) CU(cudaEventRecord(next_event(h, &a), E.stream));
-            CU(launch_mc(E, MC_RUN, 0, nullptr, 0, nullptr, E.stream));
-            if (h->profiling) { CU(cudaEventRecord(next_event(h, &b), E.stream)); h->ev_mc.push_back({a, b}); }
-            if (flush_kernels) {
-                if (h->profiling) CU(cudaEventRecord(next_event(h, &c), E.stream));
-                int s = flush_dirty(h);
-                if (s) return s;
-                if (h->profiling) { CU(cudaEventRecord(next_event(h, &e2), E.stream)); h->ev_flush.push_back({c, e2}); }
-            }
-            h->prof.kernel_launches += 1 + flush_kernels;
-            ++iter;
-        }
+        // one graph = check_every x (MC launch + potential-mesh rebuild); chunks after
+        // every replica reached its target are no-ops
+        CU(cudaGraphLaunch(h->graph_exec, E.stream));
+        h->prof.kernel_launches += (int64_t)check_every * (1 + flush_kernels);
+        iter += check_every;
         k_count_active<<<1, 256, 0, E.stream>>>(E.d.state, E.R, E.d_active);
         h->prof.kernel_launches += 1;
         CU(cudaMemcpyAsync(E.h_active, E.d_active, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
         CU(cudaStreamSynchronize(E.stream));
+        if (h->profiling) {
+            for (int k = 0; k < check_every; ++k) {
+                float ms = 0.f;
+                CU(cudaEventElapsedTime(&ms, h->gev[4 * k], h->gev[4 * k + 1]));
+                h->prof.mc_ms += ms;
+                if (flush_kernels) {
+                    CU(cudaEventElapsedTime(&ms, h->gev[4 * k + 2], h->gev[4 * k + 3]));
+                    h->prof.flush_ms += ms;
+                }
+            }
+            h->prof.mc_launches += check_every;
+            if (flush_kernels) h->prof.flush_launches += check_every;
+        }
         if (*E.h_active == 0) break;
         if (iter > max_iter) return fail(PHMC_ERR_BUDGET, "trial loop made no progress");
     }
     if (h->profiling) {
-        for (auto& pr : h->ev_mc) {
-            float ms = 0.f;
-            CU(cudaEventElapsedTime(&ms, h->ev_pool[pr.first], h->ev_pool[pr.second]));
-            h->prof.mc_ms += ms;
-        }
-        for (auto& pr : h->ev_flush) {
-            float ms = 0.f;
-            CU(cudaEventElapsedTime(&ms, h->ev_pool[pr.first], h->ev_pool[pr.second]));
-            h->prof.flush_ms += ms;
-        }
-        h->prof.mc_launches += (int64_t)h->ev_mc.size();
-        h->prof.flush_launches += (int64_t)h->ev_flush.size();
         std::vector<RepState> st1((size_t)E.R);
         CU(cudaMemcpy(st1.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
         for (int r = 0; r < E.R; ++r) {

@@ -60,4 +60,5 @@ void launch_full_energy(Engine& E, cudaStream_t st);
 // k_mc.cu
 enum { MC_RUN = 0, MC_EVAL = 1, MC_APPLY = 2 };
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* d_trials, int n, double* d_dE, cudaStream_t st);
+cudaError_t prepare_mc(Engine& E);
 size_t mc_smem_bytes(int order, int pend_max);

@@ -746,11 +746,33 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
 template <int P, int NT>
 static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
     const size_t smem = mc_smem_bytes(P, E.pend_max);
-    cudaError_t e = cudaFuncSetAttribute(k_mc<P, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     const int grid = (mode == MC_RUN) ? E.R : 1;
     k_mc<P, NT><<<grid, NT, smem, st>>>(E.d, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
+}
+
+// Raise the dynamic shared-memory cap of the engine's MC kernel instance to the
+// device maximum (minus its static shared memory), once, outside any capture.
+template <int P, int NT>
+static cudaError_t prepare_mc_t(Engine& E) {
+    int optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, k_mc<P, NT>);
+    if (e != cudaSuccess) return e;
+    const int cap = optin - (int)fa.sharedSizeBytes;
+    if ((size_t)cap < mc_smem_bytes(P, E.pend_max)) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(k_mc<P, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+}
+
+cudaError_t prepare_mc(Engine& E) {
+    const int NTh = E.threads;
+    switch (E.order) {
+        case 4: return NTh == 128 ? prepare_mc_t<4, 128>(E) : prepare_mc_t<4, 256>(E);
+        case 5: return NTh == 128 ? prepare_mc_t<5, 128>(E) : prepare_mc_t<5, 256>(E);
+        default: return NTh == 128 ? prepare_mc_t<6, 128>(E) : prepare_mc_t<6, 256>(E);
+    }
 }
 
 size_t mc_smem_bytes(int order, int pend_max) {
