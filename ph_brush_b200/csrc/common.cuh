@@ -26,6 +26,8 @@ struct RepDesc {
     long long oct_off;
     int mod_off[3];       // offsets of the B-spline moduli per axis
     int tw_off[3];        // offsets of the twiddle tables per axis
+    int tw_off_h;         // twiddle table of length nx/2 (real-to-complex path)
+    long long meshh_off;  // offset into the half-spectrum complex mesh ((nx/2+1) x ny x nz)
     int order;
     int coulomb;
     int ref_corner;

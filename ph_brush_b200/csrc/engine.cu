@@ -214,8 +214,19 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     std::vector<double> h_mod;
     std::vector<float2> h_tw;
     std::map<int, int> tw_off;
+    auto tw_table = [&](int n) {  // exp(-2 pi i j / n), j < n, one table per distinct length
+        auto it = tw_off.find(n);
+        if (it != tw_off.end()) return it->second;
+        const int off = (int)h_tw.size();
+        tw_off[n] = off;
+        for (int j = 0; j < n; ++j) h_tw.push_back(make_float2((float)std::cos(-2.0 * M_PI * j / n), (float)std::sin(-2.0 * M_PI * j / n)));
+        return off;
+    };
     int slot_off = 0, cell_off = 0;
-    long long mesh_off = 0, oct_off = 0;
+    long long mesh_off = 0, meshh_off = 0, oct_off = 0;
+    E.use_r2c = ewald;
+    for (int r = 0; r < R; ++r)
+        if (prm[r].mesh[0] % 2 != 0) E.use_r2c = false;
     for (int r = 0; r < R; ++r) {
         const phmc_system& S = sys[r];
         const phmc_params& P = prm[r];
@@ -285,21 +296,18 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                 std::vector<double> m = bspline_moduli(P.mesh[k], P.order, P.ref_moduli);
                 D.mod_off[k] = (int)h_mod.size();
                 h_mod.insert(h_mod.end(), m.begin(), m.end());
-                auto it = tw_off.find(P.mesh[k]);
-                if (it == tw_off.end()) {
-                    const int n = P.mesh[k];
-                    tw_off[n] = (int)h_tw.size();
-                    for (int j = 0; j < n; ++j) h_tw.push_back(make_float2((float)std::cos(-2.0 * M_PI * j / n), (float)std::sin(-2.0 * M_PI * j / n)));
-                }
-                D.tw_off[k] = tw_off[P.mesh[k]];
+                D.tw_off[k] = tw_table(P.mesh[k]);
             }
+            D.tw_off_h = (P.mesh[0] % 2 == 0) ? tw_table(P.mesh[0] / 2) : 0;
             D.mesh_off = mesh_off; mesh_off += (long long)D.mesh[0] * D.mesh[1] * D.mesh[2];
+            D.meshh_off = meshh_off; meshh_off += (long long)(D.mesh[0] / 2 + 1) * D.mesh[1] * D.mesh[2];
             D.oct_off = oct_off; oct_off += (long long)D.oct[0] * D.oct[1] * D.oct[2];
         }
     }
     E.total_slots = slot_off;
     E.total_cells = cell_off;
     E.total_mesh = mesh_off;
+    E.total_meshh = meshh_off;
     E.total_oct = oct_off;
 
     // ---- host particle arrays + lists ----
@@ -396,13 +404,21 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
 
     // ---- mesh ----
     if (ewald) {
-        DALLOC(d.qfix, E.total_mesh); DALLOC(d.cmesh, E.total_mesh); DALLOC(d.phi, E.total_mesh);
+        // even nx everywhere: fused spread + half-spectrum (real-to-complex) rebuild, no global
+        // charge mesh; otherwise the scatter + full-complex path
+        if (E.use_r2c) {
+            DALLOC(d.cmesh, E.total_meshh);
+        } else {
+            DALLOC(d.qfix, E.total_mesh); DALLOC(d.cmesh, E.total_mesh);
+        }
+        DALLOC(d.phi, E.total_mesh);
+        E.flush_kernels = E.use_r2c ? 4 : 5;
         DALLOC(d.goct, E.total_oct);
         DALLOC(d.moduli, h_mod.size()); DALLOC(d.twiddle, h_tw.size());
         std::vector<float> hm(h_mod.begin(), h_mod.end());
         CU(cudaMemcpy(d.moduli, hm.data(), sizeof(float) * hm.size(), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(d.twiddle, h_tw.data(), sizeof(float2) * h_tw.size(), cudaMemcpyHostToDevice));
-        CU(cudaMemset(d.qfix, 0, sizeof(unsigned long long) * E.total_mesh));
+        if (!E.use_r2c) CU(cudaMemset(d.qfix, 0, sizeof(unsigned long long) * E.total_mesh));
         std::vector<int2> pj;
         std::vector<int4> zj;
         std::vector<int> zoff;
@@ -410,9 +426,24 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
             const RepDesc& D = E.desc[r];
             for (int z = 0; z < D.mesh[2]; ++z) pj.push_back(make_int2(r, z));
             zoff.push_back((int)zj.size());
-            for (int y = 0; y < D.mesh[1]; ++y)
-                for (int x0 = 0; x0 < D.mesh[0]; x0 += ZPASS_TX) zj.push_back(make_int4(r, y, x0, 0));
-            E.plane_smem = std::max(E.plane_smem, (size_t)2 * D.mesh[0] * D.mesh[1] * sizeof(float2));
+            if (E.use_r2c) {
+                // column tiles of near-equal width <= ZPASS_TX over the nx/2+1 half-spectrum columns
+                const int nxh = D.mesh[0] / 2 + 1;
+                const int nt = (nxh + ZPASS_TX - 1) / ZPASS_TX;
+                const int w = (nxh + nt - 1) / nt;
+                for (int y = 0; y < D.mesh[1]; ++y)
+                    for (int x0 = 0; x0 < nxh; x0 += w) zj.push_back(make_int4(r, y, x0, std::min(w, nxh - x0)));
+                // + cell counts / ids of the cell layers a plane's stencils reach (<= order + 5 layers)
+                const size_t ncell = (size_t)std::min(D.ncell[2], E.order + 5) * D.ncell[0] * D.ncell[1];
+                E.rb_fwd_smem = std::max(E.rb_fwd_smem, (size_t)D.mesh[0] * D.mesh[1] * sizeof(unsigned long long) +
+                                                             (size_t)2 * nxh * D.mesh[1] * sizeof(float2) +
+                                                             (2 * ncell + 1) * sizeof(int));
+                E.rb_inv_smem = std::max(E.rb_inv_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2));
+            } else {
+                for (int y = 0; y < D.mesh[1]; ++y)
+                    for (int x0 = 0; x0 < D.mesh[0]; x0 += ZPASS_TX) zj.push_back(make_int4(r, y, x0, 0));
+                E.plane_smem = std::max(E.plane_smem, (size_t)2 * D.mesh[0] * D.mesh[1] * sizeof(float2));
+            }
             E.zpass_smem = std::max(E.zpass_smem, (size_t)2 * ZPASS_TX * D.mesh[2] * sizeof(float2));
         }
         zoff.push_back((int)zj.size());
@@ -422,7 +453,8 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         CU(cudaMemcpy(E.d_plane_jobs, pj.data(), sizeof(int2) * pj.size(), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(E.d_zjobs, zj.data(), sizeof(int4) * zj.size(), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(E.d_zjob_off, zoff.data(), sizeof(int) * zoff.size(), cudaMemcpyHostToDevice));
-        CU(mesh_set_smem_limits(E));
+        if (E.use_r2c) CU(rebuild_set_smem_limits(E));
+        else CU(mesh_set_smem_limits(E));
     }
     CU(prepare_mc(E));
     return PHMC_OK;
@@ -693,7 +725,7 @@ int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
         h->ev_mc.clear();
         h->ev_flush.clear();
     }
-    const int flush_kernels = (E.coulomb == PHMC_COUL_EWALD) ? 5 : 0;
+    const int flush_kernels = E.flush_kernels;
     long long iter = 0;
     const long long max_iter = n_trials + 8;
     int s = build_chunk_graph(h, check_every);
@@ -870,7 +902,7 @@ extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const flo
     launch_cell_build(E, s);
     h->prof.kernel_launches += 2;
     int rc = full_recompute(h);
-    h->prof.kernel_launches += (E.coulomb == PHMC_COUL_EWALD ? 5 : 0) + 2;
+    h->prof.kernel_launches += E.flush_kernels + 2;
     return rc;
 }
 

@@ -29,6 +29,11 @@ struct Engine {
     int* d_zjob_off = nullptr;
     double* d_epart = nullptr;
     size_t plane_smem = 0, zpass_smem = 0;
+    bool use_r2c = false;        // every replica has even nx: fused spread + real-to-complex rebuild
+    size_t rb_fwd_smem = 0, rb_inv_smem = 0;
+    int flush_kernels = 0;       // kernels per potential-mesh rebuild
+    bool unit_pending = false;   // next rebuild places a unit charge instead of the particles
+    long long total_meshh = 0;
     int* d_rep_of = nullptr;
     int* d_cell_rep = nullptr;   // replica of every global cell
     int* d_dirty = nullptr;      // per replica: mesh must be rebuilt
@@ -52,6 +57,10 @@ void launch_fft_pipeline(Engine& E, const int* dirty, int mode, cudaStream_t st)
 void launch_unit_charge(Engine& E, cudaStream_t st);
 void launch_extract_octant(Engine& E, int r, cudaStream_t st);
 cudaError_t mesh_set_smem_limits(Engine& E);
+
+// k_rebuild.cu
+void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st);
+cudaError_t rebuild_set_smem_limits(Engine& E);
 
 // k_pair.cu
 void launch_cell_build(Engine& E, cudaStream_t st);

@@ -1,0 +1,288 @@
+// Potential-mesh rebuild for meshes with even nx: three passes over the
+// half-spectrum mesh, spreading fused into the first.
+//
+//  k_rb_fwd  (replica, z): gather the charges whose order-P stencils reach plane
+//            z from the cell list, accumulate them in a shared-memory
+//            fixed-point plane (2^40, 64-bit shared atomics: deterministic and
+//            bit-identical to the scatter kernel's mesh), then real-to-complex
+//            FFT along x (length nx/2 complex FFT of packed pairs + split) and
+//            complex FFT along y; writes (nx/2+1) x ny complex values.
+//  k_rb_zpass (replica, y, column tile): FFT along z, E += w theta |F|^2,
+//            F *= theta, inverse FFT along z.
+//  k_rb_inv  (replica, z): inverse FFT along y, complex-to-real along x; writes
+//            the real potential plane.
+// Replaces the memset + k_spread_cubic + cuFFT R2C + influence kernel chain of
+// the reference (MC/src/pme.cu:140-249,362,384-422) and the separate global
+// charge mesh of the scatter path.
+#include "common.cuh"
+#include "engine.h"
+#include "fft.cuh"
+
+template <int P, int NT>
+__global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict__ jobs, int unit_charge,
+                                               const int* __restrict__ dirty) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int2 job = jobs[blockIdx.x];
+    const int r = job.x, z = job.y;
+    if (dirty && !dirty[r]) return;
+    const RepDesc& D = d.desc[r];
+    const int nx = D.mesh[0], ny = D.mesh[1], nz = D.mesh[2];
+    const int M = nx / 2, nxh = M + 1;
+    unsigned long long* qp = reinterpret_cast<unsigned long long*>(sm_raw);
+    float2* a = reinterpret_cast<float2*>(qp + nx * ny);
+    float2* b = a + nxh * ny;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < nx * ny; i += NT) qp[i] = 0ull;
+    __syncthreads();
+    if (unit_charge) {
+        if (z == 0 && tid == 0) qp[0] = (unsigned long long)(long long)PHMC_FIX_SCALE;
+    } else {
+        // floor(g_z) of a contributing charge lies in [z - P/2, z - P/2 + P - 1] (mod nz)
+        const float hz = D.L[2] / (float)nz;
+        const float lo = (float)(z - P / 2) * hz, hi = (float)(z - P / 2 + P) * hz;
+        const int ncz = D.ncell[2], ncxy = D.ncell[0] * D.ncell[1];
+        int c_lo = (int)floorf(lo * D.cell_scale[2]) - 1, c_hi = (int)floorf(hi * D.cell_scale[2]) + 1;
+        int nlay = c_hi - c_lo + 1;
+        if (nlay > ncz) { nlay = ncz; c_lo = 0; }
+        const int ncell = nlay * ncxy;
+        // member counts of every cell in the layers, then an exclusive scan, so that the
+        // (cell, member) items spread over all threads with independent loads
+        int* s_cnt = reinterpret_cast<int*>(b + nxh * ny);
+        int* s_cid = s_cnt + ncell + 1;
+        __shared__ int s_wsum[NT / 32 + 1];
+        for (int cc = tid; cc < ncell; cc += NT) {
+            const int lay = cc / ncxy, cxy = cc - lay * ncxy;
+            int cz = (c_lo + lay) % ncz;
+            cz += (cz < 0) ? ncz : 0;
+            const int c = cz * ncxy + cxy;
+            s_cid[cc] = c;
+            s_cnt[cc] = min(d.cell_count[D.cell_off + c], D.cell_cap);
+        }
+        __syncthreads();
+        {   // block scan: each thread a contiguous chunk, then the chunk totals
+            const int per = (ncell + NT - 1) / NT;
+            const int b0 = min(ncell, tid * per), b1 = min(ncell, b0 + per);
+            int sum = 0;
+            for (int i = b0; i < b1; ++i) sum += s_cnt[i];
+            int x = sum;
+            const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_wsum[warp] = x;
+            __syncthreads();
+            if (tid == 0) {
+                int acc = 0;
+                for (int w = 0; w < NT / 32; ++w) { const int v = s_wsum[w]; s_wsum[w] = acc; acc += v; }
+                s_wsum[NT / 32] = acc;
+            }
+            __syncthreads();
+            int run = s_wsum[warp] + x - sum;
+            for (int i = b0; i < b1; ++i) { const int v = s_cnt[i]; s_cnt[i] = run; run += v; }
+            if (tid == NT - 1) s_cnt[ncell] = s_wsum[NT / 32];
+        }
+        __syncthreads();
+        const int total = s_cnt[ncell];
+        for (int it = tid; it < total; it += NT) {
+            int lo2 = 0, hi2 = ncell - 1;  // last cell whose offset <= it
+            while (lo2 < hi2) {
+                const int mid = (lo2 + hi2 + 1) >> 1;
+                if (s_cnt[mid] <= it) lo2 = mid; else hi2 = mid - 1;
+            }
+            const int c = s_cid[lo2];
+            const int k = it - s_cnt[lo2];
+            {
+                const float4 pq = d.posq[D.slot_off + d.cell_list[((size_t)D.cell_off + c) * D.cell_cap + k]];
+                if (pq.w == 0.0f) continue;
+                const float gz = pq.z / D.L[2] * (float)nz;
+                const float flz = floorf(gz);
+                int ci = z - ((int)flz + P / 2 - P + 1);
+                ci %= nz;
+                ci += (ci < 0) ? nz : 0;
+                if (ci >= P) continue;
+                float wz[P], wx[P], wy[P];
+                bspline_weights<P>(gz - flz, wz);
+                const float gx = pq.x / D.L[0] * (float)nx, gy = pq.y / D.L[1] * (float)ny;
+                const float flx = floorf(gx), fly = floorf(gy);
+                bspline_weights<P>(gx - flx, wx);
+                bspline_weights<P>(gy - fly, wy);
+                const int bx = (int)flx + P / 2 - P + 1, by = (int)fly + P / 2 - P + 1;
+#pragma unroll
+                for (int bb = 0; bb < P; ++bb) {
+                    int yb = by + bb;
+                    yb += (yb < 0) ? ny : 0;
+                    yb -= (yb >= ny) ? ny : 0;
+                    const float wyz = pq.w * wy[bb] * wz[ci];
+#pragma unroll
+                    for (int aa = 0; aa < P; ++aa) {
+                        int xa = bx + aa;
+                        xa += (xa < 0) ? nx : 0;
+                        xa -= (xa >= nx) ? nx : 0;
+                        const long long v = __double2ll_rn((double)(wyz * wx[aa]) * PHMC_FIX_SCALE);
+                        atomicAdd(&qp[yb * nx + xa], (unsigned long long)v);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // packed real pairs: a[y*M + j] = (Q[y][2j], Q[y][2j+1])
+    for (int i = tid; i < M * ny; i += NT) {
+        const int y = i / M, j = i - y * M;
+        a[i] = make_float2((float)((double)(long long)qp[y * nx + 2 * j] * PHMC_FIX_INV),
+                           (float)((double)(long long)qp[y * nx + 2 * j + 1] * PHMC_FIX_INV));
+    }
+    __syncthreads();
+    float2* zr = fft_lines<NT>(a, b, M, ny, M, 1, d.twiddle + D.tw_off_h, -1.0f, false);
+    float2* xo = (zr == a) ? b : a;
+    const float2* twn = d.twiddle + D.tw_off[0];  // exp(-2 pi i k / nx)
+    // split: X_k = 1/2 (Z_k + conj Z_{M-k}) - i/2 W^k (Z_k - conj Z_{M-k}), k = 0..M
+    for (int i = tid; i < nxh * ny; i += NT) {
+        const int y = i / nxh, k = i - y * nxh;
+        const float2 zk = zr[y * M + (k == M ? 0 : k)];
+        float2 zc = zr[y * M + (k == 0 ? 0 : M - k)];
+        zc.y = -zc.y;
+        const float2 w = twn[k];
+        const float2 s = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+        const float2 df = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
+        const float2 wd = cmul(w, df);  // W * (Z_k - conj Z_{M-k}) / 2
+        xo[y * nxh + k] = make_float2(s.x + wd.y, s.y - wd.x);  // s - i * wd
+    }
+    __syncthreads();
+    float2* res = fft_lines<NT>(xo, zr, ny, nxh, 1, nxh, d.twiddle + D.tw_off[1], -1.0f, true);
+    float2* c = d.cmesh + D.meshh_off + (size_t)z * ny * nxh;
+    for (int i = tid; i < nxh * ny; i += NT) c[i] = res[i];
+}
+
+// z pencils of the half spectrum; job = (replica, y, x0, width <= ZPASS_TX).
+template <int NT, int TX>
+__global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restrict__ jobs, double* __restrict__ epart,
+                                                 const int* __restrict__ dirty) {
+    extern __shared__ float2 sm[];
+    __shared__ double red[40];
+    const int4 job = jobs[blockIdx.x];
+    const int r = job.x, y = job.y, x0 = job.z, tw_n = job.w;
+    if (dirty && !dirty[r]) { if (threadIdx.x == 0) epart[blockIdx.x] = 0.0; return; }
+    const RepDesc& D = d.desc[r];
+    const int nx = D.mesh[0], ny = D.mesh[1], nz = D.mesh[2];
+    const int M = nx / 2, nxh = M + 1;
+    float2* a = sm;
+    float2* b = sm + TX * nz;
+    float2* c = d.cmesh + D.meshh_off;
+    for (int e = threadIdx.x; e < nz * TX; e += NT) {
+        const int z = e / TX, tx = e - z * TX;
+        a[e] = (tx < tw_n) ? c[((size_t)z * ny + y) * nxh + x0 + tx] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* res = fft_lines<NT>(a, b, nz, TX, 1, TX, d.twiddle + D.tw_off[2], -1.0f, true);
+    const float* mx = d.moduli + D.mod_off[0];
+    const float* my = d.moduli + D.mod_off[1];
+    const float* mz = d.moduli + D.mod_off[2];
+    const int myi = (y <= ny / 2) ? y : y - ny;
+    const float kyv = (float)myi / D.L[1];
+    const float pv = 3.14159265358979323846f * (float)D.V;
+    double e_loc = 0.0;
+    for (int e = threadIdx.x; e < nz * TX; e += NT) {
+        const int kz = e / TX, tx = e - kz * TX;
+        const int kx = x0 + tx;
+        const float2 F = res[e];
+        float th = 0.0f;
+        if (tx < tw_n && !(kx == 0 && y == 0 && kz == 0)) {
+            const int mzi = (kz <= nz / 2) ? kz : kz - nz;
+            const float kxv = (float)kx / D.L[0], kzv = (float)mzi / D.L[2];
+            const float m2 = kxv * kxv + kyv * kyv + kzv * kzv;
+            const float den = m2 * pv * mx[kx] * my[y] * mz[kz];
+            if (den > 0.0f) th = D.elf * expf(-D.ewald_factor * m2) / den;
+            const float wgt = (kx == 0 || kx == M) ? 1.0f : 2.0f;  // half spectrum, Hermitian partners counted
+            e_loc += (double)(wgt * th) * ((double)F.x * F.x + (double)F.y * F.y);
+        }
+        res[e] = make_float2(F.x * th, F.y * th);
+    }
+    __syncthreads();
+    float2* oth = (res == a) ? b : a;
+    res = fft_lines<NT>(res, oth, nz, TX, 1, TX, d.twiddle + D.tw_off[2], 1.0f, true);
+    for (int e = threadIdx.x; e < nz * TX; e += NT) {
+        const int z = e / TX, tx = e - z * TX;
+        if (tx < tw_n) c[((size_t)z * ny + y) * nxh + x0 + tx] = res[e];
+    }
+    const double s = block_sum<NT>(e_loc, red);
+    if (threadIdx.x == 0) epart[blockIdx.x] = 0.5 * s;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_rb_inv(DevPtrs d, const int2* __restrict__ jobs, const int* __restrict__ dirty) {
+    extern __shared__ float2 sm[];
+    const int2 job = jobs[blockIdx.x];
+    const int r = job.x, z = job.y;
+    if (dirty && !dirty[r]) return;
+    const RepDesc& D = d.desc[r];
+    const int nx = D.mesh[0], ny = D.mesh[1];
+    const int M = nx / 2, nxh = M + 1;
+    float2* a = sm;
+    float2* b = sm + nxh * ny;
+    const float2* c = d.cmesh + D.meshh_off + (size_t)z * ny * nxh;
+    for (int i = threadIdx.x; i < nxh * ny; i += NT) a[i] = c[i];
+    __syncthreads();
+    float2* xr = fft_lines<NT>(a, b, ny, nxh, 1, nxh, d.twiddle + D.tw_off[1], 1.0f, true);
+    float2* zo = (xr == a) ? b : a;
+    const float2* twn = d.twiddle + D.tw_off[0];
+    // merge: Z'_k = (X_k + conj X_{M-k}) + i W^{-k} (X_k - conj X_{M-k}), k = 0..M-1
+    for (int i = threadIdx.x; i < M * ny; i += NT) {
+        const int y = i / M, k = i - y * M;
+        const float2 A = xr[y * nxh + k];
+        float2 B = xr[y * nxh + (M - k)];
+        B.y = -B.y;
+        float2 w = twn[k];
+        w.y = -w.y;  // W^{-k}
+        const float2 s = make_float2(A.x + B.x, A.y + B.y);
+        const float2 wd = cmul(w, make_float2(A.x - B.x, A.y - B.y));
+        zo[y * M + k] = make_float2(s.x - wd.y, s.y + wd.x);  // s + i * wd
+    }
+    __syncthreads();
+    float2* zz = fft_lines<NT>(zo, xr, M, ny, M, 1, d.twiddle + D.tw_off_h, 1.0f, false);
+    float* phi = d.phi + D.mesh_off + (size_t)z * ny * nx;
+    for (int i = threadIdx.x; i < M * ny; i += NT) {
+        const int y = i / M, j = i - y * M;
+        phi[y * nx + 2 * j] = zz[i].x;
+        phi[y * nx + 2 * j + 1] = zz[i].y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st) {
+    switch (E.order) {
+        case 4: k_rb_fwd<4, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
+        case 5: k_rb_fwd<5, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
+        default: k_rb_fwd<6, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
+    }
+    k_rb_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty);
+    k_rb_inv<256><<<E.n_plane_jobs, 256, E.rb_inv_smem, st>>>(E.d, E.d_plane_jobs, dirty);
+}
+
+template <typename K>
+static cudaError_t raise_cap(K kernel, int device, size_t need) {
+    int optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    const int cap = optin - (int)fa.sharedSizeBytes;
+    if (cap < (int)need) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+}
+
+cudaError_t rebuild_set_smem_limits(Engine& E) {
+    cudaError_t e = cudaSuccess;
+    switch (E.order) {
+        case 4: e = raise_cap(k_rb_fwd<4, 256>, E.device, E.rb_fwd_smem); break;
+        case 5: e = raise_cap(k_rb_fwd<5, 256>, E.device, E.rb_fwd_smem); break;
+        default: e = raise_cap(k_rb_fwd<6, 256>, E.device, E.rb_fwd_smem); break;
+    }
+    if (e != cudaSuccess) return e;
+    e = raise_cap(k_rb_zpass<256, ZPASS_TX>, E.device, E.zpass_smem);
+    if (e != cudaSuccess) return e;
+    return raise_cap(k_rb_inv<256>, E.device, E.rb_inv_smem);
+}
