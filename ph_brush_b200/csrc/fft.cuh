@@ -52,40 +52,69 @@ __device__ __forceinline__ int fft_plan(int n, int* rad) {
     return ns;
 }
 
+// a / b and a % b for 0 <= a < 2^22 through a float reciprocal of b, corrected to exact.
+struct FastDiv {
+    int b;
+    float rb;
+    __device__ __forceinline__ explicit FastDiv(int b_) : b(b_), rb(1.0f / (float)b_) {}
+    __device__ __forceinline__ int div(int a, int& rem) const {
+        int q = __float2int_rz((float)a * rb);
+        int r = a - q * b;
+        if (r < 0) { --q; r += b; } else if (r >= b) { ++q; r -= b; }
+        rem = r;
+        return q;
+    }
+};
+
+// One Stockham stage of radix R over all lines (R is a compile-time constant, so
+// the butterfly's R values stay in registers).
+template <int R, int NT>
+__device__ __forceinline__ void fft_stage(const float2* __restrict__ a, float2* __restrict__ b, int n, int nlines, int ls,
+                                          int es, const float2* __restrict__ tw, float sign, bool line_fastest, int Ns,
+                                          const FastDiv& dl) {
+    const int nb = n / R;
+    const int tstride = n / (Ns * R);
+    const int total = nb * nlines;
+    const FastDiv dnb(nb), dns(Ns);
+    for (int t = threadIdx.x; t < total; t += NT) {
+        int line, j, k;
+        if (line_fastest) j = dl.div(t, line);
+        else line = dnb.div(t, j);
+        const int jq = dns.div(j, k);
+        float2 v[R];
+        const float2* src = a + line * ls;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            float2 w = __ldg(&tw[r * k * tstride]);
+            if (sign > 0.0f) w.y = -w.y;
+            v[r] = cmul(v[r], w);
+        }
+        dft_radix(v, R, sign);
+        const int idx = jq * Ns * R + k;
+        float2* dst = b + line * ls;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[(idx + r * Ns) * es] = v[r];
+    }
+    __syncthreads();
+}
+
+// Radices in the order 4,...,4, 2, 3,...,3, 5,...,5 (n = 2^a 3^b 5^c).
 template <int NT>
 __device__ float2* fft_lines(float2* a, float2* b, int n, int nlines, int ls, int es, const float2* __restrict__ tw,
                              float sign, bool line_fastest) {
-    int rad[16];
-    const int ns = fft_plan(n, rad);
-    int Ns = 1;
-    for (int s = 0; s < ns; ++s) {
-        const int R = rad[s];
-        const int nb = n / R;
-        const int tstride = n / (Ns * R);
-        const int total = nb * nlines;
-        for (int t = threadIdx.x; t < total; t += NT) {
-            int line, j;
-            if (line_fastest) { line = t % nlines; j = t / nlines; }
-            else { j = t % nb; line = t / nb; }
-            const int k = j % Ns;
-            float2 v[5];
-            const float2* src = a + line * ls;
-#pragma unroll 5
-            for (int r = 0; r < 5; ++r)
-                if (r < R) v[r] = src[(j + r * nb) * es];
-            for (int r = 1; r < R; ++r) {
-                float2 w = __ldg(&tw[r * k * tstride]);
-                if (sign > 0.0f) w.y = -w.y;
-                v[r] = cmul(v[r], w);
-            }
-            dft_radix(v, R, sign);
-            const int idx = (j / Ns) * Ns * R + k;
-            float2* dst = b + line * ls;
-            for (int r = 0; r < R; ++r) dst[(idx + r * Ns) * es] = v[r];
-        }
-        __syncthreads();
+    int Ns = 1, m = n;
+    const FastDiv dl(nlines);
+    while (m > 1) {
+        int R;
+        if (m % 4 == 0) { R = 4; fft_stage<4, NT>(a, b, n, nlines, ls, es, tw, sign, line_fastest, Ns, dl); }
+        else if (m % 2 == 0) { R = 2; fft_stage<2, NT>(a, b, n, nlines, ls, es, tw, sign, line_fastest, Ns, dl); }
+        else if (m % 3 == 0) { R = 3; fft_stage<3, NT>(a, b, n, nlines, ls, es, tw, sign, line_fastest, Ns, dl); }
+        else { R = 5; fft_stage<5, NT>(a, b, n, nlines, ls, es, tw, sign, line_fastest, Ns, dl); }
         float2* t = a; a = b; b = t;
         Ns *= R;
+        m /= R;
     }
     return a;
 }

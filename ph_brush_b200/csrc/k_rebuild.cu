@@ -41,7 +41,8 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
         const float hz = D.L[2] / (float)nz;
         const float lo = (float)(z - P / 2) * hz, hi = (float)(z - P / 2 + P) * hz;
         const int ncz = D.ncell[2], ncxy = D.ncell[0] * D.ncell[1];
-        int c_lo = (int)floorf(lo * D.cell_scale[2]) - 1, c_hi = (int)floorf(hi * D.cell_scale[2]) + 1;
+        // the cell layers of [lo, hi), widened by a rounding margin (the exact test is per charge)
+        int c_lo = (int)floorf((lo - 1e-3f * hz) * D.cell_scale[2]), c_hi = (int)floorf((hi + 1e-3f * hz) * D.cell_scale[2]);
         int nlay = c_hi - c_lo + 1;
         if (nlay > ncz) { nlay = ncz; c_lo = 0; }
         const int ncell = nlay * ncxy;
@@ -120,7 +121,9 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
                         int xa = bx + aa;
                         xa += (xa < 0) ? nx : 0;
                         xa -= (xa >= nx) ? nx : 0;
-                        const long long v = __double2ll_rn((double)(wyz * wx[aa]) * PHMC_FIX_SCALE);
+                        // v * 2^40 is exact in float, so this rounds the same real number as the
+                        // scatter kernel's double conversion: identical fixed-point values
+                        const long long v = __float2ll_rn(wyz * wx[aa] * 1099511627776.0f);
                         atomicAdd(&qp[yb * nx + xa], (unsigned long long)v);
                     }
                 }
