@@ -246,6 +246,77 @@ int phmc_recip_energy_static(const float* x, const float* y, const float* z, con
                              const double box[3], const int mesh[3], int order, double ewald_alpha,
                              double epsilon_r, int ref_moduli, double* e_recip);
 
+/* ---- learned surrogate and delayed acceptance (no counterpart in the reference) ----
+ *
+ * The surrogate is an MLP n_in -> H -> H -> H -> 1 (GELU, BF16 weights and
+ * activations, FP32 accumulation on the tensor cores) trained on the GPU with
+ * Adam.  A sample is one titration or swap move: PHMC_SUR_ROWS rows of n_in
+ * features (the old and the new state of each changed particle; row layout in
+ * the design notes) with signs -1 / +1 (0 = unused row) and a target
+ * t = dE - (exact terms), where the exact terms are the direct interaction of
+ * the two changed particles and the self / net-charge / slab changes.  The
+ * estimate of a move is scale * sum_r sign_r y(row_r) + exact terms: minus the
+ * estimate of the reverse move, so delayed acceptance with it keeps detailed
+ * balance.  The engine's first stage needs n_in == PHMC_SUR_INPUTS. */
+#define PHMC_SUR_INPUTS 80
+#define PHMC_SUR_ROWS 4
+#define PHMC_SUR_DESC_STRIDE (PHMC_SUR_ROWS * PHMC_SUR_INPUTS + 2 * PHMC_SUR_ROWS + 4)
+typedef struct phmc_surrogate phmc_surrogate;
+int phmc_surrogate_create(int n_in, int hidden, uint64_t seed, phmc_surrogate** out);
+int phmc_surrogate_destroy(phmc_surrogate* s);
+int phmc_surrogate_num_params(phmc_surrogate* s);
+/* flat FP32 parameters: W1[n_in*H], b1[H], W2[H*H], b2[H], W3[H*H], b3[H], w4[H], b4;
+ * W[k*H + j] connects input k to unit j */
+int phmc_surrogate_get_params(phmc_surrogate* s, float* out, int n);
+int phmc_surrogate_set_params(phmc_surrogate* s, const float* in, int n);
+/* input standardisation (x - mu) / sd and the output scale (energy = scale * y) */
+int phmc_surrogate_set_scaling(phmc_surrogate* s, const float* mu, const float* sd, float scale);
+int phmc_surrogate_get_scaling(phmc_surrogate* s, float* mu, float* sd, float* scale);
+/* per-row outputs in energy units for n_rows host rows of n_in features */
+int phmc_surrogate_predict(phmc_surrogate* s, const float* x, int n_rows, float* y);
+/* loss 1/2 mean((pred - clip(t)) / scale)^2 and its gradient w.r.t. the flat
+ * parameters for n samples (x: n*PHMC_SUR_ROWS rows, sign: n*PHMC_SUR_ROWS) */
+int phmc_surrogate_gradient(phmc_surrogate* s, const float* x, const float* sign, const float* t, int n, float clip,
+                            double* loss, float* grad);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) over host samples; rescale = 1 first sets the
+ * standardisation and scale from the data.  *loss = mean batch loss of the last epoch. */
+int phmc_surrogate_train(phmc_surrogate* s, const float* x, const float* sign, const float* t, int n, int epochs,
+                         int batch, float lr, float clip, uint64_t seed, int rescale, double* loss);
+int phmc_surrogate_save(phmc_surrogate* s, const char* path);
+int phmc_surrogate_load(const char* path, phmc_surrogate** out);
+
+/* Record a training sample for every titration / swap trial of the following
+ * phmc_run calls (all replicas, exact dE), up to `capacity` samples; 0 stops
+ * and frees.  Each call clears the samples. */
+int phmc_harvest(phmc_engine* e, int capacity);
+int phmc_harvest_count(phmc_engine* e, int* n);
+int phmc_harvest_get(phmc_engine* e, int n, float* x, float* sign, float* t);
+/* Train s on the harvested samples on the device (rescale from the data). */
+int phmc_surrogate_fit(phmc_engine* e, phmc_surrogate* s, int epochs, int batch, float lr, float clip, uint64_t seed,
+                       double* loss);
+/* Delayed acceptance for titration and swap trials of all replicas: stage one
+ * is Metropolis on the surrogate estimate, stage two on the exact dE minus the
+ * estimate.  A replica returns to plain Metropolis when, over `window`
+ * stage-one passes, fewer than `threshold` of them are accepted by stage two.
+ * s must outlive the attachment; NULL detaches.  Resets the counters. */
+int phmc_surrogate_attach(phmc_engine* e, phmc_surrogate* s, double threshold, int window);
+typedef struct phmc_da_stats {
+    int64_t evaluated;  /* trials judged by the surrogate */
+    int64_t passed;     /* stage-one passes (exact dE computed) */
+    int64_t accepted;   /* stage-two accepts */
+    int fallback;       /* 1: replica went back to plain Metropolis */
+    int pad;
+} phmc_da_stats;
+int phmc_get_da_stats(phmc_engine* e, phmc_da_stats* out); /* n_replicas entries */
+/* Descriptor rows, signs, per-row outputs and exact terms of n trials of replica r
+ * against the current state (PHMC_SUR_DESC_STRIDE floats per trial: rows, signs,
+ * outputs, cross term, moment terms, row count, inner-cell particles); dEs gets
+ * the surrogate estimate (NaN without an attached surrogate).  For checks. */
+int phmc_surrogate_describe(phmc_engine* e, int replica, const phmc_trial* t, int n, float* out, double* dEs);
+/* With a trial log set: also record, per trial, the stage reached (0 plain,
+ * 1 rejected by the surrogate, 2 judged by the exact dE) and the estimate. */
+int phmc_set_da_log(phmc_engine* e, int* stage, double* dEs);
+
 /* ---- synthetic input (no counterpart in the reference, whose inputs are
  * LAMMPS data files, MC/src/io.cpp:79-146) ----
  * Grafted brush: chains on a square lattice at z = 0, self-avoiding random

@@ -5,7 +5,7 @@ include/phmc.h; this package holds its Python handle, the model containers
 and the workload builders.
 """
 from . import _abi
-from .engine import Engine
+from .engine import Engine, Surrogate
 from .model import ModelParams, SystemArrays, build_brush, ewald_alpha, ideal_alpha
 
-__all__ = ["Engine", "ModelParams", "SystemArrays", "build_brush", "ewald_alpha", "ideal_alpha", "_abi"]
+__all__ = ["Engine", "Surrogate", "ModelParams", "SystemArrays", "build_brush", "ewald_alpha", "ideal_alpha", "_abi"]

@@ -16,6 +16,8 @@ ERRORS = {1: "ARG", 2: "CUDA", 3: "CAPACITY", 4: "BUDGET", 5: "STATE", 6: "UNSUP
 COUL_NONE, COUL_CUT, COUL_EWALD = 0, 1, 2
 F_MOBILE, F_TITRATABLE, F_GHOST, F_CATION, F_ANION = 0x01, 0x02, 0x04, 0x08, 0x10
 MOVE_DISP, MOVE_TITR, MOVE_SWAP, MOVE_NONE = 0, 1, 2, 3
+SUR_INPUTS, SUR_ROWS = 80, 4
+SUR_DESC_STRIDE = SUR_ROWS * SUR_INPUTS + 2 * SUR_ROWS + 4
 
 _fp = C.POINTER(C.c_float)
 _ip = C.POINTER(C.c_int)
@@ -78,6 +80,14 @@ class Profile(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class DAStats(C.Structure):
+    _fields_ = [("evaluated", C.c_int64), ("passed", C.c_int64), ("accepted", C.c_int64),
+                ("fallback", C.c_int), ("pad", C.c_int)]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 class BrushSpec(C.Structure):
     _fields_ = [("chains_x", C.c_int), ("chains_y", C.c_int), ("graft_spacing", C.c_double),
                 ("len_min", C.c_int), ("len_max", C.c_int), ("n_permanent", C.c_int),
@@ -90,7 +100,13 @@ EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
            "phmc_set_state", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
-           "phmc_recip_energy_static"]
+           "phmc_recip_energy_static",
+           "phmc_surrogate_create", "phmc_surrogate_destroy", "phmc_surrogate_num_params",
+           "phmc_surrogate_get_params", "phmc_surrogate_set_params", "phmc_surrogate_set_scaling",
+           "phmc_surrogate_get_scaling", "phmc_surrogate_predict", "phmc_surrogate_gradient",
+           "phmc_surrogate_train", "phmc_surrogate_save", "phmc_surrogate_load", "phmc_harvest",
+           "phmc_harvest_count", "phmc_harvest_get", "phmc_surrogate_fit", "phmc_surrogate_attach",
+           "phmc_get_da_stats", "phmc_surrogate_describe", "phmc_set_da_log"]
 
 
 def load_library(path=LIB_PATH):
@@ -122,6 +138,27 @@ def load_library(path=LIB_PATH):
         "phmc_flush_l2": ([eng, C.c_int64], C.c_int),
         "phmc_recip_energy_static": ([_fp, _fp, _fp, _fp, C.c_int, _dp, _ip, C.c_int, C.c_double, C.c_double,
                                       C.c_int, _dp], C.c_int),
+        "phmc_surrogate_create": ([C.c_int, C.c_int, C.c_uint64, C.POINTER(eng)], C.c_int),
+        "phmc_surrogate_destroy": ([eng], C.c_int),
+        "phmc_surrogate_num_params": ([eng], C.c_int),
+        "phmc_surrogate_get_params": ([eng, _fp, C.c_int], C.c_int),
+        "phmc_surrogate_set_params": ([eng, _fp, C.c_int], C.c_int),
+        "phmc_surrogate_set_scaling": ([eng, _fp, _fp, C.c_float], C.c_int),
+        "phmc_surrogate_get_scaling": ([eng, _fp, _fp, _fp], C.c_int),
+        "phmc_surrogate_predict": ([eng, _fp, C.c_int, _fp], C.c_int),
+        "phmc_surrogate_gradient": ([eng, _fp, _fp, _fp, C.c_int, C.c_float, _dp, _fp], C.c_int),
+        "phmc_surrogate_train": ([eng, _fp, _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64,
+                                  C.c_int, _dp], C.c_int),
+        "phmc_surrogate_save": ([eng, C.c_char_p], C.c_int),
+        "phmc_surrogate_load": ([C.c_char_p, C.POINTER(eng)], C.c_int),
+        "phmc_harvest": ([eng, C.c_int], C.c_int),
+        "phmc_harvest_count": ([eng, _ip], C.c_int),
+        "phmc_harvest_get": ([eng, C.c_int, _fp, _fp, _fp], C.c_int),
+        "phmc_surrogate_fit": ([eng, eng, C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64, _dp], C.c_int),
+        "phmc_surrogate_attach": ([eng, eng, C.c_double, C.c_int], C.c_int),
+        "phmc_get_da_stats": ([eng, C.POINTER(DAStats)], C.c_int),
+        "phmc_surrogate_describe": ([eng, C.c_int, C.POINTER(Trial), C.c_int, _fp, _dp], C.c_int),
+        "phmc_set_da_log": ([eng, _ip, _dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/phmc.h"
+#include "surrogate.cuh"
 
 #define PHMC_MAX_TYPES 8
 #define PHMC_MAX_ORDER 6
@@ -59,6 +60,12 @@ struct RepDesc {
     double qcorr_coef;  // -pi * elf / (2 V alpha^2)
     double slab_coef;   // 2 pi elf / V
     double Lz2_12;      // Lz^2 / 12
+    // surrogate descriptor
+    float cell_w[3];      // cell widths L / ncell (float)
+    int dnr[3];           // cell range of the 8-sigma descriptor sphere: offsets -dnr .. -dnr + dnk - 1
+    int dnk[3];           // min(2 dnr + 1, ncell)
+    float sur_z0, sur_h;  // z feature = (z - sur_z0) / sur_h
+    float sur_pk, sur_salt;  // pKa - pH, log10(salt) features
 };
 
 // Per-replica mutable state (device-resident between launches).
@@ -78,6 +85,11 @@ struct RepState {
     double E_rec_flush; // E_rec computed at the last flush
     double alg_bytes;   // algorithmic bytes of the trials run so far
     long long trials_run;
+    // delayed acceptance: trials judged by the surrogate, first-stage passes,
+    // second-stage accepts; the same over the current agreement window
+    long long da_eval, da_pass, da_acc, da_wpass, da_wacc;
+    int da_off;         // agreement fell below the threshold: plain Metropolis from then on
+    int da_pad;
 };
 
 // Device pointers of the whole engine (all replicas concatenated).
@@ -108,7 +120,29 @@ struct DevPtrs {
     // trial log / replay (replica 0)
     int* log_move; double* log_dE; int* log_acc; long long log_cap;
     const int* replay; long long replay_n;
+    int* log_stage; double* log_dEs;  // delayed-acceptance log (replica 0): stage reached, surrogate dE
+    // per cell: present particles of each descriptor class (+1, -1, neutral titratable, permanent)
+    int4* cell_cls;
+    // delayed acceptance
+    SurDev sur;
+    float da_threshold;  // minimum second-stage acceptance among first-stage passes
+    int da_window;       // first-stage passes per agreement check
+    // training-sample harvest: rows [cap][SUR_ROWS][SUR_K], signs [cap][SUR_ROWS], targets [cap]
+    float* hv_rows; float* hv_sign; float* hv_target; int* hv_count; int hv_cap;
+    // descriptor output of MC_DESCRIBE launches (DSC_STRIDE floats per trial)
+    float* dsc_out;
 };
+
+#define DSC_STRIDE (SUR_ROWS * SUR_K + 2 * SUR_ROWS + 4)
+
+// Descriptor class of a present particle (-1: none).
+__host__ __device__ inline int desc_class(int flags, float q) {
+    if (flags & PHMC_F_GHOST) return -1;
+    if (flags & PHMC_F_TITRATABLE) return q != 0.0f ? 0 : 2;
+    if (q < 0.0f) return 1;
+    if (q > 0.0f) return (flags & PHMC_F_CATION) ? 0 : 3;  // salt cation, or a permanently charged bead
+    return -1;
+}
 
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon et al., SC'11), written from the paper's definition.

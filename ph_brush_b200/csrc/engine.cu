@@ -50,6 +50,8 @@ struct phmc_engine {
     int graph_chunks = 0;
     bool graph_prof = false;
     std::vector<cudaEvent_t> gev;  // 4 per chunk when profiling
+    // delayed-acceptance log destinations (host)
+    int* h_da_stage = nullptr; double* h_da_dEs = nullptr;
 };
 
 static void drop_graph(phmc_engine* h) {
@@ -260,6 +262,10 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
             D.ncell[k] = (int)std::floor(S.box[k] / rmax);
             if (D.ncell[k] < 3) return fail(PHMC_ERR_UNSUPPORTED, "box must hold at least 3 cells of the largest cutoff per axis");
             D.cell_scale[k] = (float)D.ncell[k] / D.L[k];
+            // surrogate descriptor: cell widths and the cell range of the 8-sigma sphere
+            D.cell_w[k] = D.L[k] / (float)D.ncell[k];
+            D.dnr[k] = std::max(1, (int)std::ceil((double)SUR_RMAX * D.ncell[k] / S.box[k]));
+            D.dnk[k] = std::min(2 * D.dnr[k] + 1, D.ncell[k]);
         }
         D.cell_off = cell_off; cell_off += D.ncell[0] * D.ncell[1] * D.ncell[2];
         D.cell_cap = E.cell_cap;
@@ -273,6 +279,10 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         D.order = E.order;
         D.walls = P.wall_hi > P.wall_lo;
         D.wall_lo = (float)P.wall_lo; D.wall_hi = (float)P.wall_hi;
+        D.sur_z0 = D.walls ? D.wall_lo : 0.0f;
+        D.sur_h = D.walls ? D.wall_hi - D.wall_lo : D.L[2];
+        D.sur_pk = (float)(P.pKa - P.pH);
+        D.sur_salt = P.salt_conc > 0 ? (float)std::log10(P.salt_conc) : -10.0f;
         D.fene_k = (float)P.fene_k; D.fene_r02 = (float)(P.fene_r0 * P.fene_r0);
         D.excl_lj = P.excl_bonded_lj; D.excl_coul = P.excl_bonded_coul;
         D.beta = P.beta;
@@ -359,6 +369,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     DALLOC(d.posq, N); DALLOC(d.type, N); DALLOC(d.flags, N); DALLOC(d.bonds, N);
     DALLOC(d.cell_of, N); DALLOC(d.cell_pos, N);
     DALLOC(d.cell_count, E.total_cells); DALLOC(d.cell_list, (size_t)E.total_cells * E.cell_cap);
+    DALLOC(d.cell_cls, E.total_cells);
     DALLOC(d.mobile, N); DALLOC(d.mobile_pos, N); DALLOC(d.anions, N); DALLOC(d.anion_pos, N);
     DALLOC(d.cations, N); DALLOC(d.cation_pos, N); DALLOC(d.freel, N); DALLOC(d.titr, N);
     DALLOC(d.desc, R); DALLOC(d.state, R); DALLOC(d.dirty, R);
@@ -530,6 +541,8 @@ extern "C" int phmc_destroy(phmc_engine* h) {
     if (h->d_trials) cudaFree(h->d_trials);
     if (h->d_dE) cudaFree(h->d_dE);
     if (E.d.log_move) { cudaFree(E.d.log_move); cudaFree(E.d.log_dE); cudaFree(E.d.log_acc); }
+    if (E.d.log_stage) { cudaFree(E.d.log_stage); cudaFree(E.d.log_dEs); }
+    if (E.d.hv_cap > 0) { cudaFree(E.d.hv_rows); cudaFree(E.d.hv_sign); cudaFree(E.d.hv_target); cudaFree(E.d.hv_count); }
     if (E.stream) cudaStreamDestroy(E.stream);
     delete h;
     return PHMC_OK;
@@ -657,7 +670,10 @@ extern "C" int phmc_set_trial_log(phmc_engine* h, int64_t cap, int* move, double
     Engine& E = h->E;
     drop_graph(h);  // captured launches hold the old log pointers
     if (E.d.log_move) { cudaFree(E.d.log_move); cudaFree(E.d.log_dE); cudaFree(E.d.log_acc); }
+    if (E.d.log_stage) { cudaFree(E.d.log_stage); cudaFree(E.d.log_dEs); }
     E.d.log_move = nullptr; E.d.log_dE = nullptr; E.d.log_acc = nullptr; E.d.log_cap = 0;
+    E.d.log_stage = nullptr; E.d.log_dEs = nullptr;
+    h->h_da_stage = nullptr; h->h_da_dEs = nullptr;
     h->h_log_move = move; h->h_log_dE = dE; h->h_log_acc = acc; h->log_cap = 0;
     if (!move || !dE || !acc || cap <= 0) return PHMC_OK;
     CU(cudaMalloc((void**)&E.d.log_move, sizeof(int) * cap));
@@ -831,6 +847,10 @@ extern "C" int phmc_run(phmc_engine* h, int64_t n_trials, phmc_run_stats* stats)
         CU(cudaMemcpy(h->h_log_move, E.d.log_move, sizeof(int) * n, cudaMemcpyDeviceToHost));
         CU(cudaMemcpy(h->h_log_dE, E.d.log_dE, sizeof(double) * n, cudaMemcpyDeviceToHost));
         CU(cudaMemcpy(h->h_log_acc, E.d.log_acc, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        if (h->h_da_stage && E.d.log_stage) {
+            CU(cudaMemcpy(h->h_da_stage, E.d.log_stage, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(h->h_da_dEs, E.d.log_dEs, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        }
     }
     if (stats) return collect_stats(h, stats);
     return PHMC_OK;
@@ -920,4 +940,153 @@ extern "C" int phmc_get_cells(phmc_engine* h, int rep, int* cell_of, int dims[3]
 extern "C" int phmc_capacity(phmc_engine* h, int rep) {
     if (!h || rep < 0 || rep >= h->E.R) return -1;
     return h->caps[rep];
+}
+
+// ---------------------------------------------------------------------------
+// learned surrogate: sample harvest, training on the harvest, attachment as the
+// first stage of delayed acceptance, descriptor readback
+// ---------------------------------------------------------------------------
+extern "C" int phmc_harvest(phmc_engine* h, int capacity) {
+    if (!h || capacity < 0) return fail(PHMC_ERR_ARG, "phmc_harvest: invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    drop_graph(h);  // captured launches hold the old buffers
+    if (E.d.hv_cap > 0) { cudaFree(E.d.hv_rows); cudaFree(E.d.hv_sign); cudaFree(E.d.hv_target); cudaFree(E.d.hv_count); }
+    E.d.hv_rows = nullptr; E.d.hv_sign = nullptr; E.d.hv_target = nullptr; E.d.hv_count = nullptr; E.d.hv_cap = 0;
+    if (capacity == 0) return PHMC_OK;
+    CU(cudaMalloc((void**)&E.d.hv_rows, sizeof(float) * (size_t)capacity * SUR_ROWS * SUR_K));
+    CU(cudaMalloc((void**)&E.d.hv_sign, sizeof(float) * (size_t)capacity * SUR_ROWS));
+    CU(cudaMalloc((void**)&E.d.hv_target, sizeof(float) * (size_t)capacity));
+    CU(cudaMalloc((void**)&E.d.hv_count, sizeof(int)));
+    CU(cudaMemset(E.d.hv_count, 0, sizeof(int)));
+    E.d.hv_cap = capacity;
+    return PHMC_OK;
+}
+
+static int harvest_n(phmc_engine* h, int* n) {
+    Engine& E = h->E;
+    int c = 0;
+    if (E.d.hv_cap > 0) {
+        CU(cudaStreamSynchronize(E.stream));
+        CU(cudaMemcpy(&c, E.d.hv_count, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    *n = std::min(c, E.d.hv_cap);
+    return PHMC_OK;
+}
+
+extern "C" int phmc_harvest_count(phmc_engine* h, int* n) {
+    if (!h || !n) return fail(PHMC_ERR_ARG, "phmc_harvest_count: null argument");
+    CU(cudaSetDevice(h->E.device));
+    return harvest_n(h, n);
+}
+
+extern "C" int phmc_harvest_get(phmc_engine* h, int n, float* x, float* sign, float* t) {
+    if (!h || n < 0 || (n > 0 && (!x || !sign || !t))) return fail(PHMC_ERR_ARG, "phmc_harvest_get: invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    int have = 0;
+    int s = harvest_n(h, &have);
+    if (s) return s;
+    if (n > have) return fail(PHMC_ERR_ARG, "phmc_harvest_get: fewer samples recorded than requested");
+    if (n == 0) return PHMC_OK;
+    CU(cudaMemcpy(x, E.d.hv_rows, sizeof(float) * (size_t)n * SUR_ROWS * SUR_K, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(sign, E.d.hv_sign, sizeof(float) * (size_t)n * SUR_ROWS, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(t, E.d.hv_target, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
+    return PHMC_OK;
+}
+
+extern "C" int phmc_surrogate_fit(phmc_engine* h, phmc_surrogate* sur, int epochs, int batch, float lr, float clip,
+                                  uint64_t seed, double* loss) {
+    if (!h || !sur) return fail(PHMC_ERR_ARG, "phmc_surrogate_fit: null argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    int n = 0;
+    int s = harvest_n(h, &n);
+    if (s) return s;
+    if (n < batch) return fail(PHMC_ERR_STATE, "phmc_surrogate_fit: fewer harvested samples than one batch");
+    if (phmc_surrogate_num_params(sur) < 0) return fail(PHMC_ERR_ARG, "bad surrogate");
+    s = sur_train_device(sur, E.d.hv_rows, E.d.hv_sign, E.d.hv_target, n, epochs, batch, lr, clip, seed, 1, loss);
+    if (s) return s;
+    // a network attached to this engine picks up the new weights
+    if (E.d.sur.H > 0) {
+        SurDev v;
+        s = sur_device_view(sur, &v);
+        if (s) return s;
+        if (E.d.sur.w[0] == v.w[0]) { E.d.sur = v; drop_graph(h); }
+    }
+    return PHMC_OK;
+}
+
+extern "C" int phmc_surrogate_attach(phmc_engine* h, phmc_surrogate* sur, double threshold, int window) {
+    if (!h || window < 0) return fail(PHMC_ERR_ARG, "phmc_surrogate_attach: invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    SurDev v;
+    std::memset(&v, 0, sizeof v);
+    if (sur) {
+        int s = sur_device_view(sur, &v);
+        if (s) return s;
+    }
+    drop_graph(h);  // captured launches hold the old kernel parameters
+    E.d.sur = v;
+    E.d.da_threshold = (float)threshold;
+    E.d.da_window = window;
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    for (RepState& x : st) { x.da_eval = x.da_pass = x.da_acc = x.da_wpass = x.da_wacc = 0; x.da_off = 0; }
+    CU(cudaMemcpy(E.d.state, st.data(), sizeof(RepState) * E.R, cudaMemcpyHostToDevice));
+    return PHMC_OK;
+}
+
+extern "C" int phmc_get_da_stats(phmc_engine* h, phmc_da_stats* out) {
+    if (!h || !out) return fail(PHMC_ERR_ARG, "phmc_get_da_stats: null argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    for (int r = 0; r < E.R; ++r) {
+        out[r].evaluated = st[r].da_eval; out[r].passed = st[r].da_pass; out[r].accepted = st[r].da_acc;
+        out[r].fallback = st[r].da_off; out[r].pad = 0;
+    }
+    return PHMC_OK;
+}
+
+extern "C" int phmc_surrogate_describe(phmc_engine* h, int rep, const phmc_trial* trials, int n, float* out, double* dEs) {
+    if (!h || (n > 0 && (!trials || !out || !dEs))) return fail(PHMC_ERR_ARG, "phmc_surrogate_describe: null argument");
+    if (n == 0) return PHMC_OK;
+    int s = check_trials(h, rep, trials, n);
+    if (s) return s;
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    s = ensure_trial_buffers(h, n);
+    if (s) return s;
+    float* d_out = nullptr;
+    CU(cudaMalloc((void**)&d_out, sizeof(float) * (size_t)n * DSC_STRIDE));
+    CU(cudaMemcpyAsync(h->d_trials, trials, sizeof(phmc_trial) * n, cudaMemcpyHostToDevice, E.stream));
+    E.d.dsc_out = d_out;
+    cudaError_t e = launch_mc(E, MC_DESCRIBE, rep, h->d_trials, n, h->d_dE, E.stream);
+    E.d.dsc_out = nullptr;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(float) * (size_t)n * DSC_STRIDE, cudaMemcpyDeviceToHost, E.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dEs, h->d_dE, sizeof(double) * n, cudaMemcpyDeviceToHost, E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string("describe: ") + cudaGetErrorString(e));
+    return check_kernel_errors(h);
+}
+
+extern "C" int phmc_set_da_log(phmc_engine* h, int* stage, double* dEs) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    Engine& E = h->E;
+    if (!E.d.log_move) return fail(PHMC_ERR_STATE, "phmc_set_da_log needs a trial log (phmc_set_trial_log) first");
+    drop_graph(h);
+    if (E.d.log_stage) { cudaFree(E.d.log_stage); cudaFree(E.d.log_dEs); }
+    E.d.log_stage = nullptr; E.d.log_dEs = nullptr;
+    h->h_da_stage = stage; h->h_da_dEs = dEs;
+    if (!stage || !dEs) return PHMC_OK;
+    CU(cudaMalloc((void**)&E.d.log_stage, sizeof(int) * E.d.log_cap));
+    CU(cudaMalloc((void**)&E.d.log_dEs, sizeof(double) * E.d.log_cap));
+    return PHMC_OK;
 }

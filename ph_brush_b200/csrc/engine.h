@@ -66,8 +66,13 @@ cudaError_t rebuild_set_smem_limits(Engine& E);
 void launch_cell_build(Engine& E, cudaStream_t st);
 void launch_full_energy(Engine& E, cudaStream_t st);
 
+// k_mlp.cu (surrogate network)
+int sur_device_view(phmc_surrogate* h, SurDev* out);
+int sur_train_device(phmc_surrogate* h, const float* d_x, const float* d_sign, const float* d_t, int ns, int epochs,
+                     int batch, float lr, float clip, uint64_t seed, int rescale, double* last_loss);
+
 // k_mc.cu
-enum { MC_RUN = 0, MC_EVAL = 1, MC_APPLY = 2 };
+enum { MC_RUN = 0, MC_EVAL = 1, MC_APPLY = 2, MC_DESCRIBE = 3 };
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* d_trials, int n, double* d_dE, cudaStream_t st);
 cudaError_t prepare_mc(Engine& E);
 size_t mc_smem_bytes(int order, int pend_max);

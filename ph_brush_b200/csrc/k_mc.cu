@@ -59,6 +59,15 @@ struct TrialS {
     int total_cand, npairs;
     // cell bookkeeping of the old states, loaded off the critical path (phase 4)
     int cell_old[2], cpos_old[2], cnt_old[2], last_old[2];
+    int fo[2];  // slot flags of the changed particles before the trial
+    // surrogate first stage
+    int desc, da, nrows, dtotal;
+    int row_k[SUR_ROWS], row_cls[SUR_ROWS];
+    float row_sign[SUR_ROWS];
+    float4 dpos[2];            // descriptor centres (new position if present, else old)
+    int dcx[2], dcy[2], dcz[2];
+    int ccell[2], ccls[2];     // current cell / class of the changed particles (-1: absent)
+    double cross, dmom, dEs;   // exact cross and charge-moment terms, surrogate dE
 };
 
 // Next trial's primary particle, loaded during the current trial's parallel
@@ -152,14 +161,16 @@ __device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const De
     const int so = D.slot_off;
     auto load_old = [&](int k, int i) {
         T.idx[k] = i;
-        T.pres_old[k] = !(d.flags[so + i] & PHMC_F_GHOST);
+        const int fl = d.flags[so + i];
+        T.fo[k] = fl;
+        T.pres_old[k] = !(fl & PHMC_F_GHOST);
         T.po[k] = d.posq[so + i]; T.to[k] = d.type[so + i]; T.bonds[k] = d.bonds[so + i];
     };
     // primary particle from the prefetch when it is still valid
     const bool use_pf = pf.valid && pf.t == T.tnum && pf.move == move;
     auto load_primary = [&](int i_from_list) {
         if (use_pf) {
-            T.idx[0] = pf.idx; T.pres_old[0] = !(pf.flags & PHMC_F_GHOST);
+            T.idx[0] = pf.idx; T.fo[0] = pf.flags; T.pres_old[0] = !(pf.flags & PHMC_F_GHOST);
             T.po[0] = pf.pq; T.to[0] = pf.type; T.bonds[0] = pf.bonds;
         } else {
             load_old(0, i_from_list);
@@ -232,7 +243,9 @@ __device__ void load_external(TrialS& T, const RepDesc& D, const DevPtrs& d, con
     for (int k = 0; k < e.n_changes; ++k) {
         const int i = e.c[k].index;
         T.idx[k] = i;
-        T.pres_old[k] = !(d.flags[so + i] & PHMC_F_GHOST);
+        const int fl = d.flags[so + i];
+        T.fo[k] = fl;
+        T.pres_old[k] = !(fl & PHMC_F_GHOST);
         T.po[k] = d.posq[so + i]; T.to[k] = d.type[so + i]; T.bonds[k] = d.bonds[so + i];
         T.pres_new[k] = e.c[k].present;
         T.pn[k] = make_float4(e.c[k].x, e.c[k].y, e.c[k].z, e.c[k].q);
@@ -303,6 +316,91 @@ __device__ __forceinline__ double slab_energy(const RepDesc& D, double Q, double
     return e;
 }
 
+// Charge-moment changes of trial T and the self / net-charge / slab energy changes.
+struct Moments {
+    double dQ, dQ2, dMz, dS2, dself, dqc, dslab;
+};
+__device__ void moment_terms(const TrialS& T, const RepDesc& D, const RepState& S, Moments& m) {
+    double dQ = 0, dQ2 = 0, dMz = 0, dS2 = 0;
+    for (int k = 0; k < T.nch; ++k) {
+        if (T.pres_new[k]) {
+            const double q = T.pn[k].w, z = T.pn[k].z;
+            dQ += q; dQ2 += q * q; dMz += q * z; dS2 += q * z * z;
+        }
+        if (T.pres_old[k]) {
+            const double q = T.po[k].w, z = T.po[k].z;
+            dQ -= q; dQ2 -= q * q; dMz -= q * z; dS2 -= q * z * z;
+        }
+    }
+    m.dQ = dQ; m.dQ2 = dQ2; m.dMz = dMz; m.dS2 = dS2;
+    m.dself = 0; m.dqc = 0; m.dslab = 0;
+    if (D.coulomb == PHMC_COUL_EWALD) {
+        m.dself = D.self_coef * dQ2;
+        const double Qn = S.Q + dQ;
+        m.dqc = D.qcorr_coef * (Qn * Qn - S.Q * S.Q);
+        m.dslab = slab_energy(D, Qn, S.Mz + dMz, S.S2 + dS2) - slab_energy(D, S.Q, S.Mz, S.S2);
+    }
+}
+
+// ---- surrogate descriptor (every float operation rounded explicitly, so a
+// host restatement reproduces the shell of every particle bit for bit) ----
+__device__ __forceinline__ float min_image_rn(float d, float L) {
+    return __fsub_rn(d, __fmul_rn(L, rintf(__fdiv_rn(d, L))));
+}
+__device__ __forceinline__ int shell_of(float dx, float dy, float dz) {
+    const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    return (int)__fmul_rn(__fsqrt_rn(r2), 2.0f);
+}
+// one-hot state index of a row: charged site, neutral site, anion, cation (-1: none)
+__device__ __forceinline__ int row_state(bool titr, float q) {
+    if (titr) return q != 0.0f ? 0 : 1;
+    return q < 0.0f ? 2 : (q > 0.0f ? 3 : -1);
+}
+// exact interaction of two changed particles: LJ plus bare Coulomb (Ewald) or the cutoff Coulomb
+__device__ double pair_cross(const RepDesc& D, float4 a, float4 b, int ta, int tb, bool bonded) {
+    const float dx = min_image(a.x - b.x, D.L[0]), dy = min_image(a.y - b.y, D.L[1]), dz = min_image(a.z - b.z, D.L[2]);
+    float elj, ec;
+    pair_energy(D, dx, dy, dz, ta, tb, a.w, b.w, bonded, elj, ec);
+    if (D.coulomb == PHMC_COUL_EWALD) {
+        const float qq = a.w * b.w;
+        ec = (qq != 0.0f && !(bonded && D.excl_coul)) ? D.elf * qq / sqrtf(dx * dx + dy * dy + dz * dz) : 0.0f;
+    }
+    return (double)elj + (double)ec;
+}
+
+// Rows, descriptor centres, exclusions and the exact terms of the first stage (one thread).
+__device__ void desc_setup(TrialS& T, const RepDesc& D, const RepState& S) {
+    int nr = 0;
+    for (int k = 0; k < T.nch; ++k) {
+        const float4 p = T.pres_new[k] ? T.pn[k] : T.po[k];
+        T.dpos[k] = p;
+        T.dcx[k] = min(D.ncell[0] - 1, max(0, (int)(p.x * D.cell_scale[0])));
+        T.dcy[k] = min(D.ncell[1] - 1, max(0, (int)(p.y * D.cell_scale[1])));
+        T.dcz[k] = min(D.ncell[2] - 1, max(0, (int)(p.z * D.cell_scale[2])));
+        T.ccell[k] = T.pres_old[k] ? cell_index(D, T.po[k].x, T.po[k].y, T.po[k].z) : -1;
+        T.ccls[k] = T.pres_old[k] ? desc_class(T.fo[k], T.po[k].w) : -1;
+        const bool titr = T.pres_old[k] && (T.fo[k] & PHMC_F_TITRATABLE);
+        if (T.pres_old[k]) { T.row_k[nr] = k; T.row_cls[nr] = row_state(titr, T.po[k].w); T.row_sign[nr] = -1.0f; ++nr; }
+        if (T.pres_new[k]) { T.row_k[nr] = k; T.row_cls[nr] = row_state(titr, T.pn[k].w); T.row_sign[nr] = 1.0f; ++nr; }
+    }
+    T.nrows = nr;
+    double cross = 0.0;
+    if (T.nch == 2) {
+        const bool bonded = in_bonds(T.bonds[0], T.idx[1]);
+        const double a = (T.pres_new[0] && T.pres_new[1]) ? pair_cross(D, T.pn[0], T.pn[1], T.tn[0], T.tn[1], bonded) : 0.0;
+        const double b = (T.pres_old[0] && T.pres_old[1]) ? pair_cross(D, T.po[0], T.po[1], T.to[0], T.to[1], bonded) : 0.0;
+        cross = a - b;
+    }
+    T.cross = cross;
+    Moments m;
+    moment_terms(T, D, S, m);
+    T.dmom = m.dself + m.dqc + m.dslab;
+}
+
+__device__ __forceinline__ void cls_add(const DevPtrs& d, const RepDesc& D, int cell, int cls, int delta) {
+    if (cls >= 0 && cell >= 0) reinterpret_cast<int*>(d.cell_cls + D.cell_off + cell)[cls] += delta;
+}
+
 template <int NT>
 __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double* red) {
 #pragma unroll
@@ -341,6 +439,11 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
     __shared__ uint32_t s_rng[32][12];  // Philox words of trials s_rng_base .. s_rng_base+31
     __shared__ long long s_rng_base;
     __shared__ Prefetch pf;
+    // surrogate first stage: shell histogram per changed particle, raw rows, outputs
+    __shared__ int s_hist[2 * SUR_SHELLS * SUR_CLASSES];
+    __shared__ float s_rows[SUR_ROWS][SUR_K];
+    __shared__ float s_F[8];
+    __shared__ int s_hv_slot, s_hv_nrows;  // harvested sample whose rows are still to be stored
 
     const int r = (mode == MC_RUN) ? blockIdx.x : ext_rep;
     const int tid = threadIdx.x;
@@ -359,6 +462,7 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
         T.stop = 0;
         s_rng_base = -64;
         pf.valid = 0;
+        s_hv_slot = -1;
     }
     __syncthreads();
 
@@ -375,7 +479,7 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 }
             }
             if (tid == 0) {
-                T.stop = 0;
+                T.stop = 0; T.desc = 0; T.da = 0;
                 if (S.error) T.stop = 1;
                 else if (mode == MC_RUN) {
                     if (S.trial >= S.target) { T.stop = 1; S.stop_reason = 0; }
@@ -385,23 +489,180 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                     if (T.ext_k >= n_ext) T.stop = 1;
                     else { load_external(T, D, d, ext[T.ext_k]); T.tnum = T.ext_k; }
                 }
-                if (!T.stop && T.skip == 0) trial_setup(T, D);
+                if (!T.stop && T.skip == 0) {
+                    trial_setup(T, D);
+                    if (mode == MC_DESCRIBE) {
+                        T.desc = 1; T.da = d.sur.H > 0;
+                    } else if (mode == MC_RUN && (T.move == PHMC_MOVE_TITR || T.move == PHMC_MOVE_SWAP)) {
+                        // delayed acceptance (not under replay, which dictates decisions)
+                        T.da = d.sur.H > 0 && !S.da_off && !(r == 0 && d.replay);
+                        T.desc = T.da || d.hv_cap > 0;
+                    }
+                    if (T.desc) desc_setup(T, D, S);
+                }
             }
+        } else {
+            // idle threads: store the previous trial's harvested rows, clear the shell histogram
+            if (s_hv_slot >= 0) {
+                float* dst = d.hv_rows + (size_t)s_hv_slot * (SUR_ROWS * SUR_K);
+                for (int e = tid - 32; e < SUR_ROWS * SUR_K; e += NT - 32)
+                    dst[e] = (e / SUR_K < s_hv_nrows) ? s_rows[e / SUR_K][e % SUR_K] : 0.0f;
+            }
+            for (int e = tid - 32; e < 2 * SUR_SHELLS * SUR_CLASSES; e += NT - 32) s_hist[e] = 0;
         }
         __syncthreads();
         if (T.stop) break;
+        if (tid == 0) s_hv_slot = -1;
+        // ---------------- surrogate first stage ----------------
+        if (T.desc) {
+            // (a) the descriptor sphere's cells: inner 27 cells -> counts for the particle
+            // pass; outer cells -> class counts binned by the distance of the cell centre
+            const int nk0 = D.dnk[0], nk1 = D.dnk[1], nk2 = D.dnk[2];
+            const int nc3 = nk0 * nk1 * nk2;
+            for (int e = tid; e < T.nch * nc3; e += NT) {
+                const int k = e / nc3, loc = e - k * nc3;
+                const int lz = loc / (nk0 * nk1), lr = loc - lz * (nk0 * nk1);
+                const int ly = lr / nk0, lx = lr - ly * nk0;
+                const int ox = lx - D.dnr[0], oy = ly - D.dnr[1], oz = lz - D.dnr[2];
+                const int cx = wrap_idx(T.dcx[k] + ox, D.ncell[0]), cy = wrap_idx(T.dcy[k] + oy, D.ncell[1]),
+                          cz = wrap_idx(T.dcz[k] + oz, D.ncell[2]);
+                const int cell = (cz * D.ncell[1] + cy) * D.ncell[0] + cx;
+                if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1) {
+                    const int sl = k * 27 + (oz + 1) * 9 + (oy + 1) * 3 + (ox + 1);
+                    s_cell[sl] = cell;
+                    s_cnt[sl] = min(d.cell_count[D.cell_off + cell], D.cell_cap);
+                } else {
+                    int4 cc = d.cell_cls[D.cell_off + cell];
+                    for (int j = 0; j < T.nch; ++j)
+                        if (T.ccell[j] == cell) {
+                            cc.x -= (T.ccls[j] == 0); cc.y -= (T.ccls[j] == 1); cc.z -= (T.ccls[j] == 2); cc.w -= (T.ccls[j] == 3);
+                        }
+                    if ((cc.x | cc.y | cc.z | cc.w) == 0) continue;
+                    const float4 p = T.dpos[k];
+                    const float xc = __fmul_rn(__fadd_rn((float)cx, 0.5f), D.cell_w[0]);
+                    const float yc = __fmul_rn(__fadd_rn((float)cy, 0.5f), D.cell_w[1]);
+                    const float zc = __fmul_rn(__fadd_rn((float)cz, 0.5f), D.cell_w[2]);
+                    const int sh = shell_of(min_image_rn(__fsub_rn(xc, p.x), D.L[0]), min_image_rn(__fsub_rn(yc, p.y), D.L[1]),
+                                            min_image_rn(__fsub_rn(zc, p.z), D.L[2]));
+                    if (sh < SUR_SHELLS) {
+                        int* hb = s_hist + k * (SUR_SHELLS * SUR_CLASSES) + sh * SUR_CLASSES;
+                        if (cc.x) atomicAdd(hb, cc.x);
+                        if (cc.y) atomicAdd(hb + 1, cc.y);
+                        if (cc.z) atomicAdd(hb + 2, cc.z);
+                        if (cc.w) atomicAdd(hb + 3, cc.w);
+                    }
+                }
+            }
+            __syncthreads();
+            const int nent_d = T.nch * 27;
+            if (tid < 32) {
+                int carry = 0;
+                for (int b0 = 0; b0 < nent_d; b0 += 32) {
+                    const int e = b0 + tid;
+                    const int v = (e < nent_d) ? s_cnt[e] : 0;
+                    int x = v;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (tid >= o) x += y;
+                    }
+                    if (e < nent_d) s_off[e] = carry + x - v;
+                    carry += __shfl_sync(0xffffffffu, x, 31);
+                }
+                if (tid == 0) { s_off[nent_d] = carry; T.dtotal = carry; }
+            }
+            __syncthreads();
+            // (b) particles of the inner cells, exact distance shells
+            for (int it = tid; it < T.dtotal; it += NT) {
+                int lo = 0, hi = nent_d - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+                }
+                const int k = lo / 27;
+                const int j = d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + (it - s_off[lo])];
+                if (j == T.idx[0] || (T.nch == 2 && j == T.idx[1])) continue;
+                const int gj = D.slot_off + j;
+                const float4 pj = d.posq[gj];
+                const int c = desc_class(d.flags[gj], pj.w);
+                if (c < 0) continue;
+                const float4 p = T.dpos[k];
+                const int sh = shell_of(min_image_rn(__fsub_rn(pj.x, p.x), D.L[0]), min_image_rn(__fsub_rn(pj.y, p.y), D.L[1]),
+                                        min_image_rn(__fsub_rn(pj.z, p.z), D.L[2]));
+                if (sh < SUR_SHELLS) atomicAdd(&s_hist[k * (SUR_SHELLS * SUR_CLASSES) + sh * SUR_CLASSES + c], 1);
+            }
+            __syncthreads();
+            // (c) rows: raw features, and standardised BF16 inputs when the network runs
+            __nv_bfloat16* act0 = reinterpret_cast<__nv_bfloat16*>(s_pair);
+            __nv_bfloat16* act1 = act0 + 16 * SUR_AST;
+            for (int e = tid; e < T.nrows * SUR_K; e += NT) {
+                const int rr = e / SUR_K, f = e - rr * SUR_K;
+                const int k = T.row_k[rr];
+                float v;
+                if (f < SUR_SHELLS * SUR_CLASSES) v = (float)s_hist[k * (SUR_SHELLS * SUR_CLASSES) + f];
+                else if (f == 64) v = __fdiv_rn(__fsub_rn(T.dpos[k].z, D.sur_z0), D.sur_h);
+                else if (f < 69) v = (f - 65 == T.row_cls[rr]) ? 1.0f : 0.0f;
+                else if (f == 69) v = D.sur_pk;
+                else if (f == 70) v = D.sur_salt;
+                else v = 0.0f;
+                s_rows[rr][f] = v;
+                if (T.da) act0[rr * SUR_AST + f] = __float2bfloat16(__fdiv_rn(__fsub_rn(v, __ldg(&d.sur.mu[f])), __ldg(&d.sur.sd[f])));
+            }
+            __syncthreads();
+            // (d) network on the rows (tensor cores), first-stage decision
+            if (T.da) sur_forward_rows<NT>(d.sur, T.nrows, act0, act1, s_F);
+            if (tid == 0) {
+                if (mode == MC_RUN) S.alg_bytes += 16.0 * T.nch * nc3 + 24.0 * T.dtotal;
+                double net = 0.0;
+                if (T.da) {
+                    // per changed particle F(new) - F(old): the estimate is antisymmetric under reversal
+                    for (int k = 0; k < T.nch; ++k) {
+                        double fo = 0.0, fn = 0.0;
+                        for (int rr = 0; rr < T.nrows; ++rr)
+                            if (T.row_k[rr] == k) { if (T.row_sign[rr] < 0.0f) fo = s_F[rr]; else fn = s_F[rr]; }
+                        net += fn - fo;
+                    }
+                    T.dEs = (net + T.cross) + T.dmom;
+                }
+                if (mode == MC_DESCRIBE) {
+                    float* o = d.dsc_out + (size_t)T.ext_k * DSC_STRIDE;
+                    for (int e = 0; e < SUR_ROWS * SUR_K; ++e) o[e] = (e / SUR_K < T.nrows) ? s_rows[e / SUR_K][e % SUR_K] : 0.0f;
+                    for (int rr = 0; rr < SUR_ROWS; ++rr) {
+                        o[SUR_ROWS * SUR_K + rr] = rr < T.nrows ? T.row_sign[rr] : 0.0f;
+                        o[SUR_ROWS * SUR_K + SUR_ROWS + rr] = (T.da && rr < T.nrows) ? s_F[rr] : 0.0f;
+                    }
+                    o[SUR_ROWS * SUR_K + 2 * SUR_ROWS] = (float)T.cross;
+                    o[SUR_ROWS * SUR_K + 2 * SUR_ROWS + 1] = (float)T.dmom;
+                    o[SUR_ROWS * SUR_K + 2 * SUR_ROWS + 2] = (float)T.nrows;
+                    o[SUR_ROWS * SUR_K + 2 * SUR_ROWS + 3] = (float)T.dtotal;
+                    T.skip = 5;
+                } else if (T.da) {
+                    // first stage: Metropolis on the surrogate dE with its own uniform (Philox counter (t, 3))
+                    uint32_t w4[4];
+                    philox4x32_10(D.key[0], D.key[1], (uint32_t)T.tnum, (uint32_t)((unsigned long long)T.tnum >> 32), 3u, 0u, w4);
+                    const double expo1 = -D.beta * T.dEs + T.logf;
+                    const bool pass = (expo1 >= 0.0) || (u53(w4[0], w4[1]) < exp(expo1));
+                    S.da_eval++;
+                    if (pass) { S.da_pass++; S.da_wpass++; }
+                    else T.skip = 4;
+                }
+            }
+            __syncthreads();
+        }
         if (T.skip) {
             if (tid == 0) {
-                if (T.move < 3) S.att[T.move]++;
+                if (mode == MC_RUN && T.move < 3) S.att[T.move]++;
                 if (mode == MC_RUN) { S.alg_bytes += 16.0; S.trials_run++; }
                 const long long li = T.tnum - S.run_start;
                 if (mode == MC_RUN && r == 0 && d.log_move && li < d.log_cap) {
                     d.log_move[li] = T.move;
                     d.log_dE[li] = (T.skip == 2) ? __longlong_as_double(0x7ff0000000000000ll) : __longlong_as_double(0x7ff8000000000000ll);
                     d.log_acc[li] = 0;
+                    if (d.log_stage) { d.log_stage[li] = (T.skip == 4) ? 1 : 0; d.log_dEs[li] = T.da ? T.dEs : 0.0; }
                 }
                 if (mode != MC_RUN) {
-                    if (ext_dE) ext_dE[T.ext_k] = __longlong_as_double(0x7ff0000000000000ll);
+                    if (ext_dE) ext_dE[T.ext_k] = (T.skip == 5) ? (T.da ? T.dEs : __longlong_as_double(0x7ff8000000000000ll))
+                                                                : __longlong_as_double(0x7ff0000000000000ll);
                     T.ext_k++;
                 }
             }
@@ -628,24 +889,10 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
         block_sum3<NT>(acc_lj, acc_c, acc_rec, red);
         // ---------------- phase 5: decision and update ----------------
         if (tid == 0) {
-            double dQ = 0, dQ2 = 0, dMz = 0, dS2 = 0;
-            for (int k = 0; k < T.nch; ++k) {
-                if (T.pres_new[k]) {
-                    const double q = T.pn[k].w, z = T.pn[k].z;
-                    dQ += q; dQ2 += q * q; dMz += q * z; dS2 += q * z * z;
-                }
-                if (T.pres_old[k]) {
-                    const double q = T.po[k].w, z = T.po[k].z;
-                    dQ -= q; dQ2 -= q * q; dMz -= q * z; dS2 -= q * z * z;
-                }
-            }
-            double dself = 0, dqc = 0, dslab = 0;
-            if (D.coulomb == PHMC_COUL_EWALD) {
-                dself = D.self_coef * dQ2;
-                const double Qn = S.Q + dQ;
-                dqc = D.qcorr_coef * (Qn * Qn - S.Q * S.Q);
-                dslab = slab_energy(D, Qn, S.Mz + dMz, S.S2 + dS2) - slab_energy(D, S.Q, S.Mz, S.S2);
-            }
+            Moments mo;
+            moment_terms(T, D, S, mo);
+            const double dQ = mo.dQ, dQ2 = mo.dQ2, dMz = mo.dMz, dS2 = mo.dS2;
+            const double dself = mo.dself, dqc = mo.dqc, dslab = mo.dslab;
             const double dlj = acc_lj + T.d_direct_lj, dc = acc_c + T.d_direct_c;
             const double dE = dlj + dc + T.d_fene + acc_rec + dself + dqc + dslab;
             int accept = 0;
@@ -653,10 +900,30 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 const long long li = T.tnum - S.run_start;
                 if (r == 0 && d.replay && li < d.replay_n) accept = d.replay[li];
                 else {
-                    const double expo = -D.beta * dE + T.logf;
+                    // delayed acceptance, second stage: the exact dE judges the surrogate's
+                    // estimate (Christen & Fox 2005; the log factor cancels)
+                    const double expo = T.da ? -D.beta * (dE - T.dEs) : -D.beta * dE + T.logf;
                     accept = (expo >= 0.0) || (u53(T.ua, T.ub) < exp(expo));
                 }
-                if (r == 0 && d.log_move && li < d.log_cap) { d.log_move[li] = T.move; d.log_dE[li] = dE; d.log_acc[li] = accept; }
+                if (T.da) {
+                    if (accept) { S.da_acc++; S.da_wacc++; }
+                    if (d.da_window > 0 && S.da_wpass >= d.da_window) {
+                        if ((double)S.da_wacc < (double)d.da_threshold * (double)S.da_wpass) S.da_off = 1;
+                        S.da_wpass = 0; S.da_wacc = 0;
+                    }
+                }
+                if (T.desc && d.hv_cap > 0) {  // training sample: rows, signs, the network's target
+                    const int slot = atomicAdd(d.hv_count, 1);
+                    if (slot < d.hv_cap) {
+                        d.hv_target[slot] = (float)(dE - T.cross - T.dmom);
+                        for (int rr = 0; rr < SUR_ROWS; ++rr) d.hv_sign[(size_t)slot * SUR_ROWS + rr] = rr < T.nrows ? T.row_sign[rr] : 0.0f;
+                        s_hv_slot = slot; s_hv_nrows = T.nrows;
+                    }
+                }
+                if (r == 0 && d.log_move && li < d.log_cap) {
+                    d.log_move[li] = T.move; d.log_dE[li] = dE; d.log_acc[li] = accept;
+                    if (d.log_stage) { d.log_stage[li] = T.da ? 2 : 0; d.log_dEs[li] = T.da ? T.dEs : 0.0; }
+                }
                 S.att[T.move]++;
                 // algorithmic bytes of this trial: float4+type of every candidate, the
                 // moved particle, the phi stencils and the pending-correction reads
@@ -675,6 +942,19 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 for (int k = 0; k < T.nch; ++k) {
                     const int i = T.idx[k];
                     const int gi = so + i;
+                    {  // descriptor class table: leave the old (cell, class), enter the new one
+                        const int c_old = T.pres_old[k] ? cell_index(D, T.po[k].x, T.po[k].y, T.po[k].z) : -1;
+                        const int k_old = T.pres_old[k] ? desc_class(T.fo[k], T.po[k].w) : -1;
+                        int fl_new = T.fo[k];
+                        if (!T.pres_old[k] && T.pres_new[k])
+                            fl_new = PHMC_F_MOBILE | (T.pn[k].w > 0.0f ? PHMC_F_CATION : (T.pn[k].w < 0.0f ? PHMC_F_ANION : 0));
+                        const int c_new = T.pres_new[k] ? cell_index(D, T.pn[k].x, T.pn[k].y, T.pn[k].z) : -1;
+                        const int k_new = T.pres_new[k] ? desc_class(fl_new, T.pn[k].w) : -1;
+                        if (c_old != c_new || k_old != k_new) {
+                            cls_add(d, D, c_old, k_old, -1);
+                            cls_add(d, D, c_new, k_new, 1);
+                        }
+                    }
                     if (T.pres_old[k] && T.pres_new[k]) {
                         d.posq[gi] = T.pn[k];
                         d.type[gi] = T.tn[k];
@@ -785,7 +1065,9 @@ size_t mc_smem_bytes(int order, int pend_max) {
     // Monte Carlo trials carry <= 2 stencils against <= pend_max pending ones;
     // external trials (<= NST_MAX stencils) always start with none pending
     const size_t npairs = std::max((size_t)2 * pend_max + 3, (size_t)(NST_MAX * (NST_MAX + 1) / 2));
-    return st * (pend_max + NST_MAX) + pk * npairs;
+    // the pair tables' space also holds the surrogate's two 16-row BF16 activation buffers
+    const size_t act = 2 * 16 * SUR_AST * sizeof(__nv_bfloat16);
+    return st * (pend_max + NST_MAX) + std::max(pk * npairs, act);
 }
 
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {

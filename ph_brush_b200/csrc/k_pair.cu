@@ -34,7 +34,14 @@ __global__ void k_cell_sort(DevPtrs d, const int* __restrict__ cell_rep, int tot
         while (b >= 0 && l[b] > v) { l[b + 1] = l[b]; --b; }
         l[b + 1] = v;
     }
-    for (int a = 0; a < n; ++a) d.cell_pos[D.slot_off + l[a]] = a;
+    int4 cc = make_int4(0, 0, 0, 0);
+    for (int a = 0; a < n; ++a) {
+        const int gi = D.slot_off + l[a];
+        d.cell_pos[gi] = a;
+        const int c = desc_class(d.flags[gi], d.posq[gi].w);
+        cc.x += (c == 0); cc.y += (c == 1); cc.z += (c == 2); cc.w += (c == 3);
+    }
+    d.cell_cls[gc] = cc;
 }
 
 void launch_cell_build(Engine& E, cudaStream_t st) {

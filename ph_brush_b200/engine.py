@@ -136,3 +136,134 @@ class Engine:
         dims = np.zeros(3, np.int32)
         _abi.check(self._lib.phmc_get_cells(self._h, replica, _abi.iptr(c), _abi.iptr(dims)))
         return c, tuple(int(v) for v in dims)
+
+    # ---- learned surrogate / delayed acceptance ----
+    def harvest(self, capacity):
+        _abi.check(self._lib.phmc_harvest(self._h, int(capacity)))
+
+    def harvest_count(self):
+        n = C.c_int()
+        _abi.check(self._lib.phmc_harvest_count(self._h, C.byref(n)))
+        return n.value
+
+    def harvest_get(self, n=None):
+        n = self.harvest_count() if n is None else int(n)
+        x = np.zeros((n, _abi.SUR_ROWS, _abi.SUR_INPUTS), np.float32)
+        sg = np.zeros((n, _abi.SUR_ROWS), np.float32)
+        t = np.zeros(n, np.float32)
+        _abi.check(self._lib.phmc_harvest_get(self._h, n, _abi.fptr(x), _abi.fptr(sg), _abi.fptr(t)))
+        return x, sg, t
+
+    def surrogate_fit(self, sur, epochs=10, batch=4096, lr=1e-3, clip=25.0, seed=1):
+        loss = C.c_double()
+        _abi.check(self._lib.phmc_surrogate_fit(self._h, sur._h, int(epochs), int(batch), float(lr), float(clip),
+                                                int(seed), C.byref(loss)))
+        return loss.value
+
+    def attach_surrogate(self, sur, threshold=0.0, window=0):
+        _abi.check(self._lib.phmc_surrogate_attach(self._h, sur._h if sur is not None else None,
+                                                   float(threshold), int(window)))
+        self._sur = sur  # keep the network alive while attached
+
+    def da_stats(self):
+        out = (_abi.DAStats * self.R)()
+        _abi.check(self._lib.phmc_get_da_stats(self._h, out))
+        return [o.asdict() for o in out]
+
+    def describe(self, trials, replica=0):
+        n = len(trials)
+        arr = (_abi.Trial * n)(*[self.make_trial(t) for t in trials])
+        out = np.zeros((n, _abi.SUR_DESC_STRIDE), np.float32)
+        dEs = np.zeros(n, np.float64)
+        _abi.check(self._lib.phmc_surrogate_describe(self._h, replica, arr, n, _abi.fptr(out), _abi.dptr(dEs)))
+        R, K = _abi.SUR_ROWS, _abi.SUR_INPUTS
+        res = []
+        for k in range(n):
+            o = out[k]
+            res.append({"rows": o[:R * K].reshape(R, K).copy(), "sign": o[R * K:R * K + R].copy(),
+                        "F": o[R * K + R:R * K + 2 * R].copy(), "cross": float(o[R * K + 2 * R]),
+                        "mom": float(o[R * K + 2 * R + 1]), "nrows": int(o[R * K + 2 * R + 2]),
+                        "inner": int(o[R * K + 2 * R + 3]), "dEs": float(dEs[k])})
+        return res
+
+    def set_da_log(self):
+        cap = len(self._log[0])
+        self._da_log = (np.full(cap, -1, np.int32), np.zeros(cap, np.float64))
+        _abi.check(self._lib.phmc_set_da_log(self._h, _abi.iptr(self._da_log[0]), _abi.dptr(self._da_log[1])))
+        return self._da_log
+
+
+class Surrogate:
+    """The MLP surrogate (include/phmc.h, phmc_surrogate_*): GPU training and inference."""
+
+    def __init__(self, n_in=_abi.SUR_INPUTS, hidden=128, seed=0, _handle=None):
+        self._lib = _abi.lib()
+        self._h = C.c_void_p()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            _abi.check(self._lib.phmc_surrogate_create(int(n_in), int(hidden), int(seed), C.byref(self._h)))
+        self.n_params = self._lib.phmc_surrogate_num_params(self._h)
+
+    @classmethod
+    def load(cls, path):
+        lib = _abi.lib()
+        h = C.c_void_p()
+        _abi.check(lib.phmc_surrogate_load(str(path).encode(), C.byref(h)))
+        return cls(_handle=h)
+
+    def save(self, path):
+        _abi.check(self._lib.phmc_surrogate_save(self._h, str(path).encode()))
+
+    def close(self):
+        if self._h:
+            self._lib.phmc_surrogate_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        p = np.zeros(self.n_params, np.float32)
+        _abi.check(self._lib.phmc_surrogate_get_params(self._h, _abi.fptr(p), self.n_params))
+        return p
+
+    def set_params(self, p):
+        p = _abi.as_f32(p)
+        _abi.check(self._lib.phmc_surrogate_set_params(self._h, _abi.fptr(p), len(p)))
+
+    def set_scaling(self, mu, sd, scale):
+        mu, sd = _abi.as_f32(mu), _abi.as_f32(sd)
+        _abi.check(self._lib.phmc_surrogate_set_scaling(self._h, _abi.fptr(mu), _abi.fptr(sd), float(scale)))
+
+    def scaling(self, n_in=_abi.SUR_INPUTS):
+        mu, sd = np.zeros(n_in, np.float32), np.zeros(n_in, np.float32)
+        sc = C.c_float()
+        _abi.check(self._lib.phmc_surrogate_get_scaling(self._h, _abi.fptr(mu), _abi.fptr(sd), C.byref(sc)))
+        return mu, sd, sc.value
+
+    def predict(self, x):
+        x = _abi.as_f32(x)
+        n = x.shape[0]
+        y = np.zeros(n, np.float32)
+        _abi.check(self._lib.phmc_surrogate_predict(self._h, _abi.fptr(x), n, _abi.fptr(y)))
+        return y
+
+    def gradient(self, x, sign, t, clip=25.0):
+        x, sign, t = _abi.as_f32(x), _abi.as_f32(sign), _abi.as_f32(t)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_double()
+        _abi.check(self._lib.phmc_surrogate_gradient(self._h, _abi.fptr(x), _abi.fptr(sign), _abi.fptr(t), len(t),
+                                                     float(clip), C.byref(loss), _abi.fptr(g)))
+        return loss.value, g
+
+    def train(self, x, sign, t, epochs=1, batch=256, lr=1e-3, clip=25.0, seed=1, rescale=True):
+        x, sign, t = _abi.as_f32(x), _abi.as_f32(sign), _abi.as_f32(t)
+        loss = C.c_double()
+        _abi.check(self._lib.phmc_surrogate_train(self._h, _abi.fptr(x), _abi.fptr(sign), _abi.fptr(t), len(t),
+                                                  int(epochs), int(batch), float(lr), float(clip), int(seed),
+                                                  int(bool(rescale)), C.byref(loss)))
+        return loss.value
