@@ -43,6 +43,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--harvest", type=int, default=262144, help="surrogate training samples harvested (config 5)")
+    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--da-threshold", type=float, default=0.3)
+    ap.add_argument("--no-alpha", action="store_true")
+    ap.add_argument("--alpha-eq", type=int, default=300, help="sweeps of equilibration in the alpha(pH) check")
+    ap.add_argument("--alpha-sample", type=int, default=200, help="sweeps sampled in the alpha(pH) check")
     return ap.parse_args()
 
 
@@ -152,30 +158,101 @@ def cpu_baseline(s, p, seconds):
             "trials_per_s": tps}
 
 
+def _alpha(stats, n_sites):
+    return [st["n_charged_sites"] / n for st, n in zip(stats, n_sites)]
+
+
+def alpha_check(local, sweeps_eq, sweeps_sample, snaps=20):
+    """alpha(pH) of delayed acceptance against the plain engine on config-5 chemistry (small
+    diblock replicas that equilibrate within the run).  The plain engine equilibrates, its
+    exact dE of the last part of the equilibration train the surrogate, a second engine takes
+    over the equilibrated states with delayed acceptance, and both engines then sample."""
+    import numpy as np
+    from ph_brush_b200 import Engine, Surrogate, configs
+    reps = configs.diblock_small()
+    S, P = [a for a, _ in reps], [b for _, b in reps]
+    for p in P:
+        p.p_disp, p.p_titr = 0.5, 0.5  # titration-heavy: alpha relaxes within the run
+    ns = [a.meta["n_sites"] for a in S]
+    nmax = max(a.n for a in S)
+    A = Engine(S, P, device=local)
+    A.autotune(2000)
+    A.run(sweeps_eq * nmax)
+    A.harvest(131072)
+    A.run(max(nmax * 10, 2 * 131072 // len(S)))
+    sur = Surrogate(seed=31)
+    loss = A.surrogate_fit(sur, epochs=12, batch=2048, lr=1e-3, clip=25.0, seed=3)
+    A.harvest(0)
+    B = Engine(S, P, device=local)
+    tn = A.tuning()
+    B.set_tuning(tn["pending_max"], tn["threads"])
+    for r in range(len(S)):
+        B.set_state(A.state(r), r)
+    B.attach_surrogate(sur, threshold=0.0, window=0)
+    per = max(1, sweeps_sample * nmax // snaps)
+    a_p, a_d = [], []
+    for _ in range(snaps):
+        a_p.append(_alpha(A.run(per), ns))
+        a_d.append(_alpha(B.run(per), ns))
+    da = B.da_stats()
+    A.close()
+    B.close()
+    a_p, a_d = np.array(a_p), np.array(a_d)
+    mp, md = a_p.mean(0), a_d.mean(0)
+    half = snaps // 2
+    drift = float(np.abs(a_p[half:].mean(0) - a_p[:half].mean(0)).mean())
+    se = np.sqrt(a_p.var(0, ddof=1) / snaps + a_d.var(0, ddof=1) / snaps)
+    pH = np.array([p.pH for p in P])
+    curve = []
+    for lo in (5.0, 6.0, 7.0, 8.0):
+        m = (pH >= lo) & (pH < lo + 1.0 + (1e-9 if lo == 8.0 else 0.0))
+        curve.append({"pH": [lo, lo + 1.0], "replicas": int(m.sum()), "alpha_plain": float(mp[m].mean()),
+                      "alpha_da": float(md[m].mean()), "diff": float(md[m].mean() - mp[m].mean()),
+                      "stderr": float(np.sqrt((se[m] ** 2).sum()) / m.sum())})
+    ev = sum(d["evaluated"] for d in da)
+    ps = sum(d["passed"] for d in da)
+    ac = sum(d["accepted"] for d in da)
+    return {"workload": "config-5 chemistry, 24 replicas of 4x4 diblock chains (20 permanent +1 + 30 titratable, "
+                        "pKa 7.3), pH 5-9, salt 0.01-0.1 M, 50% displacement / 50% protonation",
+            "sweeps_equilibrate": sweeps_eq, "sweeps_sample": sweeps_sample, "snapshots": snaps,
+            "fit_loss": loss, "exact_dE_skipped": 1.0 - ps / max(ev, 1), "second_stage_agreement": ac / max(ps, 1),
+            "pH_curve": curve, "max_curve_diff": float(max(abs(c["diff"]) for c in curve)),
+            "mean_abs_diff_per_replica": float(np.abs(md - mp).mean()), "median_stderr_per_replica": float(np.median(se)),
+            "plain_drift_between_halves": drift}
+
+
 def run_batched(args, local, n_rep=256, trials=400, plain_samples=3):
     """Config 5: 256 diblock replicas in one engine (one block per replica per MC
     phase, captured in CUDA graphs) against the plain engine, which runs the same
-    replicas one at a time.  Aggregate sweeps/s = sum over replicas of sweeps / time."""
-    from ph_brush_b200 import Engine, configs
+    replicas one at a time.  Aggregate sweeps/s = sum over replicas of sweeps / time.
+    Then the learned surrogate: exact dE harvested from the replicas, one network
+    (pH and salt among its inputs) trained on the GPU, delayed acceptance on the
+    config's move mix and on a titration-only phase."""
+    import numpy as np
+    from ph_brush_b200 import Engine, Surrogate, configs
     reps = configs.config5(n_rep=n_rep)
     ns = [s.n for s, _ in reps]
+    n_sites = [int(s.meta["n_sites"]) for s, _ in reps]
     eng = Engine([s for s, _ in reps], [p for _, p in reps], device=local)
+    tune = eng.autotune(trials)
+    tuned = eng.tuning()
     eng.run(trials // 4)
     eng.set_profiling(True)
     eng.profile(reset=True)
     eng.flush_l2(256 << 20)
     ms = eng.run_timed(trials)
     prof = eng.profile(reset=True)
-    eng.close()
+    eng.set_profiling(False)
     agg = sum(trials / n for n in ns) / (ms / 1e3)
-    # plain engine: the same replicas one at a time; its aggregate rate over the set is
-    # R sweeps / sum_r (N_r * t_r), t_r the per-trial time of replica r alone
+    # plain engine: the same replicas one at a time (each autotuned); its aggregate rate
+    # over the set is R sweeps / sum_r (N_r * t_r), t_r the per-trial time of replica r alone
     idx = sorted(range(n_rep), key=lambda r: ns[r])
     pick = [idx[0], idx[len(idx) // 2], idx[-1]][:plain_samples]
     per_sweep_s = []
     for r in pick:
         s, p = reps[r]
         e1 = Engine(s, p, device=local)
+        e1.autotune(trials)
         e1.run(trials // 4)
         e1.flush_l2(256 << 20)
         t = e1.run_timed(trials) / 1e3 / trials
@@ -191,12 +268,71 @@ def run_batched(args, local, n_rep=256, trials=400, plain_samples=3):
                               "share": prof["flush_ms"] / ms}
     for v in rl.values():
         v.update({"bound": "hbm", "peak": peak, "unit": "GB/s", "frac": v["achieved"] / peak, "peak_source": kind})
+
+    # ---- surrogate: harvest (titration-heavy mix), GPU training ----
+    p0 = reps[0][1]
+    sur = Surrogate(seed=2029)
+    eng.set_move_mix(0.5, 0.5, 0.0)
+    eng.harvest(args.harvest)
+    eng.run(2 * args.harvest // n_rep + 1)
+    n_samples = eng.harvest_count()
+    t0 = time.perf_counter()
+    loss = eng.surrogate_fit(sur, epochs=args.epochs, batch=4096, lr=1e-3, clip=25.0, seed=7)
+    t_fit = time.perf_counter() - t0
+    eng.harvest(0)
+    steps = args.epochs * (n_samples // 4096)
+    # 4 rows per sample; forward 2*(80*128 + 2*128*128 + 128) flops per row, backward twice that
+    fl_row = 2.0 * (80 * 128 + 2 * 128 * 128 + 128)
+    train = {"samples": n_samples, "epochs": args.epochs, "batch": 4096, "lr": 1e-3, "final_loss": loss,
+             "seconds": t_fit, "samples_per_s": steps * 4096 / t_fit,
+             "tflops": steps * 4096 * 4 * 3 * fl_row / t_fit / 1e12}
+
+    # ---- batched + surrogate on the config's move mix ----
+    eng.set_move_mix(p0.p_disp, p0.p_titr, p0.p_swap)
+    eng.attach_surrogate(sur, threshold=args.da_threshold, window=256)
+    eng.run(trials // 4)
+    eng.flush_l2(256 << 20)
+    ms_da = eng.run_timed(trials)
+    agg_da = sum(trials / n for n in ns) / (ms_da / 1e3)
+    da_mix = eng.da_stats()
+
+    # ---- titration-only phase (the reference's protonation phase): plain vs delayed acceptance ----
+    eng.set_move_mix(0.0, 1.0, 0.0)
+    eng.attach_surrogate(None)
+    tt = int(max(n_sites))
+    eng.run(tt)
+    eng.flush_l2(256 << 20)
+    ms_tp = eng.run_timed(tt)
+    eng.attach_surrogate(sur, threshold=0.0, window=0)
+    eng.run(tt // 4)
+    eng.flush_l2(256 << 20)
+    ms_td = eng.run_timed(tt)
+    da_t = eng.da_stats()
+    eng.close()
+    ev, ps, ac = (sum(d[k] for d in da_t) for k in ("evaluated", "passed", "accepted"))
+    evm, psm, acm = (sum(d[k] for d in da_mix) for k in ("evaluated", "passed", "accepted"))
+    tp_plain = n_rep * tt / (ms_tp / 1e3)
+    tp_da = n_rep * tt / (ms_td / 1e3)
+    surrogate = {
+        "training": train,
+        "aggregate_sweeps_per_s": agg_da, "speedup_vs_plain": agg_da / plain,
+        "speedup_vs_batched_exact": agg_da / agg,
+        "config_mix": {"exact_dE_skipped": 1.0 - psm / max(evm, 1), "second_stage_agreement": acm / max(psm, 1),
+                       "fallbacks": int(sum(d["fallback"] for d in da_mix)), "threshold": args.da_threshold},
+        "titration_phase": {"trials_per_replica": tt, "plain_trials_per_s": tp_plain, "da_trials_per_s": tp_da,
+                            "gain": tp_da / tp_plain, "exact_dE_skipped": 1.0 - ps / max(ev, 1),
+                            "second_stage_agreement": ac / max(ps, 1)},
+    }
+    if not args.no_alpha:
+        surrogate["alpha_check"] = alpha_check(local, args.alpha_eq, args.alpha_sample)
     return {"workload": "config 5: 256 diblock replicas (20 permanent +1 + 30 titratable beads, pKa 7.3), 64-144 chains, "
                         "pH 5-9, salt 0.001-0.3 M, slab 60 padded to 180, SPME order 5, lateral mesh 48-64",
             "replicas": n_rep, "particles_min_max": [min(ns), max(ns)], "trials_per_replica": trials,
+            "tuning": tuned, "autotune": tune,
             "aggregate_sweeps_per_s": agg, "trials_per_s": n_rep * trials / (ms / 1e3),
             "plain_aggregate_sweeps_per_s": plain, "plain_sampled_replicas": pick, "speedup_vs_plain": agg / plain,
-            "surrogate": False, "roofline": rl, "device_ms": ms, "gpu_launches": int(prof["kernel_launches"])}
+            "roofline": rl, "device_ms": ms, "gpu_launches": int(prof["kernel_launches"]),
+            "surrogate": surrogate}
 
 
 def run_reference(args):
@@ -254,6 +390,8 @@ def run_ours(args):
     s, p = configs.config2(seed=2026 + rank)
     N = s.n
     eng = Engine(s, p, device=local)
+    tune = eng.autotune(max(2000, N // 4))
+    tuned = eng.tuning()
     for _ in range(args.warmup):
         eng.run(N)
     # ---- device-timed region: inputs resident, L2 flushed between steps ----
@@ -320,7 +458,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32 (f64 accumulation and Metropolis)",
             "data": "synthetic (seeded brush generator, seed 2026 + rank)",
             "config": {"workload": WORKLOAD, "particles": N, "trials_per_step": N, "mesh": list(p.mesh),
-                       "order": p.order, "pending_max": p.pending_max or 16,
+                       "order": p.order, "tuning": tuned, "autotune": tune,
                        "l2": "flushed between steps (256 MiB write on the engine stream)",
                        "parallelism": f"replicas only x{world}"},
             "roofline": dict(rl[dominant], kernel=dominant) if dominant else None,

@@ -197,6 +197,29 @@ int phmc_set_trial_log(phmc_engine* e, int64_t capacity, int* move, double* dE, 
  * (replica 0, one int per trial) instead of the Metropolis test. NULL disables. */
 int phmc_set_replay(phmc_engine* e, int64_t n, const int* decisions);
 
+/* Change the move mix of replica r (-1: all) for the following runs, e.g. a
+ * titration-only phase like the reference's protonation phase
+ * (MC/src/mc.cu:320-550).  Same rules as phmc_params. */
+int phmc_set_move_mix(phmc_engine* e, int replica, double p_disp, double p_titr, double p_swap);
+
+/* ---- tuning (no counterpart in the reference) ----
+ * pending_max: stencils buffered before the potential mesh is rebuilt (each
+ * trial pays a correction per buffered stencil, each rebuild a pass over the
+ * mesh); threads: threads per replica block of the MC kernel (128 or 256).
+ * Both may change between runs.  phmc_autotune times `trials` trials per
+ * replica for each candidate (pending_max 8..64 x threads 128/256), keeps the
+ * fastest and reports every candidate; its runs are ordinary Monte Carlo
+ * trials and advance the chains.  Decisions do not depend on the tuning except
+ * through FP32 rounding of the reciprocal-space dE. */
+typedef struct phmc_tuning {
+    int pending_max;
+    int threads;
+    double us_per_trial;  /* device time per trial (all replicas), autotune only */
+} phmc_tuning;
+int phmc_set_tuning(phmc_engine* e, int pending_max, int threads);
+int phmc_get_tuning(phmc_engine* e, phmc_tuning* out);
+int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_results, int* n_results);
+
 /* ---- state ---- */
 int phmc_get_state(phmc_engine* e, int replica, float* x, float* y, float* z, float* q,
                    int* type, int* flags);

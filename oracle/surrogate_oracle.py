@@ -65,8 +65,10 @@ class Geometry:
         self.n = np.asarray(dims, np.int64)
         self.scale = np.float32(self.n.astype(np.float32) / self.L)  # float(ncell) / L
         self.w = (self.L / self.n.astype(np.float32)).astype(np.float32)
-        self.dnr = np.maximum(1, np.ceil(RMAX * self.n / np.asarray(box, np.float64)).astype(np.int64))
-        self.dnk = np.minimum(2 * self.dnr + 1, self.n)
+        r = np.maximum(1, np.ceil(RMAX * self.n / np.asarray(box, np.float64)).astype(np.int64))
+        self.dnk = np.minimum(2 * r + 1, self.n)
+        # a window over the whole axis is centred: it holds -1, 0, +1 and every other cell once
+        self.dnr = np.where(self.dnk < 2 * r + 1, (self.dnk - 1) // 2, r)
         walls = params.wall_hi > params.wall_lo
         self.z0 = f32(params.wall_lo) if walls else f32(0.0)
         self.h = f32(f32(params.wall_hi) - f32(params.wall_lo)) if walls else self.L[2]

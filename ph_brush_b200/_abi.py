@@ -88,6 +88,13 @@ class DAStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
+class Tuning(C.Structure):
+    _fields_ = [("pending_max", C.c_int), ("threads", C.c_int), ("us_per_trial", C.c_double)]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class BrushSpec(C.Structure):
     _fields_ = [("chains_x", C.c_int), ("chains_y", C.c_int), ("graft_spacing", C.c_double),
                 ("len_min", C.c_int), ("len_max", C.c_int), ("n_permanent", C.c_int),
@@ -106,7 +113,8 @@ EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy",
            "phmc_surrogate_get_scaling", "phmc_surrogate_predict", "phmc_surrogate_gradient",
            "phmc_surrogate_train", "phmc_surrogate_save", "phmc_surrogate_load", "phmc_harvest",
            "phmc_harvest_count", "phmc_harvest_get", "phmc_surrogate_fit", "phmc_surrogate_attach",
-           "phmc_get_da_stats", "phmc_surrogate_describe", "phmc_set_da_log"]
+           "phmc_get_da_stats", "phmc_surrogate_describe", "phmc_set_da_log", "phmc_set_move_mix",
+           "phmc_set_tuning", "phmc_get_tuning", "phmc_autotune"]
 
 
 def load_library(path=LIB_PATH):
@@ -159,6 +167,10 @@ def load_library(path=LIB_PATH):
         "phmc_get_da_stats": ([eng, C.POINTER(DAStats)], C.c_int),
         "phmc_surrogate_describe": ([eng, C.c_int, C.POINTER(Trial), C.c_int, _fp, _dp], C.c_int),
         "phmc_set_da_log": ([eng, _ip, _dp], C.c_int),
+        "phmc_set_move_mix": ([eng, C.c_int, C.c_double, C.c_double, C.c_double], C.c_int),
+        "phmc_set_tuning": ([eng, C.c_int, C.c_int], C.c_int),
+        "phmc_get_tuning": ([eng, C.POINTER(Tuning)], C.c_int),
+        "phmc_autotune": ([eng, C.c_int64, C.POINTER(Tuning), C.c_int, _ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -124,6 +124,26 @@ def config5(seed=2029, order=5, n_rep=256):
     return out
 
 
+def diblock_small(seed=2031, order=5, n_rep=24, side=4):
+    """Config-5 chemistry on small replicas (side x side diblock chains: 20 permanent +1 and 30
+    titratable beads, pKa 7.3), pH 5..9 evenly spaced, salt 0.01 / 0.03 / 0.1 M cycling; small enough
+    for the degree of ionisation to equilibrate within a benchmark run."""
+    out = []
+    H = 60.0
+    salts = [0.01, 0.03, 0.1]
+    for k in range(n_rep):
+        pH = 5.0 + 4.0 * k / max(n_rep - 1, 1)
+        salt = salts[k % 3]
+        L = 4.0 * side
+        nxy = smooth_mesh(max(32, L / 0.75))
+        mesh = (nxy, nxy, smooth_mesh(3 * H / 0.75))
+        s = build_brush(side, side, 4.0, 50, 50, H, 3 * H, ideal_alpha(pH, 7.3), molar_to_sigma3(salt),
+                        n_permanent=20, graft_titratable=0, seed=seed + k)
+        p = native_params(pH, 7.3, mesh, H, seed + k, order=order)
+        out.append((s, p))
+    return out
+
+
 def small_system(seed=7, chains=2, length=6, box_xy=12.0, height=12.0, salt_pairs=4, order=5, mesh=(16, 16, 48),
                  lb=L_BJERRUM, ion_frac=0.5, p_swap=0.0, salt_conc=0.0):
     """A few dozen particles for oracle-sized parity tests."""

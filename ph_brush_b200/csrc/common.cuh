@@ -62,8 +62,8 @@ struct RepDesc {
     double Lz2_12;      // Lz^2 / 12
     // surrogate descriptor
     float cell_w[3];      // cell widths L / ncell (float)
-    int dnr[3];           // cell range of the 8-sigma descriptor sphere: offsets -dnr .. -dnr + dnk - 1
-    int dnk[3];           // min(2 dnr + 1, ncell)
+    int dnr[3];           // cell window of the 8-sigma descriptor sphere: offsets -dnr .. -dnr + dnk - 1,
+    int dnk[3];           // dnk = min(2 r + 1, ncell) for the range r; dnr = r, or (dnk - 1) / 2 when dnk == ncell
     float sur_z0, sur_h;  // z feature = (z - sur_z0) / sur_h
     float sur_pk, sur_salt;  // pKa - pH, log10(salt) features
 };

@@ -266,6 +266,9 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
             D.cell_w[k] = D.L[k] / (float)D.ncell[k];
             D.dnr[k] = std::max(1, (int)std::ceil((double)SUR_RMAX * D.ncell[k] / S.box[k]));
             D.dnk[k] = std::min(2 * D.dnr[k] + 1, D.ncell[k]);
+            // when the range covers the whole axis, centre the window so that it holds the
+            // neighbours -1, 0, +1 (the inner cells) and every other cell once
+            if (D.dnk[k] < 2 * D.dnr[k] + 1) D.dnr[k] = (D.dnk[k] - 1) / 2;
         }
         D.cell_off = cell_off; cell_off += D.ncell[0] * D.ncell[1] * D.ncell[2];
         D.cell_cap = E.cell_cap;
@@ -1089,4 +1092,88 @@ extern "C" int phmc_set_da_log(phmc_engine* h, int* stage, double* dEs) {
     CU(cudaMalloc((void**)&E.d.log_stage, sizeof(int) * E.d.log_cap));
     CU(cudaMalloc((void**)&E.d.log_dEs, sizeof(double) * E.d.log_cap));
     return PHMC_OK;
+}
+
+extern "C" int phmc_set_move_mix(phmc_engine* h, int rep, double p_disp, double p_titr, double p_swap) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    Engine& E = h->E;
+    if (rep < -1 || rep >= E.R) return fail(PHMC_ERR_ARG, "replica index out of range");
+    if (p_disp < 0 || p_titr < 0 || p_swap < 0 || p_disp + p_titr + p_swap > 1.0 + 1e-12)
+        return fail(PHMC_ERR_ARG, "move probabilities must be >= 0 with sum <= 1");
+    const int r0 = rep < 0 ? 0 : rep, r1 = rep < 0 ? E.R : rep + 1;
+    for (int r = r0; r < r1; ++r)
+        if (p_swap > 0 && !(E.desc[r].salt_c2V2 > 0)) return fail(PHMC_ERR_ARG, "swap moves need salt_conc > 0");
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    for (int r = r0; r < r1; ++r) {
+        RepDesc& D = E.desc[r];
+        D.p_disp = (float)p_disp; D.p_titr = (float)p_titr; D.p_swap = (float)p_swap;
+    }
+    // the MC kernel reads the descriptor table at launch: captured launches stay valid
+    CU(cudaMemcpy(E.d.desc, E.desc.data(), sizeof(RepDesc) * E.R, cudaMemcpyHostToDevice));
+    return PHMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tuning: pending-stencil capacity (rebuild frequency against per-trial
+// correction cost) and threads per replica block; both may change between runs
+// ---------------------------------------------------------------------------
+static int apply_tuning(phmc_engine* h, int pend, int threads) {
+    Engine& E = h->E;
+    const int old_p = E.pend_max, old_t = E.threads;
+    E.pend_max = pend;
+    E.threads = threads;
+    cudaError_t e = prepare_mc(E);
+    if (e != cudaSuccess) {
+        E.pend_max = old_p; E.threads = old_t;
+        return fail(PHMC_ERR_UNSUPPORTED, std::string("tuning does not fit the device: ") + cudaGetErrorString(e));
+    }
+    for (RepDesc& D : E.desc) D.pend_max = pend;
+    CU(cudaMemcpy(E.d.desc, E.desc.data(), sizeof(RepDesc) * E.R, cudaMemcpyHostToDevice));
+    drop_graph(h);  // captured launches hold the old launch shape
+    return PHMC_OK;
+}
+
+extern "C" int phmc_set_tuning(phmc_engine* h, int pending_max, int threads) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    if (pending_max < 4 || pending_max > PHMC_MAX_PEND || (threads != 128 && threads != 256))
+        return fail(PHMC_ERR_ARG, "pending_max must be in [4, 64] and threads 128 or 256");
+    CU(cudaSetDevice(h->E.device));
+    CU(cudaStreamSynchronize(h->E.stream));
+    return apply_tuning(h, pending_max, threads);
+}
+
+extern "C" int phmc_get_tuning(phmc_engine* h, phmc_tuning* out) {
+    if (!h || !out) return fail(PHMC_ERR_ARG, "null argument");
+    out->pending_max = h->E.pend_max;
+    out->threads = h->E.threads;
+    out->us_per_trial = 0.0;
+    return PHMC_OK;
+}
+
+extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* results, int max_results, int* n_results) {
+    if (!h || trials < 16) return fail(PHMC_ERR_ARG, "phmc_autotune: need trials >= 16");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    const int pends[] = {8, 16, 24, 32, 48, 64};
+    const int ths[] = {128, 256};
+    int best_p = E.pend_max, best_t = E.threads, n = 0;
+    double best = 1e300;
+    for (int t : ths)
+        for (int pm : pends) {
+            if (pm > PHMC_MAX_PEND) continue;
+            if (apply_tuning(h, pm, t) != PHMC_OK) continue;  // does not fit: skip
+            int s = phmc_run_loop(h, std::max<int64_t>(trials / 4, 4), 4);  // warm-up (captures the graph)
+            if (s) return s;
+            double ms = 0.0;
+            s = phmc_run_timed(h, trials, &ms);
+            if (s) return s;
+            const double us = ms * 1e3 / (double)trials;
+            if (results && n < max_results) { results[n].pending_max = pm; results[n].threads = t; results[n].us_per_trial = us; }
+            ++n;
+            if (us < best) { best = us; best_p = pm; best_t = t; }
+        }
+    if (n_results) *n_results = n;
+    return apply_tuning(h, best_p, best_t);
 }

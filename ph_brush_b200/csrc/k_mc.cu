@@ -19,6 +19,7 @@
 #include <algorithm>
 #include "common.cuh"
 #include "engine.h"
+#include "fft.cuh"
 
 #define NST_MAX 4    // stencils per trial
 #define NPROBE_MAX 4 // (old, new) states of up to two particles
@@ -118,12 +119,14 @@ __device__ __forceinline__ float4 rand_pos(const RepDesc& D, uint32_t a, uint32_
     return p;
 }
 
-// The 12 Philox words of trial t: A = ctr (t, 0), B = ctr (t, 1), C = ctr (t, 2).
+// The 16 Philox words of trial t: A = ctr (t, 0), B = ctr (t, 1), C = ctr (t, 2),
+// and ctr (t, 3), whose first two words are the delayed-acceptance first-stage uniform.
 __device__ __forceinline__ void trial_words(const RepDesc& D, long long t, uint32_t* w) {
     const uint32_t lo = (uint32_t)t, hi = (uint32_t)((unsigned long long)t >> 32);
     philox4x32_10(D.key[0], D.key[1], lo, hi, 0u, 0u, w);
     philox4x32_10(D.key[0], D.key[1], lo, hi, 1u, 0u, w + 4);
     philox4x32_10(D.key[0], D.key[1], lo, hi, 2u, 0u, w + 8);
+    philox4x32_10(D.key[0], D.key[1], lo, hi, 3u, 0u, w + 12);
 }
 
 __device__ __forceinline__ int move_of(const RepDesc& D, uint32_t a0) {
@@ -274,6 +277,12 @@ __device__ __forceinline__ void make_stencil(Stencil<P>& s, const RepDesc& D, fl
 }
 
 __device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+// i mod n for |i| within a few periods (descriptor cell offsets)
+__device__ __forceinline__ int wrap_small(int i, int n) {
+    while (i < 0) i += n;
+    while (i >= n) i -= n;
+    return i;
+}
 
 __device__ __forceinline__ void list_remove(int* list, int* pos, int& n, int so, int i) {
     const int k = pos[so + i];
@@ -369,7 +378,7 @@ __device__ double pair_cross(const RepDesc& D, float4 a, float4 b, int ta, int t
 }
 
 // Rows, descriptor centres, exclusions and the exact terms of the first stage (one thread).
-__device__ void desc_setup(TrialS& T, const RepDesc& D, const RepState& S) {
+__device__ void desc_setup(TrialS& T, const RepDesc& D) {
     int nr = 0;
     for (int k = 0; k < T.nch; ++k) {
         const float4 p = T.pres_new[k] ? T.pn[k] : T.po[k];
@@ -384,6 +393,11 @@ __device__ void desc_setup(TrialS& T, const RepDesc& D, const RepState& S) {
         if (T.pres_new[k]) { T.row_k[nr] = k; T.row_cls[nr] = row_state(titr, T.pn[k].w); T.row_sign[nr] = 1.0f; ++nr; }
     }
     T.nrows = nr;
+}
+
+// Exact terms of the first stage: the changed particles' direct interaction and
+// the self / net-charge / slab changes (one thread, beside the descriptor work).
+__device__ void desc_exact_terms(TrialS& T, const RepDesc& D, const RepState& S) {
     double cross = 0.0;
     if (T.nch == 2) {
         const bool bonded = in_bonds(T.bonds[0], T.idx[1]);
@@ -422,7 +436,7 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
 }
 
 template <int P, int NT>
-__global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
+__global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
     constexpr int W = 2 * P - 1;
     constexpr int P3 = P * P * P;
@@ -436,7 +450,7 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
     __shared__ int s_cnt[NPROBE_MAX * 27], s_off[NPROBE_MAX * 27 + 1], s_cell[NPROBE_MAX * 27];
     __shared__ double red[100];
     __shared__ int s_npend;
-    __shared__ uint32_t s_rng[32][12];  // Philox words of trials s_rng_base .. s_rng_base+31
+    __shared__ uint32_t s_rng[32][16];  // Philox words of trials s_rng_base .. s_rng_base+31
     __shared__ long long s_rng_base;
     __shared__ Prefetch pf;
     // surrogate first stage: shell histogram per changed particle, raw rows, outputs
@@ -444,6 +458,17 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
     __shared__ float s_rows[SUR_ROWS][SUR_K];
     __shared__ float s_F[8];
     __shared__ int s_hv_slot, s_hv_nrows;  // harvested sample whose rows are still to be stored
+    __shared__ __align__(8) uint64_t s_mbar[3];  // completion of the staged weight copies
+    __shared__ int s_sfail;                      // a staged copy did not arrive in time
+    __shared__ float s_mu[SUR_K], s_sd[SUR_K];   // the attached network's input standardisation
+    // staged first stage (aliases the pair tables, used before phase 3): activations, weights
+    unsigned char* sur_base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(s_pair) + 127) & ~uintptr_t(127));
+    __nv_bfloat16* act0 = reinterpret_cast<__nv_bfloat16*>(sur_base);
+    __nv_bfloat16* act1 = act0 + 16 * SUR_AST;
+    uint2* wa = reinterpret_cast<uint2*>(sur_base + SUR_ACT_BYTES);
+    uint2* wb = wa + (SUR_K * SUR_HMAX * 2) / 8;
+    uint2* wc = wb + SUR_WBUF_BYTES / 8;
+    uint32_t sur_par = 0;  // parity of the weight barriers' current phase (one phase per evaluated move)
 
     const int r = (mode == MC_RUN) ? blockIdx.x : ext_rep;
     const int tid = threadIdx.x;
@@ -463,7 +488,13 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
         s_rng_base = -64;
         pf.valid = 0;
         s_hv_slot = -1;
+        s_sfail = 0;
+        sur_mbar_init(&s_mbar[0]);
+        sur_mbar_init(&s_mbar[1]);
+        sur_mbar_init(&s_mbar[2]);
     }
+    if (d.sur.H > 0)
+        for (int k = tid; k < SUR_K; k += NT) { s_mu[k] = d.sur.mu[k]; s_sd[k] = d.sur.sd[k]; }
     __syncthreads();
 
     for (;;) {
@@ -498,7 +529,7 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                         T.da = d.sur.H > 0 && !S.da_off && !(r == 0 && d.replay);
                         T.desc = T.da || d.hv_cap > 0;
                     }
-                    if (T.desc) desc_setup(T, D, S);
+                    if (T.desc) desc_setup(T, D);
                 }
             }
         } else {
@@ -509,35 +540,69 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                     dst[e] = (e / SUR_K < s_hv_nrows) ? s_rows[e / SUR_K][e % SUR_K] : 0.0f;
             }
             for (int e = tid - 32; e < 2 * SUR_SHELLS * SUR_CLASSES; e += NT - 32) s_hist[e] = 0;
+            for (int e = tid - 32; e < 2 * 27; e += NT - 32) { s_cnt[e] = 0; s_cell[e] = 0; }
         }
         __syncthreads();
         if (T.stop) break;
         if (tid == 0) s_hv_slot = -1;
         // ---------------- surrogate first stage ----------------
         if (T.desc) {
+            if (T.da && tid == 0) {  // stage the three hidden layers while the descriptor is built
+                sur_bulk_load(wa, d.sur.w[0], sur_layer_bytes(SUR_K, d.sur.H), &s_mbar[0]);
+                sur_bulk_load(wb, d.sur.w[1], sur_layer_bytes(d.sur.H, d.sur.H), &s_mbar[1]);
+                sur_bulk_load(wc, d.sur.w[2], sur_layer_bytes(d.sur.H, d.sur.H), &s_mbar[2]);
+            }
+            if (tid == NT - 1) desc_exact_terms(T, D, S);
             // (a) the descriptor sphere's cells: inner 27 cells -> counts for the particle
             // pass; outer cells -> class counts binned by the distance of the cell centre
             const int nk0 = D.dnk[0], nk1 = D.dnk[1], nk2 = D.dnk[2];
             const int nc3 = nk0 * nk1 * nk2;
-            for (int e = tid; e < T.nch * nc3; e += NT) {
-                const int k = e / nc3, loc = e - k * nc3;
-                const int lz = loc / (nk0 * nk1), lr = loc - lz * (nk0 * nk1);
-                const int ly = lr / nk0, lx = lr - ly * nk0;
-                const int ox = lx - D.dnr[0], oy = ly - D.dnr[1], oz = lz - D.dnr[2];
-                const int cx = wrap_idx(T.dcx[k] + ox, D.ncell[0]), cy = wrap_idx(T.dcy[k] + oy, D.ncell[1]),
-                          cz = wrap_idx(T.dcz[k] + oz, D.ncell[2]);
-                const int cell = (cz * D.ncell[1] + cy) * D.ncell[0] + cx;
-                if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1) {
-                    const int sl = k * 27 + (oz + 1) * 9 + (oy + 1) * 3 + (ox + 1);
-                    s_cell[sl] = cell;
-                    s_cnt[sl] = min(d.cell_count[D.cell_off + cell], D.cell_cap);
-                } else {
-                    int4 cc = d.cell_cls[D.cell_off + cell];
+            constexpr int RC = 3;
+            const FastDiv f3(nc3), f2(nk0 * nk1), f1(nk0);
+            for (int e0 = tid; e0 < T.nch * nc3; e0 += RC * NT) {
+                int cell_u[RC], k_u[RC], sl_u[RC];
+                int4 cc_u[RC];
+                int3 c3_u[RC];
+#pragma unroll
+                for (int u = 0; u < RC; ++u) {  // all loads of the batch first
+                    const int e = e0 + u * NT;
+                    cell_u[u] = -1;
+                    if (e >= T.nch * nc3) continue;
+                    int loc, lr, lx;
+                    const int k = f3.div(e, loc);
+                    const int lz = f2.div(loc, lr);
+                    const int ly = f1.div(lr, lx);
+                    const int ox = lx - D.dnr[0], oy = ly - D.dnr[1], oz = lz - D.dnr[2];
+                    const int cx = wrap_small(T.dcx[k] + ox, D.ncell[0]), cy = wrap_small(T.dcy[k] + oy, D.ncell[1]),
+                              cz = wrap_small(T.dcz[k] + oz, D.ncell[2]);
+                    const int cell = (cz * D.ncell[1] + cy) * D.ncell[0] + cx;
+                    cell_u[u] = cell; k_u[u] = k;
+                    c3_u[u] = make_int3(cx, cy, cz);
+                    if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1) {
+                        sl_u[u] = k * 27 + (oz + 1) * 9 + (oy + 1) * 3 + (ox + 1);
+                        cc_u[u].x = d.cell_count[D.cell_off + cell];
+                    } else {
+                        sl_u[u] = -1;
+                        cc_u[u] = d.cell_cls[D.cell_off + cell];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RC; ++u) {
+                    const int cell = cell_u[u];
+                    if (cell < 0) continue;
+                    if (sl_u[u] >= 0) {  // inner cell: count for the particle pass
+                        s_cell[sl_u[u]] = cell;
+                        s_cnt[sl_u[u]] = min(cc_u[u].x, D.cell_cap);
+                        continue;
+                    }
+                    int4 cc = cc_u[u];
                     for (int j = 0; j < T.nch; ++j)
                         if (T.ccell[j] == cell) {
                             cc.x -= (T.ccls[j] == 0); cc.y -= (T.ccls[j] == 1); cc.z -= (T.ccls[j] == 2); cc.w -= (T.ccls[j] == 3);
                         }
                     if ((cc.x | cc.y | cc.z | cc.w) == 0) continue;
+                    const int k = k_u[u];
+                    const int cx = c3_u[u].x, cy = c3_u[u].y, cz = c3_u[u].z;
                     const float4 p = T.dpos[k];
                     const float xc = __fmul_rn(__fadd_rn((float)cx, 0.5f), D.cell_w[0]);
                     const float yc = __fmul_rn(__fadd_rn((float)cy, 0.5f), D.cell_w[1]);
@@ -572,29 +637,47 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 if (tid == 0) { s_off[nent_d] = carry; T.dtotal = carry; }
             }
             __syncthreads();
-            // (b) particles of the inner cells, exact distance shells
-            for (int it = tid; it < T.dtotal; it += NT) {
-                int lo = 0, hi = nent_d - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+            // (b) particles of the inner cells, exact distance shells (loads batched per thread)
+            constexpr int RP = 4;
+            for (int it0 = tid; it0 < T.dtotal; it0 += RP * NT) {
+                int j_u[RP], k_u[RP];
+#pragma unroll
+                for (int u = 0; u < RP; ++u) {
+                    const int it = it0 + u * NT;
+                    j_u[u] = -1;
+                    if (it >= T.dtotal) continue;
+                    int lo = 0, hi = nent_d - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+                    }
+                    k_u[u] = lo / 27;
+                    j_u[u] = d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + (it - s_off[lo])];
                 }
-                const int k = lo / 27;
-                const int j = d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + (it - s_off[lo])];
-                if (j == T.idx[0] || (T.nch == 2 && j == T.idx[1])) continue;
-                const int gj = D.slot_off + j;
-                const float4 pj = d.posq[gj];
-                const int c = desc_class(d.flags[gj], pj.w);
-                if (c < 0) continue;
-                const float4 p = T.dpos[k];
-                const int sh = shell_of(min_image_rn(__fsub_rn(pj.x, p.x), D.L[0]), min_image_rn(__fsub_rn(pj.y, p.y), D.L[1]),
-                                        min_image_rn(__fsub_rn(pj.z, p.z), D.L[2]));
-                if (sh < SUR_SHELLS) atomicAdd(&s_hist[k * (SUR_SHELLS * SUR_CLASSES) + sh * SUR_CLASSES + c], 1);
+                float4 p_u[RP];
+                int f_u[RP];
+#pragma unroll
+                for (int u = 0; u < RP; ++u) {
+                    const int j = j_u[u];
+                    f_u[u] = PHMC_F_GHOST;
+                    if (j < 0 || j == T.idx[0] || (T.nch == 2 && j == T.idx[1])) continue;
+                    p_u[u] = d.posq[D.slot_off + j];
+                    f_u[u] = d.flags[D.slot_off + j];
+                }
+#pragma unroll
+                for (int u = 0; u < RP; ++u) {
+                    if (f_u[u] & PHMC_F_GHOST) continue;
+                    const float4 pj = p_u[u];
+                    const int c = desc_class(f_u[u], pj.w);
+                    if (c < 0) continue;
+                    const float4 p = T.dpos[k_u[u]];
+                    const int sh = shell_of(min_image_rn(__fsub_rn(pj.x, p.x), D.L[0]), min_image_rn(__fsub_rn(pj.y, p.y), D.L[1]),
+                                            min_image_rn(__fsub_rn(pj.z, p.z), D.L[2]));
+                    if (sh < SUR_SHELLS) atomicAdd(&s_hist[k_u[u] * (SUR_SHELLS * SUR_CLASSES) + sh * SUR_CLASSES + c], 1);
+                }
             }
             __syncthreads();
             // (c) rows: raw features, and standardised BF16 inputs when the network runs
-            __nv_bfloat16* act0 = reinterpret_cast<__nv_bfloat16*>(s_pair);
-            __nv_bfloat16* act1 = act0 + 16 * SUR_AST;
             for (int e = tid; e < T.nrows * SUR_K; e += NT) {
                 const int rr = e / SUR_K, f = e - rr * SUR_K;
                 const int k = T.row_k[rr];
@@ -606,11 +689,14 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                 else if (f == 70) v = D.sur_salt;
                 else v = 0.0f;
                 s_rows[rr][f] = v;
-                if (T.da) act0[rr * SUR_AST + f] = __float2bfloat16(__fdiv_rn(__fsub_rn(v, __ldg(&d.sur.mu[f])), __ldg(&d.sur.sd[f])));
+                if (T.da) act0[rr * SUR_AST + f] = __float2bfloat16(__fdiv_rn(__fsub_rn(v, s_mu[f]), s_sd[f]));
             }
             __syncthreads();
             // (d) network on the rows (tensor cores), first-stage decision
-            if (T.da) sur_forward_rows<NT>(d.sur, T.nrows, act0, act1, s_F);
+            if (T.da) {
+                sur_forward_staged<NT>(d.sur, T.nrows, act0, act1, wa, wb, wc, s_mbar, sur_par, s_F, &s_sfail);
+                sur_par ^= 1u;
+            }
             if (tid == 0) {
                 if (mode == MC_RUN) S.alg_bytes += 16.0 * T.nch * nc3 + 24.0 * T.dtotal;
                 double net = 0.0;
@@ -624,7 +710,10 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                     }
                     T.dEs = (net + T.cross) + T.dmom;
                 }
-                if (mode == MC_DESCRIBE) {
+                if (T.da && s_sfail) {  // a staged copy never arrived: stop this replica
+                    S.error = PHMC_ERR_BUDGET;
+                    T.skip = 6;
+                } else if (mode == MC_DESCRIBE) {
                     float* o = d.dsc_out + (size_t)T.ext_k * DSC_STRIDE;
                     for (int e = 0; e < SUR_ROWS * SUR_K; ++e) o[e] = (e / SUR_K < T.nrows) ? s_rows[e / SUR_K][e % SUR_K] : 0.0f;
                     for (int rr = 0; rr < SUR_ROWS; ++rr) {
@@ -638,8 +727,7 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
                     T.skip = 5;
                 } else if (T.da) {
                     // first stage: Metropolis on the surrogate dE with its own uniform (Philox counter (t, 3))
-                    uint32_t w4[4];
-                    philox4x32_10(D.key[0], D.key[1], (uint32_t)T.tnum, (uint32_t)((unsigned long long)T.tnum >> 32), 3u, 0u, w4);
+                    const uint32_t* w4 = s_rng[T.tnum - s_rng_base] + 12;
                     const double expo1 = -D.beta * T.dEs + T.logf;
                     const bool pass = (expo1 >= 0.0) || (u53(w4[0], w4[1]) < exp(expo1));
                     S.da_eval++;
@@ -1025,7 +1113,7 @@ __global__ void __launch_bounds__(NT) k_mc(DevPtrs d, int mode, int ext_rep, con
 
 template <int P, int NT>
 static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
-    const size_t smem = mc_smem_bytes(P, E.pend_max);
+    const size_t smem = mc_smem_bytes(P, E.pend_max, E.d.sur.H > 0);
     const int grid = (mode == MC_RUN) ? E.R : 1;
     k_mc<P, NT><<<grid, NT, smem, st>>>(E.d, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
@@ -1042,7 +1130,7 @@ static cudaError_t prepare_mc_t(Engine& E) {
     e = cudaFuncGetAttributes(&fa, k_mc<P, NT>);
     if (e != cudaSuccess) return e;
     const int cap = optin - (int)fa.sharedSizeBytes;
-    if ((size_t)cap < mc_smem_bytes(P, E.pend_max)) return cudaErrorInvalidValue;
+    if ((size_t)cap < mc_smem_bytes(P, E.pend_max, true)) return cudaErrorInvalidValue;
     return cudaFuncSetAttribute(k_mc<P, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
 }
 
@@ -1055,7 +1143,7 @@ cudaError_t prepare_mc(Engine& E) {
     }
 }
 
-size_t mc_smem_bytes(int order, int pend_max) {
+size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate) {
     size_t st = 0, pk = 0;
     switch (order) {
         case 4: st = sizeof(Stencil<4>); pk = sizeof(PairK<4>); break;
@@ -1065,9 +1153,8 @@ size_t mc_smem_bytes(int order, int pend_max) {
     // Monte Carlo trials carry <= 2 stencils against <= pend_max pending ones;
     // external trials (<= NST_MAX stencils) always start with none pending
     const size_t npairs = std::max((size_t)2 * pend_max + 3, (size_t)(NST_MAX * (NST_MAX + 1) / 2));
-    // the pair tables' space also holds the surrogate's two 16-row BF16 activation buffers
-    const size_t act = 2 * 16 * SUR_AST * sizeof(__nv_bfloat16);
-    return st * (pend_max + NST_MAX) + std::max(pk * npairs, act);
+    // with a surrogate attached the pair tables' space also holds its activations and staged weights
+    return st * (pend_max + NST_MAX) + std::max(pk * npairs, staged_surrogate ? (size_t)SUR_SMEM_BYTES : (size_t)0);
 }
 
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {

@@ -60,29 +60,75 @@ __device__ __forceinline__ float sur_out_dot(const __nv_bfloat16* h, const uint1
     return v;
 }
 
-// Network outputs (energy units) of rows 0..nrows-1 (nrows <= 8) held,
-// standardised, in `buf0` (bf16, row stride SUR_AST).  `buf1` is a second
-// buffer of 16 rows.  Called by all threads of the block; ends synchronised.
+// ---- bulk asynchronous copies (global -> this block's shared memory) ----
+__device__ __forceinline__ void sur_mbar_init(uint64_t* mbar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// One thread: order earlier generic accesses of the block (made visible by a
+// preceding __syncthreads) before the async copy, then copy `bytes` (multiple
+// of 16, both addresses 16-byte aligned) and count them on `mbar`.
+__device__ __forceinline__ void sur_bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    const uint32_t m = (uint32_t)__cvta_generic_to_shared(mbar);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(m), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(bytes), "r"(m)
+                 : "memory");
+}
+// Bounded wait for the completion of the phase with parity `parity`; false when the bound ran out.
+__device__ __forceinline__ bool sur_mbar_wait(uint64_t* mbar, uint32_t parity) {
+    const uint32_t m = (uint32_t)__cvta_generic_to_shared(mbar);
+    for (int it = 0; it < (1 << 20); ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(m), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__host__ __device__ inline uint32_t sur_layer_bytes(int K, int H) { return (uint32_t)K * (uint32_t)H * 2u; }
+
+// Shared-memory layout of the staged first stage: two 16-row activation
+// buffers, then the three hidden layers' weights (SUR_K x SUR_HMAX, then two
+// SUR_HMAX x SUR_HMAX, BF16, fragment-packed).
+#define SUR_ACT_BYTES (2 * 16 * SUR_AST * 2)
+#define SUR_WBUF_BYTES (SUR_HMAX * SUR_HMAX * 2)
+#define SUR_SMEM_BYTES (128 + SUR_ACT_BYTES + SUR_K * SUR_HMAX * 2 + 2 * SUR_WBUF_BYTES)
+
+// The caller's thread 0 has issued layer l -> w_l on mbar[l] (l = 0, 1, 2), each
+// barrier in the phase of parity `par`.  Computes the outputs (energy units) of
+// rows 0..nrows-1 (nrows <= 8) held, standardised, in buf0.  Returns false
+// (every thread) when a copy did not arrive within the bound.
 template <int NT>
-__device__ void sur_forward_rows(const SurDev& s, int nrows, __nv_bfloat16* buf0, __nv_bfloat16* buf1, float* out) {
+__device__ bool sur_forward_staged(const SurDev& s, int nrows, __nv_bfloat16* buf0, __nv_bfloat16* buf1, const uint2* wa,
+                                   const uint2* wb, const uint2* wc, uint64_t* mbar, uint32_t par, float* out, int* s_fail) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
     __nv_bfloat16* in = buf0;
     __nv_bfloat16* ot = buf1;
     int K = SUR_K;
     for (int l = 0; l < 3; ++l) {
+        const uint2* w = (l == 0) ? wa : (l == 1 ? wb : wc);
+        bool ok = sur_mbar_wait(&mbar[l], par);
+        if (!ok) ok = sur_mbar_wait(&mbar[l], par);  // a second bounded wait for the copy in flight
+        if (!ok) *s_fail = 1;
         const int nks = K >> 4;
         for (int cg = warp; cg < (s.H >> 4); cg += NT / 32) {
             float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll 4
             for (int ks = 0; ks < nks; ++ks) {
-                // rows g and g + 8 of the 16-row tile; rows >= nrows only feed discarded outputs
                 const __nv_bfloat16* p0 = in + g * SUR_AST + ks * 16 + 2 * t4;
                 uint32_t a[4];
                 a[0] = *reinterpret_cast<const uint32_t*>(p0);
                 a[1] = *reinterpret_cast<const uint32_t*>(p0 + 8 * SUR_AST);
                 a[2] = *reinterpret_cast<const uint32_t*>(p0 + 8);
                 a[3] = *reinterpret_cast<const uint32_t*>(p0 + 8 * SUR_AST + 8);
-                const uint2* wp = s.w[l] + sur_pack_index(cg, ks, 0, lane, nks);
-                const uint2 b0 = __ldg(wp), b1 = __ldg(wp + 32);
+                const uint2* wp = w + sur_pack_index(cg, ks, 0, lane, nks);
+                const uint2 b0 = wp[0], b1 = wp[32];
                 sur_mma(acc[0], a, b0.x, b0.y);
                 sur_mma(acc[1], a, b1.x, b1.y);
             }
@@ -106,4 +152,5 @@ __device__ void sur_forward_rows(const SurDev& s, int nrows, __nv_bfloat16* buf0
         if (lane == 0) out[warp] = __fmaf_rn(v + __ldg(s.b4), s.scale, s.offset);
     }
     __syncthreads();
+    return *s_fail == 0;
 }

@@ -99,6 +99,23 @@ class Engine:
         self._replay = np.ascontiguousarray(decisions, np.int32)
         _abi.check(self._lib.phmc_set_replay(self._h, len(self._replay), _abi.iptr(self._replay)))
 
+    def set_tuning(self, pending_max, threads):
+        _abi.check(self._lib.phmc_set_tuning(self._h, int(pending_max), int(threads)))
+
+    def tuning(self):
+        t = _abi.Tuning()
+        _abi.check(self._lib.phmc_get_tuning(self._h, C.byref(t)))
+        return t.asdict()
+
+    def autotune(self, trials):
+        res = (_abi.Tuning * 32)()
+        n = C.c_int()
+        _abi.check(self._lib.phmc_autotune(self._h, int(trials), res, 32, C.byref(n)))
+        return [res[k].asdict() for k in range(min(n.value, 32))]
+
+    def set_move_mix(self, p_disp, p_titr, p_swap=0.0, replica=-1):
+        _abi.check(self._lib.phmc_set_move_mix(self._h, int(replica), float(p_disp), float(p_titr), float(p_swap)))
+
     # ---- state ----
     def state(self, replica=0):
         n = self.caps[replica]

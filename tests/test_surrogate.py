@@ -227,16 +227,24 @@ def _oracle_rows(st, geo, trial):
     return SO.descriptor(st, geo, ch)
 
 
+def _small_four_cells():
+    # 12 x 12 sigma lateral box: 4 cells per axis, fewer than the 8-sigma window's 7
+    s, p = configs.small_system(seed=71, chains=3, length=12, box_xy=12.0, height=14.0, salt_pairs=8)
+    return s, p
+
+
 @pytest.mark.gpu
-def test_descriptor_rows_match_oracle_bit_for_bit():
-    s, p = configs.config1(seed=31)
+@pytest.mark.parametrize("case", ["config1", "four_cells"])
+def test_descriptor_rows_match_oracle_bit_for_bit(case):
+    s, p = configs.config1(seed=31) if case == "config1" else _small_four_cells()
+    height = float(s.meta["height"])
     rng = np.random.default_rng(15)
     with Engine(s, p) as e:
         e.run(20000)  # move away from the generated state
         st = e.state()
         _, dims = e.cells()
         geo = SO.Geometry(s.box, dims, p)
-        trials = _move_trials(st, s.box, 40.0, rng)
+        trials = _move_trials(st, s.box, height, rng)
         out = e.describe(trials)
     for t, o in zip(trials, out):
         rows, sg, nr = _oracle_rows(st, geo, t)

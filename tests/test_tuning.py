@@ -1,0 +1,62 @@
+"""Tuning: the pending-stencil capacity and the block size change between runs
+without changing the physics, and the autotuner keeps the fastest candidate."""
+import numpy as np
+import pytest
+
+from ph_brush_b200 import Engine, _abi, configs
+
+
+@pytest.mark.gpu
+def test_retuning_keeps_tracked_energy_consistent():
+    s, p = configs.config1(seed=51)
+    with Engine(s, p) as e:
+        for pend, th in ((8, 128), (64, 256), (16, 256), (48, 128)):
+            e.set_tuning(pend, th)
+            assert e.tuning()["pending_max"] == pend and e.tuning()["threads"] == th
+            st = e.run(3000)[0]
+            fresh = e.energy()[0]["total"]
+            assert abs(st["energy"] - fresh) <= 1e-6 * abs(fresh) + 1e-3, (pend, th, st["energy"], fresh)
+
+
+@pytest.mark.gpu
+def test_tuning_leaves_the_trial_stream_unchanged_on_a_short_run():
+    """Same seed, different tuning: the same proposals; decisions agree unless a dE
+    sits within FP32 rounding of its acceptance threshold (none on a short run)."""
+    s, p = configs.config1(seed=52)
+    logs = []
+    for pend, th in ((8, 128), (48, 256)):
+        with Engine(s, p) as e:
+            e.set_tuning(pend, th)
+            log = e.set_trial_log(4000)
+            e.run(4000)
+            logs.append((log[0].copy(), log[1].copy(), log[2].copy()))
+    (m0, d0, a0), (m1, d1, a1) = logs
+    assert np.array_equal(m0, m1)
+    assert np.array_equal(a0, a1)
+    fin = np.isfinite(d0) & np.isfinite(d1)
+    assert np.allclose(d0[fin], d1[fin], rtol=1e-5, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_the_fastest_candidate():
+    S, P = [], []
+    for k in range(4):
+        s, p = configs.config1(seed=60 + k)
+        S.append(s)
+        P.append(p)
+    with Engine(S, P) as e:
+        res = e.autotune(1500)
+        assert len(res) >= 10
+        best = min(res, key=lambda r: r["us_per_trial"])
+        t = e.tuning()
+        assert (t["pending_max"], t["threads"]) == (best["pending_max"], best["threads"])
+        st = e.run(2000)
+        fresh = e.energy()
+        for a, b in zip(st, fresh):
+            assert abs(a["energy"] - b["total"]) <= 1e-6 * abs(b["total"]) + 1e-3
+
+
+def test_tuning_arguments_are_checked_without_a_gpu():
+    lib = _abi.lib()
+    assert lib.phmc_set_tuning(None, 16, 256) != 0
+    assert lib.phmc_autotune(None, 100, None, 0, None) != 0
