@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--da-threshold", type=float, default=0.3)
     ap.add_argument("--no-alpha", action="store_true")
+    ap.add_argument("--batched-replicas", type=int, default=256)
+    ap.add_argument("--tuning", default=None, help="pending_max,threads instead of the autotuner (for profiling)")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="only the config-5 batched section (its own JSON object; for profiling)")
     ap.add_argument("--alpha-eq", type=int, default=300, help="sweeps of equilibration in the alpha(pH) check")
     ap.add_argument("--alpha-sample", type=int, default=200, help="sweeps sampled in the alpha(pH) check")
     return ap.parse_args()
@@ -158,6 +162,15 @@ def cpu_baseline(s, p, seconds):
             "trials_per_s": tps}
 
 
+def tune_engine(eng, args, trials):
+    """Autotune (pending capacity x block size), or apply --tuning."""
+    if args.tuning:
+        pm, th = (int(v) for v in args.tuning.split(","))
+        eng.set_tuning(pm, th)
+        return None
+    return eng.autotune(trials)
+
+
 def _alpha(stats, n_sites):
     return [st["n_charged_sites"] / n for st, n in zip(stats, n_sites)]
 
@@ -234,7 +247,7 @@ def run_batched(args, local, n_rep=256, trials=400, plain_samples=3):
     ns = [s.n for s, _ in reps]
     n_sites = [int(s.meta["n_sites"]) for s, _ in reps]
     eng = Engine([s for s, _ in reps], [p for _, p in reps], device=local)
-    tune = eng.autotune(trials)
+    tune = tune_engine(eng, args, trials)
     tuned = eng.tuning()
     eng.run(trials // 4)
     eng.set_profiling(True)
@@ -252,7 +265,7 @@ def run_batched(args, local, n_rep=256, trials=400, plain_samples=3):
     for r in pick:
         s, p = reps[r]
         e1 = Engine(s, p, device=local)
-        e1.autotune(trials)
+        tune_engine(e1, args, trials)
         e1.run(trials // 4)
         e1.flush_l2(256 << 20)
         t = e1.run_timed(trials) / 1e3 / trials
@@ -390,7 +403,7 @@ def run_ours(args):
     s, p = configs.config2(seed=2026 + rank)
     N = s.n
     eng = Engine(s, p, device=local)
-    tune = eng.autotune(max(2000, N // 4))
+    tune = tune_engine(eng, args, max(2000, N // 4))
     tuned = eng.tuning()
     for _ in range(args.warmup):
         eng.run(N)
@@ -468,7 +481,7 @@ def run_ours(args):
             "clocks": clk}
     eng.close()
     if rank == 0 and world == 1 and not args.no_batched:
-        line["batched"] = run_batched(args, local)
+        line["batched"] = run_batched(args, local, n_rep=args.batched_replicas)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(s, p, args.cpu_seconds)
     if world > 1:
@@ -480,6 +493,9 @@ def run_ours(args):
 
 def main():
     args = parse()
+    if args.batched_only:
+        print(json.dumps({"batched": run_batched(args, dist_env()[2], n_rep=args.batched_replicas)}))
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

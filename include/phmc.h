@@ -176,6 +176,11 @@ int phmc_energy(phmc_engine* e, phmc_energy_components* out);
  * No counterpart in the reference (it recomputes the total per trial). */
 int phmc_delta_energy(phmc_engine* e, int replica, const phmc_trial* trials, int n, double* dE);
 
+/* phmc_delta_energy split into the components of phmc_energy_components (total
+ * = their sum); lets a caller keep the reference's separate LJ and Coulomb sums. */
+int phmc_delta_energy_components(phmc_engine* e, int replica, const phmc_trial* trials, int n,
+                                 phmc_energy_components* out);
+
 /* Apply one trial to replica r (state, cell list, pending mesh changes). */
 int phmc_commit(phmc_engine* e, int replica, const phmc_trial* trial);
 

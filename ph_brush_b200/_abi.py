@@ -114,7 +114,7 @@ EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy",
            "phmc_surrogate_train", "phmc_surrogate_save", "phmc_surrogate_load", "phmc_harvest",
            "phmc_harvest_count", "phmc_harvest_get", "phmc_surrogate_fit", "phmc_surrogate_attach",
            "phmc_get_da_stats", "phmc_surrogate_describe", "phmc_set_da_log", "phmc_set_move_mix",
-           "phmc_set_tuning", "phmc_get_tuning", "phmc_autotune"]
+           "phmc_set_tuning", "phmc_get_tuning", "phmc_autotune", "phmc_delta_energy_components"]
 
 
 def load_library(path=LIB_PATH):
@@ -169,6 +169,7 @@ def load_library(path=LIB_PATH):
         "phmc_set_da_log": ([eng, _ip, _dp], C.c_int),
         "phmc_set_move_mix": ([eng, C.c_int, C.c_double, C.c_double, C.c_double], C.c_int),
         "phmc_set_tuning": ([eng, C.c_int, C.c_int], C.c_int),
+        "phmc_delta_energy_components": ([eng, C.c_int, C.POINTER(Trial), C.c_int, C.POINTER(EnergyComponents)], C.c_int),
         "phmc_get_tuning": ([eng, C.POINTER(Tuning)], C.c_int),
         "phmc_autotune": ([eng, C.c_int64, C.POINTER(Tuning), C.c_int, _ip], C.c_int),
     }

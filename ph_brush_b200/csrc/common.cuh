@@ -131,6 +131,8 @@ struct DevPtrs {
     float* hv_rows; float* hv_sign; float* hv_target; int* hv_count; int hv_cap;
     // descriptor output of MC_DESCRIBE launches (DSC_STRIDE floats per trial)
     float* dsc_out;
+    // per external trial dE components (lj, fene, coul_real, coul_recip, self, qcorr, slab), or null
+    double* ext_comp;
 };
 
 #define DSC_STRIDE (SUR_ROWS * SUR_K + 2 * SUR_ROWS + 4)

@@ -1177,3 +1177,33 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     if (n_results) *n_results = n;
     return apply_tuning(h, best_p, best_t);
 }
+
+extern "C" int phmc_delta_energy_components(phmc_engine* h, int rep, const phmc_trial* trials, int n,
+                                            phmc_energy_components* out) {
+    if (!h || (n > 0 && (!trials || !out))) return fail(PHMC_ERR_ARG, "null argument");
+    if (n == 0) return PHMC_OK;
+    int s = check_trials(h, rep, trials, n);
+    if (s) return s;
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    s = ensure_trial_buffers(h, n);
+    if (s) return s;
+    double* d_c = nullptr;
+    CU(cudaMalloc((void**)&d_c, sizeof(double) * 7 * (size_t)n));
+    cudaError_t e = cudaMemcpyAsync(h->d_trials, trials, sizeof(phmc_trial) * n, cudaMemcpyHostToDevice, E.stream);
+    E.d.ext_comp = d_c;
+    if (e == cudaSuccess) e = launch_mc(E, MC_EVAL, rep, h->d_trials, n, h->d_dE, E.stream);
+    E.d.ext_comp = nullptr;
+    std::vector<double> hc((size_t)7 * n), dE((size_t)n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hc.data(), d_c, sizeof(double) * 7 * n, cudaMemcpyDeviceToHost, E.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dE.data(), h->d_dE, sizeof(double) * n, cudaMemcpyDeviceToHost, E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    cudaFree(d_c);
+    if (e != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string("delta_energy_components: ") + cudaGetErrorString(e));
+    for (int k = 0; k < n; ++k) {
+        const double* c = hc.data() + 7 * k;
+        out[k].lj = c[0]; out[k].fene = c[1]; out[k].coul_real = c[2]; out[k].coul_recip = c[3];
+        out[k].self = c[4]; out[k].qcorr = c[5]; out[k].slab = c[6]; out[k].total = dE[(size_t)k];
+    }
+    return check_kernel_errors(h);
+}

@@ -1023,6 +1023,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 accept = 1;
                 if (ext_dE) ext_dE[T.ext_k] = dE;
             }
+            if (mode != MC_RUN && d.ext_comp) {
+                double* o = d.ext_comp + (size_t)T.ext_k * 7;
+                o[0] = dlj; o[1] = T.d_fene; o[2] = dc; o[3] = acc_rec; o[4] = dself; o[5] = dqc; o[6] = dslab;
+            }
             if (mode != MC_RUN) T.ext_k++;
             if (accept) {
                 if (mode == MC_RUN) S.acc[T.move]++;

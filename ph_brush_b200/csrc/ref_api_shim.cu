@@ -1,0 +1,395 @@
+// The reference's energy-layer API over the phmc C ABI.
+//
+// Implements the functions declared in the reference headers
+//   MC/include/energy.hpp:7-18    compute_lj_sr_energy_gpu, compute_coul_sr_energy_gpu
+//   MC/include/pme.hpp:42-49      pmeCreate, pmeDestroy, pmeEnergy
+//   MC/include/neighbor.hpp:6-13  copy_csr_to_device, build_half_neighbors_gpu
+// so that the reference's own driver and move loops (MC/src/main.cu, MC/src/mc.cu,
+// MC/src/io.cpp, MC/src/report.cpp) link against libphmc.so in place of its
+// energy sources (MC/src/energy_gpu.cu, pme.cu, neighbor.cu).  Compiled against the
+// reference headers (-I<reference>/MC/include) with the reference's precision macro.
+//
+// The reference keeps atom positions fixed and changes identities (type, q) between
+// energy calls with plain device writes (set_atom_identity, MC/src/mc.cu:33-41).
+// One engine mirrors the atoms: each energy call finds the changed atoms with a
+// device comparison against the engine's committed state; up to two changed atoms
+// are evaluated as one trial against that state (one MC-kernel launch, no mesh
+// rebuild); more changes, or moved atoms, are uploaded as a new state (full
+// recompute).  The model is the reference's: LJ cut and shifted at rc, 1-2 bonded
+// pairs excluded from LJ and Coulomb, cubic-or-higher SPME with the reference's
+// moduli and mesh rule, slab correction when pme_3dc is on.
+#include <cuda_runtime.h>
+#include <thrust/copy.h>
+#include <thrust/device_vector.h>
+#include <thrust/host_vector.h>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "energy.hpp"
+#include "neighbor.hpp"
+#include "pme.hpp"
+#include "phmc.h"
+
+namespace {
+
+void ck(int s, const char* what) {
+    if (s != PHMC_OK) throw std::runtime_error(std::string(what) + ": " + phmc_last_error());
+}
+void cu(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// smallest 2^a 3^b 5^c >= max(8, n) searched up to max(16, 2n + 32) (MC/src/pme.cu:46-51)
+int fft_dim(int n) {
+    const int nmax = std::max(16, n * 2 + 32);
+    for (int m = std::max(8, n); m <= nmax; ++m) {
+        int k = m;
+        for (int p : {2, 3, 5})
+            while (k % p == 0) k /= p;
+        if (k == 1) return m;
+    }
+    return n;
+}
+
+// erfc(alpha rc) = rtol by bisection (used only when the caller left ewald_alpha unset)
+double alpha_from_rtol(double rc, double rtol) {
+    double lo = 0.0, hi = 10.0 / rc;
+    for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (std::erfc(mid * rc) > rtol) lo = mid; else hi = mid;
+    }
+    return 0.5 * (lo + hi);
+}
+
+template <typename T>
+__global__ void k_shim_diff(int n, const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
+                            const T* __restrict__ q, const int* __restrict__ t, const float* __restrict__ mx,
+                            const float* __restrict__ my, const float* __restrict__ mz, const float* __restrict__ mq,
+                            const int* __restrict__ mt, int* __restrict__ idx, int* __restrict__ cnt, int cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool moved = (float)x[i] != mx[i] || (float)y[i] != my[i] || (float)z[i] != mz[i];
+    const bool ident = (float)q[i] != mq[i] || t[i] != mt[i];
+    if (moved) atomicOr(&cnt[1], 1);
+    if (moved || ident) {
+        const int k = atomicAdd(&cnt[0], 1);
+        if (k < cap) idx[k] = i;
+    }
+}
+
+template <typename T>
+__global__ void k_shim_mirror(int n, const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
+                              const T* __restrict__ q, const int* __restrict__ t, float* mx, float* my, float* mz,
+                              float* mq, int* mt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    mx[i] = (float)x[i]; my[i] = (float)y[i]; mz[i] = (float)z[i]; mq[i] = (float)q[i]; mt[i] = t[i];
+}
+
+// pairs i < j with r <= rc (minimum image on all axes), 1-2 bonded pairs excluded (MC/src/neighbor.cu:74-125)
+template <typename T>
+__global__ void k_shim_count_pairs(int n, const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
+                                   T Lx, T Ly, T Lz, T rc2, const int* __restrict__ head, const int* __restrict__ list,
+                                   unsigned long long* count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long c = 0;
+    for (int j = i + 1; j < n; ++j) {
+        T dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+        dx -= Lx * rint(dx / Lx); dy -= Ly * rint(dy / Ly); dz -= Lz * rint(dz / Lz);
+        if (dx * dx + dy * dy + dz * dz > rc2) continue;
+        bool bonded = false;
+        if (head)
+            for (int k = head[i]; k < head[i + 1]; ++k)
+                if (list[k] == j) { bonded = true; break; }
+        if (!bonded) ++c;
+    }
+    atomicAdd(count, c);
+}
+
+struct Shim {
+    phmc_engine* eng = nullptr;
+    int n = 0;
+    // SPME settings (pmeCreate)
+    bool pme = false;
+    int mesh[3] = {0, 0, 0};
+    int order = 4;
+    double alpha = 0.0;
+    bool slab = false;
+    // 1-2 bonds (copy_csr_to_device)
+    std::vector<int> bi, bj;
+    // device mirror of the committed state
+    float *mx = nullptr, *my = nullptr, *mz = nullptr, *mq = nullptr;
+    int* mt = nullptr;
+    int* d_idx = nullptr;
+    int* d_cnt = nullptr;
+    phmc_energy_components base{};
+    // the last evaluated difference (reused by the next energy call when unchanged)
+    int last_n = -1;
+    int last_idx[2] = {-1, -1};
+    float last_q[2] = {0, 0};
+    int last_t[2] = {0, 0};
+    phmc_energy_components cur{};
+};
+Shim g;
+
+void release() {
+    if (g.eng) phmc_destroy(g.eng);
+    for (void* p : {(void*)g.mx, (void*)g.my, (void*)g.mz, (void*)g.mq, (void*)g.mt, (void*)g.d_idx, (void*)g.d_cnt})
+        if (p) cudaFree(p);
+    const bool pme = g.pme;
+    const int mesh[3] = {g.mesh[0], g.mesh[1], g.mesh[2]};
+    const int order = g.order;
+    const double alpha = g.alpha;
+    const bool slab = g.slab;
+    std::vector<int> bi = g.bi, bj = g.bj;
+    g = Shim();
+    g.pme = pme; g.order = order; g.alpha = alpha; g.slab = slab;
+    for (int k = 0; k < 3; ++k) g.mesh[k] = mesh[k];
+    g.bi = bi; g.bj = bj;
+}
+
+template <typename V>
+std::vector<double> to_host(const V& v) {
+    thrust::host_vector<real> h(v.begin(), v.end());
+    return std::vector<double>(h.begin(), h.end());
+}
+
+void upload_state(const DeviceAtoms& a) {
+    thrust::host_vector<real> x(a.x.begin(), a.x.end()), y(a.y.begin(), a.y.end()), z(a.z.begin(), a.z.end()),
+        q(a.q.begin(), a.q.end());
+    thrust::host_vector<int> t(a.type.begin(), a.type.end());
+    std::vector<float> fx(g.n), fy(g.n), fz(g.n), fq(g.n);
+    std::vector<int> ti(t.begin(), t.end()), fl((size_t)g.n, 0);
+    for (int i = 0; i < g.n; ++i) { fx[i] = (float)x[i]; fy[i] = (float)y[i]; fz[i] = (float)z[i]; fq[i] = (float)q[i]; }
+    ck(phmc_set_state(g.eng, 0, fx.data(), fy.data(), fz.data(), fq.data(), ti.data(), fl.data()), "phmc_set_state");
+}
+
+void mirror(const DeviceAtoms& a) {
+    k_shim_mirror<real><<<(g.n + 255) / 256, 256>>>(g.n, thrust::raw_pointer_cast(a.x.data()), thrust::raw_pointer_cast(a.y.data()),
+                                                    thrust::raw_pointer_cast(a.z.data()), thrust::raw_pointer_cast(a.q.data()),
+                                                    thrust::raw_pointer_cast(a.type.data()), g.mx, g.my, g.mz, g.mq, g.mt);
+    cu(cudaDeviceSynchronize(), "shim mirror");
+}
+
+void ensure_engine(const DeviceAtoms& a, const DeviceParams& dp, const Box& box) {
+    if (g.eng) return;
+    g.n = (int)a.x.size();
+    if (g.n <= 0) throw std::runtime_error("phmc shim: no atoms");
+    const int T = dp.ntypes;
+    std::vector<double> eps = to_host(dp.lj_eps), sig = to_host(dp.lj_sig);
+    if ((int)eps.size() != T * T || (int)sig.size() != T * T) throw std::runtime_error("phmc shim: LJ tables must be ntypes^2");
+    thrust::host_vector<real> x(a.x.begin(), a.x.end()), y(a.y.begin(), a.y.end()), z(a.z.begin(), a.z.end()),
+        q(a.q.begin(), a.q.end());
+    thrust::host_vector<int> t(a.type.begin(), a.type.end());
+    std::vector<float> fx(g.n), fy(g.n), fz(g.n), fq(g.n);
+    std::vector<int> ti(t.begin(), t.end()), fl((size_t)g.n, 0);
+    for (int i = 0; i < g.n; ++i) { fx[i] = (float)x[i]; fy[i] = (float)y[i]; fz[i] = (float)z[i]; fq[i] = (float)q[i]; }
+    phmc_system s;
+    std::memset(&s, 0, sizeof s);
+    s.n_particles = g.n; s.capacity = g.n;
+    s.x = fx.data(); s.y = fy.data(); s.z = fz.data(); s.q = fq.data(); s.type = ti.data(); s.flags = fl.data();
+    s.n_bonds = (int)g.bi.size(); s.bond_i = g.bi.data(); s.bond_j = g.bj.data();
+    s.box[0] = box.Lx; s.box[1] = box.Ly; s.box[2] = box.Lz;
+    phmc_params p;
+    std::memset(&p, 0, sizeof p);
+    p.n_types = T; p.lj_eps = eps.data(); p.lj_sig = sig.data(); p.lj_rc = nullptr; p.rc_lj = dp.rc;
+    p.lj_shift = dp.lj_shift ? 1 : 0;
+    if (dp.coulombtype == "pme") {
+        if (!g.pme) throw std::runtime_error("phmc shim: pmeEnergy needs pmeCreate first");
+        p.coulomb = PHMC_COUL_EWALD;
+        for (int k = 0; k < 3; ++k) p.mesh[k] = g.mesh[k];
+        p.order = g.order; p.ewald_alpha = g.alpha; p.slab = g.slab ? 1 : 0;
+    } else if (dp.coulombtype == "coul_cut") {
+        p.coulomb = PHMC_COUL_CUT;
+    } else {
+        throw std::runtime_error("phmc shim: unsupported coulombtype " + dp.coulombtype);
+    }
+    p.rc_coul = dp.rc; p.epsilon_r = dp.epsilon_r; p.ref_moduli = 1;
+    p.excl_bonded_lj = 1; p.excl_bonded_coul = 1;
+    p.beta = 1.0; p.seed = 1;
+    int dev = 0;
+    cu(cudaGetDevice(&dev), "cudaGetDevice");
+    ck(phmc_create(1, &s, &p, dev, &g.eng), "phmc_create");
+    ck(phmc_energy(g.eng, &g.base), "phmc_energy");
+    cu(cudaMalloc((void**)&g.mx, sizeof(float) * g.n), "cudaMalloc");
+    cu(cudaMalloc((void**)&g.my, sizeof(float) * g.n), "cudaMalloc");
+    cu(cudaMalloc((void**)&g.mz, sizeof(float) * g.n), "cudaMalloc");
+    cu(cudaMalloc((void**)&g.mq, sizeof(float) * g.n), "cudaMalloc");
+    cu(cudaMalloc((void**)&g.mt, sizeof(int) * g.n), "cudaMalloc");
+    cu(cudaMalloc((void**)&g.d_idx, sizeof(int) * 2), "cudaMalloc");
+    cu(cudaMalloc((void**)&g.d_cnt, sizeof(int) * 2), "cudaMalloc");
+    mirror(a);
+    g.cur = g.base;
+    g.last_n = 0;
+}
+
+// Energy components of the atoms' current state.
+const phmc_energy_components& evaluate(const DeviceAtoms& a, const DeviceParams& dp, const Box& box) {
+    ensure_engine(a, dp, box);
+    if ((int)a.x.size() != g.n) throw std::runtime_error("phmc shim: the number of atoms changed");
+    cu(cudaMemset(g.d_cnt, 0, sizeof(int) * 2), "cudaMemset");
+    k_shim_diff<real><<<(g.n + 255) / 256, 256>>>(g.n, thrust::raw_pointer_cast(a.x.data()), thrust::raw_pointer_cast(a.y.data()),
+                                                  thrust::raw_pointer_cast(a.z.data()), thrust::raw_pointer_cast(a.q.data()),
+                                                  thrust::raw_pointer_cast(a.type.data()), g.mx, g.my, g.mz, g.mq, g.mt,
+                                                  g.d_idx, g.d_cnt, 2);
+    int cnt[2] = {0, 0};
+    cu(cudaMemcpy(cnt, g.d_cnt, sizeof cnt, cudaMemcpyDeviceToHost), "shim diff");
+    if (cnt[0] == 0) {
+        g.last_n = 0;
+        g.cur = g.base;
+        return g.cur;
+    }
+    if (cnt[0] <= 2 && !cnt[1]) {
+        int idx[2] = {-1, -1};
+        cu(cudaMemcpy(idx, g.d_idx, sizeof(int) * cnt[0], cudaMemcpyDeviceToHost), "shim diff");
+        if (cnt[0] == 2 && idx[0] > idx[1]) std::swap(idx[0], idx[1]);
+        real qv[2] = {0, 0};
+        int tv[2] = {0, 0};
+        for (int k = 0; k < cnt[0]; ++k) {
+            cu(cudaMemcpy(&qv[k], thrust::raw_pointer_cast(a.q.data()) + idx[k], sizeof(real), cudaMemcpyDeviceToHost), "shim q");
+            cu(cudaMemcpy(&tv[k], thrust::raw_pointer_cast(a.type.data()) + idx[k], sizeof(int), cudaMemcpyDeviceToHost), "shim type");
+        }
+        bool same = g.last_n == cnt[0];
+        for (int k = 0; k < cnt[0] && same; ++k)
+            same = g.last_idx[k] == idx[k] && g.last_q[k] == (float)qv[k] && g.last_t[k] == tv[k];
+        if (same) return g.cur;
+        phmc_trial tr;
+        std::memset(&tr, 0, sizeof tr);
+        tr.n_changes = cnt[0];
+        for (int k = 0; k < cnt[0]; ++k) {
+            float pos[3];
+            cu(cudaMemcpy(&pos[0], g.mx + idx[k], sizeof(float), cudaMemcpyDeviceToHost), "shim x");
+            cu(cudaMemcpy(&pos[1], g.my + idx[k], sizeof(float), cudaMemcpyDeviceToHost), "shim y");
+            cu(cudaMemcpy(&pos[2], g.mz + idx[k], sizeof(float), cudaMemcpyDeviceToHost), "shim z");
+            tr.c[k].index = idx[k]; tr.c[k].present = 1;
+            tr.c[k].x = pos[0]; tr.c[k].y = pos[1]; tr.c[k].z = pos[2];
+            tr.c[k].q = (float)qv[k]; tr.c[k].type = tv[k];
+        }
+        phmc_energy_components d;
+        ck(phmc_delta_energy_components(g.eng, 0, &tr, 1, &d), "phmc_delta_energy_components");
+        g.cur.lj = g.base.lj + d.lj; g.cur.fene = g.base.fene + d.fene;
+        g.cur.coul_real = g.base.coul_real + d.coul_real; g.cur.coul_recip = g.base.coul_recip + d.coul_recip;
+        g.cur.self = g.base.self + d.self; g.cur.qcorr = g.base.qcorr + d.qcorr; g.cur.slab = g.base.slab + d.slab;
+        g.cur.total = g.base.total + d.total;
+        g.last_n = cnt[0];
+        for (int k = 0; k < cnt[0]; ++k) { g.last_idx[k] = idx[k]; g.last_q[k] = (float)qv[k]; g.last_t[k] = tv[k]; }
+        return g.cur;
+    }
+    // more changes (or moved atoms): the current atoms become the committed state
+    upload_state(a);
+    ck(phmc_energy(g.eng, &g.base), "phmc_energy");
+    mirror(a);
+    g.cur = g.base;
+    g.last_n = 0;
+    return g.cur;
+}
+
+}  // namespace
+
+// ---- MC/include/neighbor.hpp ----
+DeviceCSR copy_csr_to_device(const CSR& host) {
+    DeviceCSR d;
+    d.rows = host.head.empty() ? 0 : (int)host.head.size() - 1;
+    d.nnz = (int)host.list.size();
+    d.head = thrust::device_vector<int>(host.head.begin(), host.head.end());
+    d.list = thrust::device_vector<int>(host.list.begin(), host.list.end());
+    // the 1-2 pairs (i < j) become the engine's bond list
+    g.bi.clear(); g.bj.clear();
+    for (int i = 0; i < d.rows; ++i)
+        for (int k = host.head[i]; k < host.head[i + 1]; ++k)
+            if (host.list[k] > i) { g.bi.push_back(i); g.bj.push_back(host.list[k]); }
+    return d;
+}
+
+DeviceCSR build_half_neighbors_gpu(const DeviceAtoms& atoms, const Box& box, const DeviceCSR& bonds12_dev, real rc) {
+    // The engine keeps its own cell list; the pair list itself is not needed.  Its
+    // size is counted (the reference reports it) without storing it.
+    DeviceCSR d;
+    d.rows = (int)atoms.x.size();
+    unsigned long long* cnt = nullptr;
+    cu(cudaMalloc((void**)&cnt, sizeof(unsigned long long)), "cudaMalloc");
+    cu(cudaMemset(cnt, 0, sizeof(unsigned long long)), "cudaMemset");
+    const int* head = bonds12_dev.rows > 0 ? thrust::raw_pointer_cast(bonds12_dev.head.data()) : nullptr;
+    const int* list = bonds12_dev.nnz > 0 ? thrust::raw_pointer_cast(bonds12_dev.list.data()) : nullptr;
+    if (!list) head = nullptr;
+    k_shim_count_pairs<real><<<(d.rows + 127) / 128, 128>>>(d.rows, thrust::raw_pointer_cast(atoms.x.data()),
+                                                           thrust::raw_pointer_cast(atoms.y.data()),
+                                                           thrust::raw_pointer_cast(atoms.z.data()), box.Lx, box.Ly, box.Lz,
+                                                           rc * rc, head, list, cnt);
+    unsigned long long h = 0;
+    cudaError_t e = cudaMemcpy(&h, cnt, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(cnt);
+    cu(e, "build_half_neighbors_gpu");
+    d.nnz = (int)h;
+    return d;
+}
+
+// ---- MC/include/energy.hpp ----
+real compute_lj_sr_energy_gpu(const DeviceAtoms& atoms, const DeviceParams& dparams, const DeviceCSR&, const Box& box) {
+    return (real)evaluate(atoms, dparams, box).lj;
+}
+
+real compute_coul_sr_energy_gpu(const DeviceAtoms& atoms, const DeviceParams& dparams, const DeviceCSR&, const Box& box) {
+    if (dparams.coulombtype != "coul_cut") throw std::runtime_error("compute_coul_sr_energy_gpu: coulombtype must be coul_cut");
+    return (real)evaluate(atoms, dparams, box).coul_real;
+}
+
+// ---- MC/include/pme.hpp ----
+namespace {
+// the parameters pmeCreate was given (pmeEnergy receives none); held on the heap and
+// released by pmeDestroy, so no device vector outlives the CUDA runtime at exit
+DeviceParams* g_pme_params = nullptr;
+}
+
+void pmeCreate(PMEPlan* plan, const DeviceParams& params, const Box& box, real rc) {
+    if (!plan) throw std::runtime_error("pmeCreate: null plan");
+    plan->order = params.pme_order;
+    plan->use3dc = params.pme_3dc_enabled;
+    plan->alpha = params.ewald_alpha > 0 ? params.ewald_alpha : (real)alpha_from_rtol(rc, params.ewald_rtol);
+    plan->ewaldFactor = (real(M_PI) / plan->alpha) * (real(M_PI) / plan->alpha);
+    plan->elFactor = real(138.935458) / params.epsilon_r;
+    plan->vol = box.Lx * box.Ly * box.Lz;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) plan->recipBox[a][b] = 0;
+    plan->recipBox[0][0] = real(1) / box.Lx; plan->recipBox[1][1] = real(1) / box.Ly; plan->recipBox[2][2] = real(1) / box.Lz;
+    plan->nx = std::max(fft_dim((int)std::ceil(box.Lx / params.pme_spacing)), plan->order);
+    plan->ny = std::max(fft_dim((int)std::ceil(box.Ly / params.pme_spacing)), plan->order);
+    plan->nz = std::max(fft_dim((int)std::ceil(box.Lz / params.pme_spacing)), plan->order);
+    plan->ngridReal = plan->nx * plan->ny * plan->nz;
+    plan->ngridK = (plan->nx / 2 + 1) * plan->ny * plan->nz;
+    plan->planR2C = 0;  // the engine's own FFT: no library plan
+    if (g.eng) release();
+    g.pme = true;
+    g.mesh[0] = plan->nx; g.mesh[1] = plan->ny; g.mesh[2] = plan->nz;
+    g.order = plan->order;
+    g.alpha = plan->alpha;
+    g.slab = plan->use3dc;
+    delete g_pme_params;
+    g_pme_params = new DeviceParams(params);
+}
+
+void pmeDestroy(PMEPlan* plan) {
+    if (!plan) return;
+    release();
+    g.pme = false;
+    delete g_pme_params;
+    g_pme_params = nullptr;
+}
+
+real pmeEnergy(PMEPlan& plan, const DeviceAtoms& atoms, const DeviceCSR&, const Box& box, PMEEnergyComponents* components) {
+    if (!g.pme || !g_pme_params) throw std::runtime_error("pmeEnergy: pmeCreate was not called");
+    DeviceParams& dp = *g_pme_params;
+    dp.coulombtype = "pme";
+    const phmc_energy_components& c = evaluate(atoms, dp, box);
+    if (components) {
+        components->real_space = (real)c.coul_real;
+        components->recip_space = (real)c.coul_recip;
+        components->self_term = (real)c.self;
+        components->qcorr_term = (real)(c.qcorr + c.slab);
+    }
+    (void)plan;
+    return (real)(c.coul_real + c.coul_recip + c.self + c.qcorr + c.slab);
+}

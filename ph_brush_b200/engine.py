@@ -70,6 +70,13 @@ class Engine:
         _abi.check(self._lib.phmc_delta_energy(self._h, replica, arr, n, _abi.dptr(dE)))
         return dE
 
+    def delta_energy_components(self, trials, replica=0):
+        n = len(trials)
+        arr = (_abi.Trial * n)(*[self.make_trial(t) for t in trials])
+        out = (_abi.EnergyComponents * n)()
+        _abi.check(self._lib.phmc_delta_energy_components(self._h, replica, arr, n, out))
+        return [o.asdict() for o in out]
+
     def commit(self, changes, replica=0):
         t = self.make_trial(changes)
         _abi.check(self._lib.phmc_commit(self._h, replica, C.byref(t)))

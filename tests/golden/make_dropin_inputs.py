@@ -1,0 +1,29 @@
+"""Writes the drop-in workflow fixture (tests/golden/inputs/dropin_small.data,
+.params): a small brush in the reference's model and input format with a W-bead
+pool, and phase settings short enough for a test, so that the reference's own
+driver (MC/src/main.cu: protonation phase and phase-2 swaps) can run it both in
+its own build and linked against the engine's reference-API shim.
+Usage: python tests/golden/make_dropin_inputs.py
+"""
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from ph_brush_b200 import configs  # noqa: E402
+
+PHASES = {"target_pct": "30", "rng_seed": "2025", "max_attempts": "1500", "patience": "400",
+          "energy_interval": "100", "gc_block_fixed": "300", "sgmc_epoch_attempt_max": "1500", "phase2_wc": "yes"}
+
+
+def main():
+    small, _ = configs.small_system(seed=9, chains=3, length=12, box_xy=12.0, height=14.0, salt_pairs=6, ion_frac=0.2)
+    s, p = configs.to_reference_semantics(small, n_w=small.meta["n_sites"], spacing=0.5, seed=6)
+    os.makedirs(os.path.join(HERE, "inputs"), exist_ok=True)
+    configs.write_lammps_data(os.path.join(HERE, "inputs", "dropin_small.data"), s)
+    configs.write_params_in(os.path.join(HERE, "inputs", "dropin_small.params"), p, 0.5, extra=PHASES)
+
+
+if __name__ == "__main__":
+    main()
