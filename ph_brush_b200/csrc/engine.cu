@@ -449,9 +449,9 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                     for (int x0 = 0; x0 < nxh; x0 += w) zj.push_back(make_int4(r, y, x0, std::min(w, nxh - x0)));
                 // + cell counts / ids of the cell layers a plane's stencils reach (<= order + 5 layers)
                 const size_t ncell = (size_t)std::min(D.ncell[2], E.order + 5) * D.ncell[0] * D.ncell[1];
-                E.rb_fwd_smem = std::max(E.rb_fwd_smem, (size_t)D.mesh[0] * D.mesh[1] * sizeof(unsigned long long) +
-                                                             (size_t)2 * nxh * D.mesh[1] * sizeof(float2) +
-                                                             (2 * ncell + 1) * sizeof(int));
+                // two complex buffers (the 64-bit charge plane lives inside them) + cell counts
+                E.rb_fwd_smem = std::max(E.rb_fwd_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2) +
+                                                             (ncell + 1) * sizeof(int));
                 E.rb_inv_smem = std::max(E.rb_inv_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2));
             } else {
                 for (int y = 0; y < D.mesh[1]; ++y)

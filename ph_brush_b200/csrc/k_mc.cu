@@ -917,23 +917,46 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         {
             const int total = T.total_cand;
             const int so = D.slot_off;
-            for (int it = tid; it < total; it += NT) {
-                int lo = 0, hi = nent - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+            // RC candidates per thread and round: all list loads, then all particle loads, then
+            // the pair terms (each thread still adds its candidates in increasing order)
+            constexpr int RC = 4;
+            for (int it0 = tid; it0 < total; it0 += RC * NT) {
+                int j_u[RC], p_u[RC];
+#pragma unroll
+                for (int u = 0; u < RC; ++u) {
+                    const int it = it0 + u * NT;
+                    j_u[u] = -1;
+                    p_u[u] = 0;
+                    if (it >= total) continue;
+                    int lo = 0, hi = nent - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+                    }
+                    p_u[u] = lo / 27;
+                    j_u[u] = d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + (it - s_off[lo])];
                 }
-                const int p = lo / 27;
-                const int j = d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + (it - s_off[lo])];
-                if (j == T.idx[0] || (T.nch == 2 && j == T.idx[1])) continue;
-                const float4 pj = d.posq[so + j];
-                const int tj = d.type[so + j];
-                const float4 pp = T.probe_p[p];
-                float elj, ec;
-                pair_energy(D, min_image(pp.x - pj.x, D.L[0]), min_image(pp.y - pj.y, D.L[1]), min_image(pp.z - pj.z, D.L[2]),
-                            T.probe_t[p], tj, pp.w, pj.w, in_bonds(T.bonds[T.probe_owner[p]], j), elj, ec);
-                acc_lj += (double)(T.probe_sign[p] * elj);
-                acc_c += (double)(T.probe_sign[p] * ec);
+                float4 pj_u[RC];
+                int tj_u[RC];
+#pragma unroll
+                for (int u = 0; u < RC; ++u) {
+                    const int j = j_u[u];
+                    if (j < 0 || j == T.idx[0] || (T.nch == 2 && j == T.idx[1])) { j_u[u] = -1; continue; }
+                    pj_u[u] = d.posq[so + j];
+                    tj_u[u] = d.type[so + j];
+                }
+#pragma unroll
+                for (int u = 0; u < RC; ++u) {
+                    if (j_u[u] < 0) continue;
+                    const int p = p_u[u];
+                    const float4 pj = pj_u[u];
+                    const float4 pp = T.probe_p[p];
+                    float elj, ec;
+                    pair_energy(D, min_image(pp.x - pj.x, D.L[0]), min_image(pp.y - pj.y, D.L[1]), min_image(pp.z - pj.z, D.L[2]),
+                                T.probe_t[p], tj_u[u], pp.w, pj.w, in_bonds(T.bonds[T.probe_owner[p]], j_u[u]), elj, ec);
+                    acc_lj += (double)(T.probe_sign[p] * elj);
+                    acc_c += (double)(T.probe_sign[p] * ec);
+                }
             }
         }
         if (D.coulomb == PHMC_COUL_EWALD) {
@@ -956,7 +979,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const int ox = D.oct[0], oy = D.oct[1];
             constexpr int W3 = W * W * W;
             const int nit = T.npairs * W3;
-            constexpr int RB = 4;
+            constexpr int RB = 8;
             (void)ox; (void)oy;
             for (int it0 = tid; it0 < nit; it0 += RB * NT) {
                 float g[RB], kk[RB];

@@ -28,9 +28,11 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
     const RepDesc& D = d.desc[r];
     const int nx = D.mesh[0], ny = D.mesh[1], nz = D.mesh[2];
     const int M = nx / 2, nxh = M + 1;
-    unsigned long long* qp = reinterpret_cast<unsigned long long*>(sm_raw);
-    float2* a = reinterpret_cast<float2*>(qp + nx * ny);
+    // shared memory: two complex buffers of nxh x ny; the 64-bit charge plane (nx x ny)
+    // lives inside them until it is converted to the real plane (the packed pairs of a)
+    float2* a = reinterpret_cast<float2*>(sm_raw);
     float2* b = a + nxh * ny;
+    unsigned long long* qp = reinterpret_cast<unsigned long long*>(sm_raw);
     const int tid = threadIdx.x;
     for (int i = tid; i < nx * ny; i += NT) qp[i] = 0ull;
     __syncthreads();
@@ -49,16 +51,16 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
         // member counts of every cell in the layers, then an exclusive scan, so that the
         // (cell, member) items spread over all threads with independent loads
         int* s_cnt = reinterpret_cast<int*>(b + nxh * ny);
-        int* s_cid = s_cnt + ncell + 1;
         __shared__ int s_wsum[NT / 32 + 1];
-        for (int cc = tid; cc < ncell; cc += NT) {
+        // cell of item cc: layer cc / ncxy (wrapped in z), in-layer index cc % ncxy
+        auto cell_of_item = [&](int cc) {
             const int lay = cc / ncxy, cxy = cc - lay * ncxy;
             int cz = (c_lo + lay) % ncz;
             cz += (cz < 0) ? ncz : 0;
-            const int c = cz * ncxy + cxy;
-            s_cid[cc] = c;
-            s_cnt[cc] = min(d.cell_count[D.cell_off + c], D.cell_cap);
-        }
+            return cz * ncxy + cxy;
+        };
+        for (int cc = tid; cc < ncell; cc += NT)
+            s_cnt[cc] = min(d.cell_count[D.cell_off + cell_of_item(cc)], D.cell_cap);
         __syncthreads();
         {   // block scan: each thread a contiguous chunk, then the chunk totals
             const int per = (ncell + NT - 1) / NT;
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
                 const int mid = (lo2 + hi2 + 1) >> 1;
                 if (s_cnt[mid] <= it) lo2 = mid; else hi2 = mid - 1;
             }
-            const int c = s_cid[lo2];
+            const int c = cell_of_item(lo2);
             const int k = it - s_cnt[lo2];
             {
                 const float4 pq = d.posq[D.slot_off + d.cell_list[((size_t)D.cell_off + c) * D.cell_cap + k]];
@@ -131,11 +133,27 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
         }
     }
     __syncthreads();
-    // packed real pairs: a[y*M + j] = (Q[y][2j], Q[y][2j+1])
-    for (int i = tid; i < M * ny; i += NT) {
-        const int y = i / M, j = i - y * M;
-        a[i] = make_float2((float)((double)(long long)qp[y * nx + 2 * j] * PHMC_FIX_INV),
-                           (float)((double)(long long)qp[y * nx + 2 * j + 1] * PHMC_FIX_INV));
+    // fixed point -> float in place, in chunks of NT * CV elements: the floats of chunk k
+    // overwrite 64-bit elements [k CH/2, (k+1) CH/2), all read in chunks <= k.  The real
+    // plane Q[y][x] (row length nx) is then the packed pairs a[y*M + j] = (Q[y][2j], Q[y][2j+1]).
+    {
+        constexpr int CV = 16, CH = NT * CV;
+        float* qf = reinterpret_cast<float*>(sm_raw);
+        const int nq = nx * ny;
+        for (int c0 = 0; c0 < nq; c0 += CH) {
+            float v[CV];
+#pragma unroll
+            for (int u = 0; u < CV; ++u) {
+                const int i = c0 + u * NT + tid;
+                v[u] = (i < nq) ? (float)((double)(long long)qp[i] * PHMC_FIX_INV) : 0.0f;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < CV; ++u) {
+                const int i = c0 + u * NT + tid;
+                if (i < nq) qf[i] = v[u];
+            }
+        }
     }
     __syncthreads();
     float2* zr = fft_lines<NT>(a, b, M, ny, M, 1, d.twiddle + D.tw_off_h, -1.0f, false);
