@@ -1,19 +1,30 @@
 #!/usr/bin/env python3
-"""Benchmark: Monte Carlo sweeps/s of the plain engine on the config-2 brush.
+"""Benchmark: aggregate MC sweeps/s of batched delayed-acceptance MC on config 5.
 
-Workload: 10x10 grafted chains x 50 titratable beads (pKa 7.5, pH 6.5), box
-40x40x100 sigma padded to 300 for the slab correction, 0.1 M salt (about 12k
-particles), SPME mesh 64x64x384 order 5, WCA + FENE + erfc Coulomb, moves 90 %
-displacement (0.3 sigma) / 10 % protonation with counterion insert/delete.
-One step = one sweep = N_particles trial moves of the replica.
+Headline workload (config 5): 256 diblock brush replicas (64-144 chains of 20
+permanent +1 and 30 titratable beads, pKa 7.3; pH 5-9 and salt 0.001-0.3 M
+drawn from the seed; 4.6k-20k particles; slab 60 sigma padded to 180; SPME
+order 5), all in one engine: one MC block per replica per launch and one fused
+potential-mesh rebuild per chunk, captured in CUDA graphs, with the learned
+surrogate (trained on the GPU on exact dE harvested from the replicas, pH and
+salt among its inputs) as the first stage of delayed acceptance.  Moves: 90 %
+displacement (0.3 sigma), 10 % protonation with counterion insert/delete.
+One step = `--trials` trials of every replica; value = sum over replicas of
+sweeps (trials / N_replica) per second, all ranks together.
+
+Beside it: the plain engine on the same replicas one at a time (the
+`speedup_vs_plain` of the metric), the titration-only phase, the alpha(pH) check
+of delayed acceptance against the plain engine, and the plain engine on config 2
+(10x10 chains x 50 titratable beads, ~12k particles) against the reference.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With N > 1 (torchrun, one process per GPU) every rank runs its own replica
+With N > 1 (torchrun, one process per GPU) every rank runs its own replica set
 (replicas only, weak scaling); the timed region is bracketed by barriers and
 the max device time over ranks is reported.  `--impl reference` runs the
-reference's own CUDA build (compiled from its sources into oracle/_ref) on the
-same system in the reference's model and prints the same metric.
+reference's own CUDA build (compiled from its sources into oracle/_ref) one
+replica at a time on sampled config-5 replicas in the reference's model, and on
+config 2, and prints the same metric.
 """
 import argparse
 import json
@@ -30,8 +41,11 @@ sys.path.insert(0, ROOT)
 METRIC = "MC sweeps/s on 1 B200: batched+surrogate vs plain, α(pH) within 0.005"
 UNIT = "sweeps/s"
 FALLBACK_HBM_GBS = 6650.0
-WORKLOAD = ("config 2: plain constant-pH MC, 10x10 chains x 50 titratable beads, 40x40x100 box padded to 300, "
-            "0.1 M salt, ~12k particles, SPME 64x64x384 order 5, rc 3, 90% displacement / 10% protonation")
+WORKLOAD = ("config 5: 256 diblock brush replicas (20 permanent +1 + 30 titratable beads per chain, pKa 7.3), "
+            "64-144 chains, pH 5-9, salt 0.001-0.3 M, slab 60 padded to 180, SPME order 5, batched in one engine, "
+            "delayed acceptance with the GPU-trained surrogate; 90% displacement / 10% protonation")
+CFG2 = ("config 2: plain constant-pH MC, 10x10 chains x 50 titratable beads, 40x40x100 box padded to 300, "
+        "0.1 M salt, ~12k particles, SPME 64x64x384 order 5, rc 3, 90% displacement / 10% protonation")
 
 
 def parse():
@@ -40,19 +54,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--harvest", type=int, default=262144, help="surrogate training samples harvested (config 5)")
+    ap.add_argument("--replicas", type=int, default=256)
+    ap.add_argument("--trials", type=int, default=1000, help="trials per replica per step")
+    ap.add_argument("--harvest", type=int, default=262144, help="surrogate training samples harvested")
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--da-threshold", type=float, default=0.3)
-    ap.add_argument("--no-alpha", action="store_true")
-    ap.add_argument("--batched-replicas", type=int, default=256)
     ap.add_argument("--tuning", default=None, help="pending_max,threads instead of the autotuner (for profiling)")
-    ap.add_argument("--batched-only", action="store_true",
-                    help="only the config-5 batched section (its own JSON object; for profiling)")
-    ap.add_argument("--alpha-eq", type=int, default=300, help="sweeps of equilibration in the alpha(pH) check")
-    ap.add_argument("--alpha-sample", type=int, default=200, help="sweeps sampled in the alpha(pH) check")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="headline only (plain comparison, phases, alpha skipped)")
+    ap.add_argument("--no-alpha", action="store_true")
+    ap.add_argument("--alpha-eq", type=int, default=600, help="sweeps of equilibration in the alpha(pH) check")
+    ap.add_argument("--alpha-sample", type=int, default=400, help="sweeps sampled in the alpha(pH) check")
     return ap.parse_args()
 
 
@@ -114,13 +127,11 @@ def measured_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic(kernel):
-    """DRAM bytes per launch from the committed ncu summary, if present."""
+def ncu_traffic_ratio(kernel):
+    """DRAM bytes per algorithmic byte of `kernel` from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if not os.path.exists(path):
-        return None
     try:
-        return json.load(open(path)).get(kernel, {}).get("dram_bytes_per_launch")
+        return json.load(open(path)).get(kernel, {}).get("dram_bytes_per_alg_byte")
     except Exception:
         return None
 
@@ -141,27 +152,6 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_baseline(s, p, seconds):
-    """The FP64 oracle's Monte Carlo (same move set, energy from scratch per trial) on the host cores."""
-    from oracle import pyoracle as O
-    mc = O.MC(s, p)
-    n = 0
-    t0 = time.perf_counter()
-    while True:
-        mc.step()
-        n += 1
-        el = time.perf_counter() - t0
-        if el > seconds and n >= 2:
-            break
-    mc.close()
-    tps = n / el
-    cores = os.cpu_count()
-    return {"value": tps / s.n, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} trials of the config-2 system in {el:.1f} s (FP64, O(N^2) pairs + FP64 FFT per trial, "
-                      f"{cores} OpenMP threads); sweeps/s = trials/s / {s.n}",
-            "trials_per_s": tps}
-
-
 def tune_engine(eng, args, trials):
     """Autotune (pending capacity x block size), or apply --tuning."""
     if args.tuning:
@@ -169,6 +159,79 @@ def tune_engine(eng, args, trials):
         eng.set_tuning(pm, th)
         return None
     return eng.autotune(trials)
+
+
+def sums(stats, keys=("evaluated", "passed", "accepted")):
+    return [sum(d[k] for d in stats) for k in keys]
+
+
+# ---------------------------------------------------------------------------
+# headline: batched + delayed acceptance on config 5
+# ---------------------------------------------------------------------------
+def build_headline(args, local, rank):
+    """Config-5 engine, autotuned, with a surrogate trained on the GPU on exact dE
+    harvested from its own replicas (all of this is set-up, outside the timed region)."""
+    from ph_brush_b200 import Engine, Surrogate, configs
+    reps = configs.config5(seed=2029 + 7919 * rank, n_rep=args.replicas)
+    eng = Engine([s for s, _ in reps], [p for _, p in reps], device=local)
+    tune = tune_engine(eng, args, 400)
+    p0 = reps[0][1]
+    sur = Surrogate(seed=2029)
+    eng.set_move_mix(0.5, 0.5, 0.0)  # titration-heavy harvest
+    eng.harvest(args.harvest)
+    eng.run(2 * args.harvest // len(reps) + 1)
+    n_samples = eng.harvest_count()
+    t0 = time.perf_counter()
+    loss = eng.surrogate_fit(sur, epochs=args.epochs, batch=4096, lr=1e-3, clip=25.0, seed=7)
+    t_fit = time.perf_counter() - t0
+    eng.harvest(0)
+    eng.set_move_mix(p0.p_disp, p0.p_titr, p0.p_swap)
+    eng.attach_surrogate(sur, threshold=args.da_threshold, window=256)
+    steps = args.epochs * (n_samples // 4096)
+    fl_row = 2.0 * (80 * 128 + 2 * 128 * 128 + 128)  # forward flops per row; backward twice that
+    train = {"samples": n_samples, "epochs": args.epochs, "batch": 4096, "lr": 1e-3, "final_loss": loss,
+             "seconds": t_fit, "samples_per_s": steps * 4096 / t_fit,
+             "tflops": steps * 4096 * 4 * 3 * fl_row / t_fit / 1e12}
+    return reps, eng, sur, tune, train
+
+
+def plain_aggregate(args, reps, local, trials, samples=3):
+    """The plain engine (exact dE, no batching) on sampled replicas one at a time;
+    aggregate rate over the set = R sweeps / sum_r (N_r t_r) estimated from the samples."""
+    from ph_brush_b200 import Engine
+    ns = [s.n for s, _ in reps]
+    idx = sorted(range(len(reps)), key=lambda r: ns[r])
+    pick = sorted({idx[0], idx[len(idx) // 2], idx[-1]})[:samples]
+    per_sweep_s = []
+    for r in pick:
+        s, p = reps[r]
+        e1 = Engine(s, p, device=local)
+        tune_engine(e1, args, trials)
+        e1.run(trials // 4)
+        e1.flush_l2(256 << 20)
+        t = e1.run_timed(trials) / 1e3 / trials
+        e1.close()
+        per_sweep_s.append(ns[r] * t)
+    return 1.0 / (sum(per_sweep_s) / len(per_sweep_s)), pick
+
+
+def titration_phase(eng, sur, n_sites, threshold):
+    """The reference's protonation phase as a move mix: titration only, plain against
+    delayed acceptance, on the same engine."""
+    eng.set_move_mix(0.0, 1.0, 0.0)
+    eng.attach_surrogate(None)
+    tt = int(max(n_sites))
+    eng.run(tt)
+    eng.flush_l2(256 << 20)
+    ms_p = eng.run_timed(tt)
+    eng.attach_surrogate(sur, threshold=0.0, window=0)
+    eng.run(tt // 4)
+    eng.flush_l2(256 << 20)
+    ms_d = eng.run_timed(tt)
+    ev, ps, ac = sums(eng.da_stats())
+    R = len(n_sites)
+    return {"trials_per_replica": tt, "plain_trials_per_s": R * tt / (ms_p / 1e3), "da_trials_per_s": R * tt / (ms_d / 1e3),
+            "gain": ms_p / ms_d, "exact_dE_skipped": 1.0 - ps / max(ev, 1), "second_stage_agreement": ac / max(ps, 1)}
 
 
 def _alpha(stats, n_sites):
@@ -199,15 +262,14 @@ def alpha_check(local, sweeps_eq, sweeps_sample, snaps=20):
     B = Engine(S, P, device=local)
     tn = A.tuning()
     B.set_tuning(tn["pending_max"], tn["threads"])
-    for r in range(len(S)):
-        B.set_state(A.state(r), r)
+    B.set_state(A.state(-1), -1)
     B.attach_surrogate(sur, threshold=0.0, window=0)
     per = max(1, sweeps_sample * nmax // snaps)
     a_p, a_d = [], []
     for _ in range(snaps):
         a_p.append(_alpha(A.run(per), ns))
         a_d.append(_alpha(B.run(per), ns))
-    da = B.da_stats()
+    ev, ps, ac = sums(B.da_stats())
     A.close()
     B.close()
     a_p, a_d = np.array(a_p), np.array(a_d)
@@ -222,9 +284,6 @@ def alpha_check(local, sweeps_eq, sweeps_sample, snaps=20):
         curve.append({"pH": [lo, lo + 1.0], "replicas": int(m.sum()), "alpha_plain": float(mp[m].mean()),
                       "alpha_da": float(md[m].mean()), "diff": float(md[m].mean() - mp[m].mean()),
                       "stderr": float(np.sqrt((se[m] ** 2).sum()) / m.sum())})
-    ev = sum(d["evaluated"] for d in da)
-    ps = sum(d["passed"] for d in da)
-    ac = sum(d["accepted"] for d in da)
     return {"workload": "config-5 chemistry, 24 replicas of 4x4 diblock chains (20 permanent +1 + 30 titratable, "
                         "pKa 7.3), pH 5-9, salt 0.01-0.1 M, 50% displacement / 50% protonation",
             "sweeps_equilibrate": sweeps_eq, "sweeps_sample": sweeps_sample, "snapshots": snaps,
@@ -234,118 +293,193 @@ def alpha_check(local, sweeps_eq, sweeps_sample, snaps=20):
             "plain_drift_between_halves": drift}
 
 
-def run_batched(args, local, n_rep=256, trials=400, plain_samples=3):
-    """Config 5: 256 diblock replicas in one engine (one block per replica per MC
-    phase, captured in CUDA graphs) against the plain engine, which runs the same
-    replicas one at a time.  Aggregate sweeps/s = sum over replicas of sweeps / time.
-    Then the learned surrogate: exact dE harvested from the replicas, one network
-    (pH and salt among its inputs) trained on the GPU, delayed acceptance on the
-    config's move mix and on a titration-only phase."""
-    import numpy as np
-    from ph_brush_b200 import Engine, Surrogate, configs
-    reps = configs.config5(n_rep=n_rep)
-    ns = [s.n for s, _ in reps]
-    n_sites = [int(s.meta["n_sites"]) for s, _ in reps]
-    eng = Engine([s for s, _ in reps], [p for _, p in reps], device=local)
-    tune = tune_engine(eng, args, trials)
-    tuned = eng.tuning()
-    eng.run(trials // 4)
+def plain_config2(args, local):
+    """The plain engine (one replica, exact dE) on config 2: the comparison with the
+    reference's CUDA build on the same system."""
+    from ph_brush_b200 import Engine, configs
+    s, p = configs.config2()
+    eng = Engine(s, p, device=local)
+    tuned = tune_engine(eng, args, max(2000, s.n // 4))
+    eng.run(s.n)
     eng.set_profiling(True)
     eng.profile(reset=True)
-    eng.flush_l2(256 << 20)
-    ms = eng.run_timed(trials)
+    ms = 0.0
+    for _ in range(3):
+        eng.flush_l2(256 << 20)
+        ms += eng.run_timed(s.n)
+    prof = eng.profile(reset=True)
+    out = {"workload": CFG2, "particles": s.n, "sweeps_per_s": 3 / (ms / 1e3), "trials_per_s": 3 * s.n / (ms / 1e3),
+           "tuning": eng.tuning(), "autotune": tuned,
+           "k_mc_share": prof["mc_ms"] / ms if ms else None,
+           "k_mc_alg_gbs": prof["mc_alg_bytes"] / (prof["mc_ms"] / 1e3) / 1e9 if prof["mc_ms"] else None}
+    eng.close()
+    return out, (s, p)
+
+
+def cpu_baseline(s, p, seconds, what):
+    """The FP64 oracle's Monte Carlo (same move set, energy from scratch per trial) on the host cores."""
+    from oracle import pyoracle as O
+    mc = O.MC(s, p)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        mc.step()
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds and n >= 2:
+            break
+    mc.close()
+    tps = n / el
+    cores = os.cpu_count()
+    return {"value": tps / s.n, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} trials of {what} ({s.n} particles) in {el:.1f} s (FP64, O(N^2) pairs + FP64 FFT per "
+                      f"trial, {cores} OpenMP threads); sweeps/s = trials/s / {s.n}: one replica's rate, the "
+                      f"host's aggregate over a replica set run one at a time",
+            "trials_per_s": tps}
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    import numpy as np
+
+    reps, eng, sur, tune, train = build_headline(args, local, rank)
+    ns = np.array([s.n for s, _ in reps], np.float64)
+    T = args.trials
+    sweeps_per_step = float((T / ns).sum())
+    for _ in range(args.warmup):
+        eng.run(T)
+    # ---- device-timed region: inputs resident, L2 flushed between steps ----
+    eng.set_profiling(True)
+    eng.profile(reset=True)
+    da0 = sums(eng.da_stats())
+    clocks = Clocks(local)
+    barrier(world)
+    dev_ms = 0.0
+    for _ in range(args.steps):
+        eng.flush_l2(256 << 20)
+        dev_ms += eng.run_timed(T)
+    barrier(world)
+    clk = clocks.stop()
     prof = eng.profile(reset=True)
     eng.set_profiling(False)
-    agg = sum(trials / n for n in ns) / (ms / 1e3)
-    # plain engine: the same replicas one at a time (each autotuned); its aggregate rate
-    # over the set is R sweeps / sum_r (N_r * t_r), t_r the per-trial time of replica r alone
-    idx = sorted(range(n_rep), key=lambda r: ns[r])
-    pick = [idx[0], idx[len(idx) // 2], idx[-1]][:plain_samples]
-    per_sweep_s = []
-    for r in pick:
-        s, p = reps[r]
-        e1 = Engine(s, p, device=local)
-        tune_engine(e1, args, trials)
-        e1.run(trials // 4)
-        e1.flush_l2(256 << 20)
-        t = e1.run_timed(trials) / 1e3 / trials
-        e1.close()
-        per_sweep_s.append(ns[r] * t)
-    plain = 1.0 / (sum(per_sweep_s) / len(per_sweep_s))
-    peak, kind = measured_peak()
-    rl = {}
-    if prof["mc_launches"] and prof["mc_ms"] > 0:
-        rl["k_mc"] = {"achieved": prof["mc_alg_bytes"] / (prof["mc_ms"] / 1e3) / 1e9, "share": prof["mc_ms"] / ms}
-    if prof["flush_launches"] and prof["flush_ms"] > 0:
-        rl["mesh_rebuild"] = {"achieved": prof["flush_alg_bytes"] / (prof["flush_ms"] / 1e3) / 1e9,
-                              "share": prof["flush_ms"] / ms}
-    for v in rl.values():
-        v.update({"bound": "hbm", "peak": peak, "unit": "GB/s", "frac": v["achieved"] / peak, "peak_source": kind})
+    da1 = sums(eng.da_stats())
+    max_ms = reduce_max(dev_ms, world, local)
+    value = world * args.steps * sweeps_per_step / (max_ms / 1e3)
 
-    # ---- surrogate: harvest (titration-heavy mix), GPU training ----
-    p0 = reps[0][1]
-    sur = Surrogate(seed=2029)
-    eng.set_move_mix(0.5, 0.5, 0.0)
-    eng.harvest(args.harvest)
-    eng.run(2 * args.harvest // n_rep + 1)
-    n_samples = eng.harvest_count()
+    # ---- end to end through the public API: pinned host state of every replica in,
+    #      state and energies out, every step ----
+    st = eng.state(-1)
+    try:
+        import torch
+        pinned = {k: torch.from_numpy(v.copy()).pin_memory().numpy() for k, v in st.items()}
+    except Exception:
+        pinned = {k: v.copy() for k, v in st.items()}
+    slots = len(st["x"])
+    barrier(world)
     t0 = time.perf_counter()
-    loss = eng.surrogate_fit(sur, epochs=args.epochs, batch=4096, lr=1e-3, clip=25.0, seed=7)
-    t_fit = time.perf_counter() - t0
-    eng.harvest(0)
-    steps = args.epochs * (n_samples // 4096)
-    # 4 rows per sample; forward 2*(80*128 + 2*128*128 + 128) flops per row, backward twice that
-    fl_row = 2.0 * (80 * 128 + 2 * 128 * 128 + 128)
-    train = {"samples": n_samples, "epochs": args.epochs, "batch": 4096, "lr": 1e-3, "final_loss": loss,
-             "seconds": t_fit, "samples_per_s": steps * 4096 / t_fit,
-             "tflops": steps * 4096 * 4 * 3 * fl_row / t_fit / 1e12}
+    for _ in range(args.steps):
+        eng.set_state(pinned, -1)
+        res = eng.run(T)
+        out = eng.state(-1)
+        energies = [r["energy"] for r in res]
+    e2e_s = time.perf_counter() - t0
+    barrier(world)
+    e2e_s = reduce_max(e2e_s, world, local)
+    e2e = {"value": world * args.steps * sweeps_per_step / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": slots * (16 + 4 + 4), "d2h_bytes_per_step": slots * (16 + 4 + 4) + 8 * len(reps),
+           "timing": "host wall clock around phmc_set_state(all replicas) + phmc_run + phmc_get_state(all replicas), "
+                     "synchronous calls"}
+    del out, energies
 
-    # ---- batched + surrogate on the config's move mix ----
-    eng.set_move_mix(p0.p_disp, p0.p_titr, p0.p_swap)
-    eng.attach_surrogate(sur, threshold=args.da_threshold, window=256)
-    eng.run(trials // 4)
-    eng.flush_l2(256 << 20)
-    ms_da = eng.run_timed(trials)
-    agg_da = sum(trials / n for n in ns) / (ms_da / 1e3)
-    da_mix = eng.da_stats()
+    # ---- roofline of the dominant kernel (MC kernel or the fused rebuild) ----
+    peak, peak_kind = measured_peak()
+    kern = []
+    if prof["mc_launches"]:
+        kern.append(("k_mc", prof["mc_ms"], prof["mc_launches"], prof["mc_alg_bytes"]))
+    if prof["flush_launches"]:
+        kern.append(("mesh_rebuild", prof["flush_ms"], prof["flush_launches"], prof["flush_alg_bytes"]))
+    kern.sort(key=lambda k: -k[1])
+    rl = {}
+    for name, tot, n_l, by in kern:
+        ms = tot / n_l
+        per = by / n_l
+        ach = per / (ms / 1e3) / 1e9
+        ratio = ncu_traffic_ratio(name)
+        rl[name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "peak_source": peak_kind, "traffic": ratio * per if ratio else None,
+                    "alg_bytes_per_launch": per, "avg_launch_ms": ms, "launches": n_l,
+                    "share_of_timed": tot / dev_ms if dev_ms else None}
+    dominant = kern[0][0] if kern else None
 
-    # ---- titration-only phase (the reference's protonation phase): plain vs delayed acceptance ----
-    eng.set_move_mix(0.0, 1.0, 0.0)
-    eng.attach_surrogate(None)
-    tt = int(max(n_sites))
-    eng.run(tt)
-    eng.flush_l2(256 << 20)
-    ms_tp = eng.run_timed(tt)
-    eng.attach_surrogate(sur, threshold=0.0, window=0)
-    eng.run(tt // 4)
-    eng.flush_l2(256 << 20)
-    ms_td = eng.run_timed(tt)
-    da_t = eng.da_stats()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 pair/mesh/FFT, f64 accumulation and Metropolis, bf16 surrogate",
+            "data": "synthetic (seeded brush generator, config-5 seed 2029 + 7919 * rank)",
+            "config": {"workload": WORKLOAD, "replicas": len(reps), "particles_min_max": [int(ns.min()), int(ns.max())],
+                       "trials_per_replica_per_step": T, "sweeps_per_step": sweeps_per_step,
+                       "tuning": eng.tuning(), "autotune": tune, "da_threshold": args.da_threshold,
+                       "l2": "flushed between steps (256 MiB write on the engine stream)",
+                       "parallelism": f"replicas only x{world}"},
+            "roofline": dict(rl[dominant], kernel=dominant) if dominant else None,
+            "roofline_other": {k: v for k, v in rl.items() if k != dominant},
+            "e2e": e2e, "gpu_launches": int(prof["kernel_launches"]),
+            "trials_per_s": world * prof["trials"] / (max_ms / 1e3) if prof["trials"] else None,
+            "surrogate": {"training": train, "exact_dE_skipped": 1.0 - (da1[1] - da0[1]) / max(da1[0] - da0[0], 1),
+                          "second_stage_agreement": (da1[2] - da0[2]) / max(da1[1] - da0[1], 1),
+                          "fallbacks": int(sum(d["fallback"] for d in eng.da_stats()))},
+            "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_extras:
+        plain, pick = plain_aggregate(args, reps, local, 400)
+        line["plain_aggregate_sweeps_per_s"] = plain
+        line["plain_sampled_replicas"] = pick
+        line["speedup_vs_plain"] = value / plain
+        # batched exact (no surrogate) on the same engine, for the split of the gain
+        eng.attach_surrogate(None)
+        eng.run(T // 4)
+        eng.flush_l2(256 << 20)
+        ms_ex = eng.run_timed(T)
+        line["batched_exact_sweeps_per_s"] = sweeps_per_step / (ms_ex / 1e3)
+        line["titration_phase"] = titration_phase(eng, sur, [int(s.meta["n_sites"]) for s, _ in reps], args.da_threshold)
     eng.close()
-    ev, ps, ac = (sum(d[k] for d in da_t) for k in ("evaluated", "passed", "accepted"))
-    evm, psm, acm = (sum(d[k] for d in da_mix) for k in ("evaluated", "passed", "accepted"))
-    tp_plain = n_rep * tt / (ms_tp / 1e3)
-    tp_da = n_rep * tt / (ms_td / 1e3)
-    surrogate = {
-        "training": train,
-        "aggregate_sweeps_per_s": agg_da, "speedup_vs_plain": agg_da / plain,
-        "speedup_vs_batched_exact": agg_da / agg,
-        "config_mix": {"exact_dE_skipped": 1.0 - psm / max(evm, 1), "second_stage_agreement": acm / max(psm, 1),
-                       "fallbacks": int(sum(d["fallback"] for d in da_mix)), "threshold": args.da_threshold},
-        "titration_phase": {"trials_per_replica": tt, "plain_trials_per_s": tp_plain, "da_trials_per_s": tp_da,
-                            "gain": tp_da / tp_plain, "exact_dE_skipped": 1.0 - ps / max(ev, 1),
-                            "second_stage_agreement": ac / max(ps, 1)},
-    }
-    if not args.no_alpha:
-        surrogate["alpha_check"] = alpha_check(local, args.alpha_eq, args.alpha_sample)
-    return {"workload": "config 5: 256 diblock replicas (20 permanent +1 + 30 titratable beads, pKa 7.3), 64-144 chains, "
-                        "pH 5-9, salt 0.001-0.3 M, slab 60 padded to 180, SPME order 5, lateral mesh 48-64",
-            "replicas": n_rep, "particles_min_max": [min(ns), max(ns)], "trials_per_replica": trials,
-            "tuning": tuned, "autotune": tune,
-            "aggregate_sweeps_per_s": agg, "trials_per_s": n_rep * trials / (ms / 1e3),
-            "plain_aggregate_sweeps_per_s": plain, "plain_sampled_replicas": pick, "speedup_vs_plain": agg / plain,
-            "roofline": rl, "device_ms": ms, "gpu_launches": int(prof["kernel_launches"]),
-            "surrogate": surrogate}
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["plain_config2"], c2 = plain_config2(args, local)
+        if not args.no_alpha:
+            line["alpha_check"] = alpha_check(local, args.alpha_eq, args.alpha_sample)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        small = min(reps, key=lambda sp: sp[0].n)
+        line["cpu_baseline"] = cpu_baseline(small[0], small[1], args.cpu_seconds, "the smallest config-5 replica")
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's CUDA build, one replica at a time
+# ---------------------------------------------------------------------------
+def ref_time(harness, sn, spacing, per_step, steps, warmup, seed):
+    """Trials/s of the reference's phase-2 identity-swap loop (MC/src/mc.cu:159-318, total
+    energy recomputed per trial) on `sn` in the reference's model."""
+    from ph_brush_b200 import configs
+    n_sites = int(((sn.flags & 2) != 0).sum())
+    n_charged = int((((sn.flags & 2) != 0) & (sn.q != 0)).sum())
+    s, p = configs.to_reference_semantics(sn, n_w=n_sites, spacing=spacing, seed=seed)
+    d = tempfile.mkdtemp()
+    configs.write_lammps_data(os.path.join(d, "in.data"), s)
+    pct = 100.0 * (n_charged + 0.5) / max(n_sites, 1)  # floor(pct/100 * sites) == current count
+    configs.write_params_in(os.path.join(d, "params.in"), p, spacing, extra={"target_pct": f"{pct:.8f}"})
+    r = subprocess.run([harness, "time", os.path.join(d, "in.data"), os.path.join(d, "params.in"),
+                        str(per_step * steps), str(per_step * warmup)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference harness failed: " + r.stderr.strip()[-200:])
+    return json.loads(r.stdout.strip().splitlines()[-1])
 
 
 def run_reference(args):
@@ -357,145 +491,44 @@ def run_reference(args):
     if not os.path.exists(harness):
         print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build missing: run `make -C oracle ref`"}))
         return
-    sn, _ = configs.config2()
-    n_sites = int(((sn.flags & 2) != 0).sum())
-    n_charged = int(((sn.flags & 2) != 0).__and__(sn.q != 0).sum())
-    spacing = 0.7  # reference mesh rule: 60x60x432 (1.56 M points) for the 40x40x300 box
-    s, p = configs.to_reference_semantics(sn, n_w=n_sites, spacing=spacing, seed=5)
-    d = tempfile.mkdtemp()
-    configs.write_lammps_data(os.path.join(d, "in.data"), s)
-    pct = 100.0 * (n_charged + 0.5) / n_sites  # floor(pct/100 * sites) == current count (build_plan needs target >= current)
-    configs.write_params_in(os.path.join(d, "params.in"), p, spacing, extra={"target_pct": f"{pct:.8f}"})
-    per_step = 20
-    r = subprocess.run([harness, "time", os.path.join(d, "in.data"), os.path.join(d, "params.in"),
-                        str(per_step * args.steps), str(per_step * args.warmup)], capture_output=True, text=True)
-    if r.returncode != 0:
-        print(json.dumps({"impl": "reference", "unavailable": "reference harness failed: " + r.stderr.strip()[-200:]}))
-        return
-    out = json.loads(r.stdout.strip().splitlines()[-1])
-    sweeps = out["trials_per_s"] / sn.n
-    line = {"impl": "reference", "metric": METRIC, "value": sweeps, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * out["seconds"] / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brush generator)",
-            "config": {"workload": WORKLOAD + " (reference model: LJ cut at 3 sigma, 1-2 exclusions, cubic SPME, "
-                                  "mesh from pme_spacing 0.7 -> %s; moves: the reference's phase-2 identity swaps)"
-                                  % out["mesh"], "particles": sn.n, "reference_atoms": out["natoms"],
-                       "trials_per_step": per_step},
-            "cpu_baseline": {"value": sweeps, "unit": UNIT, "cores": 1, "kind": "reference",
-                             "sample": f"{out['trials']} trials of phase2_swap_jitter (MC/src/mc.cu:159-318) in the "
-                                       f"reference's CUDA build on this B200 (one host thread), CUDA-event timed"},
-            "e2e": {"value": sweeps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "trials_per_s": out["trials_per_s"], "reference_seconds": out["seconds"]}
-    print(json.dumps(line))
-
-
-def run_ours(args):
-    rank, world, local = dist_env()
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    import numpy as np
-    from ph_brush_b200 import Engine, configs
-
-    s, p = configs.config2(seed=2026 + rank)
-    N = s.n
-    eng = Engine(s, p, device=local)
-    tune = tune_engine(eng, args, max(2000, N // 4))
-    tuned = eng.tuning()
-    for _ in range(args.warmup):
-        eng.run(N)
-    # ---- device-timed region: inputs resident, L2 flushed between steps ----
-    eng.set_profiling(True)
-    eng.profile(reset=True)
-    clocks = Clocks(local)
-    barrier(world)
-    dev_ms = 0.0
-    for _ in range(args.steps):
-        eng.flush_l2(256 << 20)
-        dev_ms += eng.run_timed(N)
-    barrier(world)
-    clk = clocks.stop()
-    prof = eng.profile(reset=True)
-    eng.set_profiling(False)
-    max_ms = reduce_max(dev_ms, world, local)
-    value = world * args.steps / (max_ms / 1e3)
-
-    # ---- end to end through the public API: pinned host state in, state + energy out ----
-    st = eng.state()
+    reps = configs.config5(seed=2029, n_rep=args.replicas)
+    ns = [s.n for s, _ in reps]
+    idx = sorted(range(len(reps)), key=lambda r: ns[r])
+    pick = sorted({idx[0], idx[len(idx) // 2], idx[-1]})
+    per_step = 10
     try:
-        import torch
-        pinned = {k: torch.from_numpy(v.copy()).pin_memory().numpy() for k, v in st.items()}
-    except Exception:
-        pinned = {k: v.copy() for k, v in st.items()}
-    cap = len(st["x"])
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        eng.set_state(pinned)
-        res = eng.run(N)
-        out = eng.state()
-        energy = res[0]["energy"]
-    e2e_s = time.perf_counter() - t0
-    barrier(world)
-    e2e_s = reduce_max(e2e_s, world, local)
-    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": cap * (16 + 4 + 4), "d2h_bytes_per_step": cap * (16 + 4 + 4) + 8,
-           "timing": "host wall clock around phmc_set_state + phmc_run + phmc_get_state (synchronous calls)"}
-
-    # ---- roofline of the dominant kernel ----
-    peak, peak_kind = measured_peak()
-    kern = []
-    if prof["mc_launches"]:
-        ms = prof["mc_ms"] / prof["mc_launches"]
-        by = prof["mc_alg_bytes"] / prof["mc_launches"]
-        kern.append(("k_mc", prof["mc_ms"], ms, by))
-    if prof["flush_launches"]:
-        ms = prof["flush_ms"] / prof["flush_launches"]
-        by = prof["flush_alg_bytes"] / prof["flush_launches"]
-        kern.append(("mesh_rebuild", prof["flush_ms"], ms, by))
-    kern.sort(key=lambda k: -k[1])
-    rl = {}
-    for name, tot, ms, by in kern:
-        ach = by / (ms / 1e3) / 1e9
-        rl[name] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                    "peak_source": peak_kind, "traffic": ncu_traffic(name), "alg_bytes_per_launch": by,
-                    "avg_launch_ms": ms, "launches": prof[("mc" if name == "k_mc" else "flush") + "_launches"],
-                    "share_of_timed": tot / dev_ms if dev_ms else None}
-    dominant = kern[0][0] if kern else None
-
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (f64 accumulation and Metropolis)",
-            "data": "synthetic (seeded brush generator, seed 2026 + rank)",
-            "config": {"workload": WORKLOAD, "particles": N, "trials_per_step": N, "mesh": list(p.mesh),
-                       "order": p.order, "tuning": tuned, "autotune": tune,
-                       "l2": "flushed between steps (256 MiB write on the engine stream)",
-                       "parallelism": f"replicas only x{world}"},
-            "roofline": dict(rl[dominant], kernel=dominant) if dominant else None,
-            "roofline_other": {k: v for k, v in rl.items() if k != dominant},
-            "e2e": e2e, "gpu_launches": int(prof["kernel_launches"]),
-            "trials_per_s": world * prof["trials"] / (max_ms / 1e3) if prof["trials"] else None,
-            "clocks": clk}
-    eng.close()
-    if rank == 0 and world == 1 and not args.no_batched:
-        line["batched"] = run_batched(args, local, n_rep=args.batched_replicas)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(s, p, args.cpu_seconds)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line))
+        runs = [ref_time(harness, reps[r][0], 0.7, per_step, args.steps, args.warmup, 5 + r) for r in pick]
+        s2, _ = configs.config2()
+        run2 = ref_time(harness, s2, 0.7, 20, args.steps, args.warmup, 5)
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return
+    # aggregate over the replica set run one at a time: R sweeps / sum_r N_r t_r, from the samples
+    per_sweep = [ns[r] / o["trials_per_s"] for r, o in zip(pick, runs)]
+    value = 1.0 / (sum(per_sweep) / len(per_sweep))
+    secs = sum(o["seconds"] for o in runs)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brush generator)",
+            "config": {"workload": WORKLOAD + " -- reference: no batching and no surrogate, so the replicas run one at "
+                                  "a time in its model (LJ cut at 3 sigma, 1-2 exclusions, cubic SPME, mesh from "
+                                  "pme_spacing 0.7, its phase-2 identity swaps with a full energy per trial); "
+                                  "aggregate from the smallest, median and largest replica",
+                       "sampled_replicas": pick, "particles": [ns[r] for r in pick],
+                       "reference_atoms": [o["natoms"] for o in runs], "meshes": [o["mesh"] for o in runs],
+                       "trials_per_s": [o["trials_per_s"] for o in runs], "trials_per_step": per_step},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{per_step * args.steps} timed trials per sampled replica of "
+                                       "phase2_swap_jitter (MC/src/mc.cu:159-318) in the reference's CUDA build on "
+                                       "this B200 (one host thread), CUDA-event timed"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config2": {"workload": CFG2, "trials_per_s": run2["trials_per_s"],
+                        "sweeps_per_s": run2["trials_per_s"] / configs.config2()[0].n, "mesh": run2["mesh"]}}
+    print(json.dumps(line))
 
 
 def main():
     args = parse()
-    if args.batched_only:
-        print(json.dumps({"batched": run_batched(args, dist_env()[2], n_rep=args.batched_replicas)}))
-        return
     if args.impl == "reference":
         run_reference(args)
     else:

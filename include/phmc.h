@@ -225,7 +225,9 @@ int phmc_set_tuning(phmc_engine* e, int pending_max, int threads);
 int phmc_get_tuning(phmc_engine* e, phmc_tuning* out);
 int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_results, int* n_results);
 
-/* ---- state ---- */
+/* ---- state ----
+ * replica == -1: every replica at once, arrays of sum(capacity) slots concatenated
+ * in replica order (one upload and one full recompute for the whole engine). */
 int phmc_get_state(phmc_engine* e, int replica, float* x, float* y, float* z, float* q,
                    int* type, int* flags);
 /* Replace replica r's particle state from host arrays of capacity length (bonds

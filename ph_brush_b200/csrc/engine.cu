@@ -860,29 +860,30 @@ extern "C" int phmc_run(phmc_engine* h, int64_t n_trials, phmc_run_stats* stats)
 }
 
 extern "C" int phmc_get_state(phmc_engine* h, int rep, float* x, float* y, float* z, float* q, int* type, int* flags) {
-    if (!h || rep < 0 || rep >= h->E.R) return fail(PHMC_ERR_ARG, "invalid replica");
+    if (!h || rep < -1 || rep >= h->E.R) return fail(PHMC_ERR_ARG, "invalid replica");
     Engine& E = h->E;
     CU(cudaSetDevice(E.device));
     CU(cudaStreamSynchronize(E.stream));
-    const RepDesc& D = E.desc[rep];
-    std::vector<float4> pq((size_t)D.cap);
-    CU(cudaMemcpy(pq.data(), E.d.posq + D.slot_off, sizeof(float4) * D.cap, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < D.cap; ++i) {
+    // one replica, or (rep == -1) all replicas concatenated in replica order, capacity slots each
+    const int off = rep < 0 ? 0 : E.desc[rep].slot_off;
+    const int cap = rep < 0 ? E.total_slots : E.desc[rep].cap;
+    std::vector<float4> pq((size_t)cap);
+    CU(cudaMemcpy(pq.data(), E.d.posq + off, sizeof(float4) * cap, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < cap; ++i) {
         if (x) x[i] = pq[i].x;
         if (y) y[i] = pq[i].y;
         if (z) z[i] = pq[i].z;
         if (q) q[i] = pq[i].w;
     }
-    if (type) CU(cudaMemcpy(type, E.d.type + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
-    if (flags) CU(cudaMemcpy(flags, E.d.flags + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
+    if (type) CU(cudaMemcpy(type, E.d.type + off, sizeof(int) * cap, cudaMemcpyDeviceToHost));
+    if (flags) CU(cudaMemcpy(flags, E.d.flags + off, sizeof(int) * cap, cudaMemcpyDeviceToHost));
     return PHMC_OK;
 }
 
-extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const float* y, const float* z, const float* q,
-                              const int* type, const int* flags) {
-    if (!h || rep < 0 || rep >= h->E.R || !x || !y || !z || !q || !type || !flags) return fail(PHMC_ERR_ARG, "invalid argument");
+// Host-side lists of one replica from its slot arrays, uploaded on the engine stream.
+static int stage_replica_state(phmc_engine* h, int rep, const float* x, const float* y, const float* z, const float* q,
+                               const int* type, const int* flags) {
     Engine& E = h->E;
-    CU(cudaSetDevice(E.device));
     RepDesc& D = E.desc[rep];
     const int cap = D.cap, so = D.slot_off;
     std::vector<float4> pq((size_t)cap);
@@ -908,21 +909,37 @@ extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const flo
         if (flags[i] & PHMC_F_GHOST) fr[st.n_free++] = i;
     D.n_titr = nt;
     h->n_present[rep] = npres;
-    const cudaStream_t s = E.stream;
-    CU(cudaMemcpyAsync(E.d.posq + so, pq.data(), sizeof(float4) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.type + so, type, sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.flags + so, flags, sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.mobile + so, mob.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.mobile_pos + so, mpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.anions + so, an.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.anion_pos + so, apos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.cations + so, ca.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.cation_pos + so, cpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.freel + so, fr.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.titr + so, ti.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.state + rep, &st, sizeof(RepState), cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(E.d.desc + rep, &D, sizeof(RepDesc), cudaMemcpyHostToDevice, s));
-    launch_cell_build(E, s);
+    // synchronous copies: the staging vectors are local
+    CU(cudaMemcpy(E.d.posq + so, pq.data(), sizeof(float4) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.type + so, type, sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.flags + so, flags, sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.mobile + so, mob.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.mobile_pos + so, mpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.anions + so, an.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.anion_pos + so, apos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.cations + so, ca.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.cation_pos + so, cpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.freel + so, fr.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.titr + so, ti.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.state + rep, &st, sizeof(RepState), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.desc + rep, &D, sizeof(RepDesc), cudaMemcpyHostToDevice));
+    return PHMC_OK;
+}
+
+extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const float* y, const float* z, const float* q,
+                              const int* type, const int* flags) {
+    if (!h || rep < -1 || rep >= h->E.R || !x || !y || !z || !q || !type || !flags) return fail(PHMC_ERR_ARG, "invalid argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    // one replica, or (rep == -1) all replicas from arrays concatenated in replica order
+    const int r0 = rep < 0 ? 0 : rep, r1 = rep < 0 ? E.R : rep + 1;
+    for (int r = r0; r < r1; ++r) {
+        const int o = rep < 0 ? E.desc[r].slot_off : 0;
+        const int s = stage_replica_state(h, r, x + o, y + o, z + o, q + o, type + o, flags + o);
+        if (s) return s;
+    }
+    launch_cell_build(E, E.stream);
     h->prof.kernel_launches += 2;
     int rc = full_recompute(h);
     h->prof.kernel_launches += E.flush_kernels + 2;

@@ -39,10 +39,13 @@ enum { EPI_STORE = 0, EPI_BIAS_GELU = 1, EPI_GELU_GRAD = 2 };
 // epi EPI_STORE:     Cf[i*N+j] = acc
 // epi EPI_BIAS_GELU: Z = acc + bias[j] -> Cf (fp32), H = gelu(Z) -> Hb (bf16)
 // epi EPI_GELU_GRAD: dZ = acc * gelu'(Zin[i*N+j]) -> Hb (bf16)
+// Split K: block z covers k in [z * kchunk, min(K, (z + 1) * kchunk)) and, for EPI_STORE,
+// writes its partial product to Cf + z * M * N (summed by k_sum_splits in a fixed order).
 __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __nv_bfloat16* __restrict__ A, long sai,
                                                    long sak, const __nv_bfloat16* __restrict__ B, long sbk, long sbj,
                                                    int epi, float* __restrict__ Cf, const float* __restrict__ bias,
-                                                   const float* __restrict__ Zin, __nv_bfloat16* __restrict__ Hb) {
+                                                   const float* __restrict__ Zin, __nv_bfloat16* __restrict__ Hb,
+                                                   int kchunk) {
     __shared__ __nv_bfloat16 As[64][16 + 8];
     __shared__ __nv_bfloat16 Bs[16][64 + 8];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -57,16 +60,18 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
     const __nv_bfloat16 z = __float2bfloat16(0.0f);
-    for (int k0 = 0; k0 < K; k0 += 16) {
+    const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
+    if (epi == EPI_STORE) Cf += (size_t)blockIdx.z * M * N;
+    for (int k0 = kbeg; k0 < kend; k0 += 16) {
         for (int e = tid; e < 64 * 16; e += 128) {
             const int r = e >> 4, kk = e & 15;
             const int i = i0 + r, k = k0 + kk;
-            As[r][kk] = (i < M && k < K) ? A[(long)i * sai + (long)k * sak] : z;
+            As[r][kk] = (i < M && k < kend) ? A[(long)i * sai + (long)k * sak] : z;
         }
         for (int e = tid; e < 16 * 64; e += 128) {
             const int kk = e >> 6, cc = e & 63;
             const int k = k0 + kk, j = j0 + cc;
-            Bs[kk][cc] = (k < K && j < N) ? B[(long)k * sbk + (long)j * sbj] : z;
+            Bs[kk][cc] = (k < kend && j < N) ? B[(long)k * sbk + (long)j * sbj] : z;
         }
         __syncthreads();
         uint32_t af[2][4], bfr[4][2];
@@ -114,10 +119,37 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __
                 }
 }
 
+// out[i] = sum_z part[z * n + i] in z order (deterministic)
+__global__ void k_sum_splits(const float* __restrict__ part, int splits, int n, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s = 0.0f;
+    for (int z = 0; z < splits; ++z) s += part[(size_t)z * n + i];
+    out[i] = s;
+}
+
+#define GEMM_MAX_SPLITS 64
+
 static void gemm(int M, int N, int K, const __nv_bfloat16* A, long sai, long sak, const __nv_bfloat16* B, long sbk,
-                 long sbj, int epi, float* Cf, const float* bias, const float* Zin, __nv_bfloat16* Hb, cudaStream_t st) {
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
-    k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, A, sai, sak, B, sbk, sbj, epi, Cf, bias, Zin, Hb);
+                 long sbj, int epi, float* Cf, const float* bias, const float* Zin, __nv_bfloat16* Hb, cudaStream_t st,
+                 float* split_buf = nullptr) {
+    dim3 grid((N + 63) / 64, (M + 63) / 64, 1);
+    // long-K products with few output tiles (weight gradients): split K over enough blocks to fill the GPU
+    int splits = 1;
+    if (epi == EPI_STORE && split_buf) {
+        const int tiles = grid.x * grid.y;
+        splits = std::min(GEMM_MAX_SPLITS, std::max(1, 296 / tiles));
+        splits = std::min(splits, std::max(1, K / 256));
+    }
+    const int kchunk = ((K + splits - 1) / splits + 15) / 16 * 16;
+    splits = (K + kchunk - 1) / kchunk;
+    grid.z = splits;
+    if (splits == 1) {
+        k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, A, sai, sak, B, sbk, sbj, epi, Cf, bias, Zin, Hb, kchunk);
+        return;
+    }
+    k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, A, sai, sak, B, sbk, sbj, epi, split_buf, bias, Zin, Hb, kchunk);
+    k_sum_splits<<<(M * N + 255) / 256, 256, 0, st>>>(split_buf, splits, M * N, Cf);
 }
 
 // ---------------------------------------------------------------------------
@@ -321,6 +353,7 @@ struct phmc_surrogate {
     float* grad = nullptr;
     float *adam_m = nullptr, *adam_v = nullptr;
     float* d_scale = nullptr;
+    float* split = nullptr;             // split-K partial products (GEMM_MAX_SPLITS x max(n_in, H) x H)
     int adam_t = 0;
     std::vector<void*> allocs;
 };
@@ -405,6 +438,7 @@ extern "C" int phmc_surrogate_create(int n_in, int hidden, uint64_t seed, phmc_s
         (s = malloc_t(h, &h->adam_m, h->nparam)) || (s = malloc_t(h, &h->adam_v, h->nparam)) ||
         (s = malloc_t(h, &h->mu, n_in)) || (s = malloc_t(h, &h->sd, n_in)) || (s = malloc_t(h, &h->loss, 1)) ||
         (s = malloc_t(h, &h->d_scale, 1)) || (s = malloc_t(h, &h->packed[0], (size_t)nk1 * hidden / 4)) ||
+        (s = malloc_t(h, &h->split, (size_t)GEMM_MAX_SPLITS * std::max(n_in, hidden) * hidden)) ||
         (s = malloc_t(h, &h->packed[1], (size_t)hidden * hidden / 4)) || (s = malloc_t(h, &h->packed[2], (size_t)hidden * hidden / 4))) {
         phmc_surrogate_destroy(h);
         return s;
@@ -454,15 +488,15 @@ static void backward_rows(phmc_surrogate* h, const float* d_sign, const float* d
     k_out_wgrad<<<H + 1, 256, 0, st>>>(h->dy, h->Hb[2], n, H, h->grad + off[6], h->grad + off[7]);
     k_out_backward<<<(int)((n * H + 255) / 256), 256, 0, st>>>(h->dy, h->Z[2], n, H, reinterpret_cast<const uint16_t*>(W + off[6]), h->dZ[2]);
     // layer 3: dW3 = H2^T dZ3, db3 = colsum dZ3, dZ2 = (dZ3 W3^T) * gelu'(Z2)
-    gemm(H, H, (int)n, h->Hb[1], 1, H, h->dZ[2], H, 1, EPI_STORE, h->grad + off[4], nullptr, nullptr, nullptr, st);
+    gemm(H, H, (int)n, h->Hb[1], 1, H, h->dZ[2], H, 1, EPI_STORE, h->grad + off[4], nullptr, nullptr, nullptr, st, h->split);
     k_colsum<<<H, 256, 0, st>>>(h->dZ[2], n, H, h->grad + off[5]);
     gemm((int)n, H, H, h->dZ[2], H, 1, W + off[4], 1, H, EPI_GELU_GRAD, nullptr, nullptr, h->Z[1], h->dZ[1], st);
     // layer 2
-    gemm(H, H, (int)n, h->Hb[0], 1, H, h->dZ[1], H, 1, EPI_STORE, h->grad + off[2], nullptr, nullptr, nullptr, st);
+    gemm(H, H, (int)n, h->Hb[0], 1, H, h->dZ[1], H, 1, EPI_STORE, h->grad + off[2], nullptr, nullptr, nullptr, st, h->split);
     k_colsum<<<H, 256, 0, st>>>(h->dZ[1], n, H, h->grad + off[3]);
     gemm((int)n, H, H, h->dZ[1], H, 1, W + off[2], 1, H, EPI_GELU_GRAD, nullptr, nullptr, h->Z[0], h->dZ[0], st);
     // layer 1
-    gemm(nin, H, (int)n, h->X, 1, nin, h->dZ[0], H, 1, EPI_STORE, h->grad + off[0], nullptr, nullptr, nullptr, st);
+    gemm(nin, H, (int)n, h->X, 1, nin, h->dZ[0], H, 1, EPI_STORE, h->grad + off[0], nullptr, nullptr, nullptr, st, h->split);
     k_colsum<<<H, 256, 0, st>>>(h->dZ[0], n, H, h->grad + off[1]);
 }
 

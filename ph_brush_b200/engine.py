@@ -125,7 +125,8 @@ class Engine:
 
     # ---- state ----
     def state(self, replica=0):
-        n = self.caps[replica]
+        """Slot arrays of one replica, or of all replicas concatenated (replica=-1)."""
+        n = sum(self.caps) if replica < 0 else self.caps[replica]
         x, y, z, q = (np.zeros(n, np.float32) for _ in range(4))
         t, f = np.zeros(n, np.int32), np.zeros(n, np.int32)
         _abi.check(self._lib.phmc_get_state(self._h, replica, _abi.fptr(x), _abi.fptr(y), _abi.fptr(z),
