@@ -7,7 +7,7 @@
 
 #define PHMC_MAX_TYPES 8
 #define PHMC_MAX_ORDER 6
-#define PHMC_MAX_PEND 64
+#define PHMC_MAX_PEND 128
 #define PHMC_FIX_SCALE 1099511627776.0   /* 2^40: fixed-point scale of the charge mesh */
 #define PHMC_FIX_INV (1.0 / 1099511627776.0)
 

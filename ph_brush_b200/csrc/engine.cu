@@ -699,6 +699,23 @@ extern "C" int phmc_set_replay(phmc_engine* h, int64_t n, const int* decisions) 
     return PHMC_OK;
 }
 
+// protonated (charged) titratable sites of every replica, one block per replica
+__global__ void k_count_charged(DevPtrs d, int* __restrict__ out) {
+    const int r = blockIdx.x;
+    const RepDesc& D = d.desc[r];
+    int c = 0;
+    for (int k = threadIdx.x; k < D.n_titr; k += blockDim.x) c += d.posq[D.slot_off + d.titr[D.slot_off + k]].w != 0.0f;
+    c = __reduce_add_sync(0xffffffffu, c);
+    __shared__ int s[8];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)blockDim.x / 32; ++w) t += s[w];
+        out[r] = t;
+    }
+}
+
 static int collect_stats(phmc_engine* h, phmc_run_stats* stats) {
     Engine& E = h->E;
     std::vector<RepState> st((size_t)E.R);
@@ -712,18 +729,16 @@ static int collect_stats(phmc_engine* h, phmc_run_stats* stats) {
         o.n_cations = st[r].n_cation; o.n_anions = st[r].n_anion;
         o.energy = st[r].E; o.energy_drift = st[r].drift;
     }
-    // protonated sites: count titratable sites with q != 0 (host side, small)
-    for (int r = 0; r < E.R; ++r) {
-        const RepDesc& D = E.desc[r];
-        if (D.n_titr == 0) continue;
-        std::vector<int> titr((size_t)D.n_titr);
-        std::vector<float4> pq((size_t)D.cap);
-        CU(cudaMemcpy(titr.data(), E.d.titr + D.slot_off, sizeof(int) * D.n_titr, cudaMemcpyDeviceToHost));
-        CU(cudaMemcpy(pq.data(), E.d.posq + D.slot_off, sizeof(float4) * D.cap, cudaMemcpyDeviceToHost));
-        int c = 0;
-        for (int i : titr) if (pq[i].w != 0.0f) ++c;
-        stats[r].n_charged_sites = c;
-    }
+    // protonated sites: titratable sites with q != 0, counted on the device
+    int* d_cnt = nullptr;
+    CU(cudaMalloc((void**)&d_cnt, sizeof(int) * E.R));
+    k_count_charged<<<E.R, 256, 0, E.stream>>>(E.d, d_cnt);
+    std::vector<int> cnt((size_t)E.R);
+    cudaError_t e = cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * E.R, cudaMemcpyDeviceToHost, E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    cudaFree(d_cnt);
+    if (e != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string("collect_stats: ") + cudaGetErrorString(e));
+    for (int r = 0; r < E.R; ++r) stats[r].n_charged_sites = cnt[(size_t)r];
     return PHMC_OK;
 }
 
@@ -880,16 +895,24 @@ extern "C" int phmc_get_state(phmc_engine* h, int rep, float* x, float* y, float
     return PHMC_OK;
 }
 
-// Host-side lists of one replica from its slot arrays, uploaded on the engine stream.
+// Host copies of the slot arrays and lists of replicas [r0, r1), uploaded with one copy per array.
+struct StateStage {
+    int off = 0, n = 0;
+    std::vector<float4> pq;
+    std::vector<int> type, flags, mob, mpos, an, apos, ca, cpos, fr, ti;
+};
+
+// Lists of one replica from its slot arrays into the stage (slot i of the replica at i + D.slot_off - off).
 static int stage_replica_state(phmc_engine* h, int rep, const float* x, const float* y, const float* z, const float* q,
-                               const int* type, const int* flags) {
+                               const int* type, const int* flags, StateStage& sg, RepState& st) {
     Engine& E = h->E;
     RepDesc& D = E.desc[rep];
-    const int cap = D.cap, so = D.slot_off;
-    std::vector<float4> pq((size_t)cap);
-    std::vector<int> mob(cap, -1), mpos(cap, -1), an(cap, -1), apos(cap, -1), ca(cap, -1), cpos(cap, -1), fr(cap, -1), ti(cap, -1);
-    RepState st;
-    CU(cudaMemcpy(&st, E.d.state + rep, sizeof(RepState), cudaMemcpyDeviceToHost));
+    const int cap = D.cap, o = D.slot_off - sg.off;
+    float4* pq = sg.pq.data() + o;
+    int *mob = sg.mob.data() + o, *mpos = sg.mpos.data() + o, *an = sg.an.data() + o, *apos = sg.apos.data() + o;
+    int *ca = sg.ca.data() + o, *cpos = sg.cpos.data() + o, *fr = sg.fr.data() + o, *ti = sg.ti.data() + o;
+    std::memcpy(sg.type.data() + o, type, sizeof(int) * cap);
+    std::memcpy(sg.flags.data() + o, flags, sizeof(int) * cap);
     st.n_mobile = st.n_anion = st.n_cation = st.n_free = 0;
     int nt = 0, npres = 0;
     for (int i = 0; i < cap; ++i) {
@@ -909,20 +932,6 @@ static int stage_replica_state(phmc_engine* h, int rep, const float* x, const fl
         if (flags[i] & PHMC_F_GHOST) fr[st.n_free++] = i;
     D.n_titr = nt;
     h->n_present[rep] = npres;
-    // synchronous copies: the staging vectors are local
-    CU(cudaMemcpy(E.d.posq + so, pq.data(), sizeof(float4) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.type + so, type, sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.flags + so, flags, sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.mobile + so, mob.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.mobile_pos + so, mpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.anions + so, an.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.anion_pos + so, apos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.cations + so, ca.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.cation_pos + so, cpos.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.freel + so, fr.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.titr + so, ti.data(), sizeof(int) * cap, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.state + rep, &st, sizeof(RepState), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.desc + rep, &D, sizeof(RepDesc), cudaMemcpyHostToDevice));
     return PHMC_OK;
 }
 
@@ -934,11 +943,33 @@ extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const flo
     CU(cudaStreamSynchronize(E.stream));
     // one replica, or (rep == -1) all replicas from arrays concatenated in replica order
     const int r0 = rep < 0 ? 0 : rep, r1 = rep < 0 ? E.R : rep + 1;
+    StateStage sg;
+    sg.off = E.desc[r0].slot_off;
+    sg.n = E.desc[r1 - 1].slot_off + E.desc[r1 - 1].cap - sg.off;
+    const size_t n = (size_t)sg.n;
+    sg.pq.resize(n); sg.type.resize(n); sg.flags.resize(n);
+    for (std::vector<int>* v : {&sg.mob, &sg.mpos, &sg.an, &sg.apos, &sg.ca, &sg.cpos, &sg.fr, &sg.ti}) v->assign(n, -1);
+    std::vector<RepState> st((size_t)(r1 - r0));
+    CU(cudaMemcpy(st.data(), E.d.state + r0, sizeof(RepState) * (r1 - r0), cudaMemcpyDeviceToHost));
     for (int r = r0; r < r1; ++r) {
         const int o = rep < 0 ? E.desc[r].slot_off : 0;
-        const int s = stage_replica_state(h, r, x + o, y + o, z + o, q + o, type + o, flags + o);
+        const int s = stage_replica_state(h, r, x + o, y + o, z + o, q + o, type + o, flags + o, sg, st[(size_t)(r - r0)]);
         if (s) return s;
     }
+    const int so = sg.off;
+    CU(cudaMemcpy(E.d.posq + so, sg.pq.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.type + so, sg.type.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.flags + so, sg.flags.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.mobile + so, sg.mob.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.mobile_pos + so, sg.mpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.anions + so, sg.an.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.anion_pos + so, sg.apos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.cations + so, sg.ca.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.cation_pos + so, sg.cpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.freel + so, sg.fr.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.titr + so, sg.ti.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.state + r0, st.data(), sizeof(RepState) * (r1 - r0), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(E.d.desc + r0, E.desc.data() + r0, sizeof(RepDesc) * (r1 - r0), cudaMemcpyHostToDevice));
     launch_cell_build(E, E.stream);
     h->prof.kernel_launches += 2;
     int rc = full_recompute(h);
@@ -1154,7 +1185,7 @@ static int apply_tuning(phmc_engine* h, int pend, int threads) {
 extern "C" int phmc_set_tuning(phmc_engine* h, int pending_max, int threads) {
     if (!h) return fail(PHMC_ERR_ARG, "null engine");
     if (pending_max < 4 || pending_max > PHMC_MAX_PEND || (threads != 128 && threads != 256))
-        return fail(PHMC_ERR_ARG, "pending_max must be in [4, 64] and threads 128 or 256");
+        return fail(PHMC_ERR_ARG, "pending_max must be in [4, 128] and threads 128 or 256");
     CU(cudaSetDevice(h->E.device));
     CU(cudaStreamSynchronize(h->E.stream));
     return apply_tuning(h, pending_max, threads);
@@ -1173,7 +1204,7 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     Engine& E = h->E;
     CU(cudaSetDevice(E.device));
     CU(cudaStreamSynchronize(E.stream));
-    const int pends[] = {8, 16, 24, 32, 48, 64};
+    const int pends[] = {8, 16, 24, 32, 48, 64, 96, 128};
     const int ths[] = {128, 256};
     int best_p = E.pend_max, best_t = E.threads, n = 0;
     double best = 1e300;

@@ -38,9 +38,9 @@ struct PairK {
     int f[3][2 * P - 1];  // folded octant coordinate of D + delta
     float coef;
     int pad;
-    // per (dz, dy) row: octant row offset and coef * Ky * Kz
+    // per (dz, dy) row: octant row offset (coef * Ky * Kz is recomputed where it is used,
+    // which keeps the table small enough for two MC blocks per SM at 64 pending stencils)
     int roff[(2 * P - 1) * (2 * P - 1)];
-    float kyz[(2 * P - 1) * (2 * P - 1)];
 };
 
 struct TrialS {
@@ -880,7 +880,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         }
         __syncthreads();
         if (D.coulomb == PHMC_COUL_EWALD) {
-            // phase 3b: per (pair, dz, dy) row, the octant row offset and coef * Ky * Kz
+            // phase 3b: per (pair, dz, dy) row, the octant row offset
             constexpr int W = 2 * P - 1;
             const int ox = D.oct[0], oy = D.oct[1];
             const int nrow = T.npairs * W * W;
@@ -889,7 +889,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 const int dz = rw / W, dy = rw - dz * W;
                 PairK<P>& pk = s_pair[q];
                 pk.roff[rw] = (pk.f[2][dz] * oy + pk.f[1][dy]) * ox;
-                pk.kyz[rw] = pk.coef * pk.K[1][dy] * pk.K[2][dz];
             }
             __syncthreads();
         }
@@ -990,8 +989,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                     const int rowg = itc / W, dx = itc - rowg * W;  // rowg = pair * W*W + row
                     const int q = rowg / (W * W), rw = rowg - q * (W * W);
                     const PairK<P>& pk = s_pair[q];
+                    const int dz = rw / W, dy = rw - dz * W;
                     g[u] = __ldg(&G[pk.roff[rw] + pk.f[0][dx]]);
-                    kk[u] = (it < nit) ? pk.kyz[rw] * pk.K[0][dx] : 0.0f;
+                    const float kyz = pk.coef * pk.K[1][dy] * pk.K[2][dz];
+                    kk[u] = (it < nit) ? kyz * pk.K[0][dx] : 0.0f;
                 }
 #pragma unroll
                 for (int u = 0; u < RB; ++u) acc_rec += (double)(kk[u] * g[u]);

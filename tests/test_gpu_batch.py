@@ -51,3 +51,55 @@ def test_config3_replicas_build_and_run():
     with Engine([s for s, _ in reps], [p for _, p in reps]) as e:
         st = e.run(300)
     assert all(s_["attempted"][0] > 0 for s_ in st)
+
+
+def _with_state(s, st):
+    """A copy of SystemArrays s holding every slot of state st (empty slots flagged)."""
+    import copy
+    out = copy.deepcopy(s)
+    for k in ("x", "y", "z", "q"):
+        setattr(out, k, np.ascontiguousarray(st[k], np.float32))
+    out.type = np.ascontiguousarray(st["type"], np.int32)
+    out.flags = np.ascontiguousarray(st["flags"], np.int32)
+    out.capacity = len(st["x"])
+    return out
+
+
+@pytest.mark.gpu
+def test_state_upload_one_and_all_replicas():
+    """phmc_set_state for one replica and for all replicas at once (concatenated
+    arrays): lists, cells and the potential mesh are rebuilt, the energies are those
+    of the uploaded states (FP64 oracle), and the chains continue from them."""
+    from oracle import pyoracle as O
+    reps = ragged_set()
+    S, P = [s for s, _ in reps], [p for _, p in reps]
+    with Engine(S, P) as e:
+        e.run(800)
+        st_all = e.state(-1)
+        # perturb: flip the charge state of one titratable site of replica 1 (slot arrays of all replicas)
+        off = sum(e.caps[:1])
+        f1 = st_all["flags"][off:off + e.caps[1]]
+        site = int(np.nonzero((f1 & 2) != 0)[0][0])
+        st_all["q"][off + site] = 1.0 - st_all["q"][off + site]
+        st_all["type"][off + site] = 1 - st_all["type"][off + site]
+        e.set_state(st_all, -1)
+        got = [c["total"] for c in e.energy()]
+        for r in range(len(reps)):
+            o = sum(e.caps[:r])
+            sub = {k: v[o:o + e.caps[r]] for k, v in st_all.items()}
+            ref = O.energy(_with_state(S[r], sub), P[r])["total"]
+            assert abs(got[r] - ref) <= 1e-6 * abs(ref) + 1e-4, (r, got[r], ref)
+        # one replica: put replica 2 back to its generated state
+        g = S[2]
+        cap = e.caps[2]
+        one = {"x": np.zeros(cap, np.float32), "y": np.zeros(cap, np.float32), "z": np.zeros(cap, np.float32),
+               "q": np.zeros(cap, np.float32), "type": np.zeros(cap, np.int32), "flags": np.full(cap, 4, np.int32)}
+        for k in ("x", "y", "z", "q", "type", "flags"):
+            one[k][:g.n] = getattr(g, k)
+        e.set_state(one, 2)
+        assert abs(e.energy()[2]["total"] - O.energy(g, P[2])["total"]) <= 1e-6 * abs(O.energy(g, P[2])["total"]) + 1e-4
+        st = e.run(600)
+        fresh = e.energy()
+        for a, b in zip(st, fresh):
+            assert abs(a["energy"] - b["total"]) <= 1e-6 * abs(b["total"]) + 1e-3
+        assert all(0 <= x["n_charged_sites"] <= x["n_titratable"] for x in st)
