@@ -64,8 +64,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline only (plain comparison, phases, alpha skipped)")
     ap.add_argument("--no-alpha", action="store_true")
-    ap.add_argument("--alpha-eq", type=int, default=600, help="sweeps of equilibration in the alpha(pH) check")
-    ap.add_argument("--alpha-sample", type=int, default=400, help="sweeps sampled in the alpha(pH) check")
+    ap.add_argument("--alpha-eq", type=int, default=1200, help="sweeps of equilibration in the alpha(pH) check")
+    ap.add_argument("--alpha-sample", type=int, default=600, help="sweeps sampled in the alpha(pH) check")
     return ap.parse_args()
 
 

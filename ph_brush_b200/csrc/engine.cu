@@ -52,6 +52,9 @@ struct phmc_engine {
     std::vector<cudaEvent_t> gev;  // 4 per chunk when profiling
     // delayed-acceptance log destinations (host)
     int* h_da_stage = nullptr; double* h_da_dEs = nullptr;
+    // device staging of state uploads / readbacks (allocated on first use, total_slots long)
+    float *st_x = nullptr, *st_y = nullptr, *st_z = nullptr, *st_q = nullptr;
+    int *st_t = nullptr, *st_f = nullptr, *st_err = nullptr, *st_cnt = nullptr;
 };
 
 static void drop_graph(phmc_engine* h) {
@@ -546,6 +549,9 @@ extern "C" int phmc_destroy(phmc_engine* h) {
     if (E.d.log_move) { cudaFree(E.d.log_move); cudaFree(E.d.log_dE); cudaFree(E.d.log_acc); }
     if (E.d.log_stage) { cudaFree(E.d.log_stage); cudaFree(E.d.log_dEs); }
     if (E.d.hv_cap > 0) { cudaFree(E.d.hv_rows); cudaFree(E.d.hv_sign); cudaFree(E.d.hv_target); cudaFree(E.d.hv_count); }
+    for (void* p : {(void*)h->st_x, (void*)h->st_y, (void*)h->st_z, (void*)h->st_q, (void*)h->st_t, (void*)h->st_f,
+                    (void*)h->st_err, (void*)h->st_cnt})
+        if (p) cudaFree(p);
     if (E.stream) cudaStreamDestroy(E.stream);
     delete h;
     return PHMC_OK;
@@ -874,64 +880,140 @@ extern "C" int phmc_run(phmc_engine* h, int64_t n_trials, phmc_run_stats* stats)
     return PHMC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// state upload / readback: caller arrays <-> device staging (direct copies, DMA
+// from pinned memory), interleaving, validation and list building on the device
+// ---------------------------------------------------------------------------
+static int ensure_state_staging(phmc_engine* h) {
+    if (h->st_x) return PHMC_OK;
+    const size_t n = (size_t)h->E.total_slots;
+    CU(cudaMalloc((void**)&h->st_x, sizeof(float) * n));
+    CU(cudaMalloc((void**)&h->st_y, sizeof(float) * n));
+    CU(cudaMalloc((void**)&h->st_z, sizeof(float) * n));
+    CU(cudaMalloc((void**)&h->st_q, sizeof(float) * n));
+    CU(cudaMalloc((void**)&h->st_t, sizeof(int) * n));
+    CU(cudaMalloc((void**)&h->st_f, sizeof(int) * n));
+    CU(cudaMalloc((void**)&h->st_err, sizeof(int)));
+    CU(cudaMalloc((void**)&h->st_cnt, sizeof(int) * 2 * h->E.R));
+    return PHMC_OK;
+}
+
+__global__ void k_state_egress(DevPtrs d, int off, int n, float* x, float* y, float* z, float* q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = d.posq[off + i];
+    x[i] = p.x; y[i] = p.y; z[i] = p.z; q[i] = p.w;
+}
+
+// staged slot arrays (index s - off) of replicas [r0, r0 + gridDim.x): 1 = type out of range,
+// 2 = a present particle outside [0, L)
+__global__ void k_state_check(DevPtrs d, int r0, int off, const float* __restrict__ x, const float* __restrict__ y,
+                              const float* __restrict__ z, const int* __restrict__ t, const int* __restrict__ f, int* err) {
+    const RepDesc& D = d.desc[r0 + blockIdx.x];
+    for (int i = threadIdx.x; i < D.cap; i += blockDim.x) {
+        const int s = D.slot_off + i - off;
+        if (t[s] < 0 || t[s] >= D.T) atomicMax(err, 1);
+        if (!(f[s] & PHMC_F_GHOST) && !(x[s] >= 0.0f && x[s] < D.L[0] && y[s] >= 0.0f && y[s] < D.L[1] && z[s] >= 0.0f && z[s] < D.L[2]))
+            atomicMax(err, 2);
+    }
+}
+
+// One block per replica: particle arrays, membership lists with position maps, the
+// free stack (top = lowest empty slot) and the counts, in slot order as on the host.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_state_ingest(DevPtrs d, int r0, int off, const float* __restrict__ x,
+                                                     const float* __restrict__ y, const float* __restrict__ z,
+                                                     const float* __restrict__ q, const int* __restrict__ t,
+                                                     const int* __restrict__ f, int* __restrict__ counts) {
+    const int r = r0 + blockIdx.x;
+    RepDesc& D = d.desc[r];
+    const int cap = D.cap, so = D.slot_off;
+    __shared__ int s_ghost;
+    __shared__ int s_warp[5][NT / 32];
+    __shared__ int s_base[5];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // pass 1: number of empty slots (the free stack is filled from the top of the slot range)
+    if (threadIdx.x == 0) s_ghost = 0;
+    __syncthreads();
+    int g = 0;
+    for (int i = threadIdx.x; i < cap; i += NT) g += (f[so + i - off] & PHMC_F_GHOST) != 0;
+    g = __reduce_add_sync(0xffffffffu, g);
+    if (lane == 0) atomicAdd(&s_ghost, g);
+    if (threadIdx.x < 5) s_base[threadIdx.x] = 0;
+    __syncthreads();
+    const int n_ghost = s_ghost;
+    // pass 2: chunks of NT slots, block-wide exclusive scans of the five memberships
+    for (int c0 = 0; c0 < cap; c0 += NT) {
+        const int i = c0 + threadIdx.x;
+        int fl = PHMC_F_GHOST;
+        if (i < cap) {
+            const int s = so + i - off;
+            fl = f[s];
+            d.posq[so + i] = make_float4(x[s], y[s], z[s], q[s]);
+            d.type[so + i] = t[s];
+            d.flags[so + i] = fl;
+        }
+        const bool pres = i < cap && !(fl & PHMC_F_GHOST);
+        const int m[5] = {pres && (fl & PHMC_F_MOBILE), pres && (fl & PHMC_F_ANION), pres && (fl & PHMC_F_CATION),
+                          pres && (fl & PHMC_F_TITRATABLE), i < cap && (fl & PHMC_F_GHOST)};
+        int ex[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const unsigned bal = __ballot_sync(0xffffffffu, m[k]);
+            ex[k] = __popc(bal & ((1u << lane) - 1u));
+            if (lane == 0) s_warp[k][warp] = __popc(bal);
+        }
+        __syncthreads();
+        if (threadIdx.x < 5) {  // warp totals -> exclusive warp offsets, chunk total -> base
+            const int k = threadIdx.x;
+            int acc = s_base[k];
+            for (int w = 0; w < NT / 32; ++w) { const int v = s_warp[k][w]; s_warp[k][w] = acc; acc += v; }
+            s_base[k] = acc;
+        }
+        __syncthreads();
+        if (i < cap) {
+            int pos[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) pos[k] = s_warp[k][warp] + ex[k];
+            d.mobile_pos[so + i] = m[0] ? pos[0] : -1;
+            if (m[0]) d.mobile[so + pos[0]] = i;
+            d.anion_pos[so + i] = m[1] ? pos[1] : -1;
+            if (m[1]) d.anions[so + pos[1]] = i;
+            d.cation_pos[so + i] = m[2] ? pos[2] : -1;
+            if (m[2]) d.cations[so + pos[2]] = i;
+            if (m[3]) d.titr[so + pos[3]] = i;
+            if (m[4]) d.freel[so + n_ghost - 1 - pos[4]] = i;  // the highest empty slot at the bottom
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        RepState& S = d.state[r];
+        S.n_mobile = s_base[0]; S.n_anion = s_base[1]; S.n_cation = s_base[2]; S.n_free = s_base[4];
+        D.n_titr = s_base[3];
+        counts[2 * r] = s_base[3];
+        counts[2 * r + 1] = cap - s_base[4];
+    }
+}
+
 extern "C" int phmc_get_state(phmc_engine* h, int rep, float* x, float* y, float* z, float* q, int* type, int* flags) {
     if (!h || rep < -1 || rep >= h->E.R) return fail(PHMC_ERR_ARG, "invalid replica");
     Engine& E = h->E;
     CU(cudaSetDevice(E.device));
-    CU(cudaStreamSynchronize(E.stream));
+    int s = ensure_state_staging(h);
+    if (s) return s;
     // one replica, or (rep == -1) all replicas concatenated in replica order, capacity slots each
     const int off = rep < 0 ? 0 : E.desc[rep].slot_off;
     const int cap = rep < 0 ? E.total_slots : E.desc[rep].cap;
-    std::vector<float4> pq((size_t)cap);
-    CU(cudaMemcpy(pq.data(), E.d.posq + off, sizeof(float4) * cap, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < cap; ++i) {
-        if (x) x[i] = pq[i].x;
-        if (y) y[i] = pq[i].y;
-        if (z) z[i] = pq[i].z;
-        if (q) q[i] = pq[i].w;
-    }
-    if (type) CU(cudaMemcpy(type, E.d.type + off, sizeof(int) * cap, cudaMemcpyDeviceToHost));
-    if (flags) CU(cudaMemcpy(flags, E.d.flags + off, sizeof(int) * cap, cudaMemcpyDeviceToHost));
-    return PHMC_OK;
-}
-
-// Host copies of the slot arrays and lists of replicas [r0, r1), uploaded with one copy per array.
-struct StateStage {
-    int off = 0, n = 0;
-    std::vector<float4> pq;
-    std::vector<int> type, flags, mob, mpos, an, apos, ca, cpos, fr, ti;
-};
-
-// Lists of one replica from its slot arrays into the stage (slot i of the replica at i + D.slot_off - off).
-static int stage_replica_state(phmc_engine* h, int rep, const float* x, const float* y, const float* z, const float* q,
-                               const int* type, const int* flags, StateStage& sg, RepState& st) {
-    Engine& E = h->E;
-    RepDesc& D = E.desc[rep];
-    const int cap = D.cap, o = D.slot_off - sg.off;
-    float4* pq = sg.pq.data() + o;
-    int *mob = sg.mob.data() + o, *mpos = sg.mpos.data() + o, *an = sg.an.data() + o, *apos = sg.apos.data() + o;
-    int *ca = sg.ca.data() + o, *cpos = sg.cpos.data() + o, *fr = sg.fr.data() + o, *ti = sg.ti.data() + o;
-    std::memcpy(sg.type.data() + o, type, sizeof(int) * cap);
-    std::memcpy(sg.flags.data() + o, flags, sizeof(int) * cap);
-    st.n_mobile = st.n_anion = st.n_cation = st.n_free = 0;
-    int nt = 0, npres = 0;
-    for (int i = 0; i < cap; ++i) {
-        if (type[i] < 0 || type[i] >= D.T) return fail(PHMC_ERR_ARG, "type out of range");
-        const int f = flags[i];
-        if (!(f & PHMC_F_GHOST) && !(x[i] >= 0 && x[i] < D.L[0] && y[i] >= 0 && y[i] < D.L[1] && z[i] >= 0 && z[i] < D.L[2]))
-            return fail(PHMC_ERR_ARG, "particle outside [0,L)");
-        pq[i] = make_float4(x[i], y[i], z[i], q[i]);
-        if (f & PHMC_F_GHOST) continue;
-        ++npres;
-        if (f & PHMC_F_MOBILE) { mpos[i] = st.n_mobile; mob[st.n_mobile++] = i; }
-        if (f & PHMC_F_TITRATABLE) ti[nt++] = i;
-        if (f & PHMC_F_ANION) { apos[i] = st.n_anion; an[st.n_anion++] = i; }
-        if (f & PHMC_F_CATION) { cpos[i] = st.n_cation; ca[st.n_cation++] = i; }
-    }
-    for (int i = cap - 1; i >= 0; --i)
-        if (flags[i] & PHMC_F_GHOST) fr[st.n_free++] = i;
-    D.n_titr = nt;
-    h->n_present[rep] = npres;
+    const cudaStream_t st = E.stream;
+    k_state_egress<<<(cap + 255) / 256, 256, 0, st>>>(E.d, off, cap, h->st_x, h->st_y, h->st_z, h->st_q);
+    CU(cudaGetLastError());
+    if (x) CU(cudaMemcpyAsync(x, h->st_x, sizeof(float) * cap, cudaMemcpyDeviceToHost, st));
+    if (y) CU(cudaMemcpyAsync(y, h->st_y, sizeof(float) * cap, cudaMemcpyDeviceToHost, st));
+    if (z) CU(cudaMemcpyAsync(z, h->st_z, sizeof(float) * cap, cudaMemcpyDeviceToHost, st));
+    if (q) CU(cudaMemcpyAsync(q, h->st_q, sizeof(float) * cap, cudaMemcpyDeviceToHost, st));
+    if (type) CU(cudaMemcpyAsync(type, E.d.type + off, sizeof(int) * cap, cudaMemcpyDeviceToHost, st));
+    if (flags) CU(cudaMemcpyAsync(flags, E.d.flags + off, sizeof(int) * cap, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
     return PHMC_OK;
 }
 
@@ -940,40 +1022,38 @@ extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const flo
     if (!h || rep < -1 || rep >= h->E.R || !x || !y || !z || !q || !type || !flags) return fail(PHMC_ERR_ARG, "invalid argument");
     Engine& E = h->E;
     CU(cudaSetDevice(E.device));
-    CU(cudaStreamSynchronize(E.stream));
+    int s = ensure_state_staging(h);
+    if (s) return s;
     // one replica, or (rep == -1) all replicas from arrays concatenated in replica order
-    const int r0 = rep < 0 ? 0 : rep, r1 = rep < 0 ? E.R : rep + 1;
-    StateStage sg;
-    sg.off = E.desc[r0].slot_off;
-    sg.n = E.desc[r1 - 1].slot_off + E.desc[r1 - 1].cap - sg.off;
-    const size_t n = (size_t)sg.n;
-    sg.pq.resize(n); sg.type.resize(n); sg.flags.resize(n);
-    for (std::vector<int>* v : {&sg.mob, &sg.mpos, &sg.an, &sg.apos, &sg.ca, &sg.cpos, &sg.fr, &sg.ti}) v->assign(n, -1);
-    std::vector<RepState> st((size_t)(r1 - r0));
-    CU(cudaMemcpy(st.data(), E.d.state + r0, sizeof(RepState) * (r1 - r0), cudaMemcpyDeviceToHost));
-    for (int r = r0; r < r1; ++r) {
-        const int o = rep < 0 ? E.desc[r].slot_off : 0;
-        const int s = stage_replica_state(h, r, x + o, y + o, z + o, q + o, type + o, flags + o, sg, st[(size_t)(r - r0)]);
-        if (s) return s;
-    }
-    const int so = sg.off;
-    CU(cudaMemcpy(E.d.posq + so, sg.pq.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.type + so, sg.type.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.flags + so, sg.flags.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.mobile + so, sg.mob.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.mobile_pos + so, sg.mpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.anions + so, sg.an.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.anion_pos + so, sg.apos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.cations + so, sg.ca.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.cation_pos + so, sg.cpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.freel + so, sg.fr.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.titr + so, sg.ti.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.state + r0, st.data(), sizeof(RepState) * (r1 - r0), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(E.d.desc + r0, E.desc.data() + r0, sizeof(RepDesc) * (r1 - r0), cudaMemcpyHostToDevice));
-    launch_cell_build(E, E.stream);
-    h->prof.kernel_launches += 2;
-    int rc = full_recompute(h);
+    const int r0 = rep < 0 ? 0 : rep, nr = rep < 0 ? E.R : 1;
+    const int off = E.desc[r0].slot_off;
+    const int n = E.desc[r0 + nr - 1].slot_off + E.desc[r0 + nr - 1].cap - off;
+    const cudaStream_t st = E.stream;
+    CU(cudaMemcpyAsync(h->st_x, x, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(h->st_y, y, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(h->st_z, z, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(h->st_q, q, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(h->st_t, type, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(h->st_f, flags, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(h->st_err, 0, sizeof(int), st));
+    k_state_check<<<nr, 256, 0, st>>>(E.d, r0, off, h->st_x, h->st_y, h->st_z, h->st_t, h->st_f, h->st_err);
+    int err = 0;
+    CU(cudaMemcpyAsync(&err, h->st_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (err == 1) return fail(PHMC_ERR_ARG, "type out of range");
+    if (err == 2) return fail(PHMC_ERR_ARG, "particle outside [0,L)");
+    k_state_ingest<256><<<nr, 256, 0, st>>>(E.d, r0, off, h->st_x, h->st_y, h->st_z, h->st_q, h->st_t, h->st_f, h->st_cnt);
+    CU(cudaGetLastError());
+    std::vector<int> cnt((size_t)2 * E.R);
+    CU(cudaMemcpyAsync(cnt.data() + 2 * r0, h->st_cnt + 2 * r0, sizeof(int) * 2 * nr, cudaMemcpyDeviceToHost, st));
+    launch_cell_build(E, st);
+    h->prof.kernel_launches += 4;
+    int rc = full_recompute(h);  // synchronises the stream
     h->prof.kernel_launches += E.flush_kernels + 2;
+    for (int r = r0; r < r0 + nr; ++r) {
+        E.desc[(size_t)r].n_titr = cnt[(size_t)2 * r];
+        h->n_present[(size_t)r] = cnt[(size_t)2 * r + 1];
+    }
     return rc;
 }
 
