@@ -125,6 +125,7 @@ struct DevPtrs {
     int4* cell_cls;
     // delayed acceptance
     SurDev sur;
+    int sur_late_l3;     // two-buffer staging (layer 3 copied after layer 1) to keep two MC blocks per SM
     float da_threshold;  // minimum second-stage acceptance among first-stage passes
     int da_window;       // first-stage passes per agreement check
     // training-sample harvest: rows [cap][SUR_ROWS][SUR_K], signs [cap][SUR_ROWS], targets [cap]

@@ -55,6 +55,7 @@ struct phmc_engine {
     // device staging of state uploads / readbacks (allocated on first use, total_slots long)
     float *st_x = nullptr, *st_y = nullptr, *st_z = nullptr, *st_q = nullptr;
     int *st_t = nullptr, *st_f = nullptr, *st_err = nullptr, *st_cnt = nullptr;
+    int* d_charged = nullptr;  // per replica charged-site counts of the last run
 };
 
 static void drop_graph(phmc_engine* h) {
@@ -550,7 +551,7 @@ extern "C" int phmc_destroy(phmc_engine* h) {
     if (E.d.log_stage) { cudaFree(E.d.log_stage); cudaFree(E.d.log_dEs); }
     if (E.d.hv_cap > 0) { cudaFree(E.d.hv_rows); cudaFree(E.d.hv_sign); cudaFree(E.d.hv_target); cudaFree(E.d.hv_count); }
     for (void* p : {(void*)h->st_x, (void*)h->st_y, (void*)h->st_z, (void*)h->st_q, (void*)h->st_t, (void*)h->st_f,
-                    (void*)h->st_err, (void*)h->st_cnt})
+                    (void*)h->st_err, (void*)h->st_cnt, (void*)h->d_charged})
         if (p) cudaFree(p);
     if (E.stream) cudaStreamDestroy(E.stream);
     delete h;
@@ -736,14 +737,11 @@ static int collect_stats(phmc_engine* h, phmc_run_stats* stats) {
         o.energy = st[r].E; o.energy_drift = st[r].drift;
     }
     // protonated sites: titratable sites with q != 0, counted on the device
-    int* d_cnt = nullptr;
-    CU(cudaMalloc((void**)&d_cnt, sizeof(int) * E.R));
-    k_count_charged<<<E.R, 256, 0, E.stream>>>(E.d, d_cnt);
+    if (!h->d_charged) CU(cudaMalloc((void**)&h->d_charged, sizeof(int) * E.R));
+    k_count_charged<<<E.R, 256, 0, E.stream>>>(E.d, h->d_charged);
     std::vector<int> cnt((size_t)E.R);
-    cudaError_t e = cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * E.R, cudaMemcpyDeviceToHost, E.stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
-    cudaFree(d_cnt);
-    if (e != cudaSuccess) return fail(PHMC_ERR_CUDA, std::string("collect_stats: ") + cudaGetErrorString(e));
+    CU(cudaMemcpyAsync(cnt.data(), h->d_charged, sizeof(int) * E.R, cudaMemcpyDeviceToHost, E.stream));
+    CU(cudaStreamSynchronize(E.stream));
     for (int r = 0; r < E.R; ++r) stats[r].n_charged_sites = cnt[(size_t)r];
     return PHMC_OK;
 }

@@ -75,4 +75,4 @@ int sur_train_device(phmc_surrogate* h, const float* d_x, const float* d_sign, c
 enum { MC_RUN = 0, MC_EVAL = 1, MC_APPLY = 2, MC_DESCRIBE = 3 };
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* d_trials, int n, double* d_dE, cudaStream_t st);
 cudaError_t prepare_mc(Engine& E);
-size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate = false);
+size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate = false, bool two_buffers = false);

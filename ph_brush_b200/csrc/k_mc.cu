@@ -38,9 +38,8 @@ struct PairK {
     int f[3][2 * P - 1];  // folded octant coordinate of D + delta
     float coef;
     int pad;
-    // per (dz, dy) row: octant row offset (coef * Ky * Kz is recomputed where it is used,
-    // which keeps the table small enough for two MC blocks per SM at 64 pending stencils)
-    int roff[(2 * P - 1) * (2 * P - 1)];
+    // (row offsets and coef * Ky * Kz are recomputed where they are used: 224 bytes per
+    // pair at order 5 keep two MC blocks per SM up to ~100 pending stencils)
 };
 
 struct TrialS {
@@ -466,8 +465,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     __nv_bfloat16* act0 = reinterpret_cast<__nv_bfloat16*>(sur_base);
     __nv_bfloat16* act1 = act0 + 16 * SUR_AST;
     uint2* wa = reinterpret_cast<uint2*>(sur_base + SUR_ACT_BYTES);
-    uint2* wb = wa + (SUR_K * SUR_HMAX * 2) / 8;
-    uint2* wc = wb + SUR_WBUF_BYTES / 8;
+    // three buffers (layer 1, 2, 3), or with sur_late_l3 two of SUR_HMAX^2 (layer 3 reuses layer 1's)
+    uint2* wb = d.sur_late_l3 ? wa + SUR_WBUF_BYTES / 8 : wa + (SUR_K * SUR_HMAX * 2) / 8;
+    uint2* wc = d.sur_late_l3 ? wa : wb + SUR_WBUF_BYTES / 8;
     uint32_t sur_par = 0;  // parity of the weight barriers' current phase (one phase per evaluated move)
 
     const int r = (mode == MC_RUN) ? blockIdx.x : ext_rep;
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             if (T.da && tid == 0) {  // stage the three hidden layers while the descriptor is built
                 sur_bulk_load(wa, d.sur.w[0], sur_layer_bytes(SUR_K, d.sur.H), &s_mbar[0]);
                 sur_bulk_load(wb, d.sur.w[1], sur_layer_bytes(d.sur.H, d.sur.H), &s_mbar[1]);
-                sur_bulk_load(wc, d.sur.w[2], sur_layer_bytes(d.sur.H, d.sur.H), &s_mbar[2]);
+                if (!d.sur_late_l3) sur_bulk_load(wc, d.sur.w[2], sur_layer_bytes(d.sur.H, d.sur.H), &s_mbar[2]);
             }
             if (tid == NT - 1) desc_exact_terms(T, D, S);
             // (a) the descriptor sphere's cells: inner 27 cells -> counts for the particle
@@ -694,7 +694,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             __syncthreads();
             // (d) network on the rows (tensor cores), first-stage decision
             if (T.da) {
-                sur_forward_staged<NT>(d.sur, T.nrows, act0, act1, wa, wb, wc, s_mbar, sur_par, s_F, &s_sfail);
+                sur_forward_staged<NT>(d.sur, T.nrows, act0, act1, wa, wb, wc, s_mbar, sur_par, s_F, &s_sfail,
+                                       d.sur_late_l3 != 0);
                 sur_par ^= 1u;
             }
             if (tid == 0) {
@@ -879,19 +880,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             if (tid == 32) T.npairs = npairs;
         }
         __syncthreads();
-        if (D.coulomb == PHMC_COUL_EWALD) {
-            // phase 3b: per (pair, dz, dy) row, the octant row offset
-            constexpr int W = 2 * P - 1;
-            const int ox = D.oct[0], oy = D.oct[1];
-            const int nrow = T.npairs * W * W;
-            for (int e = tid; e < nrow; e += NT) {
-                const int q = e / (W * W), rw = e - q * (W * W);
-                const int dz = rw / W, dy = rw - dz * W;
-                PairK<P>& pk = s_pair[q];
-                pk.roff[rw] = (pk.f[2][dz] * oy + pk.f[1][dy]) * ox;
-            }
-            __syncthreads();
-        }
         // ---------------- phase 4: all pair / mesh work items ----------------
         // helper loads off the critical path: the next trial's primary particle,
         // and the cell bookkeeping a commit of this trial would need
@@ -979,7 +967,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             constexpr int W3 = W * W * W;
             const int nit = T.npairs * W3;
             constexpr int RB = 8;
-            (void)ox; (void)oy;
             for (int it0 = tid; it0 < nit; it0 += RB * NT) {
                 float g[RB], kk[RB];
 #pragma unroll
@@ -990,7 +977,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                     const int q = rowg / (W * W), rw = rowg - q * (W * W);
                     const PairK<P>& pk = s_pair[q];
                     const int dz = rw / W, dy = rw - dz * W;
-                    g[u] = __ldg(&G[pk.roff[rw] + pk.f[0][dx]]);
+                    g[u] = __ldg(&G[(pk.f[2][dz] * oy + pk.f[1][dy]) * ox + pk.f[0][dx]]);
                     const float kyz = pk.coef * pk.K[1][dy] * pk.K[2][dz];
                     kk[u] = (it < nit) ? kyz * pk.K[0][dx] : 0.0f;
                 }
@@ -1141,9 +1128,22 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
 
 template <int P, int NT>
 static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
-    const size_t smem = mc_smem_bytes(P, E.pend_max, E.d.sur.H > 0);
+    DevPtrs dd = E.d;
+    size_t smem = mc_smem_bytes(P, E.pend_max, false);
+    dd.sur_late_l3 = 0;
+    if (E.d.sur.H > 0) {
+        // three staged layers when two blocks per SM still fit, else two buffers
+        cudaFuncAttributes fa;
+        cudaFuncGetAttributes(&fa, k_mc<P, NT>);
+        int per_sm = 0;
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, E.device);
+        const size_t three = mc_smem_bytes(P, E.pend_max, true);
+        const bool fits2 = 2 * (three + fa.sharedSizeBytes + 1024) <= (size_t)per_sm;
+        dd.sur_late_l3 = fits2 ? 0 : 1;
+        smem = fits2 ? three : mc_smem_bytes(P, E.pend_max, true, true);
+    }
     const int grid = (mode == MC_RUN) ? E.R : 1;
-    k_mc<P, NT><<<grid, NT, smem, st>>>(E.d, mode, rep, t, n, dE, E.pend_max);
+    k_mc<P, NT><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
 }
 
@@ -1171,7 +1171,7 @@ cudaError_t prepare_mc(Engine& E) {
     }
 }
 
-size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate) {
+size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate, bool two_buffers) {
     size_t st = 0, pk = 0;
     switch (order) {
         case 4: st = sizeof(Stencil<4>); pk = sizeof(PairK<4>); break;
@@ -1182,7 +1182,8 @@ size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate) {
     // external trials (<= NST_MAX stencils) always start with none pending
     const size_t npairs = std::max((size_t)2 * pend_max + 3, (size_t)(NST_MAX * (NST_MAX + 1) / 2));
     // with a surrogate attached the pair tables' space also holds its activations and staged weights
-    return st * (pend_max + NST_MAX) + std::max(pk * npairs, staged_surrogate ? (size_t)SUR_SMEM_BYTES : (size_t)0);
+    const size_t sur = staged_surrogate ? (size_t)(two_buffers ? SUR_SMEM2_BYTES : SUR_SMEM_BYTES) : (size_t)0;
+    return st * (pend_max + NST_MAX) + std::max(pk * npairs, sur);
 }
 
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {

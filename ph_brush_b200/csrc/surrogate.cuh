@@ -99,14 +99,18 @@ __host__ __device__ inline uint32_t sur_layer_bytes(int K, int H) { return (uint
 #define SUR_ACT_BYTES (2 * 16 * SUR_AST * 2)
 #define SUR_WBUF_BYTES (SUR_HMAX * SUR_HMAX * 2)
 #define SUR_SMEM_BYTES (128 + SUR_ACT_BYTES + SUR_K * SUR_HMAX * 2 + 2 * SUR_WBUF_BYTES)
+// two-buffer layout: layer 3 streams into layer 1's buffer once layer 1 is done
+#define SUR_SMEM2_BYTES (128 + SUR_ACT_BYTES + 2 * SUR_WBUF_BYTES)
 
-// The caller's thread 0 has issued layer l -> w_l on mbar[l] (l = 0, 1, 2), each
-// barrier in the phase of parity `par`.  Computes the outputs (energy units) of
-// rows 0..nrows-1 (nrows <= 8) held, standardised, in buf0.  Returns false
-// (every thread) when a copy did not arrive within the bound.
+// The caller's thread 0 has issued layer l -> w_l on mbar[l] (l = 0, 1, and 2
+// unless late_l3), each barrier in the phase of parity `par`; with late_l3 layer 3
+// is copied into wc (= wa) here, once layer 1 is done.  Computes the outputs
+// (energy units) of rows 0..nrows-1 (nrows <= 8) held, standardised, in buf0.
+// Returns false (every thread) when a copy did not arrive within the bound.
 template <int NT>
 __device__ bool sur_forward_staged(const SurDev& s, int nrows, __nv_bfloat16* buf0, __nv_bfloat16* buf1, const uint2* wa,
-                                   const uint2* wb, const uint2* wc, uint64_t* mbar, uint32_t par, float* out, int* s_fail) {
+                                   const uint2* wb, const uint2* wc, uint64_t* mbar, uint32_t par, float* out, int* s_fail,
+                                   bool late_l3) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
     __nv_bfloat16* in = buf0;
     __nv_bfloat16* ot = buf1;
@@ -144,6 +148,8 @@ __device__ bool sur_forward_staged(const SurDev& s, int nrows, __nv_bfloat16* bu
             }
         }
         __syncthreads();
+        if (l == 0 && late_l3 && threadIdx.x == 0)
+            sur_bulk_load(const_cast<uint2*>(wc), s.w[2], sur_layer_bytes(s.H, s.H), &mbar[2]);
         __nv_bfloat16* t = in; in = ot; ot = t;
         K = s.H;
     }
