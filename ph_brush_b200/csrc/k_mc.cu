@@ -960,29 +960,38 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 const float v = phi[((size_t)s.m[2][c] * ny + s.m[1][b]) * nx + s.m[0][a]];
                 acc_rec += (double)(s.coef * s.w[0][a] * s.w[1][b] * s.w[2][c] * v);
             }
-            // S(W_a, W_b) = sum_delta Kx Ky Kz G[fz, fy, fx]: element (pair, dz, dy, dx), dx fastest
-            // (lanes read consecutive x of a G row); each thread issues RB loads before using them
+            // S(W_a, W_b) = sum over (dz, dy) rows of coef Ky Kz sum_dx Kx G[fz, fy, fx]: one
+            // (pair, row) per thread and step, RR rows in flight, the row's W loads back to back;
+            // row sums in FP32 (W terms of one sign pattern), the total in FP64
             const float* G = d.goct + D.oct_off;
             const int ox = D.oct[0], oy = D.oct[1];
-            constexpr int W3 = W * W * W;
-            const int nit = T.npairs * W3;
-            constexpr int RB = 8;
-            for (int it0 = tid; it0 < nit; it0 += RB * NT) {
-                float g[RB], kk[RB];
+            constexpr int WW = W * W;
+            const int nrow = T.npairs * WW;
+            constexpr int RR = 2;
+            for (int r0 = tid; r0 < nrow; r0 += RR * NT) {
+                float gv[RR][W];
+                int qv[RR], rv[RR];
 #pragma unroll
-                for (int u = 0; u < RB; ++u) {
-                    const int it = it0 + u * NT;
-                    const int itc = it < nit ? it : nit - 1;
-                    const int rowg = itc / W, dx = itc - rowg * W;  // rowg = pair * W*W + row
-                    const int q = rowg / (W * W), rw = rowg - q * (W * W);
-                    const PairK<P>& pk = s_pair[q];
+                for (int u = 0; u < RR; ++u) {
+                    const int rowg = min(r0 + u * NT, nrow - 1);
+                    const int q = rowg / WW, rw = rowg - q * WW;
                     const int dz = rw / W, dy = rw - dz * W;
-                    g[u] = __ldg(&G[(pk.f[2][dz] * oy + pk.f[1][dy]) * ox + pk.f[0][dx]]);
-                    const float kyz = pk.coef * pk.K[1][dy] * pk.K[2][dz];
-                    kk[u] = (it < nit) ? kyz * pk.K[0][dx] : 0.0f;
+                    const PairK<P>& pk = s_pair[q];
+                    const float* Grow = G + (pk.f[2][dz] * oy + pk.f[1][dy]) * ox;
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) gv[u][dx] = __ldg(&Grow[pk.f[0][dx]]);
+                    qv[u] = q; rv[u] = rw;
                 }
 #pragma unroll
-                for (int u = 0; u < RB; ++u) acc_rec += (double)(kk[u] * g[u]);
+                for (int u = 0; u < RR; ++u) {
+                    if (r0 + u * NT >= nrow) continue;
+                    const PairK<P>& pk = s_pair[qv[u]];
+                    const int dz = rv[u] / W, dy = rv[u] - dz * W;
+                    float s = 0.0f;
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) s = fmaf(pk.K[0][dx], gv[u][dx], s);
+                    acc_rec += (double)(pk.coef * pk.K[1][dy] * pk.K[2][dz] * s);
+                }
             }
         }
         block_sum3<NT>(acc_lj, acc_c, acc_rec, red);
