@@ -440,6 +440,10 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         std::vector<int2> pj;
         std::vector<int4> zj;
         std::vector<int> zoff;
+        // register z pass when every replica has the same supported nz
+        E.zreg = E.use_r2c ? zreg_variant(E.desc[0].mesh[2]) : 0;
+        for (int r = 1; r < R && E.zreg; ++r)
+            if (E.desc[r].mesh[2] != E.desc[0].mesh[2]) E.zreg = 0;
         for (int r = 0; r < R; ++r) {
             const RepDesc& D = E.desc[r];
             for (int z = 0; z < D.mesh[2]; ++z) pj.push_back(make_int2(r, z));
@@ -447,10 +451,16 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
             if (E.use_r2c) {
                 // column tiles of near-equal width <= ZPASS_TX over the nx/2+1 half-spectrum columns
                 const int nxh = D.mesh[0] / 2 + 1;
-                const int nt = (nxh + ZPASS_TX - 1) / ZPASS_TX;
-                const int w = (nxh + nt - 1) / nt;
-                for (int y = 0; y < D.mesh[1]; ++y)
-                    for (int x0 = 0; x0 < nxh; x0 += w) zj.push_back(make_int4(r, y, x0, std::min(w, nxh - x0)));
+                if (E.zreg) {
+                    // ZREG_TX consecutive columns of the flattened ny x nxh plane per job
+                    const int ncol = nxh * D.mesh[1];
+                    for (int c0 = 0; c0 < ncol; c0 += ZREG_TX) zj.push_back(make_int4(r, c0, std::min(ZREG_TX, ncol - c0), 0));
+                } else {
+                    const int nt = (nxh + ZPASS_TX - 1) / ZPASS_TX;
+                    const int w = (nxh + nt - 1) / nt;
+                    for (int y = 0; y < D.mesh[1]; ++y)
+                        for (int x0 = 0; x0 < nxh; x0 += w) zj.push_back(make_int4(r, y, x0, std::min(w, nxh - x0)));
+                }
                 // + cell counts / ids of the cell layers a plane's stencils reach (<= order + 5 layers)
                 const size_t ncell = (size_t)std::min(D.ncell[2], E.order + 5) * D.ncell[0] * D.ncell[1];
                 // two complex buffers (the 64-bit charge plane lives inside them) + cell counts
@@ -462,7 +472,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                     for (int x0 = 0; x0 < D.mesh[0]; x0 += ZPASS_TX) zj.push_back(make_int4(r, y, x0, 0));
                 E.plane_smem = std::max(E.plane_smem, (size_t)2 * D.mesh[0] * D.mesh[1] * sizeof(float2));
             }
-            E.zpass_smem = std::max(E.zpass_smem, (size_t)2 * ZPASS_TX * D.mesh[2] * sizeof(float2));
+            E.zpass_smem = std::max(E.zpass_smem, E.zreg ? zreg_smem(D.mesh[2]) : (size_t)2 * ZPASS_TX * D.mesh[2] * sizeof(float2));
         }
         zoff.push_back((int)zj.size());
         E.n_plane_jobs = (int)pj.size(); E.n_zjobs = (int)zj.size();

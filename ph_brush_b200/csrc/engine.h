@@ -6,6 +6,7 @@
 #include "common.cuh"
 
 #define ZPASS_TX 16
+#define ZREG_TX 16  // columns per block of the register z pass
 
 struct Engine {
     int R = 0;
@@ -31,6 +32,7 @@ struct Engine {
     size_t plane_smem = 0, zpass_smem = 0;
     bool use_r2c = false;        // every replica has even nx: fused spread + real-to-complex rebuild
     size_t rb_fwd_smem = 0, rb_inv_smem = 0;
+    int zreg = 0;                // register z-pass variant for the shared nz (0: shared-memory z pass)
     int flush_kernels = 0;       // kernels per potential-mesh rebuild
     bool unit_pending = false;   // next rebuild places a unit charge instead of the particles
     long long total_meshh = 0;
@@ -61,6 +63,8 @@ cudaError_t mesh_set_smem_limits(Engine& E);
 // k_rebuild.cu
 void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st);
 cudaError_t rebuild_set_smem_limits(Engine& E);
+int zreg_variant(int nz);      // register z-pass variant for nz, 0 if none
+size_t zreg_smem(int nz);
 
 // k_pair.cu
 void launch_cell_build(Engine& E, cudaStream_t st);

@@ -8,14 +8,14 @@
 // graphics processors", SC'08).  Element e of line l lives at l*ls + e*es.
 // Returns the buffer that holds the result (a or b).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 // multiply by sign*i
-__device__ __forceinline__ float2 cmul_si(float2 a, float sign) { return make_float2(-sign * a.y, sign * a.x); }
+__host__ __device__ __forceinline__ float2 cmul_si(float2 a, float sign) { return make_float2(-sign * a.y, sign * a.x); }
 
-__device__ __forceinline__ void dft_radix(float2* v, int R, float sign) {
+__host__ __device__ __forceinline__ void dft_radix(float2* v, int R, float sign) {
     if (R == 2) {
         float2 a = v[0], b = v[1];
         v[0] = cadd(a, b); v[1] = csub(a, b);

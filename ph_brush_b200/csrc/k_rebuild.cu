@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "engine.h"
 #include "fft.cuh"
+#include "fft_reg.cuh"
 
 template <int P, int NT>
 __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict__ jobs, int unit_charge,
@@ -232,6 +233,121 @@ __global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restri
     if (threadIdx.x == 0) epart[blockIdx.x] = 0.5 * s;
 }
 
+// z pencils with register-resident DFTs, nz = N1 * N2: TX consecutive columns of the
+// flattened half-spectrum plane (ny x (nx/2+1)); job = (replica, first column, columns, 0).
+//   stage A: per (n2, column) the length-N1 DFT over x[N2 n1 + n2] straight from global
+//            memory, times W_nz^(n2 k1), into shared memory at [k1][n2];
+//   stage B: per (k1, column) the length-N2 DFT over n2 gives F(kz = k1 + N1 k2);
+//            E += w theta |F|^2, F *= theta; the inverse length-N2 DFT and W_nz^(-n2 k1)
+//            go back to the same shared-memory row;
+//   stage A': per (n2, column) the inverse length-N1 DFT over k1, stored to global memory.
+// Shared memory is touched twice per direction instead of once per radix stage.
+template <int N1, int N2, int NT, int TX>
+__global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restrict__ jobs, double* __restrict__ epart,
+                                                const int* __restrict__ dirty) {
+    constexpr int N = N1 * N2;
+    static_assert((TX & (TX - 1)) == 0, "TX must be a power of two");
+    extern __shared__ float2 sm[];
+    __shared__ double red[40];
+    const int4 job = jobs[blockIdx.x];
+    const int r = job.x, c0 = job.y, ncol = job.z;
+    if (dirty && !dirty[r]) { if (threadIdx.x == 0) epart[blockIdx.x] = 0.0; return; }
+    const RepDesc& D = d.desc[r];
+    const int nx = D.mesh[0], ny = D.mesh[1];
+    const int M = nx / 2, nxh = M + 1;
+    const size_t plane = (size_t)ny * nxh;
+    float2* s = sm;            // [k1][n2][column]
+    float2* tw = sm + N * TX;  // exp(-2 pi i j / nz)
+    float2* c = d.cmesh + D.meshh_off + c0;
+    for (int i = threadIdx.x; i < N; i += NT) tw[i] = d.twiddle[D.tw_off[2] + i];
+    // stage A: the loads of the first round go out before the barrier that publishes tw
+    for (int base = 0; base < N2 * TX; base += NT) {
+        const int it = base + threadIdx.x;
+        const int n2 = it / TX, col = it & (TX - 1);
+        const bool act = it < N2 * TX;
+        float2 v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1)
+            v[n1] = (act && col < ncol) ? c[(size_t)(N2 * n1 + n2) * plane + col] : make_float2(0.f, 0.f);
+        if (base == 0) __syncthreads();
+        if (act) {
+            rfft::rdft<N1, -1>(v);
+            s[n2 * TX + col] = v[0];
+#pragma unroll
+            for (int k1 = 1; k1 < N1; ++k1) s[(k1 * N2 + n2) * TX + col] = cmul(v[k1], tw[n2 * k1]);
+        }
+    }
+    __syncthreads();
+    const float* mx = d.moduli + D.mod_off[0];
+    const float* my = d.moduli + D.mod_off[1];
+    const float* mz = d.moduli + D.mod_off[2];
+    const float pv = 3.14159265358979323846f * (float)D.V;
+    double e_loc = 0.0;
+    for (int it = threadIdx.x; it < N1 * TX; it += NT) {
+        const int k1 = it / TX, col = it & (TX - 1);
+        float2 u[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) u[n2] = s[(k1 * N2 + n2) * TX + col];
+        rfft::rdft<N2, -1>(u);
+        const int idx = c0 + col;
+        const int y = idx / nxh, kx = idx - y * nxh;
+        const bool valid = col < ncol;
+        const int myi = (y <= ny / 2) ? y : y - ny;
+        const float kxv = (float)kx / D.L[0], kyv = (float)myi / D.L[1];
+        const float wgt = (kx == 0 || kx == M) ? 1.0f : 2.0f;  // half spectrum, Hermitian partners counted
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            const int kz = k1 + N1 * k2;
+            const float2 F = u[k2];
+            float th = 0.0f;
+            if (valid && !(kx == 0 && y == 0 && kz == 0)) {
+                const int mzi = (kz <= N / 2) ? kz : kz - N;
+                const float kzv = (float)mzi / D.L[2];
+                const float m2 = kxv * kxv + kyv * kyv + kzv * kzv;
+                const float den = m2 * pv * mx[kx] * my[y] * mz[kz];
+                if (den > 0.0f) th = D.elf * expf(-D.ewald_factor * m2) / den;
+                e_loc += (double)(wgt * th) * ((double)F.x * F.x + (double)F.y * F.y);
+            }
+            u[k2] = make_float2(F.x * th, F.y * th);
+        }
+        rfft::rdft<N2, 1>(u);
+        s[k1 * N2 * TX + col] = u[0];
+#pragma unroll
+        for (int n2 = 1; n2 < N2; ++n2) {
+            float2 w = tw[n2 * k1];
+            w.y = -w.y;
+            s[(k1 * N2 + n2) * TX + col] = cmul(u[n2], w);
+        }
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < N2 * TX; it += NT) {
+        const int n2 = it / TX, col = it & (TX - 1);
+        float2 v[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) v[k1] = s[(k1 * N2 + n2) * TX + col];
+        rfft::rdft<N1, 1>(v);
+        if (col < ncol) {
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) c[(size_t)(N2 * n1 + n2) * plane + col] = v[n1];
+        }
+    }
+    const double es = block_sum<NT>(e_loc, red);
+    if (threadIdx.x == 0) epart[blockIdx.x] = 0.5 * es;
+}
+
+// nz -> (N1, N2) of the register z pass; 0 = shared-memory z pass
+#define ZREG_LIST(X) X(1, 48, 8, 6) X(2, 128, 16, 8) X(3, 162, 18, 9) X(4, 192, 16, 12) X(5, 216, 24, 9) \
+                     X(6, 243, 27, 9) X(7, 256, 16, 16) X(8, 288, 32, 9) X(9, 384, 32, 12)
+constexpr int ZREG_NT(int n2) { return (n2 * ZREG_TX + 31) / 32 * 32 > 256 ? 256 : (n2 * ZREG_TX + 31) / 32 * 32; }
+
+int zreg_variant(int nz) {
+#define ZREG_CASE(id, n, a, b) if (nz == n) return id;
+    ZREG_LIST(ZREG_CASE)
+#undef ZREG_CASE
+    return 0;
+}
+size_t zreg_smem(int nz) { return (size_t)(ZREG_TX + 1) * nz * sizeof(float2); }
+
 template <int NT>
 __global__ void __launch_bounds__(NT) k_rb_inv(DevPtrs d, const int2* __restrict__ jobs, const int* __restrict__ dirty) {
     extern __shared__ float2 sm[];
@@ -278,7 +394,13 @@ void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream
         case 5: k_rb_fwd<5, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
         default: k_rb_fwd<6, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
     }
-    k_rb_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty);
+    switch (E.zreg) {
+#define ZREG_LAUNCH(id, n, a, b) \
+        case id: k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX><<<E.n_zjobs, ZREG_NT(b), E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty); break;
+        ZREG_LIST(ZREG_LAUNCH)
+#undef ZREG_LAUNCH
+        default: k_rb_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty);
+    }
     k_rb_inv<256><<<E.n_plane_jobs, 256, E.rb_inv_smem, st>>>(E.d, E.d_plane_jobs, dirty);
 }
 
@@ -303,7 +425,12 @@ cudaError_t rebuild_set_smem_limits(Engine& E) {
         default: e = raise_cap(k_rb_fwd<6, 256>, E.device, E.rb_fwd_smem); break;
     }
     if (e != cudaSuccess) return e;
-    e = raise_cap(k_rb_zpass<256, ZPASS_TX>, E.device, E.zpass_smem);
+    switch (E.zreg) {
+#define ZREG_CAP(id, n, a, b) case id: e = raise_cap(k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX>, E.device, E.zpass_smem); break;
+        ZREG_LIST(ZREG_CAP)
+#undef ZREG_CAP
+        default: e = raise_cap(k_rb_zpass<256, ZPASS_TX>, E.device, E.zpass_smem);
+    }
     if (e != cudaSuccess) return e;
     return raise_cap(k_rb_inv<256>, E.device, E.rb_inv_smem);
 }
