@@ -29,6 +29,7 @@ struct RepDesc {
     int tw_off[3];        // offsets of the twiddle tables per axis
     int tw_off_h;         // twiddle table of length nx/2 (real-to-complex path)
     long long meshh_off;  // offset into the half-spectrum complex mesh ((nx/2+1) x ny x nz)
+    int zb_lo, zb_n;      // band of planes (zb_lo + i) mod nz, i < zb_n, that the walls let hold charge (all without walls)
     int order;
     int coulomb;
     int ref_corner;

@@ -316,6 +316,16 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                 D.tw_off[k] = tw_table(P.mesh[k]);
             }
             D.tw_off_h = (P.mesh[0] % 2 == 0) ? tw_table(P.mesh[0] / 2) : 0;
+            // planes a charge inside the walls can reach: floor(g_z) of z in [wall_lo, wall_hi]
+            // (one plane of rounding margin either side) + the stencil offsets
+            // [P/2 - P + 1, P/2]; the rebuild computes and reads only these
+            D.zb_lo = 0; D.zb_n = D.mesh[2];
+            if (D.walls) {
+                const double g = (double)D.mesh[2] / (double)D.L[2];
+                const int lo = (int)std::floor(P.wall_lo * g) - 1 + E.order / 2 - E.order + 1;
+                const int hi = (int)std::floor(P.wall_hi * g) + 1 + E.order / 2;
+                if (hi - lo + 1 < D.mesh[2]) { D.zb_lo = ((lo % D.mesh[2]) + D.mesh[2]) % D.mesh[2]; D.zb_n = hi - lo + 1; }
+            }
             D.mesh_off = mesh_off; mesh_off += (long long)D.mesh[0] * D.mesh[1] * D.mesh[2];
             D.meshh_off = meshh_off; meshh_off += (long long)(D.mesh[0] / 2 + 1) * D.mesh[1] * D.mesh[2];
             D.oct_off = oct_off; oct_off += (long long)D.oct[0] * D.oct[1] * D.oct[2];
@@ -437,7 +447,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         CU(cudaMemcpy(d.moduli, hm.data(), sizeof(float) * hm.size(), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(d.twiddle, h_tw.data(), sizeof(float2) * h_tw.size(), cudaMemcpyHostToDevice));
         if (!E.use_r2c) CU(cudaMemset(d.qfix, 0, sizeof(unsigned long long) * E.total_mesh));
-        std::vector<int2> pj;
+        std::vector<int2> pj, pjb;  // all planes; the wall band's planes
         std::vector<int4> zj;
         std::vector<int> zoff;
         // register z pass when every replica has the same supported nz
@@ -447,6 +457,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         for (int r = 0; r < R; ++r) {
             const RepDesc& D = E.desc[r];
             for (int z = 0; z < D.mesh[2]; ++z) pj.push_back(make_int2(r, z));
+            for (int i = 0; i < D.zb_n; ++i) pjb.push_back(make_int2(r, (D.zb_lo + i) % D.mesh[2]));
             zoff.push_back((int)zj.size());
             if (E.use_r2c) {
                 // column tiles of near-equal width <= ZPASS_TX over the nx/2+1 half-spectrum columns
@@ -475,8 +486,10 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
             E.zpass_smem = std::max(E.zpass_smem, E.zreg ? zreg_smem(D.mesh[2]) : (size_t)2 * ZPASS_TX * D.mesh[2] * sizeof(float2));
         }
         zoff.push_back((int)zj.size());
-        E.n_plane_jobs = (int)pj.size(); E.n_zjobs = (int)zj.size();
+        E.n_plane_jobs = (int)pj.size(); E.n_zjobs = (int)zj.size(); E.n_band_jobs = (int)pjb.size();
         DALLOC(E.d_plane_jobs, pj.size()); DALLOC(E.d_zjobs, zj.size()); DALLOC(E.d_zjob_off, zoff.size());
+        DALLOC(E.d_band_jobs, pjb.size());
+        CU(cudaMemcpy(E.d_band_jobs, pjb.data(), sizeof(int2) * pjb.size(), cudaMemcpyHostToDevice));
         DALLOC(E.d_epart, zj.size());
         CU(cudaMemcpy(E.d_plane_jobs, pj.data(), sizeof(int2) * pj.size(), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(E.d_zjobs, zj.data(), sizeof(int4) * zj.size(), cudaMemcpyHostToDevice));
@@ -811,9 +824,11 @@ int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
             const RepDesc& D = E.desc[r];
             h->prof.mc_alg_bytes += st1[r].alg_bytes - st0[r].alg_bytes;
             h->prof.trials += st1[r].trials_run - st0[r].trials_run;
-            const double M = (double)D.mesh[0] * D.mesh[1] * D.mesh[2];
-            const double Mc = (double)(D.mesh[0] / 2 + 1) * D.mesh[1] * D.mesh[2];
-            h->prof.flush_alg_bytes += (double)(st1[r].flushes - st0[r].flushes) * (16.0 * h->n_present[r] + 16.0 * M + 16.0 * Mc);
+            // planes of the wall band: the first pass writes the half spectrum (8 B per complex
+            // value), the z pass reads and writes it, the last pass reads it and writes phi (4 B)
+            const double Mb = (double)D.mesh[0] * D.mesh[1] * D.zb_n;
+            const double Mcb = (double)(D.mesh[0] / 2 + 1) * D.mesh[1] * D.zb_n;
+            h->prof.flush_alg_bytes += (double)(st1[r].flushes - st0[r].flushes) * (16.0 * h->n_present[r] + 32.0 * Mcb + 4.0 * Mb);
         }
     }
     return PHMC_OK;

@@ -26,6 +26,8 @@ struct Engine {
     // flush job tables
     int n_plane_jobs = 0, n_zjobs = 0;
     int2* d_plane_jobs = nullptr;
+    int n_band_jobs = 0;
+    int2* d_band_jobs = nullptr;  // (replica, z) of the planes in each replica's wall band
     int4* d_zjobs = nullptr;
     int* d_zjob_off = nullptr;
     double* d_epart = nullptr;

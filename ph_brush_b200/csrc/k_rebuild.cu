@@ -11,6 +11,10 @@
 //            F *= theta, inverse FFT along z.
 //  k_rb_inv  (replica, z): inverse FFT along y, complex-to-real along x; writes
 //            the real potential plane.
+// With hard walls the charges stay in a band of planes (RepDesc::zb_lo, zb_n) and the
+// MC kernel reads the potential only there: the first and last passes run on the
+// band's planes, the z pass loads and stores only those (the rest of the input is
+// zero).  The unit-charge rebuild of the influence kernel computes every plane.
 // Replaces the memset + k_spread_cubic + cuFFT R2C + influence kernel chain of
 // the reference (MC/src/pme.cu:140-249,362,384-422) and the separate global
 // charge mesh of the scatter path.
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
 // z pencils of the half spectrum; job = (replica, y, x0, width <= ZPASS_TX).
 template <int NT, int TX>
 __global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restrict__ jobs, double* __restrict__ epart,
-                                                 const int* __restrict__ dirty) {
+                                                 const int* __restrict__ dirty, int full) {
     extern __shared__ float2 sm[];
     __shared__ double red[40];
     const int4 job = jobs[blockIdx.x];
@@ -193,9 +197,11 @@ __global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restri
     float2* a = sm;
     float2* b = sm + TX * nz;
     float2* c = d.cmesh + D.meshh_off;
+    const int zlo = full ? 0 : D.zb_lo, zbn = full ? nz : D.zb_n;
+    auto in_band = [&](int z) { int t = z - zlo; t += (t < 0) ? nz : 0; return t < zbn; };
     for (int e = threadIdx.x; e < nz * TX; e += NT) {
         const int z = e / TX, tx = e - z * TX;
-        a[e] = (tx < tw_n) ? c[((size_t)z * ny + y) * nxh + x0 + tx] : make_float2(0.f, 0.f);
+        a[e] = (tx < tw_n && in_band(z)) ? c[((size_t)z * ny + y) * nxh + x0 + tx] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     float2* res = fft_lines<NT>(a, b, nz, TX, 1, TX, d.twiddle + D.tw_off[2], -1.0f, true);
@@ -227,7 +233,7 @@ __global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restri
     res = fft_lines<NT>(res, oth, nz, TX, 1, TX, d.twiddle + D.tw_off[2], 1.0f, true);
     for (int e = threadIdx.x; e < nz * TX; e += NT) {
         const int z = e / TX, tx = e - z * TX;
-        if (tx < tw_n) c[((size_t)z * ny + y) * nxh + x0 + tx] = res[e];
+        if (tx < tw_n && in_band(z)) c[((size_t)z * ny + y) * nxh + x0 + tx] = res[e];
     }
     const double s = block_sum<NT>(e_loc, red);
     if (threadIdx.x == 0) epart[blockIdx.x] = 0.5 * s;
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restri
 // Shared memory is touched twice per direction instead of once per radix stage.
 template <int N1, int N2, int NT, int TX>
 __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restrict__ jobs, double* __restrict__ epart,
-                                                const int* __restrict__ dirty) {
+                                                const int* __restrict__ dirty, int full) {
     constexpr int N = N1 * N2;
     static_assert((TX & (TX - 1)) == 0, "TX must be a power of two");
     extern __shared__ float2 sm[];
@@ -259,6 +265,9 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
     float2* s = sm;            // [k1][n2][column]
     float2* tw = sm + N * TX;  // exp(-2 pi i j / nz)
     float2* c = d.cmesh + D.meshh_off + c0;
+    // planes outside the wall band hold no charge (zero input) and are not read back
+    const int zlo = full ? 0 : D.zb_lo, zbn = full ? N : D.zb_n;
+    auto in_band = [&](int z) { int t = z - zlo; t += (t < 0) ? N : 0; return t < zbn; };
     for (int i = threadIdx.x; i < N; i += NT) tw[i] = d.twiddle[D.tw_off[2] + i];
     // stage A: the loads of the first round go out before the barrier that publishes tw
     for (int base = 0; base < N2 * TX; base += NT) {
@@ -268,7 +277,8 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
         float2 v[N1];
 #pragma unroll
         for (int n1 = 0; n1 < N1; ++n1)
-            v[n1] = (act && col < ncol) ? c[(size_t)(N2 * n1 + n2) * plane + col] : make_float2(0.f, 0.f);
+            v[n1] = (act && col < ncol && in_band(N2 * n1 + n2)) ? c[(size_t)(N2 * n1 + n2) * plane + col]
+                                                                 : make_float2(0.f, 0.f);
         if (base == 0) __syncthreads();
         if (act) {
             rfft::rdft<N1, -1>(v);
@@ -328,7 +338,8 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
         rfft::rdft<N1, 1>(v);
         if (col < ncol) {
 #pragma unroll
-            for (int n1 = 0; n1 < N1; ++n1) c[(size_t)(N2 * n1 + n2) * plane + col] = v[n1];
+            for (int n1 = 0; n1 < N1; ++n1)
+                if (in_band(N2 * n1 + n2)) c[(size_t)(N2 * n1 + n2) * plane + col] = v[n1];
         }
     }
     const double es = block_sum<NT>(e_loc, red);
@@ -388,20 +399,24 @@ __global__ void __launch_bounds__(NT) k_rb_inv(DevPtrs d, const int2* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// The unit-charge rebuild (influence kernel) computes every plane; a rebuild of the
+// particles' mesh only the planes of each replica's wall band.
 void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st) {
+    const int2* pj = unit_charge ? E.d_plane_jobs : E.d_band_jobs;
+    const int npj = unit_charge ? E.n_plane_jobs : E.n_band_jobs;
     switch (E.order) {
-        case 4: k_rb_fwd<4, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
-        case 5: k_rb_fwd<5, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
-        default: k_rb_fwd<6, 256><<<E.n_plane_jobs, 256, E.rb_fwd_smem, st>>>(E.d, E.d_plane_jobs, unit_charge, dirty); break;
+        case 4: k_rb_fwd<4, 256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty); break;
+        case 5: k_rb_fwd<5, 256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty); break;
+        default: k_rb_fwd<6, 256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty); break;
     }
     switch (E.zreg) {
 #define ZREG_LAUNCH(id, n, a, b) \
-        case id: k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX><<<E.n_zjobs, ZREG_NT(b), E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty); break;
+        case id: k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX><<<E.n_zjobs, ZREG_NT(b), E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty, unit_charge); break;
         ZREG_LIST(ZREG_LAUNCH)
 #undef ZREG_LAUNCH
-        default: k_rb_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty);
+        default: k_rb_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty, unit_charge);
     }
-    k_rb_inv<256><<<E.n_plane_jobs, 256, E.rb_inv_smem, st>>>(E.d, E.d_plane_jobs, dirty);
+    k_rb_inv<256><<<npj, 256, E.rb_inv_smem, st>>>(E.d, pj, dirty);
 }
 
 template <typename K>
