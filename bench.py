@@ -415,6 +415,8 @@ def run_ours(args):
                     "peak_source": peak_kind, "traffic": ratio * per if ratio else None,
                     "alg_bytes_per_launch": per, "avg_launch_ms": ms, "launches": n_l,
                     "share_of_timed": tot / dev_ms if dev_ms else None}
+        if name == "k_mc":  # share of the launches' replica slots (one block per replica) that did work
+            rl[name]["replica_busy_fraction"] = prof["mc_busy_ms"] / (len(reps) * tot) if tot else None
     dominant = kern[0][0] if kern else None
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -224,6 +224,15 @@ typedef struct phmc_tuning {
 int phmc_set_tuning(phmc_engine* e, int pending_max, int threads);
 int phmc_get_tuning(phmc_engine* e, phmc_tuning* out);
 int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_results, int* n_results);
+/* Launch quorum, 0 < quorum <= 1: an MC launch of a batched engine ends once that
+ * fraction of the replicas still running at its start have filled their pending
+ * buffer; the others stop with theirs partly filled, and the rebuild folds both in.
+ * 1 lets every replica run until its buffer is full or its trials are done, and
+ * leaves the blocks of the replicas whose buffers fill first idle until the
+ * slowest fills.  Default 0.2.  Applied only when every replica's block is
+ * resident at once.  Decisions do not depend on it except through FP32 rounding
+ * of the reciprocal-space dE. */
+int phmc_set_quorum(phmc_engine* e, double quorum);
 
 /* ---- state ----
  * replica == -1: every replica at once, arrays of sum(capacity) slots concatenated
@@ -244,8 +253,11 @@ typedef struct phmc_profile {
     int64_t flush_launches;  /* rebuild pipelines (each = spread + 3 FFT passes + reduce) */
     int64_t kernel_launches; /* every kernel the engine launched */
     double mc_alg_bytes;     /* algorithmic bytes of all trials (per-trial model in the docs) */
-    double flush_alg_bytes;  /* algorithmic bytes of all rebuilds: 16 N + 16 M + 16 Mc per replica */
+    double flush_alg_bytes;  /* algorithmic bytes of all rebuilds: 16 N + 32 Mcb + 4 Mb per replica (N particles,
+                                Mb / Mcb real / half-spectrum mesh points of the planes between the walls) */
     int64_t trials;
+    double mc_busy_ms;       /* summed over replicas: time their MC blocks ran; mc_busy_ms / (replicas * mc_ms)
+                                is the share of the launches' replica slots that did work */
 } phmc_profile;
 /* Profiling on: per-launch CUDA events around the MC kernel and the rebuilds. */
 int phmc_set_profiling(phmc_engine* e, int on);

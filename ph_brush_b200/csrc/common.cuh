@@ -73,7 +73,7 @@ struct RepDesc {
 struct RepState {
     int n_mobile, n_anion, n_cation, n_free;
     int error;          // PHMC_ERR_* raised inside a kernel (0 = none)
-    int stop_reason;    // 0 target reached, 1 pending full
+    int stop_reason;    // 0 target reached, 1 pending full, 2 launch quorum of blocked replicas reached
     long long trial;    // next trial index (Philox counter)
     long long target;   // run until trial == target
     long long run_start; // trial index at the start of the current phmc_run (log / replay origin)
@@ -91,6 +91,7 @@ struct RepState {
     long long da_eval, da_pass, da_acc, da_wpass, da_wacc;
     int da_off;         // agreement fell below the threshold: plain Metropolis from then on
     int da_pad;
+    long long busy_ns;  // summed run time of this replica's MC blocks (globaltimer)
 };
 
 // Device pointers of the whole engine (all replicas concatenated).
@@ -127,6 +128,8 @@ struct DevPtrs {
     // delayed acceptance
     SurDev sur;
     int sur_late_l3;     // two-buffer staging (layer 3 copied after layer 1) to keep two MC blocks per SM
+    int* quorum_ctl;     // [replicas active at the MC launch's start, of them stopped by a full pending buffer]
+    float quorum;        // the launch ends once that fraction of its active replicas is blocked (>= 1: off)
     float da_threshold;  // minimum second-stage acceptance among first-stage passes
     int da_window;       // first-stage passes per agreement check
     // training-sample harvest: rows [cap][SUR_ROWS][SUR_K], signs [cap][SUR_ROWS], targets [cap]

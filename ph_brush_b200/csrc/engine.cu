@@ -390,6 +390,8 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     DALLOC(d.mobile, N); DALLOC(d.mobile_pos, N); DALLOC(d.anions, N); DALLOC(d.anion_pos, N);
     DALLOC(d.cations, N); DALLOC(d.cation_pos, N); DALLOC(d.freel, N); DALLOC(d.titr, N);
     DALLOC(d.desc, R); DALLOC(d.state, R); DALLOC(d.dirty, R);
+    DALLOC(d.quorum_ctl, 2);
+    d.quorum = 1.0f;
     DALLOC(E.d_rep_of, N);
     DALLOC(E.d_cell_rep, E.total_cells);
     int maxcap = 0;
@@ -824,6 +826,7 @@ int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
             const RepDesc& D = E.desc[r];
             h->prof.mc_alg_bytes += st1[r].alg_bytes - st0[r].alg_bytes;
             h->prof.trials += st1[r].trials_run - st0[r].trials_run;
+            h->prof.mc_busy_ms += 1e-6 * (double)(st1[r].busy_ns - st0[r].busy_ns);
             // planes of the wall band: the first pass writes the half spectrum (8 B per complex
             // value), the z pass reads and writes it, the last pass reads it and writes phi (4 B)
             const double Mb = (double)D.mesh[0] * D.mesh[1] * D.zb_n;
@@ -1292,6 +1295,16 @@ extern "C" int phmc_set_tuning(phmc_engine* h, int pending_max, int threads) {
     CU(cudaSetDevice(h->E.device));
     CU(cudaStreamSynchronize(h->E.stream));
     return apply_tuning(h, pending_max, threads);
+}
+
+extern "C" int phmc_set_quorum(phmc_engine* h, double quorum) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    if (!(quorum > 0.0 && quorum <= 1.0)) return fail(PHMC_ERR_ARG, "quorum must be in (0, 1]");
+    CU(cudaSetDevice(h->E.device));
+    CU(cudaStreamSynchronize(h->E.stream));
+    h->E.quorum = (float)quorum;
+    drop_graph(h);  // the quorum is a launch parameter of the captured MC launches
+    return PHMC_OK;
 }
 
 extern "C" int phmc_get_tuning(phmc_engine* h, phmc_tuning* out) {

@@ -20,6 +20,7 @@ struct Engine {
     long long total_oct = 0;
     int threads = 256;
     int pend_max = 16;
+    float quorum = 0.2f;         // MC launch quorum of blocked replicas (1: every replica runs until it stops)
     cudaStream_t stream = nullptr;
     DevPtrs d{};
     std::vector<RepDesc> desc;

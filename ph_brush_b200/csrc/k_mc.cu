@@ -449,6 +449,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     __shared__ int s_cnt[NPROBE_MAX * 27], s_off[NPROBE_MAX * 27 + 1], s_cell[NPROBE_MAX * 27];
     __shared__ double red[100];
     __shared__ int s_npend;
+    __shared__ int s_qin;            // counted among the launch's active replicas
+    __shared__ volatile int s_qstop; // the launch's quorum of blocked replicas was seen
     __shared__ uint32_t s_rng[32][16];  // Philox words of trials s_rng_base .. s_rng_base+31
     __shared__ long long s_rng_base;
     __shared__ Prefetch pf;
@@ -489,12 +491,17 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         pf.valid = 0;
         s_hv_slot = -1;
         s_sfail = 0;
+        s_qstop = 0;
+        s_qin = 0;
+        if (mode == MC_RUN && d.quorum < 1.0f && S.trial < S.target) { atomicAdd(&d.quorum_ctl[0], 1); s_qin = 1; }
         sur_mbar_init(&s_mbar[0]);
         sur_mbar_init(&s_mbar[1]);
         sur_mbar_init(&s_mbar[2]);
     }
     if (d.sur.H > 0)
         for (int k = tid; k < SUR_K; k += NT) { s_mu[k] = d.sur.mu[k]; s_sd[k] = d.sur.sd[k]; }
+    unsigned long long t_start = 0;
+    if (tid == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
     __syncthreads();
 
     for (;;) {
@@ -514,7 +521,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 if (S.error) T.stop = 1;
                 else if (mode == MC_RUN) {
                     if (S.trial >= S.target) { T.stop = 1; S.stop_reason = 0; }
-                    else if (s_npend + 2 > pend_max) { T.stop = 1; S.stop_reason = 1; }
+                    else if (s_npend + 2 > pend_max) {
+                        T.stop = 1; S.stop_reason = 1;
+                        if (s_qin) atomicAdd(&d.quorum_ctl[1], 1);
+                    } else if (s_qstop) { T.stop = 1; S.stop_reason = 2; }
                     else { T.tnum = S.trial; propose(T, D, S, d, s_rng[S.trial - s_rng_base], pf); S.trial++; }
                 } else {
                     if (T.ext_k >= n_ext) T.stop = 1;
@@ -533,6 +543,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 }
             }
         } else {
+            // quorum of the launch: read off the proposing warp's path, used from the next trial on
+            if (tid == 32 && s_qin) {
+                const int started = *(volatile int*)&d.quorum_ctl[0], blocked = *(volatile int*)&d.quorum_ctl[1];
+                if (blocked > 0 && (float)blocked >= d.quorum * (float)started) s_qstop = 1;
+            }
             // idle threads: store the previous trial's harvested rows, clear the shell histogram
             if (s_hv_slot >= 0) {
                 float* dst = d.hv_rows + (size_t)s_hv_slot * (SUR_ROWS * SUR_K);
@@ -1130,6 +1145,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         __syncthreads();
     }
     if (tid == 0) {
+        if (mode == MC_RUN) {
+            unsigned long long t_end;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_end));
+            S.busy_ns += (long long)(t_end - t_start);
+        }
         d.state[r] = S;
         if (s_npend > 0) d.dirty[r] = 1;  // potential mesh is stale: rebuild before the next MC launch
     }
@@ -1152,6 +1172,19 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
         smem = fits2 ? three : mc_smem_bytes(P, E.pend_max, true, true);
     }
     const int grid = (mode == MC_RUN) ? E.R : 1;
+    // launch quorum only when every replica's block is resident from the start (otherwise
+    // late blocks would count against a quorum the early ones already reached)
+    dd.quorum = 1.0f;
+    if (mode == MC_RUN && E.quorum < 1.0f) {
+        int per_sm = 0, nsm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT>, NT, smem);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
+        if ((long long)per_sm * nsm >= E.R) {
+            dd.quorum = E.quorum;
+            cudaError_t e = cudaMemsetAsync(E.d.quorum_ctl, 0, 2 * sizeof(int), st);
+            if (e != cudaSuccess) return e;
+        }
+    }
     k_mc<P, NT><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
 }

@@ -109,6 +109,10 @@ class Engine:
     def set_tuning(self, pending_max, threads):
         _abi.check(self._lib.phmc_set_tuning(self._h, int(pending_max), int(threads)))
 
+    def set_quorum(self, quorum):
+        """MC launch quorum (0, 1]: a launch ends once that fraction of its running replicas is blocked."""
+        _abi.check(self._lib.phmc_set_quorum(self._h, float(quorum)))
+
     def tuning(self):
         t = _abi.Tuning()
         _abi.check(self._lib.phmc_get_tuning(self._h, C.byref(t)))

@@ -56,7 +56,37 @@ def test_autotune_keeps_the_fastest_candidate():
             assert abs(a["energy"] - b["total"]) <= 1e-6 * abs(b["total"]) + 1e-3
 
 
+@pytest.mark.gpu
+def test_launch_quorum_keeps_the_chains_and_energies():
+    """A launch quorum ends MC launches early for the replicas that have not filled
+    their pending buffers: more rebuilds, the same proposals and decisions (up to
+    FP32 rounding of the reciprocal dE), tracked energies equal to a recompute."""
+    S, P = [], []
+    for k in range(4):
+        s, p = configs.config1(seed=70 + k)
+        S.append(s)
+        P.append(p)
+    logs, flushes = [], []
+    for q in (1.0, 0.25):
+        with Engine(S, P) as e:
+            e.set_tuning(16, 256)
+            e.set_quorum(q)
+            log = e.set_trial_log(3000)
+            st = e.run(3000)
+            logs.append((log[0].copy(), log[1].copy(), log[2].copy()))
+            flushes.append(sum(d["flushes"] for d in st))
+            for a, b in zip(st, e.energy()):
+                assert abs(a["energy"] - b["total"]) <= 1e-6 * abs(b["total"]) + 1e-3, (q, a["energy"], b["total"])
+    (m0, d0, a0), (m1, d1, a1) = logs
+    assert np.array_equal(m0, m1)
+    assert np.array_equal(a0, a1)
+    fin = np.isfinite(d0) & np.isfinite(d1)
+    assert np.allclose(d0[fin], d1[fin], rtol=1e-5, atol=1e-4)
+    assert flushes[1] >= flushes[0], flushes
+
+
 def test_tuning_arguments_are_checked_without_a_gpu():
     lib = _abi.lib()
     assert lib.phmc_set_tuning(None, 16, 256) != 0
     assert lib.phmc_autotune(None, 100, None, 0, None) != 0
+    assert lib.phmc_set_quorum(None, 0.5) != 0
