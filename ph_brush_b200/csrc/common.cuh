@@ -29,6 +29,7 @@ struct RepDesc {
     int tw_off[3];        // offsets of the twiddle tables per axis
     int tw_off_h;         // twiddle table of length nx/2 (real-to-complex path)
     long long meshh_off;  // offset into the half-spectrum complex mesh ((nx/2+1) x ny x nz)
+    long long qb_off;     // offset of this replica's fixed-point charge mesh (nx x ny x zb_n) in qband
     int zb_lo, zb_n;      // band of planes (zb_lo + i) mod nz, i < zb_n, that the walls let hold charge (all without walls)
     int order;
     int coulomb;
@@ -110,6 +111,7 @@ struct DevPtrs {
     int* freel;
     int* titr;
     unsigned long long* qfix;  // fixed-point charge mesh
+    unsigned long long* qband; // fixed-point charge mesh of the wall band, kept current by the MC kernel (even nx)
     float2* cmesh;             // complex work mesh
     float* phi;                // potential mesh (real)
     float* goct;               // influence kernel octant
@@ -196,6 +198,44 @@ __device__ __forceinline__ void bspline_weights(float t, float* w) {
     }
 #pragma unroll
     for (int j = 0; j < P; ++j) w[j] = c[P - 1 - j];
+}
+
+// The fixed-point charge mesh: stencil of a charge and its integer value per mesh
+// point, every operation rounded as written (no contraction), so that the MC
+// kernel's incremental updates and the full spread give the same integers.
+template <int P>
+__device__ __forceinline__ void qmesh_stencil(const RepDesc& D, float4 pq, float (&w)[3][P], int (&base)[3]) {
+    const float p3[3] = {pq.x, pq.y, pq.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float g = __fmul_rn(__fdiv_rn(p3[k], D.L[k]), (float)D.mesh[k]);
+        const float fl = floorf(g);
+        const float t = __fsub_rn(g, fl);
+        float c[P];
+        c[0] = t; c[1] = __fsub_rn(1.0f, t);
+#pragma unroll
+        for (int n = 3; n <= P; ++n) {
+            const float inv = 1.0f / (float)(n - 1);
+            float nc[P];
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                const float a = (i < n - 1) ? c[i] : 0.0f;
+                const float b = (i >= 1) ? c[i - 1] : 0.0f;
+                const float ta = __fmul_rn(__fadd_rn(t, (float)i), a);
+                const float tb = __fmul_rn(__fsub_rn(__fsub_rn((float)n, t), (float)i), b);
+                nc[i] = __fmul_rn(__fadd_rn(ta, tb), inv);
+            }
+#pragma unroll
+            for (int i = 0; i < n; ++i) c[i] = nc[i];
+        }
+#pragma unroll
+        for (int j = 0; j < P; ++j) w[k][j] = c[P - 1 - j];
+        base[k] = (int)fl + P / 2 - P + 1;
+    }
+}
+// q wx wy wz in units of 2^-40 (q wy wz first, as a plane's row weight)
+__device__ __forceinline__ long long qmesh_value(float q, float wx, float wy, float wz) {
+    return __float2ll_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(q, wy), wz), wx), 1099511627776.0f));
 }
 
 __device__ __forceinline__ float min_image(float d, float L) { return d - L * rintf(d / L); }

@@ -229,7 +229,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         return off;
     };
     int slot_off = 0, cell_off = 0;
-    long long mesh_off = 0, meshh_off = 0, oct_off = 0;
+    long long mesh_off = 0, meshh_off = 0, oct_off = 0, qband_off = 0;
     E.use_r2c = ewald;
     for (int r = 0; r < R; ++r)
         if (prm[r].mesh[0] % 2 != 0) E.use_r2c = false;
@@ -326,6 +326,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                 const int hi = (int)std::floor(P.wall_hi * g) + 1 + E.order / 2;
                 if (hi - lo + 1 < D.mesh[2]) { D.zb_lo = ((lo % D.mesh[2]) + D.mesh[2]) % D.mesh[2]; D.zb_n = hi - lo + 1; }
             }
+            D.qb_off = qband_off; qband_off += (long long)D.mesh[0] * D.mesh[1] * D.zb_n;
             D.mesh_off = mesh_off; mesh_off += (long long)D.mesh[0] * D.mesh[1] * D.mesh[2];
             D.meshh_off = meshh_off; meshh_off += (long long)(D.mesh[0] / 2 + 1) * D.mesh[1] * D.mesh[2];
             D.oct_off = oct_off; oct_off += (long long)D.oct[0] * D.oct[1] * D.oct[2];
@@ -335,6 +336,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     E.total_cells = cell_off;
     E.total_mesh = mesh_off;
     E.total_meshh = meshh_off;
+    E.total_qband = qband_off;
     E.total_oct = oct_off;
 
     // ---- host particle arrays + lists ----
@@ -438,6 +440,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         // charge mesh; otherwise the scatter + full-complex path
         if (E.use_r2c) {
             DALLOC(d.cmesh, E.total_meshh);
+            DALLOC(d.qband, E.total_qband);
         } else {
             DALLOC(d.qfix, E.total_mesh); DALLOC(d.cmesh, E.total_mesh);
         }
@@ -476,9 +479,10 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                 }
                 // + cell counts / ids of the cell layers a plane's stencils reach (<= order + 5 layers)
                 const size_t ncell = (size_t)std::min(D.ncell[2], E.order + 5) * D.ncell[0] * D.ncell[1];
-                // two complex buffers (the 64-bit charge plane lives inside them) + cell counts
-                E.rb_fwd_smem = std::max(E.rb_fwd_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2) +
-                                                             (ncell + 1) * sizeof(int));
+                // band spread: the 64-bit charge plane + cell counts; first pass: two complex buffers
+                E.band_spread_smem = std::max(E.band_spread_smem, (size_t)D.mesh[0] * D.mesh[1] * sizeof(unsigned long long) +
+                                                                      (ncell + 1) * sizeof(int));
+                E.rb_fwd_smem = std::max(E.rb_fwd_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2));
                 E.rb_inv_smem = std::max(E.rb_inv_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2));
             } else {
                 for (int y = 0; y < D.mesh[1]; ++y)
@@ -523,7 +527,9 @@ static int check_kernel_errors(phmc_engine* h) {
 static int full_recompute(phmc_engine* h) {
     Engine& E = h->E;
     if (E.coulomb == PHMC_COUL_EWALD) {
-        launch_spread(E, nullptr, E.stream);
+        // the charge mesh from scratch (the MC kernel keeps the band mesh current between recomputes)
+        if (E.use_r2c) launch_band_spread(E, E.stream);
+        else launch_spread(E, nullptr, E.stream);
         launch_fft_pipeline(E, nullptr, 1, E.stream);
         CU(cudaGetLastError());
     }

@@ -34,7 +34,8 @@ struct Engine {
     double* d_epart = nullptr;
     size_t plane_smem = 0, zpass_smem = 0;
     bool use_r2c = false;        // every replica has even nx: fused spread + real-to-complex rebuild
-    size_t rb_fwd_smem = 0, rb_inv_smem = 0;
+    size_t rb_fwd_smem = 0, rb_inv_smem = 0, band_spread_smem = 0;
+    long long total_qband = 0;   // points of the wall bands' fixed-point charge meshes
     int zreg = 0;                // register z-pass variant for the shared nz (0: shared-memory z pass)
     int flush_kernels = 0;       // kernels per potential-mesh rebuild
     bool unit_pending = false;   // next rebuild places a unit charge instead of the particles
@@ -66,6 +67,7 @@ cudaError_t mesh_set_smem_limits(Engine& E);
 // k_rebuild.cu
 void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st);
 cudaError_t rebuild_set_smem_limits(Engine& E);
+void launch_band_spread(Engine& E, cudaStream_t st);
 int zreg_variant(int nz);      // register z-pass variant for nz, 0 if none
 size_t zreg_smem(int nz);
 

@@ -449,6 +449,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     __shared__ int s_cnt[NPROBE_MAX * 27], s_off[NPROBE_MAX * 27 + 1], s_cell[NPROBE_MAX * 27];
     __shared__ double red[100];
     __shared__ int s_npend;
+    __shared__ float4 s_qjob[4];     // charge-mesh updates of the last accepted change: (x, y, z, q) out / in
+    __shared__ int s_qsgn[4], s_nqjob;
     __shared__ int s_qin;            // counted among the launch's active replicas
     __shared__ volatile int s_qstop; // the launch's quorum of blocked replicas was seen
     __shared__ uint32_t s_rng[32][16];  // Philox words of trials s_rng_base .. s_rng_base+31
@@ -493,6 +495,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         s_sfail = 0;
         s_qstop = 0;
         s_qin = 0;
+        s_nqjob = 0;
         if (mode == MC_RUN && d.quorum < 1.0f && S.trial < S.target) { atomicAdd(&d.quorum_ctl[0], 1); s_qin = 1; }
         sur_mbar_init(&s_mbar[0]);
         sur_mbar_init(&s_mbar[1]);
@@ -543,6 +546,43 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 }
             }
         } else {
+            // warps 1..4: the last accepted change's updates of the fixed-point charge mesh
+            // (integer adds of the same values a full spread computes, so the band mesh stays
+            // equal to a spread of the current configuration)
+            {
+                const int wj = (tid >> 5) - 1;
+                if (wj < s_nqjob) {
+                    const float4 pq = s_qjob[wj];
+                    const bool neg = s_qsgn[wj] < 0;
+                    float w[3][P];
+                    int base[3];
+                    qmesh_stencil<P>(D, pq, w, base);
+                    const int nx = D.mesh[0], ny = D.mesh[1], nz = D.mesh[2];
+                    unsigned long long* qb = d.qband + D.qb_off;
+                    const int lane = tid & 31;  // lane (bb, c) < P^2 writes the row of P points
+                    const int bb = lane % P, c = lane / P;
+                    int zr = base[2] + c - D.zb_lo;
+                    zr %= nz;
+                    zr += (zr < 0) ? nz : 0;
+                    if (lane < P * P && zr < D.zb_n) {
+                        float wy = 0.0f, wz = 0.0f;  // selects keep the weights in registers
+#pragma unroll
+                        for (int j = 0; j < P; ++j) { wy = (j == bb) ? w[1][j] : wy; wz = (j == c) ? w[2][j] : wz; }
+                        int yb = base[1] + bb;
+                        yb += (yb < 0) ? ny : 0;
+                        yb -= (yb >= ny) ? ny : 0;
+                        unsigned long long* row = qb + ((size_t)zr * ny + yb) * nx;
+#pragma unroll
+                        for (int a = 0; a < P; ++a) {
+                            int xa = base[0] + a;
+                            xa += (xa < 0) ? nx : 0;
+                            xa -= (xa >= nx) ? nx : 0;
+                            const long long v = qmesh_value(pq.w, w[0][a], wy, wz);
+                            atomicAdd(&row[xa], (unsigned long long)(neg ? -v : v));
+                        }
+                    }
+                }
+            }
             // quorum of the launch: read off the proposing warp's path, used from the next trial on
             if (tid == 32 && s_qin) {
                 const int started = *(volatile int*)&d.quorum_ctl[0], blocked = *(volatile int*)&d.quorum_ctl[1];
@@ -559,7 +599,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         }
         __syncthreads();
         if (T.stop) break;
-        if (tid == 0) s_hv_slot = -1;
+        if (tid == 0) { s_hv_slot = -1; s_nqjob = 0; }
         // ---------------- surrogate first stage ----------------
         if (T.desc) {
             if (T.da && tid == 0) {  // stage the three hidden layers while the descriptor is built
@@ -1066,6 +1106,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             if (accept) {
                 if (mode == MC_RUN) S.acc[T.move]++;
                 const int so = D.slot_off;
+                if (d.qband) {  // charge-mesh updates, applied by warps 1..4 in the next proposal phase
+                    int nj = 0;
+                    for (int k = 0; k < T.nch; ++k) {
+                        const float4 o = T.po[k], nw = T.pn[k];
+                        if (T.pres_old[k] && T.pres_new[k] && o.x == nw.x && o.y == nw.y && o.z == nw.z && o.w == nw.w) continue;
+                        if (T.pres_old[k] && o.w != 0.0f) { s_qjob[nj] = o; s_qsgn[nj] = -1; ++nj; }
+                        if (T.pres_new[k] && nw.w != 0.0f) { s_qjob[nj] = nw; s_qsgn[nj] = 1; ++nj; }
+                    }
+                    s_nqjob = nj;
+                }
                 for (int k = 0; k < T.nch; ++k) {
                     const int i = T.idx[k];
                     const int gi = so + i;

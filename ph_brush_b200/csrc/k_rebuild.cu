@@ -1,13 +1,20 @@
 // Potential-mesh rebuild for meshes with even nx: three passes over the
-// half-spectrum mesh, spreading fused into the first.
+// half-spectrum mesh of each replica's fixed-point charge mesh.
 //
-//  k_rb_fwd  (replica, z): gather the charges whose order-P stencils reach plane
-//            z from the cell list, accumulate them in a shared-memory
-//            fixed-point plane (2^40, 64-bit shared atomics: deterministic and
-//            bit-identical to the scatter kernel's mesh), then real-to-complex
-//            FFT along x (length nx/2 complex FFT of packed pairs + split) and
-//            complex FFT along y; writes (nx/2+1) x ny complex values.
-//  k_rb_zpass (replica, y, column tile): FFT along z, E += w theta |F|^2,
+//  The charge mesh Q (2^40 fixed point, 64-bit integers: deterministic, order-
+//  independent sums) covers the planes of each replica's wall band.  It is kept
+//  current incrementally: the MC kernel adds the stencil values of every accepted
+//  change (old charges out, new charges in) with integer atomics, computed with the
+//  same exactly-rounded weights as the full spread (k_band_spread, run at every full
+//  recompute), so Q always equals a fresh spread of the current configuration.
+//
+//  k_band_spread (replica, z): gather the charges whose order-P stencils reach plane
+//            z from the cell list, accumulate them in a shared-memory fixed-point
+//            plane, store it to Q.
+//  k_rb_fwd  (replica, z): Q plane -> float, real-to-complex FFT along x (length
+//            nx/2 complex FFT of packed pairs + split) and complex FFT along y;
+//            writes (nx/2+1) x ny complex values.
+//  k_rb_zpass / k_rb_zreg (column tiles): FFT along z, E += w theta |F|^2,
 //            F *= theta, inverse FFT along z.
 //  k_rb_inv  (replica, z): inverse FFT along y, complex-to-real along x; writes
 //            the real potential plane.
@@ -16,14 +23,114 @@
 // band's planes, the z pass loads and stores only those (the rest of the input is
 // zero).  The unit-charge rebuild of the influence kernel computes every plane.
 // Replaces the memset + k_spread_cubic + cuFFT R2C + influence kernel chain of
-// the reference (MC/src/pme.cu:140-249,362,384-422) and the separate global
-// charge mesh of the scatter path.
+// the reference (MC/src/pme.cu:140-249,362,384-422).
 #include "common.cuh"
 #include "engine.h"
 #include "fft.cuh"
 #include "fft_reg.cuh"
 
 template <int P, int NT>
+__global__ void __launch_bounds__(NT) k_band_spread(DevPtrs d, const int2* __restrict__ jobs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int2 job = jobs[blockIdx.x];
+    const int r = job.x, z = job.y;
+    const RepDesc& D = d.desc[r];
+    const int nx = D.mesh[0], ny = D.mesh[1], nz = D.mesh[2];
+    unsigned long long* qp = reinterpret_cast<unsigned long long*>(sm_raw);
+    int* s_cnt = reinterpret_cast<int*>(qp + nx * ny);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < nx * ny; i += NT) qp[i] = 0ull;
+    __syncthreads();
+    // floor(g_z) of a contributing charge lies in [z - P/2, z - P/2 + P - 1] (mod nz)
+    const float hz = D.L[2] / (float)nz;
+    const float lo = (float)(z - P / 2) * hz, hi = (float)(z - P / 2 + P) * hz;
+    const int ncz = D.ncell[2], ncxy = D.ncell[0] * D.ncell[1];
+    // the cell layers of [lo, hi), widened by a rounding margin (the exact test is per charge)
+    int c_lo = (int)floorf((lo - 1e-3f * hz) * D.cell_scale[2]), c_hi = (int)floorf((hi + 1e-3f * hz) * D.cell_scale[2]);
+    int nlay = c_hi - c_lo + 1;
+    if (nlay > ncz) { nlay = ncz; c_lo = 0; }
+    const int ncell = nlay * ncxy;
+    // member counts of every cell in the layers, then an exclusive scan, so that the
+    // (cell, member) items spread over all threads with independent loads
+    __shared__ int s_wsum[NT / 32 + 1];
+    // cell of item cc: layer cc / ncxy (wrapped in z), in-layer index cc % ncxy
+    auto cell_of_item = [&](int cc) {
+        const int lay = cc / ncxy, cxy = cc - lay * ncxy;
+        int cz = (c_lo + lay) % ncz;
+        cz += (cz < 0) ? ncz : 0;
+        return cz * ncxy + cxy;
+    };
+    for (int cc = tid; cc < ncell; cc += NT)
+        s_cnt[cc] = min(d.cell_count[D.cell_off + cell_of_item(cc)], D.cell_cap);
+    __syncthreads();
+    {   // block scan: each thread a contiguous chunk, then the chunk totals
+        const int per = (ncell + NT - 1) / NT;
+        const int b0 = min(ncell, tid * per), b1 = min(ncell, b0 + per);
+        int sum = 0;
+        for (int i = b0; i < b1; ++i) sum += s_cnt[i];
+        int x = sum;
+        const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_wsum[warp] = x;
+        __syncthreads();
+        if (tid == 0) {
+            int acc = 0;
+            for (int w = 0; w < NT / 32; ++w) { const int v = s_wsum[w]; s_wsum[w] = acc; acc += v; }
+            s_wsum[NT / 32] = acc;
+        }
+        __syncthreads();
+        int run = s_wsum[warp] + x - sum;
+        for (int i = b0; i < b1; ++i) { const int v = s_cnt[i]; s_cnt[i] = run; run += v; }
+        if (tid == NT - 1) s_cnt[ncell] = s_wsum[NT / 32];
+    }
+    __syncthreads();
+    const int total = s_cnt[ncell];
+    for (int it = tid; it < total; it += NT) {
+        int lo2 = 0, hi2 = ncell - 1;  // last cell whose offset <= it
+        while (lo2 < hi2) {
+            const int mid = (lo2 + hi2 + 1) >> 1;
+            if (s_cnt[mid] <= it) lo2 = mid; else hi2 = mid - 1;
+        }
+        const int c = cell_of_item(lo2);
+        const int k = it - s_cnt[lo2];
+        const float4 pq = d.posq[D.slot_off + d.cell_list[((size_t)D.cell_off + c) * D.cell_cap + k]];
+        if (pq.w == 0.0f) continue;
+        float w[3][P];
+        int base[3];
+        qmesh_stencil<P>(D, pq, w, base);
+        int ci = z - base[2];
+        ci %= nz;
+        ci += (ci < 0) ? nz : 0;
+        if (ci >= P) continue;
+        float wz = 0.0f;  // select: w[2][ci] without a dynamic index
+#pragma unroll
+        for (int j = 0; j < P; ++j) wz = (j == ci) ? w[2][j] : wz;
+#pragma unroll
+        for (int bb = 0; bb < P; ++bb) {
+            int yb = base[1] + bb;
+            yb += (yb < 0) ? ny : 0;
+            yb -= (yb >= ny) ? ny : 0;
+#pragma unroll
+            for (int aa = 0; aa < P; ++aa) {
+                int xa = base[0] + aa;
+                xa += (xa < 0) ? nx : 0;
+                xa -= (xa >= nx) ? nx : 0;
+                atomicAdd(&qp[yb * nx + xa], (unsigned long long)qmesh_value(pq.w, w[0][aa], w[1][bb], wz));
+            }
+        }
+    }
+    __syncthreads();
+    int zrel = z - D.zb_lo;
+    zrel += (zrel < 0) ? nz : 0;
+    unsigned long long* q = d.qband + D.qb_off + (size_t)zrel * nx * ny;
+    for (int i = tid; i < nx * ny; i += NT) q[i] = qp[i];
+}
+
+template <int NT>
 __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict__ jobs, int unit_charge,
                                                const int* __restrict__ dirty) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -33,131 +140,20 @@ __global__ void __launch_bounds__(NT) k_rb_fwd(DevPtrs d, const int2* __restrict
     const RepDesc& D = d.desc[r];
     const int nx = D.mesh[0], ny = D.mesh[1], nz = D.mesh[2];
     const int M = nx / 2, nxh = M + 1;
-    // shared memory: two complex buffers of nxh x ny; the 64-bit charge plane (nx x ny)
-    // lives inside them until it is converted to the real plane (the packed pairs of a)
+    // two complex buffers of nxh x ny; the real plane Q[y][x] (row length nx) is loaded as
+    // the packed pairs a[y*M + j] = (Q[y][2j], Q[y][2j+1])
     float2* a = reinterpret_cast<float2*>(sm_raw);
     float2* b = a + nxh * ny;
-    unsigned long long* qp = reinterpret_cast<unsigned long long*>(sm_raw);
     const int tid = threadIdx.x;
-    for (int i = tid; i < nx * ny; i += NT) qp[i] = 0ull;
-    __syncthreads();
-    if (unit_charge) {
-        if (z == 0 && tid == 0) qp[0] = (unsigned long long)(long long)PHMC_FIX_SCALE;
+    if (unit_charge) {  // a unit charge on mesh point 0 (the influence kernel's source)
+        for (int i = tid; i < M * ny; i += NT) a[i] = make_float2((z == 0 && i == 0) ? 1.0f : 0.0f, 0.0f);
     } else {
-        // floor(g_z) of a contributing charge lies in [z - P/2, z - P/2 + P - 1] (mod nz)
-        const float hz = D.L[2] / (float)nz;
-        const float lo = (float)(z - P / 2) * hz, hi = (float)(z - P / 2 + P) * hz;
-        const int ncz = D.ncell[2], ncxy = D.ncell[0] * D.ncell[1];
-        // the cell layers of [lo, hi), widened by a rounding margin (the exact test is per charge)
-        int c_lo = (int)floorf((lo - 1e-3f * hz) * D.cell_scale[2]), c_hi = (int)floorf((hi + 1e-3f * hz) * D.cell_scale[2]);
-        int nlay = c_hi - c_lo + 1;
-        if (nlay > ncz) { nlay = ncz; c_lo = 0; }
-        const int ncell = nlay * ncxy;
-        // member counts of every cell in the layers, then an exclusive scan, so that the
-        // (cell, member) items spread over all threads with independent loads
-        int* s_cnt = reinterpret_cast<int*>(b + nxh * ny);
-        __shared__ int s_wsum[NT / 32 + 1];
-        // cell of item cc: layer cc / ncxy (wrapped in z), in-layer index cc % ncxy
-        auto cell_of_item = [&](int cc) {
-            const int lay = cc / ncxy, cxy = cc - lay * ncxy;
-            int cz = (c_lo + lay) % ncz;
-            cz += (cz < 0) ? ncz : 0;
-            return cz * ncxy + cxy;
-        };
-        for (int cc = tid; cc < ncell; cc += NT)
-            s_cnt[cc] = min(d.cell_count[D.cell_off + cell_of_item(cc)], D.cell_cap);
-        __syncthreads();
-        {   // block scan: each thread a contiguous chunk, then the chunk totals
-            const int per = (ncell + NT - 1) / NT;
-            const int b0 = min(ncell, tid * per), b1 = min(ncell, b0 + per);
-            int sum = 0;
-            for (int i = b0; i < b1; ++i) sum += s_cnt[i];
-            int x = sum;
-            const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            if (lane == 31) s_wsum[warp] = x;
-            __syncthreads();
-            if (tid == 0) {
-                int acc = 0;
-                for (int w = 0; w < NT / 32; ++w) { const int v = s_wsum[w]; s_wsum[w] = acc; acc += v; }
-                s_wsum[NT / 32] = acc;
-            }
-            __syncthreads();
-            int run = s_wsum[warp] + x - sum;
-            for (int i = b0; i < b1; ++i) { const int v = s_cnt[i]; s_cnt[i] = run; run += v; }
-            if (tid == NT - 1) s_cnt[ncell] = s_wsum[NT / 32];
-        }
-        __syncthreads();
-        const int total = s_cnt[ncell];
-        for (int it = tid; it < total; it += NT) {
-            int lo2 = 0, hi2 = ncell - 1;  // last cell whose offset <= it
-            while (lo2 < hi2) {
-                const int mid = (lo2 + hi2 + 1) >> 1;
-                if (s_cnt[mid] <= it) lo2 = mid; else hi2 = mid - 1;
-            }
-            const int c = cell_of_item(lo2);
-            const int k = it - s_cnt[lo2];
-            {
-                const float4 pq = d.posq[D.slot_off + d.cell_list[((size_t)D.cell_off + c) * D.cell_cap + k]];
-                if (pq.w == 0.0f) continue;
-                const float gz = pq.z / D.L[2] * (float)nz;
-                const float flz = floorf(gz);
-                int ci = z - ((int)flz + P / 2 - P + 1);
-                ci %= nz;
-                ci += (ci < 0) ? nz : 0;
-                if (ci >= P) continue;
-                float wz[P], wx[P], wy[P];
-                bspline_weights<P>(gz - flz, wz);
-                const float gx = pq.x / D.L[0] * (float)nx, gy = pq.y / D.L[1] * (float)ny;
-                const float flx = floorf(gx), fly = floorf(gy);
-                bspline_weights<P>(gx - flx, wx);
-                bspline_weights<P>(gy - fly, wy);
-                const int bx = (int)flx + P / 2 - P + 1, by = (int)fly + P / 2 - P + 1;
-#pragma unroll
-                for (int bb = 0; bb < P; ++bb) {
-                    int yb = by + bb;
-                    yb += (yb < 0) ? ny : 0;
-                    yb -= (yb >= ny) ? ny : 0;
-                    const float wyz = pq.w * wy[bb] * wz[ci];
-#pragma unroll
-                    for (int aa = 0; aa < P; ++aa) {
-                        int xa = bx + aa;
-                        xa += (xa < 0) ? nx : 0;
-                        xa -= (xa >= nx) ? nx : 0;
-                        // v * 2^40 is exact in float, so this rounds the same real number as the
-                        // scatter kernel's double conversion: identical fixed-point values
-                        const long long v = __float2ll_rn(wyz * wx[aa] * 1099511627776.0f);
-                        atomicAdd(&qp[yb * nx + xa], (unsigned long long)v);
-                    }
-                }
-            }
-        }
-    }
-    __syncthreads();
-    // fixed point -> float in place, in chunks of NT * CV elements: the floats of chunk k
-    // overwrite 64-bit elements [k CH/2, (k+1) CH/2), all read in chunks <= k.  The real
-    // plane Q[y][x] (row length nx) is then the packed pairs a[y*M + j] = (Q[y][2j], Q[y][2j+1]).
-    {
-        constexpr int CV = 16, CH = NT * CV;
-        float* qf = reinterpret_cast<float*>(sm_raw);
-        const int nq = nx * ny;
-        for (int c0 = 0; c0 < nq; c0 += CH) {
-            float v[CV];
-#pragma unroll
-            for (int u = 0; u < CV; ++u) {
-                const int i = c0 + u * NT + tid;
-                v[u] = (i < nq) ? (float)((double)(long long)qp[i] * PHMC_FIX_INV) : 0.0f;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int u = 0; u < CV; ++u) {
-                const int i = c0 + u * NT + tid;
-                if (i < nq) qf[i] = v[u];
-            }
+        int zrel = z - D.zb_lo;
+        zrel += (zrel < 0) ? nz : 0;
+        const ulonglong2* q = reinterpret_cast<const ulonglong2*>(d.qband + D.qb_off + (size_t)zrel * nx * ny);
+        for (int i = tid; i < M * ny; i += NT) {
+            const ulonglong2 v = q[i];
+            a[i] = make_float2((float)((double)(long long)v.x * PHMC_FIX_INV), (float)((double)(long long)v.y * PHMC_FIX_INV));
         }
     }
     __syncthreads();
@@ -404,11 +400,7 @@ __global__ void __launch_bounds__(NT) k_rb_inv(DevPtrs d, const int2* __restrict
 void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st) {
     const int2* pj = unit_charge ? E.d_plane_jobs : E.d_band_jobs;
     const int npj = unit_charge ? E.n_plane_jobs : E.n_band_jobs;
-    switch (E.order) {
-        case 4: k_rb_fwd<4, 256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty); break;
-        case 5: k_rb_fwd<5, 256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty); break;
-        default: k_rb_fwd<6, 256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty); break;
-    }
+    k_rb_fwd<256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty);
     switch (E.zreg) {
 #define ZREG_LAUNCH(id, n, a, b) \
         case id: k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX><<<E.n_zjobs, ZREG_NT(b), E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty, unit_charge); break;
@@ -417,6 +409,15 @@ void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream
         default: k_rb_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty, unit_charge);
     }
     k_rb_inv<256><<<npj, 256, E.rb_inv_smem, st>>>(E.d, pj, dirty);
+}
+
+// Charge mesh of every replica's wall band from scratch (full recompute).
+void launch_band_spread(Engine& E, cudaStream_t st) {
+    switch (E.order) {
+        case 4: k_band_spread<4, 256><<<E.n_band_jobs, 256, E.band_spread_smem, st>>>(E.d, E.d_band_jobs); break;
+        case 5: k_band_spread<5, 256><<<E.n_band_jobs, 256, E.band_spread_smem, st>>>(E.d, E.d_band_jobs); break;
+        default: k_band_spread<6, 256><<<E.n_band_jobs, 256, E.band_spread_smem, st>>>(E.d, E.d_band_jobs); break;
+    }
 }
 
 template <typename K>
@@ -435,10 +436,12 @@ static cudaError_t raise_cap(K kernel, int device, size_t need) {
 cudaError_t rebuild_set_smem_limits(Engine& E) {
     cudaError_t e = cudaSuccess;
     switch (E.order) {
-        case 4: e = raise_cap(k_rb_fwd<4, 256>, E.device, E.rb_fwd_smem); break;
-        case 5: e = raise_cap(k_rb_fwd<5, 256>, E.device, E.rb_fwd_smem); break;
-        default: e = raise_cap(k_rb_fwd<6, 256>, E.device, E.rb_fwd_smem); break;
+        case 4: e = raise_cap(k_band_spread<4, 256>, E.device, E.band_spread_smem); break;
+        case 5: e = raise_cap(k_band_spread<5, 256>, E.device, E.band_spread_smem); break;
+        default: e = raise_cap(k_band_spread<6, 256>, E.device, E.band_spread_smem); break;
     }
+    if (e != cudaSuccess) return e;
+    e = raise_cap(k_rb_fwd<256>, E.device, E.rb_fwd_smem);
     if (e != cudaSuccess) return e;
     switch (E.zreg) {
 #define ZREG_CAP(id, n, a, b) case id: e = raise_cap(k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX>, E.device, E.zpass_smem); break;

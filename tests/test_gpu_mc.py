@@ -91,6 +91,32 @@ def test_runs_are_bit_reproducible():
 
 
 @pytest.mark.gpu
+def test_charge_mesh_kept_by_the_mc_kernel_equals_a_fresh_spread():
+    """Between full recomputes the MC kernel keeps the fixed-point charge mesh of the
+    wall band current with integer updates at every accepted change.  After thousands
+    of displacements, titrations and ion swaps, the potential rebuilt from that mesh
+    must equal the one a fresh spread of the same configuration gives: the reciprocal
+    dE of probe trials is bitwise the same on an engine given the state anew."""
+    s, p = configs.small_system(seed=11, p_swap=0.2, salt_conc=0.05)
+    with Engine(s, p) as a, Engine(s, p) as b:
+        st = a.run(20000)[0]
+        assert sum(st["accepted"]) > 2000 and st["accepted"][2] > 0, st["accepted"]
+        cur = a.state(0)
+        b.set_state(cur, 0)
+        live = np.flatnonzero(((cur["flags"] & _abi.F_GHOST) == 0) & (cur["q"] != 0.0))
+        trials = []
+        for i in live[:24]:
+            z = float(np.clip(cur["z"][i] + 0.07, p.wall_lo + 0.01, p.wall_hi - 0.01))
+            x, y = float((cur["x"][i] + 0.11) % s.box[0]), float((cur["y"][i] - 0.05) % s.box[1])
+            trials.append([{"index": i, "x": x, "y": y, "z": z,
+                            "q": cur["q"][i], "type": cur["type"][i]}])
+        ra = np.array([c["coul_recip"] for c in a.delta_energy_components(trials)])
+        rb = np.array([c["coul_recip"] for c in b.delta_energy_components(trials)])
+        assert len(ra) >= 8 and np.any(ra != 0.0)
+        assert np.array_equal(ra, rb), np.max(np.abs(ra - rb))
+
+
+@pytest.mark.gpu
 def test_tracked_energy_matches_recompute():
     s, p = configs.config1()
     with Engine(s, p) as e:
