@@ -253,7 +253,7 @@ typedef struct phmc_profile {
     int64_t flush_launches;  /* rebuild pipelines (each = spread + 3 FFT passes + reduce) */
     int64_t kernel_launches; /* every kernel the engine launched */
     double mc_alg_bytes;     /* algorithmic bytes of all trials (per-trial model in the docs) */
-    double flush_alg_bytes;  /* algorithmic bytes of all rebuilds: 16 N + 32 Mcb + 4 Mb per replica (N particles,
+    double flush_alg_bytes;  /* algorithmic bytes of all rebuilds: 16 N + 32 Mcb + 12 Mb per replica (N particles,
                                 Mb / Mcb real / half-spectrum mesh points of the planes between the walls) */
     int64_t trials;
     double mc_busy_ms;       /* summed over replicas: time their MC blocks ran; mc_busy_ms / (replicas * mc_ms)

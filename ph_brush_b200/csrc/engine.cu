@@ -833,11 +833,12 @@ int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
             h->prof.mc_alg_bytes += st1[r].alg_bytes - st0[r].alg_bytes;
             h->prof.trials += st1[r].trials_run - st0[r].trials_run;
             h->prof.mc_busy_ms += 1e-6 * (double)(st1[r].busy_ns - st0[r].busy_ns);
-            // planes of the wall band: the first pass writes the half spectrum (8 B per complex
-            // value), the z pass reads and writes it, the last pass reads it and writes phi (4 B)
+            // planes of the wall band: the first pass reads the fixed-point charge plane (8 B per
+            // point) and writes the half spectrum (8 B per complex value), the z pass reads and
+            // writes it, the last pass reads it and writes phi (4 B per point)
             const double Mb = (double)D.mesh[0] * D.mesh[1] * D.zb_n;
             const double Mcb = (double)(D.mesh[0] / 2 + 1) * D.mesh[1] * D.zb_n;
-            h->prof.flush_alg_bytes += (double)(st1[r].flushes - st0[r].flushes) * (16.0 * h->n_present[r] + 32.0 * Mcb + 4.0 * Mb);
+            h->prof.flush_alg_bytes += (double)(st1[r].flushes - st0[r].flushes) * (16.0 * h->n_present[r] + 32.0 * Mcb + 12.0 * Mb);
         }
     }
     return PHMC_OK;
