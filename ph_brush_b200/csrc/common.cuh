@@ -28,6 +28,8 @@ struct RepDesc {
     int mod_off[3];       // offsets of the B-spline moduli per axis
     int tw_off[3];        // offsets of the twiddle tables per axis
     int tw_off_h;         // twiddle table of length nx/2 (real-to-complex path)
+    int th_off[3];        // per-axis influence factors (exp(-(pi/alpha)^2 k^2) / B(k), k^2) in thtab
+    float th_c;           // elf / (pi V): theta(k) = th_c tx ty tz / |k|^2
     long long meshh_off;  // offset into the half-spectrum complex mesh ((nx/2+1) x ny x nz)
     long long qb_off;     // offset of this replica's fixed-point charge mesh (nx x ny x zb_n) in qband
     int zb_lo, zb_n;      // band of planes (zb_lo + i) mod nz, i < zb_n, that the walls let hold charge (all without walls)
@@ -117,6 +119,7 @@ struct DevPtrs {
     float* goct;               // influence kernel octant
     float* moduli;
     float2* twiddle;
+    float2* thtab;             // per-axis influence factors of the rebuild's z pass
     RepDesc* desc;
     RepState* state;
     double* partials;          // reduction scratch

@@ -218,6 +218,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     // ---- descriptors ----
     E.desc.resize(R);
     std::vector<double> h_mod;
+    std::vector<float2> h_th;
     std::vector<float2> h_tw;
     std::map<int, int> tw_off;
     auto tw_table = [&](int n) {  // exp(-2 pi i j / n), j < n, one table per distinct length
@@ -313,9 +314,21 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                 std::vector<double> m = bspline_moduli(P.mesh[k], P.order, P.ref_moduli);
                 D.mod_off[k] = (int)h_mod.size();
                 h_mod.insert(h_mod.end(), m.begin(), m.end());
+                // the influence function factorises per axis: theta(k) = elf exp(-(pi/alpha)^2 |k|^2) /
+                // (pi V |k|^2 Bx By Bz); per axis (exp(-(pi/alpha)^2 k^2) / B(k), k^2) in FP64, rounded
+                // once (a zero modulus gives a zero factor, as the reference's den > 0 test does)
+                D.th_off[k] = (int)h_th.size();
+                const double ef = (M_PI / P.ewald_alpha) * (M_PI / P.ewald_alpha);
+                for (int j = 0; j < P.mesh[k]; ++j) {
+                    const int mj = (j <= P.mesh[k] / 2) ? j : j - P.mesh[k];
+                    const double kk = (double)mj / (double)D.L[k];
+                    const double f = (m[j] > 0.0) ? std::exp(-ef * kk * kk) / m[j] : 0.0;
+                    h_th.push_back(make_float2((float)f, (float)(kk * kk)));
+                }
                 D.tw_off[k] = tw_table(P.mesh[k]);
             }
             D.tw_off_h = (P.mesh[0] % 2 == 0) ? tw_table(P.mesh[0] / 2) : 0;
+            D.th_c = (float)(elf / (M_PI * D.V));
             // planes a charge inside the walls can reach: floor(g_z) of z in [wall_lo, wall_hi]
             // (one plane of rounding margin either side) + the stencil offsets
             // [P/2 - P + 1, P/2]; the rebuild computes and reads only these
@@ -447,7 +460,8 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         DALLOC(d.phi, E.total_mesh);
         E.flush_kernels = E.use_r2c ? 4 : 5;
         DALLOC(d.goct, E.total_oct);
-        DALLOC(d.moduli, h_mod.size()); DALLOC(d.twiddle, h_tw.size());
+        DALLOC(d.moduli, h_mod.size()); DALLOC(d.twiddle, h_tw.size()); DALLOC(d.thtab, h_th.size());
+        CU(cudaMemcpy(d.thtab, h_th.data(), sizeof(float2) * h_th.size(), cudaMemcpyHostToDevice));
         std::vector<float> hm(h_mod.begin(), h_mod.end());
         CU(cudaMemcpy(d.moduli, hm.data(), sizeof(float) * hm.size(), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(d.twiddle, h_tw.data(), sizeof(float2) * h_tw.size(), cudaMemcpyHostToDevice));

@@ -201,12 +201,9 @@ __global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restri
     }
     __syncthreads();
     float2* res = fft_lines<NT>(a, b, nz, TX, 1, TX, d.twiddle + D.tw_off[2], -1.0f, true);
-    const float* mx = d.moduli + D.mod_off[0];
-    const float* my = d.moduli + D.mod_off[1];
-    const float* mz = d.moduli + D.mod_off[2];
-    const int myi = (y <= ny / 2) ? y : y - ny;
-    const float kyv = (float)myi / D.L[1];
-    const float pv = 3.14159265358979323846f * (float)D.V;
+    const float2* thx = d.thtab + D.th_off[0];
+    const float2 fy = d.thtab[D.th_off[1] + y];
+    const float2* thz = d.thtab + D.th_off[2];
     double e_loc = 0.0;
     for (int e = threadIdx.x; e < nz * TX; e += NT) {
         const int kz = e / TX, tx = e - kz * TX;
@@ -214,11 +211,9 @@ __global__ void __launch_bounds__(NT) k_rb_zpass(DevPtrs d, const int4* __restri
         const float2 F = res[e];
         float th = 0.0f;
         if (tx < tw_n && !(kx == 0 && y == 0 && kz == 0)) {
-            const int mzi = (kz <= nz / 2) ? kz : kz - nz;
-            const float kxv = (float)kx / D.L[0], kzv = (float)mzi / D.L[2];
-            const float m2 = kxv * kxv + kyv * kyv + kzv * kzv;
-            const float den = m2 * pv * mx[kx] * my[y] * mz[kz];
-            if (den > 0.0f) th = D.elf * expf(-D.ewald_factor * m2) / den;
+            // theta = th_c tx ty tz / |k|^2 from the per-axis factor tables
+            const float2 fx = __ldg(&thx[kx]), fz = __ldg(&thz[kz]);
+            th = __fdividef(D.th_c * fx.x * fy.x * fz.x, fx.y + fy.y + fz.y);
             const float wgt = (kx == 0 || kx == M) ? 1.0f : 2.0f;  // half spectrum, Hermitian partners counted
             e_loc += (double)(wgt * th) * ((double)F.x * F.x + (double)F.y * F.y);
         }
@@ -260,11 +255,12 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
     const size_t plane = (size_t)ny * nxh;
     float2* s = sm;            // [k1][n2][column]
     float2* tw = sm + N * TX;  // exp(-2 pi i j / nz)
+    float2* thz = tw + N;      // z influence factor and k_z^2 per kz
     float2* c = d.cmesh + D.meshh_off + c0;
     // planes outside the wall band hold no charge (zero input) and are not read back
     const int zlo = full ? 0 : D.zb_lo, zbn = full ? N : D.zb_n;
     auto in_band = [&](int z) { int t = z - zlo; t += (t < 0) ? N : 0; return t < zbn; };
-    for (int i = threadIdx.x; i < N; i += NT) tw[i] = d.twiddle[D.tw_off[2] + i];
+    for (int i = threadIdx.x; i < N; i += NT) { tw[i] = d.twiddle[D.tw_off[2] + i]; thz[i] = d.thtab[D.th_off[2] + i]; }
     // stage A: the loads of the first round go out before the barrier that publishes tw
     for (int base = 0; base < N2 * TX; base += NT) {
         const int it = base + threadIdx.x;
@@ -284,10 +280,6 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
         }
     }
     __syncthreads();
-    const float* mx = d.moduli + D.mod_off[0];
-    const float* my = d.moduli + D.mod_off[1];
-    const float* mz = d.moduli + D.mod_off[2];
-    const float pv = 3.14159265358979323846f * (float)D.V;
     double e_loc = 0.0;
     for (int it = threadIdx.x; it < N1 * TX; it += NT) {
         const int k1 = it / TX, col = it & (TX - 1);
@@ -298,8 +290,10 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
         const int idx = c0 + col;
         const int y = idx / nxh, kx = idx - y * nxh;
         const bool valid = col < ncol;
-        const int myi = (y <= ny / 2) ? y : y - ny;
-        const float kxv = (float)kx / D.L[0], kyv = (float)myi / D.L[1];
+        // theta = th_c tx ty tz / |k|^2 from the per-axis factor tables (column part once)
+        const float2 fx = valid ? d.thtab[D.th_off[0] + kx] : make_float2(0.0f, 1.0f);
+        const float2 fy = valid ? d.thtab[D.th_off[1] + y] : make_float2(0.0f, 1.0f);
+        const float cxy = D.th_c * fx.x * fy.x, kxy2 = fx.y + fy.y;
         const float wgt = (kx == 0 || kx == M) ? 1.0f : 2.0f;  // half spectrum, Hermitian partners counted
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) {
@@ -307,11 +301,8 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
             const float2 F = u[k2];
             float th = 0.0f;
             if (valid && !(kx == 0 && y == 0 && kz == 0)) {
-                const int mzi = (kz <= N / 2) ? kz : kz - N;
-                const float kzv = (float)mzi / D.L[2];
-                const float m2 = kxv * kxv + kyv * kyv + kzv * kzv;
-                const float den = m2 * pv * mx[kx] * my[y] * mz[kz];
-                if (den > 0.0f) th = D.elf * expf(-D.ewald_factor * m2) / den;
+                const float2 fz = thz[kz];
+                th = __fdividef(cxy * fz.x, kxy2 + fz.y);
                 e_loc += (double)(wgt * th) * ((double)F.x * F.x + (double)F.y * F.y);
             }
             u[k2] = make_float2(F.x * th, F.y * th);
@@ -353,7 +344,7 @@ int zreg_variant(int nz) {
 #undef ZREG_CASE
     return 0;
 }
-size_t zreg_smem(int nz) { return (size_t)(ZREG_TX + 1) * nz * sizeof(float2); }
+size_t zreg_smem(int nz) { return (size_t)(ZREG_TX + 2) * nz * sizeof(float2); }
 
 template <int NT>
 __global__ void __launch_bounds__(NT) k_rb_inv(DevPtrs d, const int2* __restrict__ jobs, const int* __restrict__ dirty) {
