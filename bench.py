@@ -378,23 +378,25 @@ def run_ours(args):
     try:
         import torch
         pinned = {k: torch.from_numpy(v.copy()).pin_memory().numpy() for k, v in st.items()}
+        readback = {k: torch.from_numpy(v.copy()).pin_memory().numpy() for k, v in st.items()}
     except Exception:
         pinned = {k: v.copy() for k, v in st.items()}
+        readback = {k: v.copy() for k, v in st.items()}
     slots = len(st["x"])
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         eng.set_state(pinned, -1)
         res = eng.run(T)
-        out = eng.state(-1)
+        out = eng.state(-1, out=readback)
         energies = [r["energy"] for r in res]
     e2e_s = time.perf_counter() - t0
     barrier(world)
     e2e_s = reduce_max(e2e_s, world, local)
     e2e = {"value": world * args.steps * sweeps_per_step / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": slots * (16 + 4 + 4), "d2h_bytes_per_step": slots * (16 + 4 + 4) + 8 * len(reps),
-           "timing": "host wall clock around phmc_set_state(all replicas) + phmc_run + phmc_get_state(all replicas), "
-                     "synchronous calls"}
+           "timing": "host wall clock around phmc_set_state(all replicas, from pinned host arrays) + phmc_run + "
+                     "phmc_get_state(all replicas, into pinned host arrays), synchronous calls"}
     del out, energies
 
     # ---- roofline of the dominant kernel (MC kernel or the fused rebuild) ----

@@ -128,11 +128,19 @@ class Engine:
         _abi.check(self._lib.phmc_set_move_mix(self._h, int(replica), float(p_disp), float(p_titr), float(p_swap)))
 
     # ---- state ----
-    def state(self, replica=0):
-        """Slot arrays of one replica, or of all replicas concatenated (replica=-1)."""
+    def state(self, replica=0, out=None):
+        """Slot arrays of one replica, or of all replicas concatenated (replica=-1).  `out`: a dict
+        of preallocated arrays (x, y, z, q float32; type, flags int32; e.g. in pinned memory) to
+        fill instead of new ones."""
         n = sum(self.caps) if replica < 0 else self.caps[replica]
-        x, y, z, q = (np.zeros(n, np.float32) for _ in range(4))
-        t, f = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        if out is not None:
+            x, y, z, q, t, f = (out[k] for k in ("x", "y", "z", "q", "type", "flags"))
+            for a, dt in ((x, np.float32), (y, np.float32), (z, np.float32), (q, np.float32), (t, np.int32), (f, np.int32)):
+                if a.dtype != dt or a.shape != (n,) or not a.flags.c_contiguous:
+                    raise ValueError(f"state(out=...): arrays must be contiguous {n}-element float32 / int32")
+        else:
+            x, y, z, q = (np.zeros(n, np.float32) for _ in range(4))
+            t, f = np.zeros(n, np.int32), np.zeros(n, np.int32)
         _abi.check(self._lib.phmc_get_state(self._h, replica, _abi.fptr(x), _abi.fptr(y), _abi.fptr(z),
                                             _abi.fptr(q), _abi.iptr(t), _abi.iptr(f)))
         return {"x": x, "y": y, "z": z, "q": q, "type": t, "flags": f}
