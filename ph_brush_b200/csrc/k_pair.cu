@@ -68,24 +68,31 @@ __global__ void __launch_bounds__(NT) k_full_energy(DevPtrs d, int bpr) {
         if (D.walls && (pi.z < D.wall_lo || pi.z >= D.wall_hi)) acc[2] = __longlong_as_double(0x7ff0000000000000ll);
         const int c = d.cell_of[gi];
         const int cx = c % D.ncell[0], cy = (c / D.ncell[0]) % D.ncell[1], cz = c / (D.ncell[0] * D.ncell[1]);
-        for (int dz = -1; dz <= 1; ++dz)
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int nc = (wrap_idx(cz + dz, D.ncell[2]) * D.ncell[1] + wrap_idx(cy + dy, D.ncell[1])) * D.ncell[0] +
-                                   wrap_idx(cx + dx, D.ncell[0]);
-                    const int cnt = min(d.cell_count[D.cell_off + nc], D.cell_cap);
-                    const int* l = d.cell_list + ((size_t)D.cell_off + nc) * D.cell_cap;
-                    for (int k = 0; k < cnt; ++k) {
-                        const int j = l[k];
-                        if (j <= i) continue;
-                        const float4 pj = d.posq[D.slot_off + j];
-                        const int tj = d.type[D.slot_off + j];
-                        float elj, ec;
-                        pair_energy(D, min_image(pi.x - pj.x, D.L[0]), min_image(pi.y - pj.y, D.L[1]),
-                                    min_image(pi.z - pj.z, D.L[2]), ti, tj, pi.w, pj.w, in_bonds(bi, j), elj, ec);
-                        acc[0] += elj; acc[1] += ec;
-                    }
-                }
+        // each unordered pair once: the own cell with j > i, and every particle of the 13
+        // neighbour cells in the forward half shell (first non-zero offset of (dz, dy, dx)
+        // positive; with at least 3 cells per axis these are 13 distinct cells)
+        for (int h = 0; h < 14; ++h) {
+            const int dz = (h == 0) ? 0 : (h < 5 ? 0 : 1), rem = (h == 0) ? 0 : (h < 5 ? h - 1 : h - 5);
+            int dy, dx;
+            if (h == 0) { dy = 0; dx = 0; }
+            else if (h == 1) { dy = 0; dx = 1; }
+            else if (h < 5) { dy = 1; dx = rem - 2; }            // h = 2..4: (0, 1, -1..1)
+            else { dy = rem / 3 - 1; dx = rem % 3 - 1; }         // h = 5..13: (1, -1..1, -1..1)
+            const int nc = (wrap_idx(cz + dz, D.ncell[2]) * D.ncell[1] + wrap_idx(cy + dy, D.ncell[1])) * D.ncell[0] +
+                           wrap_idx(cx + dx, D.ncell[0]);
+            const int cnt = min(d.cell_count[D.cell_off + nc], D.cell_cap);
+            const int* l = d.cell_list + ((size_t)D.cell_off + nc) * D.cell_cap;
+            for (int k = 0; k < cnt; ++k) {
+                const int j = l[k];
+                if (h == 0 && j <= i) continue;
+                const float4 pj = d.posq[D.slot_off + j];
+                const int tj = d.type[D.slot_off + j];
+                float elj, ec;
+                pair_energy(D, min_image(pi.x - pj.x, D.L[0]), min_image(pi.y - pj.y, D.L[1]),
+                            min_image(pi.z - pj.z, D.L[2]), ti, tj, pi.w, pj.w, in_bonds(bi, j), elj, ec);
+                acc[0] += elj; acc[1] += ec;
+            }
+        }
         if (D.fene_k > 0.0f) {
             const int bl[4] = {bi.x, bi.y, bi.z, bi.w};
             for (int k = 0; k < 4; ++k) {
