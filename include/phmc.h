@@ -234,6 +234,21 @@ int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_
  * of the reciprocal-space dE. */
 int phmc_set_quorum(phmc_engine* e, double quorum);
 
+/* ---- checkpoint / exact resume (no counterpart in the reference: its LAMMPS data
+ * output, MC/src/io.cpp:326-368, keeps positions and identities but not the chain's
+ * random-number counter, list order or tracked energies) ----
+ * phmc_checkpoint_save writes every replica's particle arrays, the index lists the
+ * proposals draw from and the cell lists (their order included), the per-replica
+ * counters (trial index = Philox counter, accept counts, delayed-acceptance window)
+ * and tracked FP64 energies and charge moments, the move mix, the tuning, the
+ * launch quorum and the fixed-point charge mesh.  phmc_checkpoint_load restores
+ * them into an engine created from the same systems and parameters (other
+ * replicas, capacities or cells are refused with PHMC_ERR_IO) and recomputes the
+ * potential; runs continue bit for bit as the saved engine's would.  An attached surrogate is
+ * not part of the checkpoint (phmc_surrogate_save / _load, then attach). */
+int phmc_checkpoint_save(phmc_engine* e, const char* path);
+int phmc_checkpoint_load(phmc_engine* e, const char* path);
+
 /* ---- state ----
  * replica == -1: every replica at once, arrays of sum(capacity) slots concatenated
  * in replica order (one upload and one full recompute for the whole engine). */

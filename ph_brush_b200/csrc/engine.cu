@@ -1392,3 +1392,125 @@ extern "C" int phmc_delta_energy_components(phmc_engine* h, int rep, const phmc_
     }
     return check_kernel_errors(h);
 }
+
+// ---------------------------------------------------------------------------
+// checkpoint / exact resume: everything that decides the chain's continuation
+// (particle arrays, the index lists whose order the proposals draw from, the
+// cell lists whose order fixes the summation order, per-replica counters and
+// tracked FP64 energies and moments, move mix, tuning, and the fixed-point charge
+// mesh of the wall bands); the potential is recomputed from the charge mesh
+// ---------------------------------------------------------------------------
+namespace {
+const char kCkptMagic[8] = {'P', 'H', 'M', 'C', 'C', 'K', '0', '1'};
+struct CkptRep {
+    int cap, slot_off, ncell[3], mesh[3];
+    float p_disp, p_titr, p_swap;
+};
+template <typename T>
+bool ck_write_dev(FILE* f, const T* dptr, size_t n, std::vector<unsigned char>& buf) {
+    buf.resize(n * sizeof(T));
+    if (cudaMemcpy(buf.data(), dptr, n * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    return fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+}
+template <typename T>
+bool ck_read_dev(FILE* f, T* dptr, size_t n, std::vector<unsigned char>& buf) {
+    buf.resize(n * sizeof(T));
+    if (fread(buf.data(), 1, buf.size(), f) != buf.size()) return false;
+    return cudaMemcpy(dptr, buf.data(), n * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+}  // namespace
+
+extern "C" int phmc_checkpoint_save(phmc_engine* h, const char* path) {
+    if (!h || !path) return fail(PHMC_ERR_ARG, "phmc_checkpoint_save: null argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(PHMC_ERR_IO, std::string("cannot write ") + path);
+    const DevPtrs& d = E.d;
+    const size_t N = (size_t)E.total_slots, C = (size_t)E.total_cells;
+    const int hdr[7] = {1, E.R, E.total_slots, E.total_cells, E.cell_cap, (int)sizeof(RepState), E.pend_max};
+    bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(hdr, sizeof(int), 7, f) == 7 &&
+              fwrite(&E.threads, sizeof(int), 1, f) == 1 && fwrite(&E.quorum, sizeof(float), 1, f) == 1;
+    for (int r = 0; r < E.R && ok; ++r) {
+        const RepDesc& D = E.desc[r];
+        const CkptRep cr = {D.cap, D.slot_off, {D.ncell[0], D.ncell[1], D.ncell[2]}, {D.mesh[0], D.mesh[1], D.mesh[2]},
+                            D.p_disp, D.p_titr, D.p_swap};
+        ok = fwrite(&cr, sizeof cr, 1, f) == 1;
+    }
+    std::vector<unsigned char> buf;
+    ok = ok && ck_write_dev(f, d.posq, N, buf) && ck_write_dev(f, d.type, N, buf) && ck_write_dev(f, d.flags, N, buf) &&
+         ck_write_dev(f, d.bonds, N, buf) && ck_write_dev(f, d.cell_of, N, buf) && ck_write_dev(f, d.cell_pos, N, buf) &&
+         ck_write_dev(f, d.mobile, N, buf) && ck_write_dev(f, d.mobile_pos, N, buf) && ck_write_dev(f, d.anions, N, buf) &&
+         ck_write_dev(f, d.anion_pos, N, buf) && ck_write_dev(f, d.cations, N, buf) && ck_write_dev(f, d.cation_pos, N, buf) &&
+         ck_write_dev(f, d.freel, N, buf) && ck_write_dev(f, d.titr, N, buf) && ck_write_dev(f, d.cell_count, C, buf) &&
+         ck_write_dev(f, d.cell_list, C * E.cell_cap, buf) && ck_write_dev(f, d.cell_cls, C, buf) &&
+         ck_write_dev(f, d.state, (size_t)E.R, buf);
+    // the fixed-point charge mesh of the wall bands, last in the file
+    if (ok && E.use_r2c) ok = ck_write_dev(f, d.qband, (size_t)E.total_qband, buf);
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return fail(PHMC_ERR_IO, std::string("phmc_checkpoint_save: short write or device copy to ") + path);
+    return PHMC_OK;
+}
+
+extern "C" int phmc_checkpoint_load(phmc_engine* h, const char* path) {
+    if (!h || !path) return fail(PHMC_ERR_ARG, "phmc_checkpoint_load: null argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(PHMC_ERR_IO, std::string("cannot read ") + path);
+    auto bad = [&](const std::string& why) { fclose(f); return fail(PHMC_ERR_IO, "phmc_checkpoint_load: " + why + " (" + path + ")"); };
+    char magic[8];
+    int hdr[7], threads = 0;
+    float quorum = 1.0f;
+    if (fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return bad("not a checkpoint");
+    if (fread(hdr, sizeof(int), 7, f) != 7 || fread(&threads, sizeof(int), 1, f) != 1 || fread(&quorum, sizeof(float), 1, f) != 1)
+        return bad("truncated header");
+    if (hdr[0] != 1 || hdr[1] != E.R || hdr[2] != E.total_slots || hdr[3] != E.total_cells || hdr[4] != E.cell_cap ||
+        hdr[5] != (int)sizeof(RepState))
+        return bad("written by an engine with other replicas, capacities or cells");
+    std::vector<CkptRep> reps((size_t)E.R);
+    for (int r = 0; r < E.R; ++r) {
+        if (fread(&reps[r], sizeof(CkptRep), 1, f) != 1) return bad("truncated replica table");
+        const RepDesc& D = E.desc[r];
+        const CkptRep& c = reps[r];
+        if (c.cap != D.cap || c.slot_off != D.slot_off || c.ncell[0] != D.ncell[0] || c.ncell[1] != D.ncell[1] ||
+            c.ncell[2] != D.ncell[2] || c.mesh[0] != D.mesh[0] || c.mesh[1] != D.mesh[1] || c.mesh[2] != D.mesh[2])
+            return bad("replica " + std::to_string(r) + " differs from this engine's");
+    }
+    const DevPtrs& d = E.d;
+    const size_t N = (size_t)E.total_slots, C = (size_t)E.total_cells;
+    std::vector<unsigned char> buf;
+    const bool ok = ck_read_dev(f, d.posq, N, buf) && ck_read_dev(f, d.type, N, buf) && ck_read_dev(f, d.flags, N, buf) &&
+                    ck_read_dev(f, d.bonds, N, buf) && ck_read_dev(f, d.cell_of, N, buf) && ck_read_dev(f, d.cell_pos, N, buf) &&
+                    ck_read_dev(f, d.mobile, N, buf) && ck_read_dev(f, d.mobile_pos, N, buf) && ck_read_dev(f, d.anions, N, buf) &&
+                    ck_read_dev(f, d.anion_pos, N, buf) && ck_read_dev(f, d.cations, N, buf) &&
+                    ck_read_dev(f, d.cation_pos, N, buf) && ck_read_dev(f, d.freel, N, buf) && ck_read_dev(f, d.titr, N, buf) &&
+                    ck_read_dev(f, d.cell_count, C, buf) && ck_read_dev(f, d.cell_list, C * E.cell_cap, buf) &&
+                    ck_read_dev(f, d.cell_cls, C, buf) && ck_read_dev(f, d.state, (size_t)E.R, buf) &&
+                    (!E.use_r2c || ck_read_dev(f, d.qband, (size_t)E.total_qband, buf));
+    fclose(f);
+    if (!ok) return fail(PHMC_ERR_IO, std::string("phmc_checkpoint_load: truncated file or device copy (") + path +
+                                          "); the engine's state is undefined until the next phmc_set_state");
+    // move mix and tuning as they were
+    for (int r = 0; r < E.R; ++r) {
+        E.desc[r].p_disp = reps[r].p_disp; E.desc[r].p_titr = reps[r].p_titr; E.desc[r].p_swap = reps[r].p_swap;
+    }
+    CU(cudaMemcpy(E.d.desc, E.desc.data(), sizeof(RepDesc) * E.R, cudaMemcpyHostToDevice));
+    if (hdr[6] != E.pend_max || threads != E.threads) {
+        const int s = apply_tuning(h, hdr[6], threads);
+        if (s) return s;
+    }
+    E.quorum = quorum;
+    drop_graph(h);
+    // potential from the restored charge mesh (the full-complex path spreads it from the
+    // positions); the restored tracked energies stay
+    CU(cudaMemsetAsync(E.d.dirty, 0, sizeof(int) * E.R, E.stream));
+    if (E.coulomb == PHMC_COUL_EWALD) {
+        if (!E.use_r2c) launch_spread(E, nullptr, E.stream);
+        launch_fft_pipeline(E, nullptr, 1, E.stream);
+        CU(cudaGetLastError());
+    }
+    return check_kernel_errors(h);
+}

@@ -109,6 +109,14 @@ class Engine:
     def set_tuning(self, pending_max, threads):
         _abi.check(self._lib.phmc_set_tuning(self._h, int(pending_max), int(threads)))
 
+    def checkpoint_save(self, path):
+        """Everything the chains' continuation depends on, for an exact resume (not the surrogate)."""
+        _abi.check(self._lib.phmc_checkpoint_save(self._h, str(path).encode()))
+
+    def checkpoint_load(self, path):
+        """Restore a checkpoint written by an engine of the same systems and parameters."""
+        _abi.check(self._lib.phmc_checkpoint_load(self._h, str(path).encode()))
+
     def set_quorum(self, quorum):
         """MC launch quorum (0, 1]: a launch ends once that fraction of its running replicas is blocked."""
         _abi.check(self._lib.phmc_set_quorum(self._h, float(quorum)))
