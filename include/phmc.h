@@ -234,6 +234,46 @@ int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_
  * of the reciprocal-space dE. */
 int phmc_set_quorum(phmc_engine* e, double quorum);
 
+/* ---- input files of the reference's driver (host side, no device use) ----
+ * LAMMPS "full" data files: phmc_lammps_header reads the header (counts, box
+ * lengths), phmc_lammps_read the Atoms and Bonds sections into caller arrays in
+ * file order (bond atoms as 0-based indices; bonds naming unknown atom ids are
+ * dropped; wrap != 0 wraps positions into [0, L)), with the reference reader's
+ * section rules and number conversions (MC/src/io.cpp:79-146, wrap :303-316), so
+ * the values are bit-identical to the reference's.  phmc_lammps_write writes a
+ * file (box from 0; FP32 values with 9 significant digits) that both readers read
+ * back to the same arrays (replaces write_lammps_full, MC/src/io.cpp:326-368). */
+typedef struct phmc_lammps_info {
+    int natoms, nbonds, nbonds_read, ntypes;
+    double box[3];
+} phmc_lammps_info;
+int phmc_lammps_header(const char* path, phmc_lammps_info* out);
+int phmc_lammps_read(const char* path, int wrap, int cap_atoms, int cap_bonds, int* id, int* mol, int* type,
+                     float* q, float* x, float* y, float* z, int* bond_type, int* bond_i, int* bond_j,
+                     phmc_lammps_info* info);
+int phmc_lammps_write(const char* path, int natoms, const int* id, const int* mol, const int* type, const float* q,
+                      const float* x, const float* y, const float* z, int nbonds, const int* bond_type,
+                      const int* bond_i, const int* bond_j, int ntypes, const double* box);
+/* params.in (replaces read_params, MC/src/io.cpp:171-301): the reference's keys with
+ * its defaults, derived values (Ewald alpha from ewald_rtol, the LJ shift table at
+ * rc) and checks, values rounded to FP32 as the reference holds them; lj_eps /
+ * lj_sig / lj_shift_tbl hold ntypes x ntypes.  Superset: the native model's keys
+ * pH, pKa, salt_conc, wall_lo, wall_hi, fene_k, fene_r0, p_disp, p_titr, p_swap,
+ * disp_max (NaN when absent) and pme_mesh = nx ny nz (0 when absent), which the
+ * reference ignores.  Unknown entries are listed comma-separated in `unknown`;
+ * with strict != 0 they are an error (PHMC_ERR_IO) instead of being ignored. */
+typedef struct phmc_file_params {
+    double rc, epsilon_r, ewald_rtol, ewald_alpha, pme_spacing, pme_3dc_zfac, beta, target_pct, w_z_extra_nm,
+        mu_eta, nacc_frac_round;
+    int lj_shift, coulomb /* PHMC_COUL_CUT, PHMC_COUL_EWALD, -1 unknown */, pme_order, pme_3dc, nh_n_type,
+        nh_p_type, w_type, cl_type, rng_seed, energy_interval, patience, max_attempts, direct_pct_threshold,
+        gc_block_fixed, epoch_attempt_max, phase2_wc;
+    double pH, pKa, salt_conc, wall_lo, wall_hi, fene_k, fene_r0, p_disp, p_titr, p_swap, disp_max;
+    int mesh[3];
+} phmc_file_params;
+int phmc_params_read(const char* path, int ntypes, int strict, phmc_file_params* p, double* lj_eps, double* lj_sig,
+                     double* lj_shift_tbl, char* unknown, int unknown_len);
+
 /* ---- checkpoint / exact resume (no counterpart in the reference: its LAMMPS data
  * output, MC/src/io.cpp:326-368, keeps positions and identities but not the chain's
  * random-number counter, list order or tracked energies) ----

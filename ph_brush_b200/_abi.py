@@ -49,6 +49,25 @@ class Params(C.Structure):
                 ("cell_cap", C.c_int), ("pending_max", C.c_int), ("threads", C.c_int)]
 
 
+class LammpsInfo(C.Structure):
+    _fields_ = [("natoms", C.c_int), ("nbonds", C.c_int), ("nbonds_read", C.c_int), ("ntypes", C.c_int),
+                ("box", C.c_double * 3)]
+
+
+FILE_PARAMS_D1 = ("rc", "epsilon_r", "ewald_rtol", "ewald_alpha", "pme_spacing", "pme_3dc_zfac", "beta", "target_pct",
+                  "w_z_extra_nm", "mu_eta", "nacc_frac_round")
+FILE_PARAMS_I = ("lj_shift", "coulomb", "pme_order", "pme_3dc", "nh_n_type", "nh_p_type", "w_type", "cl_type", "rng_seed",
+                 "energy_interval", "patience", "max_attempts", "direct_pct_threshold", "gc_block_fixed",
+                 "epoch_attempt_max", "phase2_wc")
+FILE_PARAMS_D2 = ("pH", "pKa", "salt_conc", "wall_lo", "wall_hi", "fene_k", "fene_r0", "p_disp", "p_titr", "p_swap",
+                  "disp_max")
+
+
+class FileParams(C.Structure):
+    _fields_ = ([(k, C.c_double) for k in FILE_PARAMS_D1] + [(k, C.c_int) for k in FILE_PARAMS_I] +
+                [(k, C.c_double) for k in FILE_PARAMS_D2] + [("mesh", C.c_int * 3)])
+
+
 class EnergyComponents(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("lj", "fene", "coul_real", "coul_recip", "self", "qcorr", "slab", "total")]
 
@@ -106,7 +125,7 @@ class BrushSpec(C.Structure):
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
-           "phmc_set_state", "phmc_set_quorum", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
+           "phmc_set_state", "phmc_set_quorum", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
            "phmc_recip_energy_static",
            "phmc_surrogate_create", "phmc_surrogate_destroy", "phmc_surrogate_num_params",
            "phmc_surrogate_get_params", "phmc_surrogate_set_params", "phmc_surrogate_set_scaling",
@@ -141,6 +160,10 @@ def load_library(path=LIB_PATH):
         "phmc_build_brush": ([C.POINTER(BrushSpec), C.c_int, _fp, _fp, _fp, _fp, _ip, _ip, C.c_int, _ip, _ip, _ip, _dp], C.c_int),
         "phmc_set_state": ([eng, C.c_int, _fp, _fp, _fp, _fp, _ip, _ip], C.c_int),
         "phmc_set_profiling": ([eng, C.c_int], C.c_int),
+        "phmc_lammps_header": ([C.c_char_p, C.POINTER(LammpsInfo)], C.c_int),
+        "phmc_lammps_read": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(LammpsInfo)], C.c_int),
+        "phmc_lammps_write": ([C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_double)], C.c_int),
+        "phmc_params_read": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(FileParams), C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_char_p, C.c_int], C.c_int),
         "phmc_checkpoint_save": ([eng, C.c_char_p], C.c_int),
         "phmc_checkpoint_load": ([eng, C.c_char_p], C.c_int),
         "phmc_set_quorum": ([eng, C.c_double], C.c_int),
