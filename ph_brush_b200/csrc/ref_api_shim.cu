@@ -14,15 +14,19 @@
 // One engine mirrors the atoms: each energy call finds the changed atoms with a
 // device comparison against the engine's committed state; up to two changed atoms
 // are evaluated as one trial against that state (one MC-kernel launch, no mesh
-// rebuild); more changes, or moved atoms, are uploaded as a new state (full
-// recompute).  The model is the reference's: LJ cut and shifted at rc, 1-2 bonded
+// rebuild); up to SHIM_MAX_CHANGES identity changes (the four-atom swaps of the
+// reference's phase 2, a rejected swap's revert plus the next one) are committed
+// pair by pair until two remain, which are then evaluated; moved atoms or more
+// changes are uploaded as a new state (full recompute).  The model is the reference's: LJ cut and shifted at rc, 1-2 bonded
 // pairs excluded from LJ and Coulomb, cubic-or-higher SPME with the reference's
 // moduli and mesh rule, slab correction when pme_3dc is on.
 #include <cuda_runtime.h>
 #include <thrust/copy.h>
 #include <thrust/device_vector.h>
 #include <thrust/host_vector.h>
+#include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -79,6 +83,24 @@ __global__ void k_shim_diff(int n, const T* __restrict__ x, const T* __restrict_
     }
 }
 
+#define SHIM_MAX_CHANGES 16
+// the changed atoms' identities and positions, gathered for one copy to the host
+struct ShimDiff {
+    int cnt[2];
+    int idx[SHIM_MAX_CHANGES];
+    float q[SHIM_MAX_CHANGES], x[SHIM_MAX_CHANGES], y[SHIM_MAX_CHANGES], z[SHIM_MAX_CHANGES];
+    int t[SHIM_MAX_CHANGES];
+};
+template <typename T>
+__global__ void k_shim_gather(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
+                              const T* __restrict__ q, const int* __restrict__ t, ShimDiff* __restrict__ out) {
+    const int k = threadIdx.x;
+    if (k >= min(out->cnt[0], SHIM_MAX_CHANGES)) return;
+    const int i = out->idx[k];
+    out->q[k] = (float)q[i]; out->t[k] = t[i];
+    out->x[k] = (float)x[i]; out->y[k] = (float)y[i]; out->z[k] = (float)z[i];
+}
+
 template <typename T>
 __global__ void k_shim_mirror(int n, const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
                               const T* __restrict__ q, const int* __restrict__ t, float* mx, float* my, float* mz,
@@ -123,8 +145,7 @@ struct Shim {
     // device mirror of the committed state
     float *mx = nullptr, *my = nullptr, *mz = nullptr, *mq = nullptr;
     int* mt = nullptr;
-    int* d_idx = nullptr;
-    int* d_cnt = nullptr;
+    ShimDiff* d_diff = nullptr;
     phmc_energy_components base{};
     // the last evaluated difference (reused by the next energy call when unchanged)
     int last_n = -1;
@@ -137,7 +158,7 @@ Shim g;
 
 void release() {
     if (g.eng) phmc_destroy(g.eng);
-    for (void* p : {(void*)g.mx, (void*)g.my, (void*)g.mz, (void*)g.mq, (void*)g.mt, (void*)g.d_idx, (void*)g.d_cnt})
+    for (void* p : {(void*)g.mx, (void*)g.my, (void*)g.mz, (void*)g.mq, (void*)g.mt, (void*)g.d_diff})
         if (p) cudaFree(p);
     const bool pme = g.pme;
     const int mesh[3] = {g.mesh[0], g.mesh[1], g.mesh[2]};
@@ -219,8 +240,7 @@ void ensure_engine(const DeviceAtoms& a, const DeviceParams& dp, const Box& box)
     cu(cudaMalloc((void**)&g.mz, sizeof(float) * g.n), "cudaMalloc");
     cu(cudaMalloc((void**)&g.mq, sizeof(float) * g.n), "cudaMalloc");
     cu(cudaMalloc((void**)&g.mt, sizeof(int) * g.n), "cudaMalloc");
-    cu(cudaMalloc((void**)&g.d_idx, sizeof(int) * 2), "cudaMalloc");
-    cu(cudaMalloc((void**)&g.d_cnt, sizeof(int) * 2), "cudaMalloc");
+    cu(cudaMalloc((void**)&g.d_diff, sizeof(ShimDiff)), "cudaMalloc");
     mirror(a);
     g.cur = g.base;
     g.last_n = 0;
@@ -230,52 +250,77 @@ void ensure_engine(const DeviceAtoms& a, const DeviceParams& dp, const Box& box)
 const phmc_energy_components& evaluate(const DeviceAtoms& a, const DeviceParams& dp, const Box& box) {
     ensure_engine(a, dp, box);
     if ((int)a.x.size() != g.n) throw std::runtime_error("phmc shim: the number of atoms changed");
-    cu(cudaMemset(g.d_cnt, 0, sizeof(int) * 2), "cudaMemset");
-    k_shim_diff<real><<<(g.n + 255) / 256, 256>>>(g.n, thrust::raw_pointer_cast(a.x.data()), thrust::raw_pointer_cast(a.y.data()),
-                                                  thrust::raw_pointer_cast(a.z.data()), thrust::raw_pointer_cast(a.q.data()),
-                                                  thrust::raw_pointer_cast(a.type.data()), g.mx, g.my, g.mz, g.mq, g.mt,
-                                                  g.d_idx, g.d_cnt, 2);
-    int cnt[2] = {0, 0};
-    cu(cudaMemcpy(cnt, g.d_cnt, sizeof cnt, cudaMemcpyDeviceToHost), "shim diff");
-    if (cnt[0] == 0) {
+    cu(cudaMemset(g.d_diff, 0, sizeof(int) * 2), "cudaMemset");
+    const real *ax = thrust::raw_pointer_cast(a.x.data()), *ay = thrust::raw_pointer_cast(a.y.data()),
+               *az = thrust::raw_pointer_cast(a.z.data()), *aq = thrust::raw_pointer_cast(a.q.data());
+    const int* at = thrust::raw_pointer_cast(a.type.data());
+    char* dd = reinterpret_cast<char*>(g.d_diff);
+    k_shim_diff<real><<<(g.n + 255) / 256, 256>>>(g.n, ax, ay, az, aq, at, g.mx, g.my, g.mz, g.mq, g.mt,
+                                                  reinterpret_cast<int*>(dd + offsetof(ShimDiff, idx)),
+                                                  reinterpret_cast<int*>(dd + offsetof(ShimDiff, cnt)), SHIM_MAX_CHANGES);
+    k_shim_gather<real><<<1, SHIM_MAX_CHANGES>>>(ax, ay, az, aq, at, g.d_diff);
+    ShimDiff df;
+    cu(cudaMemcpy(&df, g.d_diff, sizeof df, cudaMemcpyDeviceToHost), "shim diff");
+    const int nch = df.cnt[0];
+    if (nch == 0) {
         g.last_n = 0;
         g.cur = g.base;
         return g.cur;
     }
-    if (cnt[0] <= 2 && !cnt[1]) {
-        int idx[2] = {-1, -1};
-        cu(cudaMemcpy(idx, g.d_idx, sizeof(int) * cnt[0], cudaMemcpyDeviceToHost), "shim diff");
-        if (cnt[0] == 2 && idx[0] > idx[1]) std::swap(idx[0], idx[1]);
-        real qv[2] = {0, 0};
-        int tv[2] = {0, 0};
-        for (int k = 0; k < cnt[0]; ++k) {
-            cu(cudaMemcpy(&qv[k], thrust::raw_pointer_cast(a.q.data()) + idx[k], sizeof(real), cudaMemcpyDeviceToHost), "shim q");
-            cu(cudaMemcpy(&tv[k], thrust::raw_pointer_cast(a.type.data()) + idx[k], sizeof(int), cudaMemcpyDeviceToHost), "shim type");
+    if (!df.cnt[1] && nch <= SHIM_MAX_CHANGES) {
+        // changes in ascending atom order
+        int ord[SHIM_MAX_CHANGES];
+        for (int k = 0; k < nch; ++k) ord[k] = k;
+        std::sort(ord, ord + nch, [&](int u, int v) { return df.idx[u] < df.idx[v]; });
+        auto change = [&](phmc_trial& tr, int slot, int k) {
+            tr.c[slot].index = df.idx[k]; tr.c[slot].present = 1;
+            tr.c[slot].x = df.x[k]; tr.c[slot].y = df.y[k]; tr.c[slot].z = df.z[k];
+            tr.c[slot].q = df.q[k]; tr.c[slot].type = df.t[k];
+        };
+        auto add = [](phmc_energy_components& e, const phmc_energy_components& d) {
+            e.lj += d.lj; e.fene += d.fene; e.coul_real += d.coul_real; e.coul_recip += d.coul_recip;
+            e.self += d.self; e.qcorr += d.qcorr; e.slab += d.slab; e.total += d.total;
+        };
+        // commit while more than two changes remain (ones or twos, so that two are left)
+        int k0 = 0;
+        while (nch - k0 > 2) {
+            const int m = std::min(2, nch - k0 - 2);
+            phmc_trial tr;
+            std::memset(&tr, 0, sizeof tr);
+            tr.n_changes = m;
+            for (int j = 0; j < m; ++j) change(tr, j, ord[k0 + j]);
+            phmc_energy_components d;
+            ck(phmc_delta_energy_components(g.eng, 0, &tr, 1, &d), "phmc_delta_energy_components");
+            ck(phmc_commit(g.eng, 0, &tr), "phmc_commit");
+            add(g.base, d);
+            for (int j = 0; j < m; ++j) {  // the mirror follows the committed state
+                const int k = ord[k0 + j], i = df.idx[k];
+                cu(cudaMemcpy(g.mq + i, &df.q[k], sizeof(float), cudaMemcpyHostToDevice), "shim mirror q");
+                cu(cudaMemcpy(g.mt + i, &df.t[k], sizeof(int), cudaMemcpyHostToDevice), "shim mirror type");
+            }
+            g.last_n = -1;
+            k0 += m;
         }
-        bool same = g.last_n == cnt[0];
-        for (int k = 0; k < cnt[0] && same; ++k)
-            same = g.last_idx[k] == idx[k] && g.last_q[k] == (float)qv[k] && g.last_t[k] == tv[k];
+        const int rem = nch - k0;
+        bool same = g.last_n == rem;
+        for (int j = 0; j < rem && same; ++j) {
+            const int k = ord[k0 + j];
+            same = g.last_idx[j] == df.idx[k] && g.last_q[j] == df.q[k] && g.last_t[j] == df.t[k];
+        }
         if (same) return g.cur;
         phmc_trial tr;
         std::memset(&tr, 0, sizeof tr);
-        tr.n_changes = cnt[0];
-        for (int k = 0; k < cnt[0]; ++k) {
-            float pos[3];
-            cu(cudaMemcpy(&pos[0], g.mx + idx[k], sizeof(float), cudaMemcpyDeviceToHost), "shim x");
-            cu(cudaMemcpy(&pos[1], g.my + idx[k], sizeof(float), cudaMemcpyDeviceToHost), "shim y");
-            cu(cudaMemcpy(&pos[2], g.mz + idx[k], sizeof(float), cudaMemcpyDeviceToHost), "shim z");
-            tr.c[k].index = idx[k]; tr.c[k].present = 1;
-            tr.c[k].x = pos[0]; tr.c[k].y = pos[1]; tr.c[k].z = pos[2];
-            tr.c[k].q = (float)qv[k]; tr.c[k].type = tv[k];
-        }
+        tr.n_changes = rem;
+        for (int j = 0; j < rem; ++j) change(tr, j, ord[k0 + j]);
         phmc_energy_components d;
         ck(phmc_delta_energy_components(g.eng, 0, &tr, 1, &d), "phmc_delta_energy_components");
-        g.cur.lj = g.base.lj + d.lj; g.cur.fene = g.base.fene + d.fene;
-        g.cur.coul_real = g.base.coul_real + d.coul_real; g.cur.coul_recip = g.base.coul_recip + d.coul_recip;
-        g.cur.self = g.base.self + d.self; g.cur.qcorr = g.base.qcorr + d.qcorr; g.cur.slab = g.base.slab + d.slab;
-        g.cur.total = g.base.total + d.total;
-        g.last_n = cnt[0];
-        for (int k = 0; k < cnt[0]; ++k) { g.last_idx[k] = idx[k]; g.last_q[k] = (float)qv[k]; g.last_t[k] = tv[k]; }
+        g.cur = g.base;
+        add(g.cur, d);
+        g.last_n = rem;
+        for (int j = 0; j < rem; ++j) {
+            const int k = ord[k0 + j];
+            g.last_idx[j] = df.idx[k]; g.last_q[j] = df.q[k]; g.last_t[j] = df.t[k];
+        }
         return g.cur;
     }
     // more changes (or moved atoms): the current atoms become the committed state
