@@ -471,6 +471,9 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         std::vector<int> zoff;
         // register z pass when every replica has the same supported nz
         E.zreg = E.use_r2c ? zreg_variant(E.desc[0].mesh[2]) : 0;
+        E.plane_reg = E.use_r2c;
+        for (int r = 0; r < R && E.plane_reg; ++r)
+            if (!plane_reg_supported(E.desc[r].mesh[0], E.desc[r].mesh[1])) E.plane_reg = false;
         for (int r = 1; r < R && E.zreg; ++r)
             if (E.desc[r].mesh[2] != E.desc[0].mesh[2]) E.zreg = 0;
         for (int r = 0; r < R; ++r) {
@@ -496,8 +499,9 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                 // band spread: the 64-bit charge plane + cell counts; first pass: two complex buffers
                 E.band_spread_smem = std::max(E.band_spread_smem, (size_t)D.mesh[0] * D.mesh[1] * sizeof(unsigned long long) +
                                                                       (ncell + 1) * sizeof(int));
-                E.rb_fwd_smem = std::max(E.rb_fwd_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2));
-                E.rb_inv_smem = std::max(E.rb_inv_smem, (size_t)2 * nxh * D.mesh[1] * sizeof(float2));
+                const size_t plane_smem = E.plane_reg ? plane_reg_smem(D.mesh[0]) : (size_t)2 * nxh * D.mesh[1] * sizeof(float2);
+                E.rb_fwd_smem = std::max(E.rb_fwd_smem, plane_smem);
+                E.rb_inv_smem = std::max(E.rb_inv_smem, plane_smem);
             } else {
                 for (int y = 0; y < D.mesh[1]; ++y)
                     for (int x0 = 0; x0 < D.mesh[0]; x0 += ZPASS_TX) zj.push_back(make_int4(r, y, x0, 0));

@@ -37,6 +37,7 @@ struct Engine {
     size_t rb_fwd_smem = 0, rb_inv_smem = 0, band_spread_smem = 0;
     long long total_qband = 0;   // points of the wall bands' fixed-point charge meshes
     int zreg = 0;                // register z-pass variant for the shared nz (0: shared-memory z pass)
+    bool plane_reg = false;      // register first / last passes (every replica's lateral mesh square and supported)
     int flush_kernels = 0;       // kernels per potential-mesh rebuild
     bool unit_pending = false;   // next rebuild places a unit charge instead of the particles
     long long total_meshh = 0;
@@ -70,6 +71,8 @@ cudaError_t rebuild_set_smem_limits(Engine& E);
 void launch_band_spread(Engine& E, cudaStream_t st);
 int zreg_variant(int nz);      // register z-pass variant for nz, 0 if none
 size_t zreg_smem(int nz);
+bool plane_reg_supported(int nx, int ny);
+size_t plane_reg_smem(int n);
 
 // k_pair.cu
 void launch_cell_build(Engine& E, cudaStream_t st);

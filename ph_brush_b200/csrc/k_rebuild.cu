@@ -386,12 +386,205 @@ __global__ void __launch_bounds__(NT) k_rb_inv(DevPtrs d, const int2* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// First and last passes with register-resident DFTs, for square lateral meshes
+// n = nx = ny in the PLANE_LIST set (one block per (replica, z) plane, the
+// replica's n picked at run time).  x: one thread per row, the row's n/2 packed
+// complex values in registers (a row stride of odd length in float2 keeps the
+// rows' shared-memory accesses free of bank conflicts); y: n = N1 * N2 in two
+// register stages over the n/2 + 1 columns.  Shared memory is passed once per
+// stage instead of once per radix stage.
+// ---------------------------------------------------------------------------
+#define PLANE_LIST(X) X(16, 4, 4) X(32, 8, 4) X(36, 6, 6) X(48, 8, 6) X(54, 9, 6) X(64, 8, 8)
+constexpr int plane_ms(int m) { return (m % 2 == 0) ? m + 1 : m + 2; }  // odd row stride (float2)
+constexpr int PLANE_NT = 128;
+
+template <int N, int N1, int N2, int NT>
+__device__ void plane_fwd(const DevPtrs& d, const RepDesc& D, int z, int unit_charge, float2* sa, float2* sb) {
+    constexpr int M = N / 2, NXH = M + 1, MS = plane_ms(M);
+    static_assert(N1 * N2 == N, "y split");
+    const int tid = threadIdx.x;
+    float2* xa = sa;  // [y][j] packed real pairs, row stride MS; later the y stage-A output [k1 N2 + n2][k]
+    float2* xb = sb;  // [y][k] after the split, row stride NXH
+    if (unit_charge) {  // a unit charge on mesh point 0 (the influence kernel's source)
+        for (int i = tid; i < N * M; i += NT) {
+            const int y = i / M, j = i - y * M;
+            xa[y * MS + j] = make_float2((z == 0 && i == 0) ? 1.0f : 0.0f, 0.0f);
+        }
+    } else {
+        int zrel = z - D.zb_lo;
+        zrel += (zrel < 0) ? D.mesh[2] : 0;
+        const ulonglong2* q = reinterpret_cast<const ulonglong2*>(d.qband + D.qb_off + (size_t)zrel * N * N);
+        for (int i = tid; i < N * M; i += NT) {
+            const int y = i / M, j = i - y * M;
+            const ulonglong2 v = q[i];
+            xa[y * MS + j] = make_float2((float)((double)(long long)v.x * PHMC_FIX_INV), (float)((double)(long long)v.y * PHMC_FIX_INV));
+        }
+    }
+    __syncthreads();
+    for (int y = tid; y < N; y += NT) {  // x: length-M DFT of the packed pairs of row y
+        float2 v[M];
+#pragma unroll
+        for (int j = 0; j < M; ++j) v[j] = xa[y * MS + j];
+        rfft::rdft<M, -1>(v);
+#pragma unroll
+        for (int j = 0; j < M; ++j) xa[y * MS + j] = v[j];
+    }
+    __syncthreads();
+    const float2* twn = d.twiddle + D.tw_off[0];  // exp(-2 pi i k / nx)
+    // split: X_k = 1/2 (Z_k + conj Z_{M-k}) - i/2 W^k (Z_k - conj Z_{M-k}), k = 0..M
+    for (int i = tid; i < N * NXH; i += NT) {
+        const int y = i / NXH, k = i - y * NXH;
+        const float2 zk = xa[y * MS + (k == M ? 0 : k)];
+        float2 zc = xa[y * MS + (k == 0 ? 0 : M - k)];
+        zc.y = -zc.y;
+        const float2 w = twn[k];
+        const float2 s = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+        const float2 df = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
+        const float2 wd = cmul(w, df);
+        xb[y * NXH + k] = make_float2(s.x + wd.y, s.y - wd.x);
+    }
+    __syncthreads();
+    const float2* twy = d.twiddle + D.tw_off[1];  // exp(-2 pi i j / ny)
+    for (int it = tid; it < N2 * NXH; it += NT) {  // y stage A: DFT over n1 of rows N2 n1 + n2, times W^(n2 k1)
+        const int n2 = it / NXH, k = it - n2 * NXH;
+        float2 v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = xb[(N2 * n1 + n2) * NXH + k];
+        rfft::rdft<N1, -1>(v);
+        xa[n2 * NXH + k] = v[0];
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1) xa[(k1 * N2 + n2) * NXH + k] = cmul(v[k1], twy[n2 * k1]);
+    }
+    __syncthreads();
+    float2* c = d.cmesh + D.meshh_off + (size_t)z * N * NXH;
+    for (int it = tid; it < N1 * NXH; it += NT) {  // y stage B: DFT over n2 gives row ky = k1 + N1 k2
+        const int k1 = it / NXH, k = it - k1 * NXH;
+        float2 u[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) u[n2] = xa[(k1 * N2 + n2) * NXH + k];
+        rfft::rdft<N2, -1>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) c[(k1 + N1 * k2) * NXH + k] = u[k2];
+    }
+}
+
+template <int N, int N1, int N2, int NT>
+__device__ void plane_inv(const DevPtrs& d, const RepDesc& D, int z, float2* sa, float2* sb) {
+    constexpr int M = N / 2, NXH = M + 1, MS = plane_ms(M);
+    const int tid = threadIdx.x;
+    float2* xa = sa;
+    float2* xb = sb;
+    const float2* c = d.cmesh + D.meshh_off + (size_t)z * N * NXH;
+    const float2* twy = d.twiddle + D.tw_off[1];
+    for (int it = tid; it < N1 * NXH; it += NT) {  // inverse y stage B: over k2, then W^(-n2 k1)
+        const int k1 = it / NXH, k = it - k1 * NXH;
+        float2 u[N2];
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) u[k2] = c[(k1 + N1 * k2) * NXH + k];
+        rfft::rdft<N2, 1>(u);
+        xa[k1 * N2 * NXH + k] = u[0];
+#pragma unroll
+        for (int n2 = 1; n2 < N2; ++n2) {
+            float2 w = twy[n2 * k1];
+            w.y = -w.y;
+            xa[(k1 * N2 + n2) * NXH + k] = cmul(u[n2], w);
+        }
+    }
+    __syncthreads();
+    for (int it = tid; it < N2 * NXH; it += NT) {  // inverse y stage A: over k1 gives row N2 n1 + n2
+        const int n2 = it / NXH, k = it - n2 * NXH;
+        float2 v[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) v[k1] = xa[(k1 * N2 + n2) * NXH + k];
+        rfft::rdft<N1, 1>(v);
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) xb[(N2 * n1 + n2) * NXH + k] = v[n1];
+    }
+    __syncthreads();
+    const float2* twn = d.twiddle + D.tw_off[0];
+    // merge: Z'_k = (X_k + conj X_{M-k}) + i W^{-k} (X_k - conj X_{M-k}), k = 0..M-1
+    for (int i = tid; i < N * M; i += NT) {
+        const int y = i / M, k = i - y * M;
+        const float2 A = xb[y * NXH + k];
+        float2 B = xb[y * NXH + (M - k)];
+        B.y = -B.y;
+        float2 w = twn[k];
+        w.y = -w.y;
+        const float2 s = make_float2(A.x + B.x, A.y + B.y);
+        const float2 wd = cmul(w, make_float2(A.x - B.x, A.y - B.y));
+        xa[y * MS + k] = make_float2(s.x - wd.y, s.y + wd.x);
+    }
+    __syncthreads();
+    for (int y = tid; y < N; y += NT) {  // inverse x: length-M DFT of row y's packed pairs
+        float2 v[M];
+#pragma unroll
+        for (int j = 0; j < M; ++j) v[j] = xa[y * MS + j];
+        rfft::rdft<M, 1>(v);
+#pragma unroll
+        for (int j = 0; j < M; ++j) xa[y * MS + j] = v[j];
+    }
+    __syncthreads();
+    float2* phi = reinterpret_cast<float2*>(d.phi + D.mesh_off + (size_t)z * N * N);
+    for (int i = tid; i < N * M; i += NT) {  // the real plane: row y, points 2j and 2j + 1
+        const int y = i / M, j = i - y * M;
+        phi[i] = xa[y * MS + j];
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_rb_fwd_reg(DevPtrs d, const int2* __restrict__ jobs, int unit_charge,
+                                                   const int* __restrict__ dirty) {
+    extern __shared__ __align__(16) float2 psm[];
+    const int2 job = jobs[blockIdx.x];
+    const int r = job.x, z = job.y;
+    if (dirty && !dirty[r]) return;
+    const RepDesc& D = d.desc[r];
+    const int n = D.mesh[0];
+    float2* sa = psm;
+    float2* sb = psm + n * plane_ms(n / 2);
+    switch (n) {
+#define PLANE_FWD(nn, a, b) case nn: plane_fwd<nn, a, b, NT>(d, D, z, unit_charge, sa, sb); break;
+        PLANE_LIST(PLANE_FWD)
+#undef PLANE_FWD
+        default: break;
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_rb_inv_reg(DevPtrs d, const int2* __restrict__ jobs, const int* __restrict__ dirty) {
+    extern __shared__ __align__(16) float2 psm[];
+    const int2 job = jobs[blockIdx.x];
+    const int r = job.x, z = job.y;
+    if (dirty && !dirty[r]) return;
+    const RepDesc& D = d.desc[r];
+    const int n = D.mesh[0];
+    float2* sa = psm;
+    float2* sb = psm + n * plane_ms(n / 2);
+    switch (n) {
+#define PLANE_INV(nn, a, b) case nn: plane_inv<nn, a, b, NT>(d, D, z, sa, sb); break;
+        PLANE_LIST(PLANE_INV)
+#undef PLANE_INV
+        default: break;
+    }
+}
+
+bool plane_reg_supported(int nx, int ny) {
+    if (nx != ny) return false;
+#define PLANE_OK(nn, a, b) if (nx == nn) return true;
+    PLANE_LIST(PLANE_OK)
+#undef PLANE_OK
+    return false;
+}
+size_t plane_reg_smem(int n) { return ((size_t)n * plane_ms(n / 2) + (size_t)n * (n / 2 + 1)) * sizeof(float2); }
+
 // The unit-charge rebuild (influence kernel) computes every plane; a rebuild of the
 // particles' mesh only the planes of each replica's wall band.
 void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st) {
     const int2* pj = unit_charge ? E.d_plane_jobs : E.d_band_jobs;
     const int npj = unit_charge ? E.n_plane_jobs : E.n_band_jobs;
-    k_rb_fwd<256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty);
+    if (E.plane_reg) k_rb_fwd_reg<PLANE_NT><<<npj, PLANE_NT, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty);
+    else k_rb_fwd<256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty);
     switch (E.zreg) {
 #define ZREG_LAUNCH(id, n, a, b) \
         case id: k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX><<<E.n_zjobs, ZREG_NT(b), E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty, unit_charge); break;
@@ -399,7 +592,8 @@ void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream
 #undef ZREG_LAUNCH
         default: k_rb_zpass<256, ZPASS_TX><<<E.n_zjobs, 256, E.zpass_smem, st>>>(E.d, E.d_zjobs, E.d_epart, dirty, unit_charge);
     }
-    k_rb_inv<256><<<npj, 256, E.rb_inv_smem, st>>>(E.d, pj, dirty);
+    if (E.plane_reg) k_rb_inv_reg<PLANE_NT><<<npj, PLANE_NT, E.rb_inv_smem, st>>>(E.d, pj, dirty);
+    else k_rb_inv<256><<<npj, 256, E.rb_inv_smem, st>>>(E.d, pj, dirty);
 }
 
 // Charge mesh of every replica's wall band from scratch (full recompute).
@@ -432,7 +626,7 @@ cudaError_t rebuild_set_smem_limits(Engine& E) {
         default: e = raise_cap(k_band_spread<6, 256>, E.device, E.band_spread_smem); break;
     }
     if (e != cudaSuccess) return e;
-    e = raise_cap(k_rb_fwd<256>, E.device, E.rb_fwd_smem);
+    e = E.plane_reg ? raise_cap(k_rb_fwd_reg<PLANE_NT>, E.device, E.rb_fwd_smem) : raise_cap(k_rb_fwd<256>, E.device, E.rb_fwd_smem);
     if (e != cudaSuccess) return e;
     switch (E.zreg) {
 #define ZREG_CAP(id, n, a, b) case id: e = raise_cap(k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX>, E.device, E.zpass_smem); break;
@@ -441,5 +635,5 @@ cudaError_t rebuild_set_smem_limits(Engine& E) {
         default: e = raise_cap(k_rb_zpass<256, ZPASS_TX>, E.device, E.zpass_smem);
     }
     if (e != cudaSuccess) return e;
-    return raise_cap(k_rb_inv<256>, E.device, E.rb_inv_smem);
+    return E.plane_reg ? raise_cap(k_rb_inv_reg<PLANE_NT>, E.device, E.rb_inv_smem) : raise_cap(k_rb_inv<256>, E.device, E.rb_inv_smem);
 }
