@@ -174,7 +174,6 @@ def build_headline(args, local, rank):
     from ph_brush_b200 import Engine, Surrogate, configs
     reps = configs.config5(seed=2029 + 7919 * rank, n_rep=args.replicas)
     eng = Engine([s for s, _ in reps], [p for _, p in reps], device=local)
-    tune = tune_engine(eng, args, 400)
     p0 = reps[0][1]
     sur = Surrogate(seed=2029)
     eng.set_move_mix(0.5, 0.5, 0.0)  # titration-heavy harvest
@@ -187,6 +186,8 @@ def build_headline(args, local, rank):
     eng.harvest(0)
     eng.set_move_mix(p0.p_disp, p0.p_titr, p0.p_swap)
     eng.attach_surrogate(sur, threshold=args.da_threshold, window=256)
+    # tuned as the timed steps run: surrogate attached, the step's trials per candidate
+    tune = tune_engine(eng, args, args.trials)
     steps = args.epochs * (n_samples // 4096)
     fl_row = 2.0 * (80 * 128 + 2 * 128 * 128 + 128)  # forward flops per row; backward twice that
     train = {"samples": n_samples, "epochs": args.epochs, "batch": 4096, "lr": 1e-3, "final_loss": loss,
