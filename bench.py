@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline only (plain comparison, phases, alpha skipped)")
     ap.add_argument("--no-alpha", action="store_true")
+    ap.add_argument("--plain-config2-only", action="store_true",
+                    help="only the plain engine on config 2 (one JSON line of its figures; for profiling)")
     ap.add_argument("--alpha-eq", type=int, default=1200, help="sweeps of equilibration in the alpha(pH) check")
     ap.add_argument("--alpha-sample", type=int, default=600, help="sweeps sampled in the alpha(pH) check")
     return ap.parse_args()
@@ -534,6 +536,12 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.plain_config2_only:
+        rank, world, local = dist_env()
+        out, _ = plain_config2(args, local)
+        if rank == 0:
+            print(json.dumps(out))
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

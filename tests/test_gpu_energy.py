@@ -158,3 +158,20 @@ def test_commit_sequence_matches_oracle():
             e.commit(tr)
             cur = after_sys
             assert_components(e.energy()[0], O.energy(cur, p))
+
+
+@pytest.mark.gpu
+def test_register_plane_passes_match_the_oracle_at_every_lateral_size():
+    """The rebuild's first and last passes run in registers for square lateral meshes
+    16, 32, 36, 48, 54 and 64 (one kernel, the replica's size picked at run time):
+    each size alone, and all four of the larger ones batched in one engine, give the
+    oracle's reciprocal energy (and every other component) within the tolerance."""
+    sizes = (36, 48, 54, 64)
+    reps = [configs.small_system(seed=20 + k, mesh=(n, n, 48)) for k, n in enumerate(sizes)]
+    refs = [O.energy(s, p) for s, p in reps]
+    for (s, p), ref in zip(reps, refs):
+        with Engine(s, p) as e:
+            assert_components(e.energy()[0], ref)
+    with Engine([s for s, _ in reps], [p for _, p in reps]) as e:
+        for got, ref in zip(e.energy(), refs):
+            assert_components(got, ref)
