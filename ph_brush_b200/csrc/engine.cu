@@ -449,8 +449,8 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
 
     // ---- mesh ----
     if (ewald) {
-        // even nx everywhere: fused spread + half-spectrum (real-to-complex) rebuild, no global
-        // charge mesh; otherwise the scatter + full-complex path
+        // even nx everywhere: the wall band's fixed-point charge mesh (kept by the MC kernel) +
+        // half-spectrum (real-to-complex) rebuild; otherwise the scatter + full-complex path
         if (E.use_r2c) {
             DALLOC(d.cmesh, E.total_meshh);
             DALLOC(d.qband, E.total_qband);

@@ -33,7 +33,7 @@ struct Engine {
     int* d_zjob_off = nullptr;
     double* d_epart = nullptr;
     size_t plane_smem = 0, zpass_smem = 0;
-    bool use_r2c = false;        // every replica has even nx: fused spread + real-to-complex rebuild
+    bool use_r2c = false;        // every replica has even nx: band charge mesh + real-to-complex rebuild
     size_t rb_fwd_smem = 0, rb_inv_smem = 0, band_spread_smem = 0;
     long long total_qband = 0;   // points of the wall bands' fixed-point charge meshes
     int zreg = 0;                // register z-pass variant for the shared nz (0: shared-memory z pass)
