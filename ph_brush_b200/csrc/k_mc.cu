@@ -464,6 +464,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     __shared__ __align__(8) uint64_t s_mbar[3];  // completion of the staged weight copies
     __shared__ int s_sfail;                      // a staged copy did not arrive in time
     __shared__ float s_mu[SUR_K], s_sd[SUR_K];   // the attached network's input standardisation
+    __shared__ uint16_t s_w4[SUR_HMAX];          // its output weights
     // staged first stage (aliases the pair tables, used before phase 3): activations, weights
     unsigned char* sur_base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(s_pair) + 127) & ~uintptr_t(127));
     __nv_bfloat16* act0 = reinterpret_cast<__nv_bfloat16*>(sur_base);
@@ -501,8 +502,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         sur_mbar_init(&s_mbar[1]);
         sur_mbar_init(&s_mbar[2]);
     }
-    if (d.sur.H > 0)
+    if (d.sur.H > 0) {
         for (int k = tid; k < SUR_K; k += NT) { s_mu[k] = d.sur.mu[k]; s_sd[k] = d.sur.sd[k]; }
+        for (int k = tid; k < d.sur.H; k += NT) s_w4[k] = d.sur.w4[k];
+    }
     unsigned long long t_start = 0;
     if (tid == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
     __syncthreads();
@@ -750,7 +753,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             // (d) network on the rows (tensor cores), first-stage decision
             if (T.da) {
                 sur_forward_staged<NT>(d.sur, T.nrows, act0, act1, wa, wb, wc, s_mbar, sur_par, s_F, &s_sfail,
-                                       d.sur_late_l3 != 0);
+                                       d.sur_late_l3 != 0, s_w4);
                 sur_par ^= 1u;
             }
             if (tid == 0) {

@@ -54,7 +54,7 @@ __device__ __forceinline__ void sur_mma(float* c, const uint32_t* a, uint32_t b0
 __device__ __forceinline__ float sur_out_dot(const __nv_bfloat16* h, const uint16_t* w4, int H, int lane) {
     float v = 0.0f;
     for (int k = lane; k < H; k += 32)
-        v += __bfloat162float(h[k]) * __bfloat162float(__ushort_as_bfloat16(__ldg(&w4[k])));
+        v += __bfloat162float(h[k]) * __bfloat162float(__ushort_as_bfloat16(w4[k]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
@@ -110,7 +110,7 @@ __host__ __device__ inline uint32_t sur_layer_bytes(int K, int H) { return (uint
 template <int NT>
 __device__ bool sur_forward_staged(const SurDev& s, int nrows, __nv_bfloat16* buf0, __nv_bfloat16* buf1, const uint2* wa,
                                    const uint2* wb, const uint2* wc, uint64_t* mbar, uint32_t par, float* out, int* s_fail,
-                                   bool late_l3) {
+                                   bool late_l3, const uint16_t* w4) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
     __nv_bfloat16* in = buf0;
     __nv_bfloat16* ot = buf1;
@@ -122,7 +122,9 @@ __device__ bool sur_forward_staged(const SurDev& s, int nrows, __nv_bfloat16* bu
         if (!ok) *s_fail = 1;
         const int nks = K >> 4;
         for (int cg = warp; cg < (s.H >> 4); cg += NT / 32) {
+            // even and odd k-steps accumulate separately (two independent MMA chains per n-tile)
             float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+            float acc2[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
 #pragma unroll 4
             for (int ks = 0; ks < nks; ++ks) {
                 const __nv_bfloat16* p0 = in + g * SUR_AST + ks * 16 + 2 * t4;
@@ -133,9 +135,18 @@ __device__ bool sur_forward_staged(const SurDev& s, int nrows, __nv_bfloat16* bu
                 a[3] = *reinterpret_cast<const uint32_t*>(p0 + 8 * SUR_AST + 8);
                 const uint2* wp = w + sur_pack_index(cg, ks, 0, lane, nks);
                 const uint2 b0 = wp[0], b1 = wp[32];
-                sur_mma(acc[0], a, b0.x, b0.y);
-                sur_mma(acc[1], a, b1.x, b1.y);
+                if (ks & 1) {
+                    sur_mma(acc2[0], a, b0.x, b0.y);
+                    sur_mma(acc2[1], a, b1.x, b1.y);
+                } else {
+                    sur_mma(acc[0], a, b0.x, b0.y);
+                    sur_mma(acc[1], a, b1.x, b1.y);
+                }
             }
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[nt][q] += acc2[nt][q];
             if (g < nrows) {
 #pragma unroll
                 for (int nt = 0; nt < 2; ++nt)
@@ -154,7 +165,7 @@ __device__ bool sur_forward_staged(const SurDev& s, int nrows, __nv_bfloat16* bu
         K = s.H;
     }
     if (warp < nrows) {
-        const float v = sur_out_dot(in + warp * SUR_AST, s.w4, s.H, lane);
+        const float v = sur_out_dot(in + warp * SUR_AST, w4, s.H, lane);
         if (lane == 0) out[warp] = __fmaf_rn(v + __ldg(s.b4), s.scale, s.offset);
     }
     __syncthreads();
