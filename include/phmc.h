@@ -212,8 +212,8 @@ int phmc_set_move_mix(phmc_engine* e, int replica, double p_disp, double p_titr,
  * trial pays a correction per buffered stencil, each rebuild a pass over the
  * mesh); threads: threads per replica block of the MC kernel (128 or 256).
  * Both may change between runs.  phmc_autotune times `trials` trials per
- * replica for each candidate (pending_max 8..128 x threads 128/256), keeps the
- * fastest and reports every candidate; its runs are ordinary Monte Carlo
+ * replica for each candidate (pending_max 8..128 x threads 128/256) in two
+ * interleaved passes, keeps the fastest and reports every candidate's better time; its runs are ordinary Monte Carlo
  * trials and advance the chains.  Decisions do not depend on the tuning except
  * through FP32 rounding of the reciprocal-space dE. */
 typedef struct phmc_tuning {

@@ -1347,21 +1347,35 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     CU(cudaStreamSynchronize(E.stream));
     const int pends[] = {8, 16, 24, 32, 48, 64, 96, 128};
     const int ths[] = {128, 256};
-    int best_p = E.pend_max, best_t = E.threads, n = 0;
+    // two passes over the candidates, each candidate's faster one kept: the chains move on
+    // while the tuner runs, and interleaving keeps that drift from favouring one candidate
+    std::vector<double> best_us(16, 1e300);
+    std::vector<char> fits(16, 0);
+    for (int pass = 0; pass < 2; ++pass) {
+        int c = 0;
+        for (int t : ths)
+            for (int pm : pends) {
+                const int k = c++;
+                if (pm > PHMC_MAX_PEND || (pass == 1 && !fits[k])) continue;
+                if (apply_tuning(h, pm, t) != PHMC_OK) continue;  // does not fit: skip
+                fits[k] = 1;
+                int s = phmc_run_loop(h, std::max<int64_t>(trials / 4, 4), 4);  // warm-up (captures the graph)
+                if (s) return s;
+                double ms = 0.0;
+                s = phmc_run_timed(h, trials, &ms);
+                if (s) return s;
+                best_us[k] = std::min(best_us[k], ms * 1e3 / (double)trials);
+            }
+    }
+    int best_p = E.pend_max, best_t = E.threads, n = 0, c = 0;
     double best = 1e300;
     for (int t : ths)
         for (int pm : pends) {
-            if (pm > PHMC_MAX_PEND) continue;
-            if (apply_tuning(h, pm, t) != PHMC_OK) continue;  // does not fit: skip
-            int s = phmc_run_loop(h, std::max<int64_t>(trials / 4, 4), 4);  // warm-up (captures the graph)
-            if (s) return s;
-            double ms = 0.0;
-            s = phmc_run_timed(h, trials, &ms);
-            if (s) return s;
-            const double us = ms * 1e3 / (double)trials;
-            if (results && n < max_results) { results[n].pending_max = pm; results[n].threads = t; results[n].us_per_trial = us; }
+            const int k = c++;
+            if (!fits[k]) continue;
+            if (results && n < max_results) { results[n].pending_max = pm; results[n].threads = t; results[n].us_per_trial = best_us[k]; }
             ++n;
-            if (us < best) { best = us; best_p = pm; best_t = t; }
+            if (best_us[k] < best) { best = best_us[k]; best_p = pm; best_t = t; }
         }
     if (n_results) *n_results = n;
     return apply_tuning(h, best_p, best_t);
