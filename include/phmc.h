@@ -438,6 +438,79 @@ typedef struct phmc_brush_spec {
 int phmc_build_brush(const phmc_brush_spec* spec, int capacity, float* x, float* y, float* z, float* q, int* type,
                      int* flags, int max_bonds, int* bond_i, int* bond_j, int* counts, double* box_out);
 
+/* ---- the reference's grand-canonical mu-control phase on the device ----
+ * Replaces phase_gc_mu_control (MC/include/mc.hpp:73-82, MC/src/mc.cu:320-548):
+ * pair flips NH_N + W -> NH_P(+1) + Cl(-1) and back, forward with probability
+ * a c / (a c + b d) (a = |NH_N|, b = |NH_P|, c = |W|, d = |Cl| pools), accepted
+ * when -beta (dE - s mu) + ln(S_before / S_after), clamped to +-40, is >= 0 or
+ * its exponential beats a uniform draw; blocks of gc_block trials; at the end
+ * of each epoch (accept target or attempt limit reached) mu moves by
+ * kT eta (logit f - logit f*) w_info; the phase ends when the protonated count
+ * reaches floor(target_pct / 100 Nh), or when no pair can flip.
+ * The whole phase runs in persistent MC-kernel launches (one block per job),
+ * with the reference's own random stream: the caller hands over its
+ * std::mt19937 (625 words: the 624 state words and the position, in the order
+ * the generator's stream output writes them) and gets it back where the
+ * phase left it, so the draws, the pool order (erase + push_back) and the
+ * float arithmetic of the reference's energies, mu update and acceptance are
+ * the reference's.  Jobs touch distinct replicas; their pools hold distinct
+ * present slots. */
+#define PHMC_GC_EV_CHUNK 1     /* a block of gc_block trials ended */
+#define PHMC_GC_EV_MU 2        /* an epoch ended: mu updated */
+#define PHMC_GC_EV_REACHED 3   /* the protonated count reached its target: the phase ends */
+#define PHMC_GC_EV_NO_PAIRS 4  /* neither direction has a pair: the phase ends */
+#define PHMC_GC_EV_ALREADY 5   /* at the target before the first trial */
+#define PHMC_GC_STOP_REACHED 1
+#define PHMC_GC_STOP_NO_PAIRS 2
+#define PHMC_GC_STOP_MAX_TRIALS 3
+#define PHMC_GC_STOP_ALREADY 4
+typedef struct phmc_gc_event {
+    int kind;                   /* PHMC_GC_EV_* */
+    int epoch;                  /* 0-based epoch */
+    int step_in_block;          /* REACHED: trials of the current block so far, this one included */
+    int acc_since_mu, att_since_mu;
+    int block_accepted, block_attempted;
+    int nprot, remaining;       /* protonated sites; max(0, target - nprot) */
+    int cause_amax;             /* MU: 1 the epoch hit the attempt limit short of the accept target, else 0 */
+    int64_t fwd_total, bwd_total;
+    float mu_kT;                /* beta mu_eff (MU: after the update) */
+    float f, w_info;            /* MU: protonated fraction, weight of the update */
+    float E;                    /* REACHED, ALREADY: the phase's energy */
+    float acc_rate;             /* CHUNK: block_accepted / block_attempted */
+} phmc_gc_event;
+typedef struct phmc_gc_job {
+    int replica;
+    int nh_n_type, nh_p_type, w_type, cl_type; /* engine types (0-based) */
+    float q_nh_p, q_cl;                        /* charges given to NH_P and Cl (the reference: +1, -1) */
+    double beta;                               /* 1 / kT */
+    double target_pct;                         /* target_protonation_pct */
+    double mu_eta;                             /* <= 0: 0.3 */
+    double nacc_frac;                          /* sgmc_nacc_frac_round, <= 0: 0.10 */
+    int gc_block;                              /* gc_block_fixed, <= 0: 2000 */
+    int epoch_attempt_max;                     /* sgmc_epoch_attempt_max, <= 0: 100000 */
+    int64_t max_trials;                        /* this call's trials at most (<= 0: 10^9); the reference has no bound */
+    const int* nh_n; int n_nh_n;               /* pools in the reference's order (slot indices) */
+    const int* nh_p; int n_nh_p;
+    const int* w; int n_w;
+    const int* cl; int n_cl;
+    uint32_t* mt_state;                        /* in / out: the caller's generator, 625 words */
+} phmc_gc_job;
+typedef struct phmc_gc_result {
+    int attempted, accepted, accepted_forward, accepted_backward, blocks_done;
+    int Nh, Nprot, target_count, reached_target;
+    int stop;                                  /* PHMC_GC_STOP_* */
+    float E, mu_eff;                           /* the phase's last energy and mu (the reference's real) */
+    int R0, Nacc_target, epoch_attempt_max, gc_block; /* settings derived as the reference derives them */
+    int n_events, events_dropped;              /* events stored for this job / beyond event_cap */
+} phmc_gc_result;
+/* events: n_jobs x event_cap records (job k at k * event_cap), or null. */
+int phmc_gc_phase(phmc_engine* e, int n_jobs, const phmc_gc_job* jobs, phmc_gc_result* results,
+                  phmc_gc_event* events, int event_cap);
+/* The reference's report.txt line of an event (MC/src/mc.cu:367-373, 377, 461-474,
+ * 506-516, 532-545), fixed notation at its precision 6, without the newline.
+ * Returns the line's length (the line is cut at cap - 1 characters). */
+int phmc_gc_event_format(const phmc_gc_event* ev, const phmc_gc_result* res, char* buf, int cap);
+
 #ifdef __cplusplus
 }
 #endif

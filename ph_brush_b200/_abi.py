@@ -122,6 +122,45 @@ class BrushSpec(C.Structure):
                 ("min_dist", C.c_double), ("seed", C.c_uint64)]
 
 
+GC_EV_CHUNK, GC_EV_MU, GC_EV_REACHED, GC_EV_NO_PAIRS, GC_EV_ALREADY = 1, 2, 3, 4, 5
+GC_STOP_REACHED, GC_STOP_NO_PAIRS, GC_STOP_MAX_TRIALS, GC_STOP_ALREADY = 1, 2, 3, 4
+
+
+class GcEvent(C.Structure):
+    _fields_ = [("kind", C.c_int), ("epoch", C.c_int), ("step_in_block", C.c_int),
+                ("acc_since_mu", C.c_int), ("att_since_mu", C.c_int),
+                ("block_accepted", C.c_int), ("block_attempted", C.c_int),
+                ("nprot", C.c_int), ("remaining", C.c_int), ("cause_amax", C.c_int),
+                ("fwd_total", C.c_int64), ("bwd_total", C.c_int64),
+                ("mu_kT", C.c_float), ("f", C.c_float), ("w_info", C.c_float), ("E", C.c_float),
+                ("acc_rate", C.c_float)]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GcJob(C.Structure):
+    _fields_ = [("replica", C.c_int), ("nh_n_type", C.c_int), ("nh_p_type", C.c_int), ("w_type", C.c_int),
+                ("cl_type", C.c_int), ("q_nh_p", C.c_float), ("q_cl", C.c_float), ("beta", C.c_double),
+                ("target_pct", C.c_double), ("mu_eta", C.c_double), ("nacc_frac", C.c_double),
+                ("gc_block", C.c_int), ("epoch_attempt_max", C.c_int), ("max_trials", C.c_int64),
+                ("nh_n", _ip), ("n_nh_n", C.c_int), ("nh_p", _ip), ("n_nh_p", C.c_int),
+                ("w", _ip), ("n_w", C.c_int), ("cl", _ip), ("n_cl", C.c_int),
+                ("mt_state", C.POINTER(C.c_uint32))]
+
+
+class GcResult(C.Structure):
+    _fields_ = [("attempted", C.c_int), ("accepted", C.c_int), ("accepted_forward", C.c_int),
+                ("accepted_backward", C.c_int), ("blocks_done", C.c_int), ("Nh", C.c_int), ("Nprot", C.c_int),
+                ("target_count", C.c_int), ("reached_target", C.c_int), ("stop", C.c_int),
+                ("E", C.c_float), ("mu_eff", C.c_float), ("R0", C.c_int), ("Nacc_target", C.c_int),
+                ("epoch_attempt_max", C.c_int), ("gc_block", C.c_int), ("n_events", C.c_int),
+                ("events_dropped", C.c_int)]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
@@ -133,7 +172,8 @@ EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy",
            "phmc_surrogate_train", "phmc_surrogate_save", "phmc_surrogate_load", "phmc_harvest",
            "phmc_harvest_count", "phmc_harvest_get", "phmc_surrogate_fit", "phmc_surrogate_attach",
            "phmc_get_da_stats", "phmc_surrogate_describe", "phmc_set_da_log", "phmc_set_move_mix",
-           "phmc_set_tuning", "phmc_get_tuning", "phmc_autotune", "phmc_delta_energy_components"]
+           "phmc_set_tuning", "phmc_get_tuning", "phmc_autotune", "phmc_delta_energy_components",
+           "phmc_gc_phase", "phmc_gc_event_format"]
 
 
 def load_library(path=LIB_PATH):
@@ -198,6 +238,8 @@ def load_library(path=LIB_PATH):
         "phmc_delta_energy_components": ([eng, C.c_int, C.POINTER(Trial), C.c_int, C.POINTER(EnergyComponents)], C.c_int),
         "phmc_get_tuning": ([eng, C.POINTER(Tuning)], C.c_int),
         "phmc_autotune": ([eng, C.c_int64, C.POINTER(Tuning), C.c_int, _ip], C.c_int),
+        "phmc_gc_phase": ([eng, C.c_int, C.POINTER(GcJob), C.POINTER(GcResult), C.POINTER(GcEvent), C.c_int], C.c_int),
+        "phmc_gc_event_format": ([C.POINTER(GcEvent), C.POINTER(GcResult), C.c_char_p, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -11,6 +11,32 @@
 #define PHMC_FIX_SCALE 1099511627776.0   /* 2^40: fixed-point scale of the charge mesh */
 #define PHMC_FIX_INV (1.0 / 1099511627776.0)
 
+#include "mt_std.cuh"
+
+// State of one job of the grand-canonical mu-control phase (MC/src/mc.cu:320-548),
+// carried across MC-kernel launches; the reference's `real` quantities are floats.
+enum { GC_NHN = 0, GC_NHP = 1, GC_W = 2, GC_CL = 3 };
+struct GcDev {
+    MtState mt;              // the reference's generator
+    int replica;
+    int type[4];             // engine types of NH_N, NH_P, W, Cl
+    float q_nhp, q_cl;
+    float beta, eta, f0;     // 1/kT, mu step factor, clamped target fraction
+    float mu;                // mu_eff
+    float E;                 // the phase's energy as the reference tracks it (R.E)
+    int Nh, Nprot, target, gc_block, amax, nacc_target;
+    int n[4];                // pool sizes
+    int attempted, accepted, fwd, bwd;
+    int epoch, block_t, block_att, block_acc, acc_mu, att_mu, blocks_done;
+    int max_trials;          // bound on attempted trials of the call
+    int launch_cap;          // trials per launch at most
+    int stop;                // PHMC_GC_STOP_* once the phase ended
+    int n_ev, ev_cap;        // events of the current launch
+    // the trial in flight
+    int dir;                 // +1 forward, -1 backward
+    long long s_before, s_after;
+};
+
 // Per-replica constant description (the ragged descriptor table).
 struct RepDesc {
     // particles
@@ -143,6 +169,12 @@ struct DevPtrs {
     float* dsc_out;
     // per external trial dE components (lj, fene, coul_real, coul_recip, self, qcorr, slab), or null
     double* ext_comp;
+    // grand-canonical mu-control phase: per job state, pools (4 x total slots: NH_N, NH_P, W,
+    // Cl of each replica at its slot offset) and event records (ev_cap per job)
+    struct GcDev* gc;
+    int* gc_pool;
+    int gc_pool_stride;
+    phmc_gc_event* gc_ev;
 };
 
 #define DSC_STRIDE (SUR_ROWS * SUR_K + 2 * SUR_ROWS + 4)

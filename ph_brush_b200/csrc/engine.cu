@@ -56,6 +56,10 @@ struct phmc_engine {
     float *st_x = nullptr, *st_y = nullptr, *st_z = nullptr, *st_q = nullptr;
     int *st_t = nullptr, *st_f = nullptr, *st_err = nullptr, *st_cnt = nullptr;
     int* d_charged = nullptr;  // per replica charged-site counts of the last run
+    // grand-canonical phase: job states, pools, events (allocated on first use)
+    GcDev* d_gc = nullptr;
+    int* d_gc_pool = nullptr;
+    phmc_gc_event* d_gc_ev = nullptr;
 };
 
 static void drop_graph(phmc_engine* h) {
@@ -600,7 +604,8 @@ extern "C" int phmc_destroy(phmc_engine* h) {
     if (E.d.log_stage) { cudaFree(E.d.log_stage); cudaFree(E.d.log_dEs); }
     if (E.d.hv_cap > 0) { cudaFree(E.d.hv_rows); cudaFree(E.d.hv_sign); cudaFree(E.d.hv_target); cudaFree(E.d.hv_count); }
     for (void* p : {(void*)h->st_x, (void*)h->st_y, (void*)h->st_z, (void*)h->st_q, (void*)h->st_t, (void*)h->st_f,
-                    (void*)h->st_err, (void*)h->st_cnt, (void*)h->d_charged})
+                    (void*)h->st_err, (void*)h->st_cnt, (void*)h->d_charged, (void*)h->d_gc, (void*)h->d_gc_pool,
+                    (void*)h->d_gc_ev})
         if (p) cudaFree(p);
     if (E.stream) cudaStreamDestroy(E.stream);
     delete h;
@@ -1106,6 +1111,156 @@ extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const flo
         h->n_present[(size_t)r] = cnt[(size_t)2 * r + 1];
     }
     return rc;
+}
+
+// ---- grand-canonical mu-control phase (MC/src/mc.cu:320-548) ----
+
+#define GC_LAUNCH_TRIALS 2048                      // trials per MC launch at most
+#define GC_EV_CAP (2 * GC_LAUNCH_TRIALS + 4)       // events one launch can record (chunk + mu per trial)
+
+static float gc_clampf(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// The phase's energy as the reference tracks it: the LJ part and the Coulomb part of the
+// energy components each rounded to its real, then added (MC/src/mc.cu:43-60).
+static float gc_energy_real(const RepState& s, int coulomb) {
+    const double ec = coulomb == PHMC_COUL_EWALD ? s.E_pair_c + s.E_rec + s.E_self + s.E_qcorr + s.E_slab : s.E_pair_c;
+    return (float)s.E_pair_lj + (float)ec;
+}
+
+extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs, phmc_gc_result* results,
+                             phmc_gc_event* events, int event_cap) {
+    if (!h || n_jobs < 1 || !jobs || !results || event_cap < 0) return fail(PHMC_ERR_ARG, "invalid argument");
+    Engine& E = h->E;
+    if (n_jobs > E.R) return fail(PHMC_ERR_ARG, "more jobs than replicas");
+    CU(cudaSetDevice(E.device));
+    std::vector<int> seen((size_t)E.R, 0);
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    std::vector<GcDev> G((size_t)n_jobs);
+    for (int k = 0; k < n_jobs; ++k) {
+        const phmc_gc_job& J = jobs[k];
+        if (J.replica < 0 || J.replica >= E.R || seen[J.replica]++) return fail(PHMC_ERR_ARG, "job replicas must be distinct and in range");
+        const RepDesc& D = E.desc[J.replica];
+        for (int t : {J.nh_n_type, J.nh_p_type, J.w_type, J.cl_type})
+            if (t < 0 || t >= D.T) return fail(PHMC_ERR_ARG, "job type out of range");
+        if (!J.mt_state || J.mt_state[MT_N] > MT_N) return fail(PHMC_ERR_ARG, "job needs a generator state (624 words, position <= 624)");
+        if (!(J.beta > 0.0)) return fail(PHMC_ERR_ARG, "beta must be positive");
+        const int* pools[4] = {J.nh_n, J.nh_p, J.w, J.cl};
+        const int npool[4] = {J.n_nh_n, J.n_nh_p, J.n_w, J.n_cl};
+        std::vector<int> flags((size_t)D.cap);
+        CU(cudaMemcpy(flags.data(), E.d.flags + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
+        std::vector<char> used((size_t)D.cap, 0);
+        for (int p = 0; p < 4; ++p) {
+            if (npool[p] < 0 || (npool[p] > 0 && !pools[p])) return fail(PHMC_ERR_ARG, "job pool pointer / size invalid");
+            for (int i = 0; i < npool[p]; ++i) {
+                const int v = pools[p][i];
+                if (v < 0 || v >= D.cap || used[v]++) return fail(PHMC_ERR_ARG, "pool slots must be distinct and in range");
+                if (flags[v] & PHMC_F_GHOST) return fail(PHMC_ERR_ARG, "pool slot is empty");
+            }
+        }
+        // settings derived as the reference derives them, in its real (MC/src/mc.cu:339-357)
+        GcDev& g = G[k];
+        std::memset(&g, 0, sizeof g);
+        for (int i = 0; i < MT_N; ++i) g.mt.x[i] = J.mt_state[i];
+        g.mt.p = (int)J.mt_state[MT_N];
+        g.replica = J.replica;
+        g.type[GC_NHN] = J.nh_n_type; g.type[GC_NHP] = J.nh_p_type; g.type[GC_W] = J.w_type; g.type[GC_CL] = J.cl_type;
+        g.q_nhp = J.q_nh_p; g.q_cl = J.q_cl;
+        g.beta = (float)J.beta;
+        for (int p = 0; p < 4; ++p) g.n[p] = npool[p];
+        g.Nh = J.n_nh_n + J.n_nh_p;
+        g.Nprot = J.n_nh_p;
+        const float pct = (float)J.target_pct;
+        g.target = (int)std::floor(pct / 100.0 * g.Nh);
+        const float lo = (float)1e-6, hi = (float)(1.0 - 1e-6);
+        const float fstar = gc_clampf((float)(pct / 100.0), lo, hi);
+        g.f0 = fstar;
+        const float bound = 10.0f / g.beta;
+        g.mu = gc_clampf((1.0f / g.beta) * std::log(fstar / (1.0f - fstar)), -bound, bound);
+        g.gc_block = J.gc_block > 0 ? J.gc_block : 2000;
+        g.amax = J.epoch_attempt_max > 0 ? J.epoch_attempt_max : 100000;
+        const int R0 = std::max(0, g.target - g.Nprot);
+        const float frac = J.nacc_frac > 0.0 ? (float)J.nacc_frac : 0.10f;
+        g.nacc_target = std::max(1, (int)std::ceil((double)frac * (double)R0));
+        g.eta = J.mu_eta > 0.0 ? (float)J.mu_eta : 0.3f;
+        g.E = gc_energy_real(st[(size_t)J.replica], D.coulomb);
+        g.max_trials = (int)std::min<int64_t>(J.max_trials > 0 ? J.max_trials : 1000000000, 1000000000);
+        g.launch_cap = GC_LAUNCH_TRIALS;
+        g.ev_cap = GC_EV_CAP;
+        if (g.Nprot == g.target) g.stop = PHMC_GC_STOP_ALREADY;
+        phmc_gc_result& R = results[k];
+        std::memset(&R, 0, sizeof R);
+        R.R0 = R0; R.Nacc_target = g.nacc_target; R.epoch_attempt_max = g.amax; R.gc_block = g.gc_block;
+    }
+    // device buffers on first use
+    if (!h->d_gc) {
+        CU(cudaMalloc((void**)&h->d_gc, sizeof(GcDev) * E.R));
+        CU(cudaMalloc((void**)&h->d_gc_pool, sizeof(int) * 4 * (size_t)E.total_slots));
+        CU(cudaMalloc((void**)&h->d_gc_ev, sizeof(phmc_gc_event) * GC_EV_CAP * (size_t)E.R));
+    }
+    E.d.gc = h->d_gc; E.d.gc_pool = h->d_gc_pool; E.d.gc_pool_stride = E.total_slots; E.d.gc_ev = h->d_gc_ev;
+    for (int k = 0; k < n_jobs; ++k) {
+        const phmc_gc_job& J = jobs[k];
+        const int* pools[4] = {J.nh_n, J.nh_p, J.w, J.cl};
+        const int npool[4] = {J.n_nh_n, J.n_nh_p, J.n_w, J.n_cl};
+        for (int p = 0; p < 4; ++p)
+            if (npool[p] > 0)
+                CU(cudaMemcpyAsync(h->d_gc_pool + (size_t)p * E.total_slots + E.desc[J.replica].slot_off, pools[p],
+                                   sizeof(int) * npool[p], cudaMemcpyHostToDevice, E.stream));
+    }
+    CU(cudaMemcpyAsync(h->d_gc, G.data(), sizeof(GcDev) * n_jobs, cudaMemcpyHostToDevice, E.stream));
+    // events kept on the host (the device buffer holds one launch's)
+    std::vector<std::vector<phmc_gc_event>> evs((size_t)n_jobs);
+    for (int k = 0; k < n_jobs; ++k)
+        if (G[k].stop == PHMC_GC_STOP_ALREADY) {
+            phmc_gc_event ev;
+            std::memset(&ev, 0, sizeof ev);
+            ev.kind = PHMC_GC_EV_ALREADY; ev.nprot = G[k].Nprot; ev.mu_kT = G[k].beta * G[k].mu; ev.E = G[k].E;
+            evs[k].push_back(ev);
+        }
+    std::vector<phmc_gc_event> evbuf;
+    // every launch runs at least pend_max / 2 trials of each unfinished job, so the loop ends
+    const long long max_launches = 2LL * 1000000000LL / std::max(1, E.pend_max / 2) + 8;
+    for (long long it = 0;; ++it) {
+        CU(launch_mc_gc(E, n_jobs, E.stream));
+        int s = flush_dirty(h);
+        if (s) return s;
+        CU(cudaMemcpyAsync(G.data(), h->d_gc, sizeof(GcDev) * n_jobs, cudaMemcpyDeviceToHost, E.stream));
+        s = check_kernel_errors(h);  // synchronises the stream
+        if (s) return s;
+        bool all = true;
+        for (int k = 0; k < n_jobs; ++k) {
+            const int n = std::min(G[k].n_ev, GC_EV_CAP);
+            if (n > 0) {
+                evbuf.resize((size_t)n);
+                CU(cudaMemcpy(evbuf.data(), h->d_gc_ev + (size_t)k * GC_EV_CAP, sizeof(phmc_gc_event) * n, cudaMemcpyDeviceToHost));
+                evs[k].insert(evs[k].end(), evbuf.begin(), evbuf.end());
+            }
+            if (G[k].n_ev > GC_EV_CAP) return fail(PHMC_ERR_CAPACITY, "grand-canonical phase: event buffer overflow");
+            all = all && G[k].stop != 0;
+        }
+        if (all) break;
+        if (it > max_launches) return fail(PHMC_ERR_BUDGET, "grand-canonical phase made no progress");
+    }
+    for (int k = 0; k < n_jobs; ++k) {
+        const GcDev& g = G[k];
+        const phmc_gc_job& J = jobs[k];
+        for (int i = 0; i < MT_N; ++i) J.mt_state[i] = g.mt.x[i];
+        J.mt_state[MT_N] = (uint32_t)g.mt.p;
+        phmc_gc_result& R = results[k];
+        R.attempted = g.attempted; R.accepted = g.accepted;
+        R.accepted_forward = g.fwd; R.accepted_backward = g.bwd; R.blocks_done = g.blocks_done;
+        R.Nh = g.Nh; R.Nprot = g.Nprot; R.target_count = g.target;
+        R.reached_target = (g.stop == PHMC_GC_STOP_REACHED || g.stop == PHMC_GC_STOP_ALREADY) ? 1 : 0;
+        R.stop = g.stop;
+        R.E = g.E; R.mu_eff = g.mu;
+        const int n = (int)evs[k].size();
+        const int kept = events ? std::min(n, event_cap) : 0;
+        for (int i = 0; i < kept; ++i) events[(size_t)k * event_cap + i] = evs[k][(size_t)i];
+        R.n_events = kept;
+        R.events_dropped = n - kept;
+    }
+    return PHMC_OK;
 }
 
 extern "C" int phmc_get_cells(phmc_engine* h, int rep, int* cell_of, int dims[3]) {

@@ -17,6 +17,7 @@
 //  * self / net-charge / slab terms from FP64 charge moments;
 //  * Metropolis in FP64 with the move's log factor (MC/src/mc.cu:438-440).
 #include <algorithm>
+#include <type_traits>
 #include "common.cuh"
 #include "engine.h"
 #include "fft.cuh"
@@ -410,6 +411,162 @@ __device__ void desc_exact_terms(TrialS& T, const RepDesc& D, const RepState& S)
     T.dmom = m.dself + m.dqc + m.dslab;
 }
 
+// ---- the reference's grand-canonical mu-control phase (MC/src/mc.cu:320-548) ----
+
+__device__ __forceinline__ int* gc_pool(const DevPtrs& d, const RepDesc& D, int k) {
+    return d.gc_pool + (size_t)k * d.gc_pool_stride + D.slot_off;
+}
+
+__device__ void gc_event(GcDev& G, const DevPtrs& d, const phmc_gc_event& ev) {
+    const int k = G.n_ev++;
+    if (k < G.ev_cap) d.gc_ev[(size_t)blockIdx.x * G.ev_cap + k] = ev;
+}
+
+__device__ __forceinline__ phmc_gc_event gc_event_base(const GcDev& G, int kind) {
+    phmc_gc_event ev;
+    memset(&ev, 0, sizeof ev);
+    ev.kind = kind; ev.epoch = G.epoch;
+    ev.acc_since_mu = G.acc_mu; ev.att_since_mu = G.att_mu;
+    ev.block_accepted = G.block_acc; ev.block_attempted = G.block_att;
+    ev.nprot = G.Nprot; ev.remaining = max(0, G.target - G.Nprot);
+    ev.fwd_total = G.fwd; ev.bwd_total = G.bwd;
+    ev.mu_kT = __fmul_rn(G.beta, G.mu);
+    ev.E = G.E;
+    return ev;
+}
+
+// natural log of a float as the host library's correctly rounded logf gives it
+__device__ __forceinline__ float gc_logf(float x) { return (float)log((double)x); }
+__device__ __forceinline__ float gc_clamp(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// Proposal of the next pair flip (one thread): direction, then NH site, then W / Cl
+// partner, each from the reference's generator (MC/src/mc.cu:383-417).  Sets T.stop
+// when the launch or the phase ends.
+__device__ void gc_propose(TrialS& T, GcDev& G, const RepDesc& D, const DevPtrs& d, int npend, int pend_max, int& launch_trials) {
+    if (G.stop || npend + 2 > pend_max || launch_trials >= G.launch_cap) { T.stop = 1; return; }
+    if (G.attempted >= G.max_trials) { G.stop = PHMC_GC_STOP_MAX_TRIALS; T.stop = 1; return; }
+    const long long a = G.n[GC_NHN], b = G.n[GC_NHP], c = G.n[GC_W], e = G.n[GC_CL];
+    const long long wf = a * c, wb = b * e;
+    bool fwd;
+    if (wf > 0 && wb > 0) {
+        const float sum = (float)(wf + wb);
+        fwd = mt_unit_float(G.mt) < __fdiv_rn((float)wf, sum);
+    } else if (wf > 0) {
+        fwd = true;
+    } else if (wb > 0) {
+        fwd = false;
+    } else {
+        gc_event(G, d, gc_event_base(G, PHMC_GC_EV_NO_PAIRS));
+        G.stop = PHMC_GC_STOP_NO_PAIRS;
+        T.stop = 1;
+        return;
+    }
+    const int i = gc_pool(d, D, fwd ? GC_NHN : GC_NHP)[mt_index(G.mt, (uint32_t)(fwd ? a : b))];
+    const int j = gc_pool(d, D, fwd ? GC_W : GC_CL)[mt_index(G.mt, (uint32_t)(fwd ? c : e))];
+    G.dir = fwd ? 1 : -1;
+    G.s_before = wf + wb;
+    G.s_after = fwd ? (a - 1) * (c - 1) + (b + 1) * (e + 1) : (a + 1) * (c + 1) + (b - 1) * (e - 1);
+    ++launch_trials;
+    T.move = PHMC_MOVE_NONE; T.skip = 0; T.nch = 2; T.logf = 0.0; T.tnum = G.attempted;
+    const int so = D.slot_off;
+    const int idx[2] = {i, j};
+    for (int k = 0; k < 2; ++k) {
+        const int s = idx[k];
+        T.idx[k] = s;
+        T.fo[k] = d.flags[so + s];
+        T.pres_old[k] = 1; T.pres_new[k] = 1;
+        T.po[k] = d.posq[so + s]; T.to[k] = d.type[so + s]; T.bonds[k] = d.bonds[so + s];
+        T.pn[k] = T.po[k];
+    }
+    T.pn[0].w = fwd ? G.q_nhp : 0.0f; T.tn[0] = G.type[fwd ? GC_NHP : GC_NHN];
+    T.pn[1].w = fwd ? G.q_cl : 0.0f;  T.tn[1] = G.type[fwd ? GC_CL : GC_W];
+}
+
+// Decision and the phase's bookkeeping after the exact dE of the flip (one thread,
+// MC/src/mc.cu:422-545).  The energies are the reference's: the LJ part and the
+// Coulomb part of the trial state each rounded to the reference's real, summed,
+// and differenced with the phase's last accepted energy.  Returns the decision.
+__device__ int gc_decide(GcDev& G, const RepDesc& D, const RepState& S, const DevPtrs& d, double dlj, double dc, double drec,
+                         double dself, double dqc, double dslab) {
+    const double lj = S.E_pair_lj + dlj;
+    const double ec = D.coulomb == PHMC_COUL_EWALD
+                          ? (S.E_pair_c + dc) + (S.E_rec + drec) + (S.E_self + dself) + (S.E_qcorr + dqc) + (S.E_slab + dslab)
+                          : S.E_pair_c + dc;
+    const float Et = __fadd_rn(__double2float_rn(lj), __double2float_rn(ec));
+    const float dEf = __fsub_rn(Et, G.E);
+    const float arg = __fmul_rn(-G.beta, __fsub_rn(dEf, __fmul_rn((float)G.dir, G.mu)));
+    double logH = 0.0;
+    if (G.s_before > 0 && G.s_after > 0) logH = log((double)G.s_before) - log((double)G.s_after);
+    double expo = (double)arg + logH;
+    expo = expo < -40.0 ? -40.0 : (expo > 40.0 ? 40.0 : expo);
+    const int accept = (expo >= 0.0) || (exp(expo) > (double)mt_unit_float(G.mt));
+    G.attempted++; G.block_att++; G.att_mu++;
+    if (accept) {
+        G.accepted++; G.block_acc++; G.acc_mu++;
+        if (G.dir > 0) G.fwd++; else G.bwd++;
+        G.E = Et;
+        G.Nprot += G.dir;
+        if (G.Nprot == G.target) {
+            phmc_gc_event ev = gc_event_base(G, PHMC_GC_EV_REACHED);
+            ev.step_in_block = G.block_t + 1;
+            gc_event(G, d, ev);
+            G.stop = PHMC_GC_STOP_REACHED;
+            return accept;
+        }
+    }
+    if (++G.block_t == G.gc_block) {
+        phmc_gc_event ev = gc_event_base(G, PHMC_GC_EV_CHUNK);
+        ev.acc_rate = __fdiv_rn((float)G.block_acc, (float)G.block_att);
+        gc_event(G, d, ev);
+        G.block_t = 0; G.block_att = 0; G.block_acc = 0;
+        if (!(G.acc_mu < G.nacc_target && G.att_mu < G.amax)) {  // the epoch ends: mu update
+            const float f = G.Nh > 0 ? __fdiv_rn((float)G.Nprot, (float)G.Nh) : 0.0f;
+            const float lo = (float)1e-6, hi = (float)(1.0 - 1e-6);
+            const float f1 = gc_clamp(f, lo, hi);
+            const float logit_diff = __fsub_rn(gc_logf(__fdiv_rn(f1, __fsub_rn(1.0f, f1))),
+                                               gc_logf(__fdiv_rn(G.f0, __fsub_rn(1.0f, G.f0))));
+            const bool early = (G.att_mu >= G.amax) && (G.acc_mu < G.nacc_target);
+            const float w_info = G.nacc_target > 0
+                                     ? gc_clamp(__fdiv_rn((float)G.acc_mu, (float)max(1, G.nacc_target)), 0.0f, 1.0f)
+                                     : 1.0f;
+            const float step = __fmul_rn(__fmul_rn(__fmul_rn(__fdiv_rn(1.0f, G.beta), G.eta), logit_diff), w_info);
+            G.mu = __fsub_rn(G.mu, step);
+            G.blocks_done = G.epoch + 1;
+            phmc_gc_event mu = gc_event_base(G, PHMC_GC_EV_MU);
+            mu.cause_amax = early ? 1 : 0;
+            mu.f = f;
+            mu.w_info = w_info;
+            gc_event(G, d, mu);
+            G.epoch++; G.acc_mu = 0; G.att_mu = 0;
+        }
+    }
+    return accept;
+}
+
+// Move slot v from pool src to the end of pool dst, keeping the order of the rest
+// (std::vector erase + push_back); all threads of the block.
+template <int NT>
+__device__ void gc_pool_move(int* src, int* dst, int& n_src, int& n_dst, int v, int* s_find) {
+    if (threadIdx.x == 0) *s_find = 0x7fffffff;
+    __syncthreads();
+    const int n = n_src;
+    for (int k = threadIdx.x; k < n; k += NT)
+        if (src[k] == v) atomicMin(s_find, k);
+    __syncthreads();
+    const int k0 = *s_find;
+    if (k0 < n) {
+        for (int b = k0; b < n - 1; b += NT) {  // shift the tail down by one, NT entries per step
+            const int k = b + threadIdx.x;
+            const int val = (k < n - 1) ? src[k + 1] : 0;
+            __syncthreads();
+            if (k < n - 1) src[k] = val;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) { dst[n_dst] = v; n_dst = n_dst + 1; n_src = n - 1; }
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ void cls_add(const DevPtrs& d, const RepDesc& D, int cell, int cls, int delta) {
     if (cls >= 0 && cell >= 0) reinterpret_cast<int*>(d.cell_cls + D.cell_off + cell)[cls] += delta;
 }
@@ -434,7 +591,7 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
     a = red[96]; b = red[97]; c = red[98];
 }
 
-template <int P, int NT>
+template <int P, int NT, bool GC>
 __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
     constexpr int W = 2 * P - 1;
@@ -474,9 +631,20 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     uint2* wb = d.sur_late_l3 ? wa + SUR_WBUF_BYTES / 8 : wa + (SUR_K * SUR_HMAX * 2) / 8;
     uint2* wc = d.sur_late_l3 ? wa : wb + SUR_WBUF_BYTES / 8;
     uint32_t sur_par = 0;  // parity of the weight barriers' current phase (one phase per evaluated move)
+    // grand-canonical mu-control phase: the job's state (block blockIdx.x runs job blockIdx.x)
+    __shared__ __align__(16) typename std::conditional<GC, GcDev, int>::type sG;
+    __shared__ int s_gc_ops, s_gc_find, s_gc_lt;
 
-    const int r = (mode == MC_RUN) ? blockIdx.x : ext_rep;
+    const int r = GC ? d.gc[blockIdx.x].replica : ((mode == MC_RUN) ? blockIdx.x : ext_rep);
     const int tid = threadIdx.x;
+    if constexpr (GC) {
+        const int* src = reinterpret_cast<const int*>(d.gc + blockIdx.x);
+        int* dst = reinterpret_cast<int*>(&sG);
+        for (int k = tid; k < (int)(sizeof(GcDev) / sizeof(int)); k += NT) dst[k] = src[k];
+        if (tid == 0) { s_gc_ops = 0; s_gc_lt = 0; }
+        __syncthreads();
+        if (tid == 0) sG.n_ev = 0;
+    }
     // the replica's descriptor lives in shared memory for the whole launch
     __shared__ __align__(16) RepDesc sD;
     {
@@ -525,7 +693,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             if (tid == 0) {
                 T.stop = 0; T.desc = 0; T.da = 0;
                 if (S.error) T.stop = 1;
-                else if (mode == MC_RUN) {
+                else if (GC) {
+                    if constexpr (GC) gc_propose(T, sG, D, d, s_npend, pend_max, s_gc_lt);
+                } else if (mode == MC_RUN) {
                     if (S.trial >= S.target) { T.stop = 1; S.stop_reason = 0; }
                     else if (s_npend + 2 > pend_max) {
                         T.stop = 1; S.stop_reason = 1;
@@ -1062,7 +1232,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const double dlj = acc_lj + T.d_direct_lj, dc = acc_c + T.d_direct_c;
             const double dE = dlj + dc + T.d_fene + acc_rec + dself + dqc + dslab;
             int accept = 0;
-            if (mode == MC_RUN) {
+            if (GC) {
+                if constexpr (GC) {
+                    accept = gc_decide(sG, D, S, d, dlj, dc, acc_rec, dself, dqc, dslab);
+                    s_gc_ops = accept;
+                }
+            } else if (mode == MC_RUN) {
                 const long long li = T.tnum - S.run_start;
                 if (r == 0 && d.replay && li < d.replay_n) accept = d.replay[li];
                 else {
@@ -1196,6 +1371,22 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             }
         }
         __syncthreads();
+        if constexpr (GC) {
+            if (s_gc_ops) {  // the accepted flip's pool updates (MC/src/mc.cu:446-458)
+                const bool fwd = sG.dir > 0;
+                const int ka = fwd ? GC_NHN : GC_NHP, kb = fwd ? GC_NHP : GC_NHN;
+                const int kc = fwd ? GC_W : GC_CL, kd = fwd ? GC_CL : GC_W;
+                gc_pool_move<NT>(gc_pool(d, D, ka), gc_pool(d, D, kb), sG.n[ka], sG.n[kb], T.idx[0], &s_gc_find);
+                gc_pool_move<NT>(gc_pool(d, D, kc), gc_pool(d, D, kd), sG.n[kc], sG.n[kd], T.idx[1], &s_gc_find);
+                if (tid == 0) s_gc_ops = 0;
+                __syncthreads();
+            }
+        }
+    }
+    if constexpr (GC) {
+        const int* src = reinterpret_cast<const int*>(&sG);
+        int* dst = reinterpret_cast<int*>(d.gc + blockIdx.x);
+        for (int k = tid; k < (int)(sizeof(GcDev) / sizeof(int)); k += NT) dst[k] = src[k];
     }
     if (tid == 0) {
         if (mode == MC_RUN) {
@@ -1216,7 +1407,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     if (E.d.sur.H > 0) {
         // three staged layers when two blocks per SM still fit, else two buffers
         cudaFuncAttributes fa;
-        cudaFuncGetAttributes(&fa, k_mc<P, NT>);
+        cudaFuncGetAttributes(&fa, k_mc<P, NT, false>);
         int per_sm = 0;
         cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, E.device);
         const size_t three = mc_smem_bytes(P, E.pend_max, true);
@@ -1230,7 +1421,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     dd.quorum = 1.0f;
     if (mode == MC_RUN && E.quorum < 1.0f) {
         int per_sm = 0, nsm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT>, NT, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT, false>, NT, smem);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
         if ((long long)per_sm * nsm >= E.R) {
             dd.quorum = E.quorum;
@@ -1238,8 +1429,40 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
             if (e != cudaSuccess) return e;
         }
     }
-    k_mc<P, NT><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
+    k_mc<P, NT, false><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
+}
+
+// One block per job of the grand-canonical phase (128 threads; no surrogate, no quorum).
+template <int P>
+static cudaError_t launch_mc_gc_t(Engine& E, int n_jobs, cudaStream_t st) {
+    DevPtrs dd = E.d;
+    dd.quorum = 1.0f;
+    dd.ext_comp = nullptr;
+    dd.hv_cap = 0;
+    dd.log_move = nullptr;
+    dd.replay = nullptr;
+    dd.sur.H = 0;
+    const size_t smem = mc_smem_bytes(P, E.pend_max, false);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_mc<P, 128, true>);
+    if (e != cudaSuccess) return e;
+    int optin = 0;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
+    if (e != cudaSuccess) return e;
+    if (smem + fa.sharedSizeBytes > (size_t)optin) return cudaErrorInvalidValue;
+    e = cudaFuncSetAttribute(k_mc<P, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_mc<P, 128, true><<<n_jobs, 128, smem, st>>>(dd, MC_GC, 0, nullptr, 0, nullptr, E.pend_max);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mc_gc(Engine& E, int n_jobs, cudaStream_t st) {
+    switch (E.order) {
+        case 4: return launch_mc_gc_t<4>(E, n_jobs, st);
+        case 5: return launch_mc_gc_t<5>(E, n_jobs, st);
+        default: return launch_mc_gc_t<6>(E, n_jobs, st);
+    }
 }
 
 // Raise the dynamic shared-memory cap of the engine's MC kernel instance to the
@@ -1250,11 +1473,11 @@ static cudaError_t prepare_mc_t(Engine& E) {
     cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
     if (e != cudaSuccess) return e;
     cudaFuncAttributes fa;
-    e = cudaFuncGetAttributes(&fa, k_mc<P, NT>);
+    e = cudaFuncGetAttributes(&fa, k_mc<P, NT, false>);
     if (e != cudaSuccess) return e;
     const int cap = optin - (int)fa.sharedSizeBytes;
     if ((size_t)cap < mc_smem_bytes(P, E.pend_max, true)) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(k_mc<P, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+    return cudaFuncSetAttribute(k_mc<P, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
 }
 
 cudaError_t prepare_mc(Engine& E) {

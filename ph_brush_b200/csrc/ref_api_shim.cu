@@ -31,10 +31,14 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include <sstream>
 #include "energy.hpp"
+#include "gc_report.hpp"
+#include "mc.hpp"
 #include "neighbor.hpp"
 #include "pme.hpp"
 #include "phmc.h"
+#include "report.hpp"
 
 namespace {
 
@@ -437,4 +441,95 @@ real pmeEnergy(PMEPlan& plan, const DeviceAtoms& atoms, const DeviceCSR&, const 
     }
     (void)plan;
     return (real)(c.coul_real + c.coul_recip + c.self + c.qcorr + c.slab);
+}
+
+// ---- MC/include/mc.hpp: the grand-canonical mu-control phase on the device ----
+// phase_gc_mu_control (MC/include/mc.hpp:73-82, MC/src/mc.cu:320-548) with the same
+// arguments, results, report lines and generator stream, run by phmc_gc_phase in
+// persistent MC-kernel launches instead of one host round trip per trial.  A driver
+// calls it in place of phase_gc_mu_control (MC/src/main.cu:190).
+PhaseGCResult phmc_ref_phase_gc_mu_control(System& sys, DeviceAtoms& d_atoms, const DeviceParams& d_params,
+                                           const DeviceCSR&, const Box& box, PMEPlan*, Params& p, const MCPlan& mcplan,
+                                           std::mt19937& rng, Phase1Result* seed_out) {
+    // the engine takes the atoms' current state
+    ensure_engine(d_atoms, d_params, box);
+    upload_state(d_atoms);
+    ck(phmc_energy(g.eng, &g.base), "phmc_energy");
+    mirror(d_atoms);
+    g.cur = g.base;
+    g.last_n = 0;
+    // pools as the reference builds them (MC/src/mc.cu:332-342)
+    std::vector<int> nh_n = mcplan.idx_nh_n, nh_p = mcplan.idx_nh_p, w = mcplan.idx_w, cl;
+    for (int j = 0; j < sys.natoms; ++j)
+        if (sys.atoms[j].type == p.Cl_type && sys.atoms[j].z < mcplan.z_cut) cl.push_back(j);
+    // the generator's state words and position, in its stream format
+    std::vector<uint32_t> mt(625);
+    {
+        std::stringstream ss;
+        ss << rng;
+        for (uint32_t& v : mt) { unsigned long x = 0; ss >> x; v = (uint32_t)x; }
+    }
+    phmc_gc_job J;
+    std::memset(&J, 0, sizeof J);
+    J.replica = 0;
+    J.nh_n_type = p.NH_N_type - 1; J.nh_p_type = p.NH_P_type - 1; J.w_type = p.W_type - 1; J.cl_type = p.Cl_type - 1;
+    J.q_nh_p = 1.0f; J.q_cl = -1.0f;
+    J.beta = p.beta; J.target_pct = p.target_protonation_pct; J.mu_eta = p.mu_eta; J.nacc_frac = p.sgmc_nacc_frac_round;
+    J.gc_block = p.gc_block_fixed; J.epoch_attempt_max = p.sgmc_epoch_attempt_max;
+    J.nh_n = nh_n.data(); J.n_nh_n = (int)nh_n.size();
+    J.nh_p = nh_p.data(); J.n_nh_p = (int)nh_p.size();
+    J.w = w.data(); J.n_w = (int)w.size();
+    J.cl = cl.data(); J.n_cl = (int)cl.size();
+    J.mt_state = mt.data();
+    phmc_gc_result R;
+    std::vector<phmc_gc_event> ev((size_t)1 << 16);
+    ck(phmc_gc_phase(g.eng, 1, &J, &R, ev.data(), (int)ev.size()), "phmc_gc_phase");
+    {
+        std::stringstream ss;
+        for (uint32_t v : mt) ss << v << ' ';
+        ss >> rng;
+    }
+    for (int i = 0; i < R.n_events; ++i) phmc_gc_write_event(mc_report(), ev[(size_t)i], R);
+    if (R.events_dropped > 0) mc_report() << "[sgmc] " << R.events_dropped << " further report lines not kept" << std::endl;
+    // the atoms take the engine's identities
+    std::vector<float> q((size_t)g.n);
+    std::vector<int> t((size_t)g.n);
+    ck(phmc_get_state(g.eng, 0, nullptr, nullptr, nullptr, q.data(), t.data(), nullptr), "phmc_get_state");
+    thrust::host_vector<real> hq(d_atoms.q.begin(), d_atoms.q.end());
+    thrust::host_vector<int> ht(d_atoms.type.begin(), d_atoms.type.end());
+    for (int i = 0; i < g.n; ++i)
+        if (t[(size_t)i] != ht[i] || q[(size_t)i] != (float)hq[i]) {
+            ht[i] = t[(size_t)i]; hq[i] = (real)q[(size_t)i];
+            sys.atoms[(size_t)i].type = t[(size_t)i] + 1;
+            sys.atoms[(size_t)i].q = (real)q[(size_t)i];
+        }
+    d_atoms.q = hq;
+    d_atoms.type = ht;
+    mirror(d_atoms);
+    ck(phmc_energy(g.eng, &g.base), "phmc_energy");
+    g.cur = g.base;
+    g.last_n = 0;
+    PhaseGCResult out;
+    out.attempted = R.attempted; out.accepted = R.accepted;
+    out.accepted_forward = R.accepted_forward; out.accepted_backward = R.accepted_backward;
+    out.blocks_done = R.blocks_done;
+    out.Nh = R.Nh; out.Nprot = R.Nprot; out.target_count = R.target_count;
+    out.reached_target = R.reached_target != 0;
+    out.E = (real)R.E;
+    out.mu_eff = (real)R.mu_eff;
+    p.mu_eff = out.mu_eff;
+    if (seed_out && R.stop == PHMC_GC_STOP_REACHED) {  // pools for phase 2 (MC/src/mc.cu:475-492)
+        seed_out->nh_p_mc.clear(); seed_out->nh_n_remaining.clear();
+        seed_out->w_remaining.clear(); seed_out->cl_mc.clear();
+        for (int idx = 0; idx < sys.natoms; ++idx) {
+            const int ty = sys.atoms[(size_t)idx].type;
+            const real zz = sys.atoms[(size_t)idx].z;
+            if (ty == p.NH_P_type) seed_out->nh_p_mc.push_back(idx);
+            else if (ty == p.NH_N_type) seed_out->nh_n_remaining.push_back(idx);
+            else if (ty == p.W_type) { if (zz < mcplan.z_cut) seed_out->w_remaining.push_back(idx); }
+            else if (ty == p.Cl_type) { if (zz < mcplan.z_cut) seed_out->cl_mc.push_back(idx); }
+        }
+        seed_out->E = out.E;
+    }
+    return out;
 }

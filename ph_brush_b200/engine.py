@@ -153,6 +153,42 @@ class Engine:
                                             _abi.fptr(q), _abi.iptr(t), _abi.iptr(f)))
         return {"x": x, "y": y, "z": z, "q": q, "type": t, "flags": f}
 
+    def gc_phase(self, jobs, event_cap=1 << 14):
+        """The reference's grand-canonical mu-control phase (MC/src/mc.cu:320-548) on the
+        device, one job per replica.  Each job is a dict with the keys of phmc_gc_job:
+        replica, nh_n_type, nh_p_type, w_type, cl_type (engine types), q_nh_p, q_cl, beta,
+        target_pct, optional mu_eta, nacc_frac, gc_block, epoch_attempt_max, max_trials,
+        the pools nh_n, nh_p, w, cl (slot indices in the reference's order) and mt_state
+        (uint32[625], updated in place).  Returns [(result dict, [event dicts])]."""
+        n = len(jobs)
+        J = (_abi.GcJob * n)()
+        keep = []
+        for k, j in enumerate(jobs):
+            st = j["mt_state"]
+            assert isinstance(st, np.ndarray) and st.dtype == np.uint32 and st.shape == (625,) and st.flags.c_contiguous
+            J[k].replica = j.get("replica", k)
+            for key in ("nh_n_type", "nh_p_type", "w_type", "cl_type"):
+                setattr(J[k], key, int(j[key]))
+            J[k].q_nh_p = j.get("q_nh_p", 1.0)
+            J[k].q_cl = j.get("q_cl", -1.0)
+            J[k].beta = j["beta"]
+            J[k].target_pct = j["target_pct"]
+            J[k].mu_eta = j.get("mu_eta", 0.0)
+            J[k].nacc_frac = j.get("nacc_frac", 0.0)
+            J[k].gc_block = j.get("gc_block", 0)
+            J[k].epoch_attempt_max = j.get("epoch_attempt_max", 0)
+            J[k].max_trials = j.get("max_trials", 0)
+            for key in ("nh_n", "nh_p", "w", "cl"):
+                a = _abi.as_i32(j[key])
+                keep.append(a)
+                setattr(J[k], key, _abi.iptr(a))
+                setattr(J[k], "n_" + key, len(a))
+            J[k].mt_state = st.ctypes.data_as(C.POINTER(C.c_uint32))
+        R = (_abi.GcResult * n)()
+        E = (_abi.GcEvent * (n * event_cap))()
+        _abi.check(self._lib.phmc_gc_phase(self._h, n, J, R, E, event_cap))
+        return [(R[k].asdict(), [E[k * event_cap + i].asdict() for i in range(R[k].n_events)]) for k in range(n)]
+
     def set_state(self, st, replica=0):
         a = [_abi.as_f32(st[k]) for k in ("x", "y", "z", "q")] + [_abi.as_i32(st["type"]), _abi.as_i32(st["flags"])]
         _abi.check(self._lib.phmc_set_state(self._h, replica, *(_abi.fptr(v) for v in a[:4]), _abi.iptr(a[4]),

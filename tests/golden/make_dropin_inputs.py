@@ -3,6 +3,7 @@
 pool, and phase settings short enough for a test, so that the reference's own
 driver (MC/src/main.cu: protonation phase and phase-2 swaps) can run it both in
 its own build and linked against the engine's reference-API shim.
+dropin_gc.params runs the same system through a longer protonation phase.
 Usage: python tests/golden/make_dropin_inputs.py
 """
 import os
@@ -15,6 +16,8 @@ from ph_brush_b200 import configs  # noqa: E402
 
 PHASES = {"target_pct": "30", "rng_seed": "2025", "max_attempts": "1500", "patience": "400",
           "energy_interval": "100", "gc_block_fixed": "300", "sgmc_epoch_attempt_max": "1500", "phase2_wc": "yes"}
+# the same system with a protonation phase of many blocks and mu updates (dropin_gc.params)
+PHASES_GC = dict(PHASES, target_pct="35", gc_block_fixed="10", sgmc_epoch_attempt_max="40")
 
 
 def main():
@@ -23,6 +26,7 @@ def main():
     os.makedirs(os.path.join(HERE, "inputs"), exist_ok=True)
     configs.write_lammps_data(os.path.join(HERE, "inputs", "dropin_small.data"), s)
     configs.write_params_in(os.path.join(HERE, "inputs", "dropin_small.params"), p, 0.5, extra=PHASES)
+    configs.write_params_in(os.path.join(HERE, "inputs", "dropin_gc.params"), p, 0.5, extra=PHASES_GC)
 
 
 if __name__ == "__main__":

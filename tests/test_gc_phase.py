@@ -1,0 +1,236 @@
+"""The reference's grand-canonical mu-control phase (MC/src/mc.cu:320-548) on the
+device (phmc_gc_phase) and its report lines written from device event records.
+
+* CPU: the device's restatement of the reference's random stream (std::mt19937,
+  uniform_int_distribution<int>, uniform_real_distribution<float>; GCC 13
+  libstdc++) against libstdc++ itself, draw for draw, plus the generator's
+  stream format; the report formatter against the reference's statements.
+* GPU: the reference's own driver with its phase_gc_mu_control call renamed to
+  the device phase (oracle/_ref/MC_phmc_gc) against the reference's complete
+  build (oracle/_ref/MC_ref) on the same input and seed: every report line, the
+  [sgmc] lines of the device phase and the phase-2 lines that follow it (which
+  only agree if the device phase left the same atoms and generator state); and
+  through the Python handle: pools, energies and determinism.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from ph_brush_b200 import Engine, _abi, configs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MT_HEADER = os.path.join(ROOT, "ph_brush_b200", "csrc", "mt_std.cuh")
+
+MT_CHECK = r"""
+#include <cstdio>
+#include <random>
+#include <sstream>
+#include "mt_std.cuh"
+int main() {
+    long long bad = 0, n = 0;
+    for (unsigned seed : {2025u, 1u, 0u, 4294967295u, 12345u}) {
+        std::mt19937 g(seed);
+        MtState s;
+        mt_seed(s, seed);
+        for (int k = 0; k < 200000; ++k) {
+            if (k % 3 == 0) {
+                uint32_t m = 1 + (k * 2654435761u) % 5000;
+                if (k % 7 == 0) m = 1;
+                if (k % 11 == 0) m = 2000000000u;
+                std::uniform_int_distribution<int> d(0, (int)m - 1);
+                if (d(g) != mt_index(s, m)) ++bad;
+            } else {
+                std::uniform_real_distribution<float> u(0.0f, 1.0f);
+                if (u(g) != mt_unit_float(s)) ++bad;
+            }
+            ++n;
+        }
+        // the stream format: 624 words, then the position
+        std::stringstream ss;
+        ss << g;
+        MtState t;
+        for (int i = 0; i < 624; ++i) ss >> t.x[i];
+        ss >> t.p;
+        for (int i = 0; i < 624; ++i) bad += t.x[i] != s.x[i];
+        bad += t.p != s.p;
+    }
+    printf("%lld %lld\n", n, bad);
+    return 0;
+}
+"""
+
+
+def test_generator_restatement_matches_libstdcxx(tmp_path):
+    src = tmp_path / "mt_check.cpp"
+    src.write_text(MT_CHECK)
+    exe = tmp_path / "mt_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.dirname(MT_HEADER), "-o", str(exe), str(src)], check=True)
+    n, bad = map(int, subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split())
+    assert n == 1000000 and bad == 0
+
+
+def fmt(ev, res):
+    buf = __import__("ctypes").create_string_buffer(512)
+    n = _abi.lib().phmc_gc_event_format(ev, res, buf, 512)
+    assert n == len(buf.value)
+    return buf.value.decode()
+
+
+def f6(x):
+    return f"{float(np.float32(x)):.6f}"
+
+
+def test_report_lines_follow_the_reference_statements():
+    res = _abi.GcResult(Nh=40, target_count=12, R0=9, Nacc_target=1, epoch_attempt_max=1500, gc_block=300)
+    ev = _abi.GcEvent(kind=_abi.GC_EV_CHUNK, acc_since_mu=3, att_since_mu=300, acc_rate=np.float32(3 / 300),
+                      fwd_total=3, bwd_total=0, remaining=6)
+    assert fmt(ev, res) == (f"[sgmc] chunk acc=3/1 attempts=300 acc_rate={f6(3 / 300)} fwd_total=3 bwd_total=0 "
+                            "gc_block=300 remaining=6")
+    mu = np.float32(-0.8472979)
+    ev = _abi.GcEvent(kind=_abi.GC_EV_MU, epoch=0, cause_amax=0, mu_kT=mu, f=np.float32(0.175), acc_since_mu=3,
+                      att_since_mu=300, fwd_total=3, bwd_total=0, remaining=6, w_info=1.0)
+    assert fmt(ev, res) == (f"[sgmc] mu-update#1 cause=Nacc mu/kT={f6(mu)} f={f6(0.175)} acc=3/1 attempts=300/1500 "
+                            "fwd_total=3 bwd_total=0 remaining=6 R0=9 w_info=1.000000")
+    ev.cause_amax = 1
+    assert " cause=Amax " in fmt(ev, res)
+    E = np.float32(-1234.5678)
+    ev = _abi.GcEvent(kind=_abi.GC_EV_REACHED, epoch=2, step_in_block=17, nprot=12, mu_kT=mu, E=E, fwd_total=10,
+                      bwd_total=1)
+    assert fmt(ev, res) == (f"[sgmc] reached target in epoch=2 step_in_block=17 Nprot=12/40 mu/kT={f6(mu)} E={f6(E)} "
+                            "fwd_acc=10 bwd_acc=1 remaining=0")
+    ev = _abi.GcEvent(kind=_abi.GC_EV_NO_PAIRS)
+    assert fmt(ev, res) == "[sgmc] no valid pairs to flip; stop."
+    ev = _abi.GcEvent(kind=_abi.GC_EV_ALREADY, nprot=12, mu_kT=mu, E=E)
+    assert fmt(ev, res) == f"[sgmc] already at target: Nprot=12/40 target=12 mu/kT={f6(mu)} E={f6(E)} remaining=0"
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "MC_ref")
+GC_BIN = os.path.join(ROOT, "oracle", "_ref", "MC_phmc_gc")
+
+
+def run_driver(binary, workdir, params):
+    import shutil
+    inputs = os.path.join(ROOT, "tests", "golden", "inputs")
+    os.makedirs(workdir)
+    shutil.copy(os.path.join(inputs, "dropin_small.data"), os.path.join(workdir, "in.data"))
+    shutil.copy(os.path.join(inputs, params), os.path.join(workdir, "params.in"))
+    r = subprocess.run([binary, "in.data", "params.in"], cwd=workdir, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (binary, r.returncode, r.stderr[-500:])
+    return open(os.path.join(workdir, "report.txt")).read().splitlines()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("params,long_phase", [("dropin_small.params", False), ("dropin_gc.params", True)])
+def test_device_gc_phase_reproduces_the_reference_driver(tmp_path, params, long_phase):
+    if not (os.path.exists(REF_BIN) and os.path.exists(GC_BIN)):
+        pytest.skip("reference driver binaries not built (make -C oracle mc-ref dropin-gc, needs the reference sources)")
+    from test_dropin import RTOL, numbers
+    ref = run_driver(REF_BIN, str(tmp_path / "ref"), params)
+    got = run_driver(GC_BIN, str(tmp_path / "gc"), params)
+    assert len(ref) == len(got), (len(ref), len(got), ref[-5:], got[-5:])
+    sgmc = [line for line in got if line.startswith("[sgmc]")]
+    assert any("reached target" in line for line in sgmc), sgmc
+    if long_phase:  # chunk lines and mu updates of several epochs
+        assert sum("mu-update#" in line for line in sgmc) >= 2 and sum("chunk" in line for line in sgmc) >= 3, sgmc
+    for a, b in zip(ref, got):
+        if a == b:
+            continue
+        na, nb = numbers(a), numbers(b)
+        assert len(na) == len(nb) and re_words(a) == re_words(b), (a, b)
+        for x, y in zip(na, nb):
+            if not any(c in x + y for c in ".eE"):
+                assert x == y, (a, b)  # counts, steps, pools
+            else:
+                assert abs(float(x) - float(y)) <= RTOL * abs(float(x)) + 1e-3, (a, b)
+    assert any("[phase2]" in line and "accepted=" in line for line in got)
+
+
+def re_words(line):
+    import re
+    return re.sub(r"-?\d+(?:\.\d+)?(?:[eE][-+]?\d+)?", "#", line)
+
+
+def mt_seeded(seed):
+    """std::mt19937(seed)'s state words and position (Knuth's initialisation)."""
+    x = np.zeros(625, np.uint32)
+    v = seed & 0xFFFFFFFF
+    x[0] = v
+    for i in range(1, 624):
+        v = (1812433253 * (v ^ (v >> 30)) + i) & 0xFFFFFFFF
+        x[i] = v
+    x[624] = 624
+    return x
+
+
+NHN, NHP, W, CL = 3, 4, 6, 7  # the reference's types 4, 5, 7, 8, 0-based
+
+
+def gc_setup(seed=11, n_w=60, target_pct=60.0):
+    s0, _ = configs.small_system(seed=seed, chains=3, length=8, box_xy=12.0, height=12.0, salt_pairs=6)
+    s, p = configs.to_reference_semantics(s0, n_w=n_w, seed=seed)
+    t = s.type
+    sites = np.where((t == NHN) | (t == NHP))[0]
+    z_cut = float(np.max(s.z[sites])) + 1.0
+    pools = {"nh_n": np.where(t == NHN)[0], "nh_p": np.where(t == NHP)[0],
+             "w": np.where((t == W) & (s.z < z_cut))[0], "cl": np.where((t == CL) & (s.z < z_cut))[0]}
+    job = dict(replica=0, nh_n_type=NHN, nh_p_type=NHP, w_type=W, cl_type=CL, q_nh_p=1.0, q_cl=-1.0, beta=1.0,
+               target_pct=target_pct, gc_block=50, epoch_attempt_max=200, **pools)
+    return s, p, job
+
+
+@pytest.mark.gpu
+def test_gc_phase_through_the_python_handle():
+    s, p, job = gc_setup()
+    runs = []
+    for _ in range(2):
+        mt = mt_seeded(2025)
+        with Engine(s, p) as e:
+            (res, evs), = e.gc_phase([dict(job, mt_state=mt)])
+            st = e.state()
+            comp = e.energy()[0]
+        runs.append((res, evs, mt.copy(), st))
+        assert res["stop"] in (_abi.GC_STOP_REACHED, _abi.GC_STOP_ALREADY), res
+        assert res["reached_target"] == 1 and res["Nprot"] == res["target_count"]
+        Nh = len(job["nh_n"]) + len(job["nh_p"])
+        assert res["Nh"] == Nh and res["target_count"] == int(np.floor(np.float32(job["target_pct"]) / 100.0 * Nh))
+        # the engine's identities follow the accepted flips: protonated sites, and as many
+        # new Cl as net forward flips
+        t, q = st["type"], st["q"]
+        sites = np.concatenate([job["nh_n"], job["nh_p"]])
+        assert int(np.sum(t[sites] == NHP)) == res["Nprot"]
+        assert np.all(q[sites][t[sites] == NHP] == 1.0) and np.all(q[sites][t[sites] == NHN] == 0.0)
+        ions = np.concatenate([job["w"], job["cl"]])
+        assert int(np.sum(t[ions] == CL)) - len(job["cl"]) == res["accepted_forward"] - res["accepted_backward"]
+        assert res["accepted_forward"] - res["accepted_backward"] == res["Nprot"] - len(job["nh_p"])
+        # the phase's tracked energy (the reference's real) against a fresh recompute
+        e_ref = np.float32(comp["lj"]) + np.float32(comp["coul_real"] + comp["coul_recip"] + comp["self"] +
+                                                     comp["qcorr"] + comp["slab"])
+        assert abs(float(res["E"]) - float(e_ref)) <= 2e-5 * abs(float(e_ref)) + 1e-3, (res["E"], e_ref)
+        # events: one chunk line per completed block, the last one the target
+        kinds = [ev["kind"] for ev in evs]
+        assert kinds[-1] in (_abi.GC_EV_REACHED, _abi.GC_EV_ALREADY)
+        if kinds[-1] == _abi.GC_EV_REACHED:  # the block the target was reached in reports no chunk line
+            assert kinds.count(_abi.GC_EV_CHUNK) == (res["attempted"] - 1) // 50
+        assert res["attempted"] > 0 and not np.array_equal(mt, mt_seeded(2025))
+    # one block per job, no launch quorum: the phase is deterministic
+    (r0, e0, m0, s0), (r1, e1, m1, s1) = runs
+    assert r0 == r1 and e0 == e1 and np.array_equal(m0, m1)
+    assert np.array_equal(s0["type"], s1["type"]) and np.array_equal(s0["q"], s1["q"])
+
+
+@pytest.mark.gpu
+def test_gc_phase_rejects_bad_jobs():
+    s, p, job = gc_setup()
+    with Engine(s, p) as e:
+        bad = dict(job, mt_state=mt_seeded(1))
+        bad["w"] = np.concatenate([job["w"], job["nh_n"][:1]])  # a slot in two pools
+        with pytest.raises(_abi.PhmcError):
+            e.gc_phase([bad])
+        with pytest.raises(_abi.PhmcError):
+            e.gc_phase([dict(job, mt_state=mt_seeded(1), cl_type=99)])
