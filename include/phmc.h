@@ -506,6 +506,64 @@ typedef struct phmc_gc_result {
 /* events: n_jobs x event_cap records (job k at k * event_cap), or null. */
 int phmc_gc_phase(phmc_engine* e, int n_jobs, const phmc_gc_job* jobs, phmc_gc_result* results,
                   phmc_gc_event* events, int event_cap);
+
+/* ---- the reference's phase 2 (swap / jitter with patience) on the device ----
+ * Replaces phase2_swap_jitter (MC/include/mc.hpp:62-71, MC/src/mc.cu:159-318):
+ * four-point moves NH_P -> NH_N, NH_N -> NH_P, Cl -> W, W -> Cl (or, with no
+ * NH_N left or no four-point move possible, the Cl/W pair alone), plain
+ * Metropolis on the reference's float energies, a report line every
+ * energy_interval attempts, and a stop after patience attempts without a new
+ * best energy or after max_attempts.  A four-point move runs as two
+ * two-atom evaluations (the NH half applied, the Cl/W half judged with it in
+ * place; a rejection restores the NH half), so its energy change is the
+ * four-atom one.  The caller's generator, pools and event records work as for
+ * phmc_gc_phase; the W and Cl pools are the ones the reference keeps (below
+ * z_cut), z_cut itself only enters the pools line. */
+#define PHMC_P2_EV_POOLS 11         /* the pool sizes before the first attempt */
+#define PHMC_P2_EV_NONE_AT_START 12 /* neither a four-point nor a Cl/W move possible: the phase ends */
+#define PHMC_P2_EV_WC_EMPTY 13      /* Cl/W moves wanted, their pools empty: the phase ends */
+#define PHMC_P2_EV_NONE 14          /* no valid proposal at an attempt: the phase ends */
+#define PHMC_P2_EV_STEP 15          /* every energy_interval attempts */
+#define PHMC_P2_EV_PATIENCE 16      /* patience reached: the phase ends */
+#define PHMC_P2_STOP_PATIENCE 1
+#define PHMC_P2_STOP_MAX_ATTEMPTS 2
+#define PHMC_P2_STOP_NO_PROPOSALS 3
+typedef struct phmc_phase2_event {
+    int kind;                   /* PHMC_P2_EV_* */
+    int attempted, accepted;    /* STEP */
+    int since_best, patience;   /* STEP, PATIENCE */
+    int mode_wc;                /* STEP: 1 the last attempt was a Cl/W move, 0 a four-point move */
+    int n_nh_p, n_nh_n, n_cl, n_w;  /* POOLS */
+    float E, acc;               /* STEP: the phase's energy, accepted / attempted */
+    float z_cut;                /* POOLS */
+    int pad;
+} phmc_phase2_event;
+typedef struct phmc_phase2_job {
+    int replica;
+    int nh_n_type, nh_p_type, w_type, cl_type; /* engine types (0-based) */
+    float q_nh_p, q_cl;                        /* charges given to NH_P and Cl (the reference: +1, -1) */
+    double beta;
+    int max_attempts, patience, energy_interval;
+    float z_cut;                               /* reported with the pools */
+    const int* nh_p; int n_nh_p;               /* pools in the reference's order (slot indices) */
+    const int* nh_n; int n_nh_n;
+    const int* w; int n_w;                     /* W below z_cut */
+    const int* cl; int n_cl;                   /* Cl below z_cut */
+    uint32_t* mt_state;                        /* in / out: the caller's generator, 625 words */
+} phmc_phase2_job;
+typedef struct phmc_phase2_result {
+    int attempted, accepted;
+    float E, best_E;                           /* the reference's real */
+    int stop;                                  /* PHMC_P2_STOP_* (0: ended before the first attempt) */
+    int since_best;
+    int n_events, events_dropped;
+} phmc_phase2_result;
+int phmc_phase2(phmc_engine* e, int n_jobs, const phmc_phase2_job* jobs, phmc_phase2_result* results,
+                phmc_phase2_event* events, int event_cap);
+/* The reference's report line of a phase-2 event (MC/src/mc.cu:191-208, 219, 296-308,
+ * 310-312), fixed notation, precision 6 where the reference's stream carries no
+ * precision of its own, without the newline; returns the length. */
+int phmc_phase2_event_format(const phmc_phase2_event* ev, char* buf, int cap);
 /* The reference's report.txt line of an event (MC/src/mc.cu:367-373, 377, 461-474,
  * 506-516, 532-545), fixed notation at its precision 6, without the newline.
  * Returns the line's length (the line is cut at cap - 1 characters). */

@@ -161,6 +161,37 @@ class GcResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+P2_EV_POOLS, P2_EV_NONE_AT_START, P2_EV_WC_EMPTY, P2_EV_NONE, P2_EV_STEP, P2_EV_PATIENCE = 11, 12, 13, 14, 15, 16
+P2_STOP_PATIENCE, P2_STOP_MAX_ATTEMPTS, P2_STOP_NO_PROPOSALS = 1, 2, 3
+
+
+class Phase2Event(C.Structure):
+    _fields_ = [("kind", C.c_int), ("attempted", C.c_int), ("accepted", C.c_int), ("since_best", C.c_int),
+                ("patience", C.c_int), ("mode_wc", C.c_int), ("n_nh_p", C.c_int), ("n_nh_n", C.c_int),
+                ("n_cl", C.c_int), ("n_w", C.c_int), ("E", C.c_float), ("acc", C.c_float), ("z_cut", C.c_float),
+                ("pad", C.c_int)]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+class Phase2Job(C.Structure):
+    _fields_ = [("replica", C.c_int), ("nh_n_type", C.c_int), ("nh_p_type", C.c_int), ("w_type", C.c_int),
+                ("cl_type", C.c_int), ("q_nh_p", C.c_float), ("q_cl", C.c_float), ("beta", C.c_double),
+                ("max_attempts", C.c_int), ("patience", C.c_int), ("energy_interval", C.c_int), ("z_cut", C.c_float),
+                ("nh_p", _ip), ("n_nh_p", C.c_int), ("nh_n", _ip), ("n_nh_n", C.c_int),
+                ("w", _ip), ("n_w", C.c_int), ("cl", _ip), ("n_cl", C.c_int),
+                ("mt_state", C.POINTER(C.c_uint32))]
+
+
+class Phase2Result(C.Structure):
+    _fields_ = [("attempted", C.c_int), ("accepted", C.c_int), ("E", C.c_float), ("best_E", C.c_float),
+                ("stop", C.c_int), ("since_best", C.c_int), ("n_events", C.c_int), ("events_dropped", C.c_int)]
+
+    def asdict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
@@ -173,7 +204,7 @@ EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy",
            "phmc_harvest_count", "phmc_harvest_get", "phmc_surrogate_fit", "phmc_surrogate_attach",
            "phmc_get_da_stats", "phmc_surrogate_describe", "phmc_set_da_log", "phmc_set_move_mix",
            "phmc_set_tuning", "phmc_get_tuning", "phmc_autotune", "phmc_delta_energy_components",
-           "phmc_gc_phase", "phmc_gc_event_format"]
+           "phmc_gc_phase", "phmc_gc_event_format", "phmc_phase2", "phmc_phase2_event_format"]
 
 
 def load_library(path=LIB_PATH):
@@ -240,6 +271,9 @@ def load_library(path=LIB_PATH):
         "phmc_autotune": ([eng, C.c_int64, C.POINTER(Tuning), C.c_int, _ip], C.c_int),
         "phmc_gc_phase": ([eng, C.c_int, C.POINTER(GcJob), C.POINTER(GcResult), C.POINTER(GcEvent), C.c_int], C.c_int),
         "phmc_gc_event_format": ([C.POINTER(GcEvent), C.POINTER(GcResult), C.c_char_p, C.c_int], C.c_int),
+        "phmc_phase2": ([eng, C.c_int, C.POINTER(Phase2Job), C.POINTER(Phase2Result), C.POINTER(Phase2Event), C.c_int],
+                        C.c_int),
+        "phmc_phase2_event_format": ([C.POINTER(Phase2Event), C.c_char_p, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -35,6 +35,17 @@ struct GcDev {
     // the trial in flight
     int dir;                 // +1 forward, -1 backward
     long long s_before, s_after;
+    // phase 2 (MC/src/mc.cu:159-318): phase 1 = grand-canonical mu control, 2 = swaps with patience
+    int phase;
+    int role;                // 0 next attempt, 1 NH half of a four-point move (applied), 2 judged move, 3 NH half restored
+    int four;                // the current attempt is a four-point move
+    int prefer_wc;
+    int max_attempts, patience, energy_interval, since_best;
+    float best_E;
+    int iP, iN, jCl, jW;     // the attempt's atoms
+    int o_type[2];           // identities of iP, iN before the attempt
+    float o_q[2];
+    int stop_after_restore;  // phase ends once the NH half is restored
 };
 
 // Per-replica constant description (the ragged descriptor table).
@@ -174,7 +185,7 @@ struct DevPtrs {
     struct GcDev* gc;
     int* gc_pool;
     int gc_pool_stride;
-    phmc_gc_event* gc_ev;
+    unsigned char* gc_ev;  // event records of either phase (phmc_gc_event / phmc_phase2_event)
 };
 
 #define DSC_STRIDE (SUR_ROWS * SUR_K + 2 * SUR_ROWS + 4)

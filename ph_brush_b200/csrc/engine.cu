@@ -2,6 +2,7 @@
 // uploads, influence-kernel construction, the trial/rebuild loop and state
 // readback.  All entry points return a status code and never throw.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -59,7 +60,7 @@ struct phmc_engine {
     // grand-canonical phase: job states, pools, events (allocated on first use)
     GcDev* d_gc = nullptr;
     int* d_gc_pool = nullptr;
-    phmc_gc_event* d_gc_ev = nullptr;
+    unsigned char* d_gc_ev = nullptr;
 };
 
 static void drop_graph(phmc_engine* h) {
@@ -1113,10 +1114,12 @@ extern "C" int phmc_set_state(phmc_engine* h, int rep, const float* x, const flo
     return rc;
 }
 
-// ---- grand-canonical mu-control phase (MC/src/mc.cu:320-548) ----
+// ---- the reference's phases on the device: grand-canonical mu control (MC/src/mc.cu:320-548)
+// and swaps with patience (MC/src/mc.cu:159-318) ----
 
-#define GC_LAUNCH_TRIALS 2048                      // trials per MC launch at most
-#define GC_EV_CAP (2 * GC_LAUNCH_TRIALS + 4)       // events one launch can record (chunk + mu per trial)
+#define GC_LAUNCH_TRIALS 2048                      // two-atom evaluations per MC launch at most
+#define GC_EV_CAP (2 * GC_LAUNCH_TRIALS + 4)       // events one launch can record (two per evaluation)
+static_assert(sizeof(phmc_gc_event) <= GC_EV_BYTES && sizeof(phmc_phase2_event) <= GC_EV_BYTES, "event record size");
 
 static float gc_clampf(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
@@ -1125,6 +1128,99 @@ static float gc_clampf(float x, float lo, float hi) { return x < lo ? lo : (x > 
 static float gc_energy_real(const RepState& s, int coulomb) {
     const double ec = coulomb == PHMC_COUL_EWALD ? s.E_pair_c + s.E_rec + s.E_self + s.E_qcorr + s.E_slab : s.E_pair_c;
     return (float)s.E_pair_lj + (float)ec;
+}
+
+// Checks shared by both phases' jobs; fills the common part of the device state.
+static int gc_job_common(phmc_engine* h, int replica, std::vector<int>& seen, const int types[4], const uint32_t* mt,
+                         double beta, const int* const pools[4], const int npool[4], GcDev& g) {
+    Engine& E = h->E;
+    if (replica < 0 || replica >= E.R || seen[replica]++) return fail(PHMC_ERR_ARG, "job replicas must be distinct and in range");
+    const RepDesc& D = E.desc[replica];
+    for (int k = 0; k < 4; ++k)
+        if (types[k] < 0 || types[k] >= D.T) return fail(PHMC_ERR_ARG, "job type out of range");
+    if (!mt || mt[MT_N] > MT_N) return fail(PHMC_ERR_ARG, "job needs a generator state (624 words, position <= 624)");
+    if (!(beta > 0.0)) return fail(PHMC_ERR_ARG, "beta must be positive");
+    std::vector<int> flags((size_t)D.cap);
+    CU(cudaMemcpy(flags.data(), E.d.flags + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
+    std::vector<char> used((size_t)D.cap, 0);
+    for (int p = 0; p < 4; ++p) {
+        if (npool[p] < 0 || (npool[p] > 0 && !pools[p])) return fail(PHMC_ERR_ARG, "job pool pointer / size invalid");
+        for (int i = 0; i < npool[p]; ++i) {
+            const int v = pools[p][i];
+            if (v < 0 || v >= D.cap || used[(size_t)v]++) return fail(PHMC_ERR_ARG, "pool slots must be distinct and in range");
+            if (flags[(size_t)v] & PHMC_F_GHOST) return fail(PHMC_ERR_ARG, "pool slot is empty");
+        }
+    }
+    std::memset(&g, 0, sizeof g);
+    for (int i = 0; i < MT_N; ++i) g.mt.x[i] = mt[i];
+    g.mt.p = (int)mt[MT_N];
+    g.replica = replica;
+    for (int k = 0; k < 4; ++k) { g.type[k] = types[k]; g.n[k] = npool[k]; }
+    g.beta = (float)beta;
+    g.launch_cap = GC_LAUNCH_TRIALS;
+    g.ev_cap = GC_EV_CAP;
+    return PHMC_OK;
+}
+
+// Upload pools and job states, run MC launches (each followed by the potential-mesh
+// rebuild of its replicas) until every job has stopped, collect the event records
+// (ev_size bytes each) and return the final job states in G.
+static int gc_run(phmc_engine* h, std::vector<GcDev>& G, const std::vector<const int* const*>& pools,
+                  const std::vector<const int*>& npools, size_t ev_size, std::vector<std::vector<unsigned char>>& evs) {
+    Engine& E = h->E;
+    const int n_jobs = (int)G.size();
+    if (!h->d_gc) {
+        CU(cudaMalloc((void**)&h->d_gc, sizeof(GcDev) * E.R));
+        CU(cudaMalloc((void**)&h->d_gc_pool, sizeof(int) * 4 * (size_t)E.total_slots));
+        CU(cudaMalloc((void**)&h->d_gc_ev, (size_t)GC_EV_BYTES * GC_EV_CAP * E.R));
+    }
+    E.d.gc = h->d_gc; E.d.gc_pool = h->d_gc_pool; E.d.gc_pool_stride = E.total_slots; E.d.gc_ev = h->d_gc_ev;
+    for (int k = 0; k < n_jobs; ++k)
+        for (int p = 0; p < 4; ++p)
+            if (npools[k][p] > 0)
+                CU(cudaMemcpyAsync(h->d_gc_pool + (size_t)p * E.total_slots + E.desc[G[k].replica].slot_off, pools[k][p],
+                                   sizeof(int) * npools[k][p], cudaMemcpyHostToDevice, E.stream));
+    CU(cudaMemcpyAsync(h->d_gc, G.data(), sizeof(GcDev) * n_jobs, cudaMemcpyHostToDevice, E.stream));
+    std::vector<unsigned char> buf;
+    // every launch makes progress on each unfinished job (pending room for an attempt is
+    // always there at a launch's start), so the loop ends; the bound is a guard
+    const long long max_launches = 4LL * 1000000000LL + 8;
+    for (long long it = 0;; ++it) {
+        CU(launch_mc_gc(E, n_jobs, E.stream));
+        int s = flush_dirty(h);
+        if (s) return s;
+        CU(cudaMemcpyAsync(G.data(), h->d_gc, sizeof(GcDev) * n_jobs, cudaMemcpyDeviceToHost, E.stream));
+        s = check_kernel_errors(h);  // synchronises the stream
+        if (s) return s;
+        bool all = true;
+        for (int k = 0; k < n_jobs; ++k) {
+            if (G[k].n_ev > GC_EV_CAP) return fail(PHMC_ERR_CAPACITY, "device phase: event buffer overflow");
+            if (G[k].n_ev > 0) {
+                buf.resize((size_t)G[k].n_ev * ev_size);
+                CU(cudaMemcpy(buf.data(), h->d_gc_ev + (size_t)k * GC_EV_CAP * GC_EV_BYTES, buf.size(), cudaMemcpyDeviceToHost));
+                evs[k].insert(evs[k].end(), buf.begin(), buf.end());
+            }
+            all = all && G[k].stop != 0;
+        }
+        if (all) break;
+        if (it > max_launches) return fail(PHMC_ERR_BUDGET, "device phase made no progress");
+    }
+    return PHMC_OK;
+}
+
+template <class Ev>
+static void gc_host_event(std::vector<unsigned char>& out, const Ev& ev) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(&ev);
+    out.insert(out.end(), p, p + sizeof ev);
+}
+
+// Copy a job's collected events to the caller's records; returns (kept, dropped).
+template <class Ev>
+static std::pair<int, int> gc_events_out(const std::vector<unsigned char>& evs, Ev* out, int cap) {
+    const int n = (int)(evs.size() / sizeof(Ev));
+    const int kept = out ? std::min(n, cap) : 0;
+    if (kept > 0) std::memcpy(out, evs.data(), sizeof(Ev) * kept);
+    return {kept, n - kept};
 }
 
 extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs, phmc_gc_result* results,
@@ -1137,37 +1233,24 @@ extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs
     std::vector<RepState> st((size_t)E.R);
     CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
     std::vector<GcDev> G((size_t)n_jobs);
+    std::vector<const int* const*> pools((size_t)n_jobs);
+    std::vector<const int*> npools((size_t)n_jobs);
+    std::vector<std::array<const int*, 4>> pool_arr((size_t)n_jobs);
+    std::vector<std::array<int, 4>> npool_arr((size_t)n_jobs);
+    std::vector<std::vector<unsigned char>> evs((size_t)n_jobs);
     for (int k = 0; k < n_jobs; ++k) {
         const phmc_gc_job& J = jobs[k];
-        if (J.replica < 0 || J.replica >= E.R || seen[J.replica]++) return fail(PHMC_ERR_ARG, "job replicas must be distinct and in range");
-        const RepDesc& D = E.desc[J.replica];
-        for (int t : {J.nh_n_type, J.nh_p_type, J.w_type, J.cl_type})
-            if (t < 0 || t >= D.T) return fail(PHMC_ERR_ARG, "job type out of range");
-        if (!J.mt_state || J.mt_state[MT_N] > MT_N) return fail(PHMC_ERR_ARG, "job needs a generator state (624 words, position <= 624)");
-        if (!(J.beta > 0.0)) return fail(PHMC_ERR_ARG, "beta must be positive");
-        const int* pools[4] = {J.nh_n, J.nh_p, J.w, J.cl};
-        const int npool[4] = {J.n_nh_n, J.n_nh_p, J.n_w, J.n_cl};
-        std::vector<int> flags((size_t)D.cap);
-        CU(cudaMemcpy(flags.data(), E.d.flags + D.slot_off, sizeof(int) * D.cap, cudaMemcpyDeviceToHost));
-        std::vector<char> used((size_t)D.cap, 0);
-        for (int p = 0; p < 4; ++p) {
-            if (npool[p] < 0 || (npool[p] > 0 && !pools[p])) return fail(PHMC_ERR_ARG, "job pool pointer / size invalid");
-            for (int i = 0; i < npool[p]; ++i) {
-                const int v = pools[p][i];
-                if (v < 0 || v >= D.cap || used[v]++) return fail(PHMC_ERR_ARG, "pool slots must be distinct and in range");
-                if (flags[v] & PHMC_F_GHOST) return fail(PHMC_ERR_ARG, "pool slot is empty");
-            }
-        }
-        // settings derived as the reference derives them, in its real (MC/src/mc.cu:339-357)
+        pool_arr[k] = {J.nh_n, J.nh_p, J.w, J.cl};
+        npool_arr[k] = {J.n_nh_n, J.n_nh_p, J.n_w, J.n_cl};
+        pools[k] = pool_arr[k].data();
+        npools[k] = npool_arr[k].data();
+        const int types[4] = {J.nh_n_type, J.nh_p_type, J.w_type, J.cl_type};
         GcDev& g = G[k];
-        std::memset(&g, 0, sizeof g);
-        for (int i = 0; i < MT_N; ++i) g.mt.x[i] = J.mt_state[i];
-        g.mt.p = (int)J.mt_state[MT_N];
-        g.replica = J.replica;
-        g.type[GC_NHN] = J.nh_n_type; g.type[GC_NHP] = J.nh_p_type; g.type[GC_W] = J.w_type; g.type[GC_CL] = J.cl_type;
+        int s = gc_job_common(h, J.replica, seen, types, J.mt_state, J.beta, pools[k], npools[k], g);
+        if (s) return s;
+        // settings derived as the reference derives them, in its real (MC/src/mc.cu:339-357)
+        g.phase = 1;
         g.q_nhp = J.q_nh_p; g.q_cl = J.q_cl;
-        g.beta = (float)J.beta;
-        for (int p = 0; p < 4; ++p) g.n[p] = npool[p];
         g.Nh = J.n_nh_n + J.n_nh_p;
         g.Nprot = J.n_nh_p;
         const float pct = (float)J.target_pct;
@@ -1183,65 +1266,21 @@ extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs
         const float frac = J.nacc_frac > 0.0 ? (float)J.nacc_frac : 0.10f;
         g.nacc_target = std::max(1, (int)std::ceil((double)frac * (double)R0));
         g.eta = J.mu_eta > 0.0 ? (float)J.mu_eta : 0.3f;
-        g.E = gc_energy_real(st[(size_t)J.replica], D.coulomb);
+        g.E = gc_energy_real(st[(size_t)J.replica], E.desc[J.replica].coulomb);
         g.max_trials = (int)std::min<int64_t>(J.max_trials > 0 ? J.max_trials : 1000000000, 1000000000);
-        g.launch_cap = GC_LAUNCH_TRIALS;
-        g.ev_cap = GC_EV_CAP;
-        if (g.Nprot == g.target) g.stop = PHMC_GC_STOP_ALREADY;
+        if (g.Nprot == g.target) {
+            g.stop = PHMC_GC_STOP_ALREADY;
+            phmc_gc_event ev;
+            std::memset(&ev, 0, sizeof ev);
+            ev.kind = PHMC_GC_EV_ALREADY; ev.nprot = g.Nprot; ev.mu_kT = g.beta * g.mu; ev.E = g.E;
+            gc_host_event(evs[k], ev);
+        }
         phmc_gc_result& R = results[k];
         std::memset(&R, 0, sizeof R);
         R.R0 = R0; R.Nacc_target = g.nacc_target; R.epoch_attempt_max = g.amax; R.gc_block = g.gc_block;
     }
-    // device buffers on first use
-    if (!h->d_gc) {
-        CU(cudaMalloc((void**)&h->d_gc, sizeof(GcDev) * E.R));
-        CU(cudaMalloc((void**)&h->d_gc_pool, sizeof(int) * 4 * (size_t)E.total_slots));
-        CU(cudaMalloc((void**)&h->d_gc_ev, sizeof(phmc_gc_event) * GC_EV_CAP * (size_t)E.R));
-    }
-    E.d.gc = h->d_gc; E.d.gc_pool = h->d_gc_pool; E.d.gc_pool_stride = E.total_slots; E.d.gc_ev = h->d_gc_ev;
-    for (int k = 0; k < n_jobs; ++k) {
-        const phmc_gc_job& J = jobs[k];
-        const int* pools[4] = {J.nh_n, J.nh_p, J.w, J.cl};
-        const int npool[4] = {J.n_nh_n, J.n_nh_p, J.n_w, J.n_cl};
-        for (int p = 0; p < 4; ++p)
-            if (npool[p] > 0)
-                CU(cudaMemcpyAsync(h->d_gc_pool + (size_t)p * E.total_slots + E.desc[J.replica].slot_off, pools[p],
-                                   sizeof(int) * npool[p], cudaMemcpyHostToDevice, E.stream));
-    }
-    CU(cudaMemcpyAsync(h->d_gc, G.data(), sizeof(GcDev) * n_jobs, cudaMemcpyHostToDevice, E.stream));
-    // events kept on the host (the device buffer holds one launch's)
-    std::vector<std::vector<phmc_gc_event>> evs((size_t)n_jobs);
-    for (int k = 0; k < n_jobs; ++k)
-        if (G[k].stop == PHMC_GC_STOP_ALREADY) {
-            phmc_gc_event ev;
-            std::memset(&ev, 0, sizeof ev);
-            ev.kind = PHMC_GC_EV_ALREADY; ev.nprot = G[k].Nprot; ev.mu_kT = G[k].beta * G[k].mu; ev.E = G[k].E;
-            evs[k].push_back(ev);
-        }
-    std::vector<phmc_gc_event> evbuf;
-    // every launch runs at least pend_max / 2 trials of each unfinished job, so the loop ends
-    const long long max_launches = 2LL * 1000000000LL / std::max(1, E.pend_max / 2) + 8;
-    for (long long it = 0;; ++it) {
-        CU(launch_mc_gc(E, n_jobs, E.stream));
-        int s = flush_dirty(h);
-        if (s) return s;
-        CU(cudaMemcpyAsync(G.data(), h->d_gc, sizeof(GcDev) * n_jobs, cudaMemcpyDeviceToHost, E.stream));
-        s = check_kernel_errors(h);  // synchronises the stream
-        if (s) return s;
-        bool all = true;
-        for (int k = 0; k < n_jobs; ++k) {
-            const int n = std::min(G[k].n_ev, GC_EV_CAP);
-            if (n > 0) {
-                evbuf.resize((size_t)n);
-                CU(cudaMemcpy(evbuf.data(), h->d_gc_ev + (size_t)k * GC_EV_CAP, sizeof(phmc_gc_event) * n, cudaMemcpyDeviceToHost));
-                evs[k].insert(evs[k].end(), evbuf.begin(), evbuf.end());
-            }
-            if (G[k].n_ev > GC_EV_CAP) return fail(PHMC_ERR_CAPACITY, "grand-canonical phase: event buffer overflow");
-            all = all && G[k].stop != 0;
-        }
-        if (all) break;
-        if (it > max_launches) return fail(PHMC_ERR_BUDGET, "grand-canonical phase made no progress");
-    }
+    int s = gc_run(h, G, pools, npools, sizeof(phmc_gc_event), evs);
+    if (s) return s;
     for (int k = 0; k < n_jobs; ++k) {
         const GcDev& g = G[k];
         const phmc_gc_job& J = jobs[k];
@@ -1254,11 +1293,79 @@ extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs
         R.reached_target = (g.stop == PHMC_GC_STOP_REACHED || g.stop == PHMC_GC_STOP_ALREADY) ? 1 : 0;
         R.stop = g.stop;
         R.E = g.E; R.mu_eff = g.mu;
-        const int n = (int)evs[k].size();
-        const int kept = events ? std::min(n, event_cap) : 0;
-        for (int i = 0; i < kept; ++i) events[(size_t)k * event_cap + i] = evs[k][(size_t)i];
-        R.n_events = kept;
-        R.events_dropped = n - kept;
+        const auto ke = gc_events_out(evs[k], events ? events + (size_t)k * event_cap : nullptr, event_cap);
+        R.n_events = ke.first; R.events_dropped = ke.second;
+    }
+    return PHMC_OK;
+}
+
+extern "C" int phmc_phase2(phmc_engine* h, int n_jobs, const phmc_phase2_job* jobs, phmc_phase2_result* results,
+                           phmc_phase2_event* events, int event_cap) {
+    if (!h || n_jobs < 1 || !jobs || !results || event_cap < 0) return fail(PHMC_ERR_ARG, "invalid argument");
+    Engine& E = h->E;
+    if (n_jobs > E.R) return fail(PHMC_ERR_ARG, "more jobs than replicas");
+    CU(cudaSetDevice(E.device));
+    std::vector<int> seen((size_t)E.R, 0);
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    std::vector<GcDev> G((size_t)n_jobs);
+    std::vector<const int* const*> pools((size_t)n_jobs);
+    std::vector<const int*> npools((size_t)n_jobs);
+    std::vector<std::array<const int*, 4>> pool_arr((size_t)n_jobs);
+    std::vector<std::array<int, 4>> npool_arr((size_t)n_jobs);
+    std::vector<std::vector<unsigned char>> evs((size_t)n_jobs);
+    for (int k = 0; k < n_jobs; ++k) {
+        const phmc_phase2_job& J = jobs[k];
+        pool_arr[k] = {J.nh_n, J.nh_p, J.w, J.cl};
+        npool_arr[k] = {J.n_nh_n, J.n_nh_p, J.n_w, J.n_cl};
+        pools[k] = pool_arr[k].data();
+        npools[k] = npool_arr[k].data();
+        const int types[4] = {J.nh_n_type, J.nh_p_type, J.w_type, J.cl_type};
+        GcDev& g = G[k];
+        int s = gc_job_common(h, J.replica, seen, types, J.mt_state, J.beta, pools[k], npools[k], g);
+        if (s) return s;
+        g.phase = 2;
+        g.q_nhp = J.q_nh_p; g.q_cl = J.q_cl;
+        g.max_attempts = std::max(0, J.max_attempts);
+        g.patience = J.patience;
+        g.energy_interval = J.energy_interval;
+        g.E = gc_energy_real(st[(size_t)J.replica], E.desc[J.replica].coulomb);
+        g.best_E = g.E;
+        // the pools line and the checks before the first attempt (MC/src/mc.cu:185-208)
+        phmc_phase2_event ev;
+        std::memset(&ev, 0, sizeof ev);
+        ev.kind = PHMC_P2_EV_POOLS;
+        ev.n_nh_p = J.n_nh_p; ev.n_nh_n = J.n_nh_n; ev.n_cl = J.n_cl; ev.n_w = J.n_w; ev.z_cut = J.z_cut;
+        gc_host_event(evs[k], ev);
+        const bool can_wc = J.n_w > 0 && J.n_cl > 0;
+        const bool can_four = can_wc && J.n_nh_p > 0 && J.n_nh_n > 0;
+        g.prefer_wc = J.n_nh_n == 0;
+        if (!g.prefer_wc && !can_four && can_wc) g.prefer_wc = 1;
+        int pre = 0;
+        if (!g.prefer_wc && !can_four && !can_wc) pre = PHMC_P2_EV_NONE_AT_START;
+        else if (g.prefer_wc && !can_wc) pre = PHMC_P2_EV_WC_EMPTY;
+        if (pre) {
+            std::memset(&ev, 0, sizeof ev);
+            ev.kind = pre;
+            gc_host_event(evs[k], ev);
+            g.stop = PHMC_P2_STOP_NO_PROPOSALS;
+        }
+    }
+    int s = gc_run(h, G, pools, npools, sizeof(phmc_phase2_event), evs);
+    if (s) return s;
+    for (int k = 0; k < n_jobs; ++k) {
+        const GcDev& g = G[k];
+        const phmc_phase2_job& J = jobs[k];
+        for (int i = 0; i < MT_N; ++i) J.mt_state[i] = g.mt.x[i];
+        J.mt_state[MT_N] = (uint32_t)g.mt.p;
+        phmc_phase2_result& R = results[k];
+        std::memset(&R, 0, sizeof R);
+        R.attempted = g.attempted; R.accepted = g.accepted;
+        R.E = g.E; R.best_E = g.best_E;
+        R.stop = g.attempted > 0 || g.stop != PHMC_P2_STOP_NO_PROPOSALS ? g.stop : 0;
+        R.since_best = g.since_best;
+        const auto ke = gc_events_out(evs[k], events ? events + (size_t)k * event_cap : nullptr, event_cap);
+        R.n_events = ke.first; R.events_dropped = ke.second;
     }
     return PHMC_OK;
 }

@@ -87,5 +87,6 @@ int sur_train_device(phmc_surrogate* h, const float* d_x, const float* d_sign, c
 enum { MC_RUN = 0, MC_EVAL = 1, MC_APPLY = 2, MC_DESCRIBE = 3, MC_GC = 4 };
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* d_trials, int n, double* d_dE, cudaStream_t st);
 cudaError_t prepare_mc(Engine& E);
+#define GC_EV_BYTES 80  // bytes of one event record of either device phase
 cudaError_t launch_mc_gc(Engine& E, int n_jobs, cudaStream_t st);  // grand-canonical phase: one block per job
 size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate = false, bool two_buffers = false);

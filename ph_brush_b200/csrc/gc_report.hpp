@@ -1,10 +1,14 @@
-// report.txt lines of the grand-canonical mu-control phase, written from the
-// device's event records (phmc_gc_event) exactly as the reference's statements
-// write them into its report stream (MC/src/mc.cu:367-373 already at target,
-// :377 no valid pairs, :461-474 reached target, :506-516 chunk, :532-545 mu
-// update): the same text, the same stream manipulators (precision 6 where the
-// reference sets it, the stream's own precision where it does not), one line per
-// event ended by std::endl.  Host C++ only.
+// report.txt lines of the reference's phases run on the device, written from the
+// device's event records exactly as the reference's statements write them into
+// its report stream: the same text, the same stream manipulators (the precision
+// the reference sets, the stream's own precision where it sets none) and the same
+// line ends (std::endl or a newline).
+//   grand-canonical mu control (phmc_gc_event): MC/src/mc.cu:367-373 already at
+//   target, :377 no valid pairs, :461-474 reached target, :506-516 chunk, :532-545
+//   mu update;
+//   phase 2 (phmc_phase2_event): MC/src/mc.cu:185-189 pools, :200-206 no proposals
+//   before the first attempt, :214 no proposals, :296-308 step, :310-312 patience.
+// Host C++ only.
 #pragma once
 #include <algorithm>
 #include <iomanip>
@@ -37,6 +41,35 @@ void phmc_gc_write_event(OS& os, const phmc_gc_event& e, const phmc_gc_result& r
                << " attempts=" << e.att_since_mu << "/" << r.epoch_attempt_max << " fwd_total=" << e.fwd_total
                << " bwd_total=" << e.bwd_total << " remaining=" << e.remaining << " R0=" << r.R0 << " w_info=" << e.w_info
                << std::endl;
+            break;
+        default:
+            break;
+    }
+}
+
+template <class OS>
+void phmc_p2_write_event(OS& os, const phmc_phase2_event& e) {
+    switch (e.kind) {
+        case PHMC_P2_EV_POOLS:
+            os << "[phase2] pools: NH_P=" << e.n_nh_p << " NH_N=" << e.n_nh_n << " Cl=" << e.n_cl << " W=" << e.n_w
+               << " (z_cut=" << e.z_cut << ")\n";
+            break;
+        case PHMC_P2_EV_NONE_AT_START:
+            os << "[phase2] no valid proposals (no 4-pt and no wc-only). Stop.\n";
+            break;
+        case PHMC_P2_EV_WC_EMPTY:
+            os << "[phase2] wc-only requested but pools empty; Stop.\n";
+            break;
+        case PHMC_P2_EV_NONE:
+            os << "[phase2] no valid proposals; Stop.\n";
+            break;
+        case PHMC_P2_EV_STEP:
+            os << std::setprecision(6) << "[phase2] step=" << e.attempted << " E=" << e.E << " accepted=" << e.accepted
+               << " acc=" << std::setprecision(3) << e.acc << " since_best=" << e.since_best << "/" << e.patience
+               << (e.mode_wc ? " mode=wc-only\n" : " mode=4-pt\n");
+            break;
+        case PHMC_P2_EV_PATIENCE:
+            os << "[phase2] patience reached: " << e.since_best << "/" << e.patience << ". Stop.\n";
             break;
         default:
             break;

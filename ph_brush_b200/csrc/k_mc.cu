@@ -417,9 +417,10 @@ __device__ __forceinline__ int* gc_pool(const DevPtrs& d, const RepDesc& D, int 
     return d.gc_pool + (size_t)k * d.gc_pool_stride + D.slot_off;
 }
 
-__device__ void gc_event(GcDev& G, const DevPtrs& d, const phmc_gc_event& ev) {
+template <class Ev>
+__device__ void gc_event(GcDev& G, const DevPtrs& d, const Ev& ev) {
     const int k = G.n_ev++;
-    if (k < G.ev_cap) d.gc_ev[(size_t)blockIdx.x * G.ev_cap + k] = ev;
+    if (k < G.ev_cap) reinterpret_cast<Ev*>(d.gc_ev + (size_t)blockIdx.x * G.ev_cap * GC_EV_BYTES)[k] = ev;
 }
 
 __device__ __forceinline__ phmc_gc_event gc_event_base(const GcDev& G, int kind) {
@@ -567,6 +568,130 @@ __device__ void gc_pool_move(int* src, int* dst, int& n_src, int& n_dst, int v, 
     __syncthreads();
 }
 
+// ---- the reference's phase 2: swaps with patience (MC/src/mc.cu:159-318) ----
+
+__device__ __forceinline__ void p2_change(TrialS& T, const DevPtrs& d, const RepDesc& D, int k, int slot, int type, float q) {
+    const int so = D.slot_off;
+    T.idx[k] = slot;
+    T.fo[k] = d.flags[so + slot];
+    T.pres_old[k] = 1; T.pres_new[k] = 1;
+    T.po[k] = d.posq[so + slot]; T.to[k] = d.type[so + slot]; T.bonds[k] = d.bonds[so + slot];
+    T.pn[k] = T.po[k]; T.pn[k].w = q; T.tn[k] = type;
+}
+
+// Next two-atom evaluation of phase 2 (one thread).  An attempt draws its atoms in the
+// reference's order (NH_P, NH_N, Cl, W; or Cl, W) and starts with the NH half of a
+// four-point move, or is a Cl/W move; the Cl/W half follows; a rejected four-point
+// move ends with the NH half restored.  Attempts start only with room for all of their
+// pending stencils, so a launch never ends inside one.
+__device__ void p2_propose(TrialS& T, GcDev& G, const RepDesc& D, const DevPtrs& d, int npend, int pend_max, int& launch_trials) {
+    T.move = PHMC_MOVE_NONE; T.skip = 0; T.nch = 2; T.logf = 0.0; T.tnum = G.attempted;
+    if (G.role == 1) {  // the Cl/W half, judged with the NH half in place
+        p2_change(T, d, D, 0, G.jCl, G.type[GC_W], 0.0f);
+        p2_change(T, d, D, 1, G.jW, G.type[GC_CL], G.q_cl);
+        G.role = 2; ++launch_trials;
+        return;
+    }
+    if (G.role == 3) {  // restore the NH half of the rejected move
+        p2_change(T, d, D, 0, G.iP, G.o_type[0], G.o_q[0]);
+        p2_change(T, d, D, 1, G.iN, G.o_type[1], G.o_q[1]);
+        ++launch_trials;
+        return;
+    }
+    if (G.stop || launch_trials >= G.launch_cap) { T.stop = 1; return; }
+    if (G.attempted >= G.max_attempts) { G.stop = PHMC_P2_STOP_MAX_ATTEMPTS; T.stop = 1; return; }
+    const bool can_wc = G.n[GC_W] > 0 && G.n[GC_CL] > 0;
+    const bool four = !G.prefer_wc && can_wc && G.n[GC_NHP] > 0 && G.n[GC_NHN] > 0;
+    const bool wc = G.prefer_wc || (!four && can_wc);
+    if (!four && !wc) {
+        phmc_phase2_event ev;
+        memset(&ev, 0, sizeof ev);
+        ev.kind = PHMC_P2_EV_NONE;
+        gc_event(G, d, ev);
+        G.stop = PHMC_P2_STOP_NO_PROPOSALS; T.stop = 1;
+        return;
+    }
+    if (npend + (four ? 6 : 2) > pend_max) { T.stop = 1; return; }
+    G.attempted++;
+    G.four = four ? 1 : 0;
+    const int so = D.slot_off;
+    if (four) {
+        G.iP = gc_pool(d, D, GC_NHP)[mt_index(G.mt, (uint32_t)G.n[GC_NHP])];
+        G.iN = gc_pool(d, D, GC_NHN)[mt_index(G.mt, (uint32_t)G.n[GC_NHN])];
+        G.jCl = gc_pool(d, D, GC_CL)[mt_index(G.mt, (uint32_t)G.n[GC_CL])];
+        G.jW = gc_pool(d, D, GC_W)[mt_index(G.mt, (uint32_t)G.n[GC_W])];
+        G.o_type[0] = d.type[so + G.iP]; G.o_q[0] = d.posq[so + G.iP].w;
+        G.o_type[1] = d.type[so + G.iN]; G.o_q[1] = d.posq[so + G.iN].w;
+        p2_change(T, d, D, 0, G.iP, G.type[GC_NHN], 0.0f);
+        p2_change(T, d, D, 1, G.iN, G.type[GC_NHP], G.q_nhp);
+        G.role = 1;
+    } else {
+        G.jCl = gc_pool(d, D, GC_CL)[mt_index(G.mt, (uint32_t)G.n[GC_CL])];
+        G.jW = gc_pool(d, D, GC_W)[mt_index(G.mt, (uint32_t)G.n[GC_W])];
+        p2_change(T, d, D, 0, G.jCl, G.type[GC_W], 0.0f);
+        p2_change(T, d, D, 1, G.jW, G.type[GC_CL], G.q_cl);
+        G.role = 2;
+    }
+    ++launch_trials;
+}
+
+// Decision of a phase-2 evaluation (one thread).  The NH half and its restoration are
+// applied unconditionally; the judged move follows the reference (MC/src/mc.cu:241-293):
+// dE from the reference's float energies, accepted if dE <= 0 or exp(clamp(-beta dE))
+// beats a uniform draw; then the best-energy / patience bookkeeping and the report line.
+// Returns the decision; *pool_ops gets 2 (four-point pools), 3 (Cl/W pools) or 0.
+__device__ int p2_decide(GcDev& G, const RepDesc& D, const RepState& S, const DevPtrs& d, double dlj, double dc, double drec,
+                         double dself, double dqc, double dslab, int* pool_ops) {
+    *pool_ops = 0;
+    if (G.role == 1) return 1;  // the NH half: applied, judged with the Cl/W half
+    if (G.role == 3) {          // restored
+        G.role = 0;
+        if (G.stop_after_restore) G.stop = G.stop_after_restore;
+        return 1;
+    }
+    const double lj = S.E_pair_lj + dlj;
+    const double ec = D.coulomb == PHMC_COUL_EWALD
+                          ? (S.E_pair_c + dc) + (S.E_rec + drec) + (S.E_self + dself) + (S.E_qcorr + dqc) + (S.E_slab + dslab)
+                          : S.E_pair_c + dc;
+    const float Et = __fadd_rn(__double2float_rn(lj), __double2float_rn(ec));
+    const float dEf = __fsub_rn(Et, G.E);
+    float expo = __fmul_rn(-G.beta, dEf);
+    expo = expo < -40.0f ? -40.0f : (expo > 40.0f ? 40.0f : expo);
+    const int accept = (dEf <= 0.0f) || ((float)exp((double)expo) > mt_unit_float(G.mt));
+    if (accept) {
+        G.accepted++;
+        G.E = Et;
+        if (G.E < __fsub_rn(G.best_E, 1e-9f)) { G.best_E = G.E; G.since_best = 0; }
+        else ++G.since_best;
+        *pool_ops = G.four ? 2 : 3;
+        G.role = 0;
+    } else {
+        ++G.since_best;
+        G.role = G.four ? 3 : 0;
+    }
+    if (G.attempted % max(1, G.energy_interval) == 0) {
+        phmc_phase2_event ev;
+        memset(&ev, 0, sizeof ev);
+        ev.kind = PHMC_P2_EV_STEP;
+        ev.attempted = G.attempted; ev.accepted = G.accepted;
+        ev.since_best = G.since_best; ev.patience = G.patience;
+        ev.mode_wc = G.four ? 0 : 1;
+        ev.E = G.E;
+        ev.acc = G.attempted > 0 ? __fdiv_rn((float)G.accepted, (float)G.attempted) : 0.0f;
+        gc_event(G, d, ev);
+    }
+    if (G.since_best >= G.patience) {
+        phmc_phase2_event ev;
+        memset(&ev, 0, sizeof ev);
+        ev.kind = PHMC_P2_EV_PATIENCE;
+        ev.since_best = G.since_best; ev.patience = G.patience;
+        gc_event(G, d, ev);
+        if (G.role == 3) G.stop_after_restore = PHMC_P2_STOP_PATIENCE;  // the rejected move is undone first
+        else G.stop = PHMC_P2_STOP_PATIENCE;
+    }
+    return accept;
+}
+
 __device__ __forceinline__ void cls_add(const DevPtrs& d, const RepDesc& D, int cell, int cls, int delta) {
     if (cls >= 0 && cell >= 0) reinterpret_cast<int*>(d.cell_cls + D.cell_off + cell)[cls] += delta;
 }
@@ -694,7 +819,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 T.stop = 0; T.desc = 0; T.da = 0;
                 if (S.error) T.stop = 1;
                 else if (GC) {
-                    if constexpr (GC) gc_propose(T, sG, D, d, s_npend, pend_max, s_gc_lt);
+                    if constexpr (GC) {
+                        if (sG.phase == 2) p2_propose(T, sG, D, d, s_npend, pend_max, s_gc_lt);
+                        else gc_propose(T, sG, D, d, s_npend, pend_max, s_gc_lt);
+                    }
                 } else if (mode == MC_RUN) {
                     if (S.trial >= S.target) { T.stop = 1; S.stop_reason = 0; }
                     else if (s_npend + 2 > pend_max) {
@@ -1234,8 +1362,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             int accept = 0;
             if (GC) {
                 if constexpr (GC) {
-                    accept = gc_decide(sG, D, S, d, dlj, dc, acc_rec, dself, dqc, dslab);
-                    s_gc_ops = accept;
+                    if (sG.phase == 2) {
+                        int ops = 0;
+                        accept = p2_decide(sG, D, S, d, dlj, dc, acc_rec, dself, dqc, dslab, &ops);
+                        s_gc_ops = ops;
+                    } else {
+                        accept = gc_decide(sG, D, S, d, dlj, dc, acc_rec, dself, dqc, dslab);
+                        s_gc_ops = accept;
+                    }
                 }
             } else if (mode == MC_RUN) {
                 const long long li = T.tnum - S.run_start;
@@ -1372,12 +1506,22 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         }
         __syncthreads();
         if constexpr (GC) {
-            if (s_gc_ops) {  // the accepted flip's pool updates (MC/src/mc.cu:446-458)
+            const int ops = s_gc_ops;
+            if (ops == 1) {  // the accepted flip's pool updates (MC/src/mc.cu:446-458)
                 const bool fwd = sG.dir > 0;
                 const int ka = fwd ? GC_NHN : GC_NHP, kb = fwd ? GC_NHP : GC_NHN;
                 const int kc = fwd ? GC_W : GC_CL, kd = fwd ? GC_CL : GC_W;
                 gc_pool_move<NT>(gc_pool(d, D, ka), gc_pool(d, D, kb), sG.n[ka], sG.n[kb], T.idx[0], &s_gc_find);
                 gc_pool_move<NT>(gc_pool(d, D, kc), gc_pool(d, D, kd), sG.n[kc], sG.n[kd], T.idx[1], &s_gc_find);
+            } else if (ops >= 2) {  // phase 2's accepted move (MC/src/mc.cu:252-256, 286-287)
+                if (ops == 2) {
+                    gc_pool_move<NT>(gc_pool(d, D, GC_NHP), gc_pool(d, D, GC_NHN), sG.n[GC_NHP], sG.n[GC_NHN], sG.iP, &s_gc_find);
+                    gc_pool_move<NT>(gc_pool(d, D, GC_NHN), gc_pool(d, D, GC_NHP), sG.n[GC_NHN], sG.n[GC_NHP], sG.iN, &s_gc_find);
+                }
+                gc_pool_move<NT>(gc_pool(d, D, GC_CL), gc_pool(d, D, GC_W), sG.n[GC_CL], sG.n[GC_W], sG.jCl, &s_gc_find);
+                gc_pool_move<NT>(gc_pool(d, D, GC_W), gc_pool(d, D, GC_CL), sG.n[GC_W], sG.n[GC_CL], sG.jW, &s_gc_find);
+            }
+            if (ops) {
                 if (tid == 0) s_gc_ops = 0;
                 __syncthreads();
             }

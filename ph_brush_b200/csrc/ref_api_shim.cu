@@ -448,50 +448,20 @@ real pmeEnergy(PMEPlan& plan, const DeviceAtoms& atoms, const DeviceCSR&, const 
 // arguments, results, report lines and generator stream, run by phmc_gc_phase in
 // persistent MC-kernel launches instead of one host round trip per trial.  A driver
 // calls it in place of phase_gc_mu_control (MC/src/main.cu:190).
-PhaseGCResult phmc_ref_phase_gc_mu_control(System& sys, DeviceAtoms& d_atoms, const DeviceParams& d_params,
-                                           const DeviceCSR&, const Box& box, PMEPlan*, Params& p, const MCPlan& mcplan,
-                                           std::mt19937& rng, Phase1Result* seed_out) {
-    // the engine takes the atoms' current state
+namespace {
+
+// The engine takes the atoms' current state (a device phase starts from it).
+void adopt_atoms(const DeviceAtoms& d_atoms, const DeviceParams& d_params, const Box& box) {
     ensure_engine(d_atoms, d_params, box);
     upload_state(d_atoms);
     ck(phmc_energy(g.eng, &g.base), "phmc_energy");
     mirror(d_atoms);
     g.cur = g.base;
     g.last_n = 0;
-    // pools as the reference builds them (MC/src/mc.cu:332-342)
-    std::vector<int> nh_n = mcplan.idx_nh_n, nh_p = mcplan.idx_nh_p, w = mcplan.idx_w, cl;
-    for (int j = 0; j < sys.natoms; ++j)
-        if (sys.atoms[j].type == p.Cl_type && sys.atoms[j].z < mcplan.z_cut) cl.push_back(j);
-    // the generator's state words and position, in its stream format
-    std::vector<uint32_t> mt(625);
-    {
-        std::stringstream ss;
-        ss << rng;
-        for (uint32_t& v : mt) { unsigned long x = 0; ss >> x; v = (uint32_t)x; }
-    }
-    phmc_gc_job J;
-    std::memset(&J, 0, sizeof J);
-    J.replica = 0;
-    J.nh_n_type = p.NH_N_type - 1; J.nh_p_type = p.NH_P_type - 1; J.w_type = p.W_type - 1; J.cl_type = p.Cl_type - 1;
-    J.q_nh_p = 1.0f; J.q_cl = -1.0f;
-    J.beta = p.beta; J.target_pct = p.target_protonation_pct; J.mu_eta = p.mu_eta; J.nacc_frac = p.sgmc_nacc_frac_round;
-    J.gc_block = p.gc_block_fixed; J.epoch_attempt_max = p.sgmc_epoch_attempt_max;
-    J.nh_n = nh_n.data(); J.n_nh_n = (int)nh_n.size();
-    J.nh_p = nh_p.data(); J.n_nh_p = (int)nh_p.size();
-    J.w = w.data(); J.n_w = (int)w.size();
-    J.cl = cl.data(); J.n_cl = (int)cl.size();
-    J.mt_state = mt.data();
-    phmc_gc_result R;
-    std::vector<phmc_gc_event> ev((size_t)1 << 16);
-    ck(phmc_gc_phase(g.eng, 1, &J, &R, ev.data(), (int)ev.size()), "phmc_gc_phase");
-    {
-        std::stringstream ss;
-        for (uint32_t v : mt) ss << v << ' ';
-        ss >> rng;
-    }
-    for (int i = 0; i < R.n_events; ++i) phmc_gc_write_event(mc_report(), ev[(size_t)i], R);
-    if (R.events_dropped > 0) mc_report() << "[sgmc] " << R.events_dropped << " further report lines not kept" << std::endl;
-    // the atoms take the engine's identities
+}
+
+// The atoms take the engine's identities after a device phase (host mirror and device arrays).
+void take_identities(System& sys, DeviceAtoms& d_atoms) {
     std::vector<float> q((size_t)g.n);
     std::vector<int> t((size_t)g.n);
     ck(phmc_get_state(g.eng, 0, nullptr, nullptr, nullptr, q.data(), t.data(), nullptr), "phmc_get_state");
@@ -509,6 +479,52 @@ PhaseGCResult phmc_ref_phase_gc_mu_control(System& sys, DeviceAtoms& d_atoms, co
     ck(phmc_energy(g.eng, &g.base), "phmc_energy");
     g.cur = g.base;
     g.last_n = 0;
+}
+
+// std::mt19937's state words and position in its stream format, and back.
+std::vector<uint32_t> rng_words(const std::mt19937& rng) {
+    std::vector<uint32_t> mt(625);
+    std::stringstream ss;
+    ss << rng;
+    for (uint32_t& v : mt) { unsigned long x = 0; ss >> x; v = (uint32_t)x; }
+    return mt;
+}
+void rng_set(std::mt19937& rng, const std::vector<uint32_t>& mt) {
+    std::stringstream ss;
+    for (uint32_t v : mt) ss << v << ' ';
+    ss >> rng;
+}
+
+}  // namespace
+
+PhaseGCResult phmc_ref_phase_gc_mu_control(System& sys, DeviceAtoms& d_atoms, const DeviceParams& d_params,
+                                           const DeviceCSR&, const Box& box, PMEPlan*, Params& p, const MCPlan& mcplan,
+                                           std::mt19937& rng, Phase1Result* seed_out) {
+    adopt_atoms(d_atoms, d_params, box);
+    // pools as the reference builds them (MC/src/mc.cu:332-342)
+    std::vector<int> nh_n = mcplan.idx_nh_n, nh_p = mcplan.idx_nh_p, w = mcplan.idx_w, cl;
+    for (int j = 0; j < sys.natoms; ++j)
+        if (sys.atoms[j].type == p.Cl_type && sys.atoms[j].z < mcplan.z_cut) cl.push_back(j);
+    std::vector<uint32_t> mt = rng_words(rng);
+    phmc_gc_job J;
+    std::memset(&J, 0, sizeof J);
+    J.replica = 0;
+    J.nh_n_type = p.NH_N_type - 1; J.nh_p_type = p.NH_P_type - 1; J.w_type = p.W_type - 1; J.cl_type = p.Cl_type - 1;
+    J.q_nh_p = 1.0f; J.q_cl = -1.0f;
+    J.beta = p.beta; J.target_pct = p.target_protonation_pct; J.mu_eta = p.mu_eta; J.nacc_frac = p.sgmc_nacc_frac_round;
+    J.gc_block = p.gc_block_fixed; J.epoch_attempt_max = p.sgmc_epoch_attempt_max;
+    J.nh_n = nh_n.data(); J.n_nh_n = (int)nh_n.size();
+    J.nh_p = nh_p.data(); J.n_nh_p = (int)nh_p.size();
+    J.w = w.data(); J.n_w = (int)w.size();
+    J.cl = cl.data(); J.n_cl = (int)cl.size();
+    J.mt_state = mt.data();
+    phmc_gc_result R;
+    std::vector<phmc_gc_event> ev((size_t)1 << 16);
+    ck(phmc_gc_phase(g.eng, 1, &J, &R, ev.data(), (int)ev.size()), "phmc_gc_phase");
+    rng_set(rng, mt);
+    for (int i = 0; i < R.n_events; ++i) phmc_gc_write_event(mc_report(), ev[(size_t)i], R);
+    if (R.events_dropped > 0) mc_report() << "[sgmc] " << R.events_dropped << " further report lines not kept" << std::endl;
+    take_identities(sys, d_atoms);
     PhaseGCResult out;
     out.attempted = R.attempted; out.accepted = R.accepted;
     out.accepted_forward = R.accepted_forward; out.accepted_backward = R.accepted_backward;
@@ -531,5 +547,50 @@ PhaseGCResult phmc_ref_phase_gc_mu_control(System& sys, DeviceAtoms& d_atoms, co
         }
         seed_out->E = out.E;
     }
+    return out;
+}
+
+// phase2_swap_jitter (MC/include/mc.hpp:62-71, MC/src/mc.cu:159-318) with the same
+// arguments, result, report lines and generator stream, run by phmc_phase2.  A driver
+// calls it in place of phase2_swap_jitter (MC/src/main.cu:201).
+Phase2Result phmc_ref_phase2_swap_jitter(System& sys, DeviceAtoms& d_atoms, const DeviceParams& d_params, const DeviceCSR&,
+                                         const Box& box, PMEPlan*, const Params& p, const MCPlan& mcplan,
+                                         const Phase1Result& ph1, std::mt19937& rng) {
+    adopt_atoms(d_atoms, d_params, box);
+    // pools as the reference keeps them (MC/src/mc.cu:173-183)
+    std::vector<int> nh_p = ph1.nh_p_mc, nh_n = ph1.nh_n_remaining, w = ph1.w_remaining, cl = ph1.cl_mc;
+    auto under_z = [&](std::vector<int>& pool) {
+        pool.erase(std::remove_if(pool.begin(), pool.end(),
+                                  [&](int i) { return i < 0 || i >= sys.natoms || sys.atoms[(size_t)i].z >= mcplan.z_cut; }),
+                   pool.end());
+    };
+    under_z(w);
+    under_z(cl);
+    std::vector<uint32_t> mt = rng_words(rng);
+    phmc_phase2_job J;
+    std::memset(&J, 0, sizeof J);
+    J.replica = 0;
+    J.nh_n_type = p.NH_N_type - 1; J.nh_p_type = p.NH_P_type - 1; J.w_type = p.W_type - 1; J.cl_type = p.Cl_type - 1;
+    J.q_nh_p = 1.0f; J.q_cl = -1.0f;
+    J.beta = p.beta;
+    J.max_attempts = p.max_attempts; J.patience = p.patience; J.energy_interval = p.energy_interval;
+    J.z_cut = (float)mcplan.z_cut;
+    J.nh_p = nh_p.data(); J.n_nh_p = (int)nh_p.size();
+    J.nh_n = nh_n.data(); J.n_nh_n = (int)nh_n.size();
+    J.w = w.data(); J.n_w = (int)w.size();
+    J.cl = cl.data(); J.n_cl = (int)cl.size();
+    J.mt_state = mt.data();
+    phmc_phase2_result R;
+    std::vector<phmc_phase2_event> ev((size_t)1 << 16);
+    ck(phmc_phase2(g.eng, 1, &J, &R, ev.data(), (int)ev.size()), "phmc_phase2");
+    rng_set(rng, mt);
+    for (int i = 0; i < R.n_events; ++i) phmc_p2_write_event(mc_report(), ev[(size_t)i]);
+    if (R.events_dropped > 0) mc_report() << "[phase2] " << R.events_dropped << " further report lines not kept\n";
+    take_identities(sys, d_atoms);
+    Phase2Result out;
+    out.attempted = R.attempted;
+    out.accepted = R.accepted;
+    out.E = (real)R.E;
+    out.best_E = (real)R.best_E;
     return out;
 }

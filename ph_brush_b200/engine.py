@@ -189,6 +189,37 @@ class Engine:
         _abi.check(self._lib.phmc_gc_phase(self._h, n, J, R, E, event_cap))
         return [(R[k].asdict(), [E[k * event_cap + i].asdict() for i in range(R[k].n_events)]) for k in range(n)]
 
+    def phase2(self, jobs, event_cap=1 << 14):
+        """The reference's phase 2, swaps with patience (MC/src/mc.cu:159-318), on the device,
+        one job per replica.  Each job is a dict with the keys of phmc_phase2_job: replica,
+        nh_n_type, nh_p_type, w_type, cl_type, q_nh_p, q_cl, beta, max_attempts, patience,
+        energy_interval, z_cut, the pools nh_p, nh_n, w, cl (W and Cl below z_cut, the
+        reference's order) and mt_state (uint32[625], updated in place).
+        Returns [(result dict, [event dicts])]."""
+        n = len(jobs)
+        J = (_abi.Phase2Job * n)()
+        keep = []
+        for k, j in enumerate(jobs):
+            st = j["mt_state"]
+            assert isinstance(st, np.ndarray) and st.dtype == np.uint32 and st.shape == (625,) and st.flags.c_contiguous
+            J[k].replica = j.get("replica", k)
+            for key in ("nh_n_type", "nh_p_type", "w_type", "cl_type", "max_attempts", "patience", "energy_interval"):
+                setattr(J[k], key, int(j[key]))
+            J[k].q_nh_p = j.get("q_nh_p", 1.0)
+            J[k].q_cl = j.get("q_cl", -1.0)
+            J[k].beta = j["beta"]
+            J[k].z_cut = j.get("z_cut", 0.0)
+            for key in ("nh_p", "nh_n", "w", "cl"):
+                a = _abi.as_i32(j[key])
+                keep.append(a)
+                setattr(J[k], key, _abi.iptr(a))
+                setattr(J[k], "n_" + key, len(a))
+            J[k].mt_state = st.ctypes.data_as(C.POINTER(C.c_uint32))
+        R = (_abi.Phase2Result * n)()
+        E = (_abi.Phase2Event * (n * event_cap))()
+        _abi.check(self._lib.phmc_phase2(self._h, n, J, R, E, event_cap))
+        return [(R[k].asdict(), [E[k * event_cap + i].asdict() for i in range(R[k].n_events)]) for k in range(n)]
+
     def set_state(self, st, replica=0):
         a = [_abi.as_f32(st[k]) for k in ("x", "y", "z", "q")] + [_abi.as_i32(st["type"]), _abi.as_i32(st["flags"])]
         _abi.check(self._lib.phmc_set_state(self._h, replica, *(_abi.fptr(v) for v in a[:4]), _abi.iptr(a[4]),

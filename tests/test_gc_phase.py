@@ -1,16 +1,18 @@
-"""The reference's grand-canonical mu-control phase (MC/src/mc.cu:320-548) on the
-device (phmc_gc_phase) and its report lines written from device event records.
+"""The reference's move phases on the device: grand-canonical mu control
+(MC/src/mc.cu:320-548, phmc_gc_phase) and swaps with patience (MC/src/mc.cu:159-318,
+phmc_phase2), with their report lines written from device event records.
 
 * CPU: the device's restatement of the reference's random stream (std::mt19937,
   uniform_int_distribution<int>, uniform_real_distribution<float>; GCC 13
   libstdc++) against libstdc++ itself, draw for draw, plus the generator's
   stream format; the report formatter against the reference's statements.
-* GPU: the reference's own driver with its phase_gc_mu_control call renamed to
-  the device phase (oracle/_ref/MC_phmc_gc) against the reference's complete
-  build (oracle/_ref/MC_ref) on the same input and seed: every report line, the
-  [sgmc] lines of the device phase and the phase-2 lines that follow it (which
-  only agree if the device phase left the same atoms and generator state); and
-  through the Python handle: pools, energies and determinism.
+* GPU: the reference's own driver with its phase_gc_mu_control and
+  phase2_swap_jitter calls renamed to the device phases (oracle/_ref/MC_phmc_dev)
+  against the reference's complete build (oracle/_ref/MC_ref) on the same input
+  and seed: every report line, [sgmc] and [phase2] (phase 2 only agrees if the
+  first phase left the same atoms and generator state); and through the Python
+  handle: pools, energies, the restored half of rejected four-point moves, and
+  determinism.
 """
 import os
 import subprocess
@@ -106,12 +108,35 @@ def test_report_lines_follow_the_reference_statements():
     assert fmt(ev, res) == f"[sgmc] already at target: Nprot=12/40 target=12 mu/kT={f6(mu)} E={f6(E)} remaining=0"
 
 
+def test_phase2_report_lines_follow_the_reference_statements():
+    def f2(ev):
+        buf = __import__("ctypes").create_string_buffer(512)
+        n = _abi.lib().phmc_phase2_event_format(ev, buf, 512)
+        assert n == len(buf.value)
+        return buf.value.decode()
+    E, acc = np.float32(-98.765432), np.float32(283 / 500)
+    ev = _abi.Phase2Event(kind=_abi.P2_EV_STEP, attempted=500, accepted=283, since_best=0, patience=400, mode_wc=0,
+                          E=E, acc=acc)
+    assert f2(ev) == f"[phase2] step=500 E={f6(E)} accepted=283 acc={float(acc):.3f} since_best=0/400 mode=4-pt"
+    ev.mode_wc = 1
+    assert f2(ev).endswith(" mode=wc-only")
+    z = np.float32(5.3329029)
+    ev = _abi.Phase2Event(kind=_abi.P2_EV_POOLS, n_nh_p=32, n_nh_n=76, n_cl=12, n_w=39, z_cut=z)
+    assert f2(ev) == f"[phase2] pools: NH_P=32 NH_N=76 Cl=12 W=39 (z_cut={f6(z)})"
+    assert f2(_abi.Phase2Event(kind=_abi.P2_EV_PATIENCE, since_best=400, patience=400)) == \
+        "[phase2] patience reached: 400/400. Stop."
+    assert f2(_abi.Phase2Event(kind=_abi.P2_EV_NONE_AT_START)) == \
+        "[phase2] no valid proposals (no 4-pt and no wc-only). Stop."
+    assert f2(_abi.Phase2Event(kind=_abi.P2_EV_WC_EMPTY)) == "[phase2] wc-only requested but pools empty; Stop."
+    assert f2(_abi.Phase2Event(kind=_abi.P2_EV_NONE)) == "[phase2] no valid proposals; Stop."
+
+
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "MC_ref")
-GC_BIN = os.path.join(ROOT, "oracle", "_ref", "MC_phmc_gc")
+DEV_BIN = os.path.join(ROOT, "oracle", "_ref", "MC_phmc_dev")
 
 
 def run_driver(binary, workdir, params):
@@ -128,11 +153,11 @@ def run_driver(binary, workdir, params):
 @pytest.mark.gpu
 @pytest.mark.parametrize("params,long_phase", [("dropin_small.params", False), ("dropin_gc.params", True)])
 def test_device_gc_phase_reproduces_the_reference_driver(tmp_path, params, long_phase):
-    if not (os.path.exists(REF_BIN) and os.path.exists(GC_BIN)):
-        pytest.skip("reference driver binaries not built (make -C oracle mc-ref dropin-gc, needs the reference sources)")
+    if not (os.path.exists(REF_BIN) and os.path.exists(DEV_BIN)):
+        pytest.skip("reference driver binaries not built (make -C oracle mc-ref dropin-dev, needs the reference sources)")
     from test_dropin import RTOL, numbers
     ref = run_driver(REF_BIN, str(tmp_path / "ref"), params)
-    got = run_driver(GC_BIN, str(tmp_path / "gc"), params)
+    got = run_driver(DEV_BIN, str(tmp_path / "dev"), params)
     assert len(ref) == len(got), (len(ref), len(got), ref[-5:], got[-5:])
     sgmc = [line for line in got if line.startswith("[sgmc]")]
     assert any("reached target" in line for line in sgmc), sgmc
@@ -148,7 +173,7 @@ def test_device_gc_phase_reproduces_the_reference_driver(tmp_path, params, long_
                 assert x == y, (a, b)  # counts, steps, pools
             else:
                 assert abs(float(x) - float(y)) <= RTOL * abs(float(x)) + 1e-3, (a, b)
-    assert any("[phase2]" in line and "accepted=" in line for line in got)
+    assert sum(line.startswith("[phase2] step=") for line in got) >= 3, got
 
 
 def re_words(line):
@@ -234,3 +259,48 @@ def test_gc_phase_rejects_bad_jobs():
             e.gc_phase([bad])
         with pytest.raises(_abi.PhmcError):
             e.gc_phase([dict(job, mt_state=mt_seeded(1), cl_type=99)])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wc_only", [False, True])
+def test_phase2_through_the_python_handle(wc_only):
+    s, p, job = gc_setup()
+    pools = {k: job[k] for k in ("nh_p", "nh_n", "w", "cl")}
+    if wc_only:
+        pools["nh_n"] = pools["nh_n"][:0]  # no NH_N left: Cl/W moves only
+    p2 = dict(replica=0, nh_n_type=NHN, nh_p_type=NHP, w_type=W, cl_type=CL, q_nh_p=1.0, q_cl=-1.0, beta=1.0,
+              max_attempts=300, patience=120, energy_interval=50, z_cut=5.0, **pools)
+    t0 = s.type.copy()
+    runs = []
+    for _ in range(2):
+        mt = mt_seeded(77)
+        with Engine(s, p) as e:
+            (res, evs), = e.phase2([dict(p2, mt_state=mt)])
+            st = e.state()
+            comp = e.energy()[0]
+        runs.append((res, evs, mt.copy(), st))
+        assert 0 < res["attempted"] <= 300
+        assert res["stop"] in (_abi.P2_STOP_PATIENCE, _abi.P2_STOP_MAX_ATTEMPTS)
+        if res["stop"] == _abi.P2_STOP_PATIENCE:
+            assert res["since_best"] >= 120
+        # identities are exchanged, never created: every type keeps its count, and the
+        # changed atoms are pool members
+        t = st["type"]
+        for ty in (NHN, NHP, W, CL):
+            assert int(np.sum(t == ty)) == int(np.sum(t0 == ty))
+        changed = np.where(t != t0)[0]
+        assert set(changed) <= set(np.concatenate([pools[k] for k in pools]).tolist())
+        if wc_only:
+            assert not np.any(np.isin(changed, np.concatenate([job["nh_p"], job["nh_n"]])))
+        # tracked energy (accepted moves only) against a fresh recompute: the NH half of
+        # every rejected four-point move was restored
+        e_ref = np.float32(comp["lj"]) + np.float32(comp["coul_real"] + comp["coul_recip"] + comp["self"] +
+                                                     comp["qcorr"] + comp["slab"])
+        assert abs(float(res["E"]) - float(e_ref)) <= 2e-5 * abs(float(e_ref)) + 1e-3, (res["E"], e_ref)
+        assert res["best_E"] <= res["E"] + 1e-6
+        kinds = [ev["kind"] for ev in evs]
+        assert kinds[0] == _abi.P2_EV_POOLS and kinds.count(_abi.P2_EV_STEP) == res["attempted"] // 50
+        steps = [ev for ev in evs if ev["kind"] == _abi.P2_EV_STEP]
+        assert all(ev["mode_wc"] == (1 if wc_only else 0) for ev in steps)
+    (r0, e0, m0, s0), (r1, e1, m1, s1) = runs
+    assert r0 == r1 and e0 == e1 and np.array_equal(m0, m1) and np.array_equal(s0["type"], s1["type"])
