@@ -4,7 +4,11 @@ pool, and phase settings short enough for a test, so that the reference's own
 driver (MC/src/main.cu: protonation phase and phase-2 swaps) can run it both in
 its own build and linked against the engine's reference-API shim.
 dropin_gc.params runs the same system through a longer protonation phase.
-Usage: python tests/golden/make_dropin_inputs.py
+With --large DIR it writes instead the timing input of the drop-in builds: the
+config-2 system (10x10 chains of 50, ~17k atoms with the W pool) in the
+reference's model, target 95 % (the direct protonation phase) and 3000
+phase-2 attempts.
+Usage: python tests/golden/make_dropin_inputs.py [--large DIR]
 """
 import os
 import sys
@@ -20,7 +24,22 @@ PHASES = {"target_pct": "30", "rng_seed": "2025", "max_attempts": "1500", "patie
 PHASES_GC = dict(PHASES, target_pct="35", gc_block_fixed="10", sgmc_epoch_attempt_max="40")
 
 
+LARGE = {"target_pct": "95", "rng_seed": "2025", "max_attempts": "3000", "patience": "100000",
+         "energy_interval": "500", "gc_block_fixed": "1000", "sgmc_epoch_attempt_max": "3000", "phase2_wc": "yes"}
+
+
+def large(out):
+    s2, _ = configs.config2()
+    s, p = configs.to_reference_semantics(s2, n_w=s2.meta["n_sites"], spacing=0.5, seed=6)
+    os.makedirs(out, exist_ok=True)
+    configs.write_lammps_data(os.path.join(out, "in.data"), s)
+    configs.write_params_in(os.path.join(out, "params.in"), p, 0.5, extra=LARGE)
+
+
 def main():
+    if len(sys.argv) == 3 and sys.argv[1] == "--large":
+        large(sys.argv[2])
+        return
     small, _ = configs.small_system(seed=9, chains=3, length=12, box_xy=12.0, height=14.0, salt_pairs=6, ion_frac=0.2)
     s, p = configs.to_reference_semantics(small, n_w=small.meta["n_sites"], spacing=0.5, seed=6)
     os.makedirs(os.path.join(HERE, "inputs"), exist_ok=True)
