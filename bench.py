@@ -319,6 +319,42 @@ def plain_config2(args, local):
     return out, (s, p)
 
 
+def reference_phase2_on_device(local, attempts=2000, spacing=0.7, seed=5):
+    """The reference's phase 2 (MC/src/mc.cu:159-318) run on the device (phmc_phase2) on the
+    system and settings the reference arm's harness times it on (config 2 in the reference's
+    model, mesh from pme_spacing 0.7, pools by type, W and Cl below z_cut): attempts/s of the
+    same loop, the same draws and the same acceptance rule, device loop against host loop."""
+    import numpy as np
+    from ph_brush_b200 import Engine, configs
+    s2, _ = configs.config2()
+    n_sites = int(((s2.flags & 2) != 0).sum())
+    s, p = configs.to_reference_semantics(s2, n_w=n_sites, spacing=spacing, seed=seed)
+    t = s.type
+    nhn, nhp, w, cl = 3, 4, 6, 7  # the reference's types 4, 5, 7, 8, 0-based
+    sites = np.where((t == nhn) | (t == nhp))[0]
+    z_cut = float(np.max(s.z[sites])) + 1.0  # w_z_extra_nm's default (MC/include/types.hpp)
+    job = dict(replica=0, nh_n_type=nhn, nh_p_type=nhp, w_type=w, cl_type=cl, beta=1.0, patience=1 << 30,
+               energy_interval=1 << 30, z_cut=z_cut, nh_p=np.where(t == nhp)[0], nh_n=np.where(t == nhn)[0],
+               w=np.where((t == w) & (s.z < z_cut))[0], cl=np.where((t == cl) & (s.z < z_cut))[0])
+    mt = np.zeros(625, np.uint32)  # std::mt19937(2025)
+    v = 2025
+    mt[0] = v
+    for i in range(1, 624):
+        v = (1812433253 * (v ^ (v >> 30)) + i) & 0xFFFFFFFF
+        mt[i] = v
+    mt[624] = 624
+    with Engine(s, p, device=local) as eng:
+        eng.phase2([dict(job, mt_state=mt, max_attempts=50)])  # warm-up
+        t0 = time.perf_counter()
+        (res, _), = eng.phase2([dict(job, mt_state=mt, max_attempts=attempts)])
+        sec = time.perf_counter() - t0
+    return {"workload": "config 2 in the reference's model (" + str(s.n) + " atoms), its phase 2 on the device "
+                        "(four-point identity swaps, float Metropolis on the reference's energies)",
+            "attempts": res["attempted"], "accepted": res["accepted"], "seconds": sec,
+            "attempts_per_s": res["attempted"] / sec, "mesh": list(p.mesh),
+            "timing": "host wall clock around the synchronous call (launches, rebuilds, event copies)"}
+
+
 def cpu_baseline(s, p, seconds, what):
     """The FP64 oracle's Monte Carlo (same move set, energy from scratch per trial) on the host cores."""
     from oracle import pyoracle as O
@@ -456,6 +492,10 @@ def run_ours(args):
     eng.close()
     if rank == 0 and world == 1 and not args.no_extras:
         line["plain_config2"], c2 = plain_config2(args, local)
+        try:
+            line["reference_phase2_on_device"] = reference_phase2_on_device(local)
+        except Exception as e:  # an extra: the headline line is printed regardless
+            line["reference_phase2_on_device"] = {"error": str(e)[:300]}
         if not args.no_alpha:
             line["alpha_check"] = alpha_check(local, args.alpha_eq, args.alpha_sample)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
