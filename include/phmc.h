@@ -518,7 +518,8 @@ int phmc_gc_phase(phmc_engine* e, int n_jobs, const phmc_gc_job* jobs, phmc_gc_r
  * place; a rejection restores the NH half), so its energy change is the
  * four-atom one.  The caller's generator, pools and event records work as for
  * phmc_gc_phase; the W and Cl pools are the ones the reference keeps (below
- * z_cut), z_cut itself only enters the pools line. */
+ * z_cut), z_cut itself only enters the pools line.  Needs the engine's
+ * pending_max >= 6 (PHMC_ERR_UNSUPPORTED otherwise). */
 #define PHMC_P2_EV_POOLS 11         /* the pool sizes before the first attempt */
 #define PHMC_P2_EV_NONE_AT_START 12 /* neither a four-point nor a Cl/W move possible: the phase ends */
 #define PHMC_P2_EV_WC_EMPTY 13      /* Cl/W moves wanted, their pools empty: the phase ends */

@@ -1304,6 +1304,8 @@ extern "C" int phmc_phase2(phmc_engine* h, int n_jobs, const phmc_phase2_job* jo
     if (!h || n_jobs < 1 || !jobs || !results || event_cap < 0) return fail(PHMC_ERR_ARG, "invalid argument");
     Engine& E = h->E;
     if (n_jobs > E.R) return fail(PHMC_ERR_ARG, "more jobs than replicas");
+    // a four-point attempt starts only with room for six pending stencils
+    if (E.pend_max < 6) return fail(PHMC_ERR_UNSUPPORTED, "phase 2 needs pending_max >= 6 (phmc_set_tuning)");
     CU(cudaSetDevice(E.device));
     std::vector<int> seen((size_t)E.R, 0);
     std::vector<RepState> st((size_t)E.R);
