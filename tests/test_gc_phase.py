@@ -304,3 +304,25 @@ def test_phase2_through_the_python_handle(wc_only):
         assert all(ev["mode_wc"] == (1 if wc_only else 0) for ev in steps)
     (r0, e0, m0, s0), (r1, e1, m1, s1) = runs
     assert r0 == r1 and e0 == e1 and np.array_equal(m0, m1) and np.array_equal(s0["type"], s1["type"])
+
+
+@pytest.mark.gpu
+def test_phases_batched_over_replicas_equal_single_runs():
+    """Two jobs on a two-replica engine run in the same launches (one block each) and
+    give exactly what each job gives alone."""
+    s, p, job = gc_setup()
+    seeds = (2025, 99)
+    single = []
+    for sd in seeds:
+        mt = mt_seeded(sd)
+        with Engine(s, p) as e:
+            (res, evs), = e.gc_phase([dict(job, mt_state=mt)])
+            single.append((res, evs, mt.copy(), e.state()["type"].copy()))
+    mts = [mt_seeded(sd) for sd in seeds]
+    with Engine([s, s], [p, p]) as e:
+        out = e.gc_phase([dict(job, replica=k, mt_state=mts[k]) for k in range(2)])
+        types = [e.state(k)["type"].copy() for k in range(2)]
+    for k in range(2):
+        res, evs, mt, t = single[k]
+        assert out[k][0] == res and out[k][1] == evs
+        assert np.array_equal(mts[k], mt) and np.array_equal(types[k], t)
