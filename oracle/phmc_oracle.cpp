@@ -20,6 +20,8 @@
 #include <vector>
 #include <algorithm>
 #include <limits>
+#include <random>
+#include <sstream>
 #include <stdexcept>
 #include "../include/phmc.h"
 
@@ -891,4 +893,25 @@ extern "C" void orc_cells(void* h, int cx, int cy, int cz, int* cell_of) {
         int c = std::min(cz - 1, std::max(0, (int)((float)mc->s.z[i] * iz)));
         cell_of[i] = (c * cy + b) * cx + a;
     }
+}
+
+// ---- the reference driver's random stream, from libstdc++ itself ----
+// std::mt19937 and the two distributions the reference's move loops draw with
+// (MC/src/mc.cu:62-65 choose_one, uniform_real_distribution<real>(0, 1) at
+// :204,353-354), for the CPU restatement of its move phases.
+extern "C" void* orc_mt_create(uint32_t seed) { return new std::mt19937(seed); }
+extern "C" void orc_mt_destroy(void* h) { delete (std::mt19937*)h; }
+extern "C" int orc_mt_index(void* h, int n) {
+    std::uniform_int_distribution<int> d(0, n - 1);
+    return d(*(std::mt19937*)h);
+}
+extern "C" float orc_mt_unit_float(void* h) {
+    std::uniform_real_distribution<float> u(0.0f, 1.0f);
+    return u(*(std::mt19937*)h);
+}
+// the generator's 624 state words and position, in its stream format
+extern "C" void orc_mt_state(void* h, uint32_t* out) {
+    std::stringstream ss;
+    ss << *(std::mt19937*)h;
+    for (int i = 0; i < 625; ++i) { unsigned long v = 0; ss >> v; out[i] = (uint32_t)v; }
 }

@@ -131,6 +131,73 @@ def test_phase2_report_lines_follow_the_reference_statements():
     assert f2(_abi.Phase2Event(kind=_abi.P2_EV_NONE)) == "[phase2] no valid proposals; Stop."
 
 
+# The oracle's restatement of the phases (oracle/pyoracle.py: libstdc++'s own
+# std::mt19937 and distributions, FP64 reference-model energies rounded as the
+# reference's float build rounds them).  Pinned to the reference's output: on
+# the drop-in fixture the reference build's report line of its GC phase (MC_ref
+# on a B200; the device phase printed the same line, counts equal and energies
+# within 2e-5, in test_device_gc_phase_reproduces_the_reference_driver) is
+#   [sgmc] reached target in epoch=0 step_in_block=41 Nprot=32/108
+#          mu/kT=-0.847298 E=110.129379 fwd_acc=6 bwd_acc=3 remaining=0
+REF_GC_LINE = {"epoch": 0, "step_in_block": 41, "nprot": 32, "Nh": 108, "mu_kT": -0.847298, "E": 110.129379,
+               "fwd_total": 6, "bwd_total": 3}
+
+
+def oracle_inputs(params):
+    from oracle import pyoracle as O
+    if not os.path.exists(O.REF_HOST):
+        pytest.skip("reference host library not built (make -C oracle ref-host)")
+    inputs = os.path.join(ROOT, "tests", "golden", "inputs")
+    return O, O.ref_host_read(os.path.join(inputs, "dropin_small.data"), os.path.join(inputs, params))
+
+
+def test_oracle_gc_phase_reproduces_the_reference_line():
+    O, (s, p, raw) = oracle_inputs("dropin_small.params")
+    plan = O.ref_plan(s, raw)
+    res, evs = O.ref_gc_phase(s, p, raw, plan, O.RefGenerator(raw["rng_seed"]))
+    assert len(evs) == 1 and evs[0]["kind"] == _abi.GC_EV_REACHED
+    ev = evs[0]
+    for k in ("epoch", "step_in_block", "nprot", "fwd_total", "bwd_total"):
+        assert ev[k] == REF_GC_LINE[k], (k, ev[k])
+    assert res["Nh"] == REF_GC_LINE["Nh"] and res["attempted"] == 41
+    assert abs(ev["mu_kT"] - REF_GC_LINE["mu_kT"]) < 5e-7
+    assert abs(ev["E"] - REF_GC_LINE["E"]) <= 2e-5 * abs(REF_GC_LINE["E"]) + 1e-3
+
+
+def test_oracle_workflow_bookkeeping():
+    """plan -> grand-canonical phase -> phase 2 on the longer-phase input: the restatement's
+    own bookkeeping (events, blocks, epochs, patience, identities exchanged, not created)."""
+    O, (s, p, raw) = oracle_inputs("dropin_gc.params")
+    plan = O.ref_plan(s, raw)
+    gen = O.RefGenerator(raw["rng_seed"])
+    t0 = s.type.copy()
+    res, evs = O.ref_gc_phase(s, p, raw, plan, gen)
+    assert res["stop"] == 1 and res["Nprot"] == res["target_count"]
+    kinds = [e["kind"] for e in evs]
+    assert kinds[-1] == _abi.GC_EV_REACHED
+    assert kinds.count(_abi.GC_EV_CHUNK) == (res["attempted"] - 1) // raw["gc_block_fixed"]
+    assert kinds.count(_abi.GC_EV_MU) == res["blocks_done"] >= 2
+    assert res["accepted_forward"] - res["accepted_backward"] == plan["to_flip"]
+    NHN, NHP, W, CL = (raw[k] - 1 for k in ("NH_N_type", "NH_P_type", "W_type", "Cl_type"))
+    t = s.type
+    assert int(np.sum(t == NHP)) - int(np.sum(t0 == NHP)) == plan["to_flip"]
+    assert int(np.sum(t == CL)) - int(np.sum(t0 == CL)) == plan["to_flip"]
+    z = np.asarray(s.z, np.float32)
+    pools = {"nh_p": list(np.where(t == NHP)[0]), "nh_n": list(np.where(t == NHN)[0]),
+             "w": list(np.where((t == W) & (z < plan["z_cut"]))[0]), "cl": list(np.where((t == CL) & (z < plan["z_cut"]))[0])}
+    t1 = t.copy()
+    r2, e2 = O.ref_phase2(s, p, raw, pools, plan["z_cut"], gen)
+    assert e2[0]["kind"] == _abi.P2_EV_POOLS and e2[0]["n_nh_p"] == len(pools["nh_p"])
+    steps = [e for e in e2 if e["kind"] == _abi.P2_EV_STEP]
+    assert len(steps) == r2["attempted"] // raw["energy_interval"]
+    assert r2["stop"] in (1, 2)
+    if r2["stop"] == 1:
+        assert e2[-1]["kind"] == _abi.P2_EV_PATIENCE and r2["since_best"] >= raw["patience"]
+    for ty in (NHN, NHP, W, CL):
+        assert int(np.sum(s.type == ty)) == int(np.sum(t1 == ty))
+    assert r2["best_E"] <= r2["E"]
+
+
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
