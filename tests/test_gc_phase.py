@@ -393,3 +393,18 @@ def test_phases_batched_over_replicas_equal_single_runs():
         res, evs, mt, t = single[k]
         assert out[k][0] == res and out[k][1] == evs
         assert np.array_equal(mts[k], mt) and np.array_equal(types[k], t)
+
+
+def test_report_formatters_truncate_and_refuse_nulls():
+    import ctypes
+    lib = _abi.lib()
+    res = _abi.GcResult(Nh=40, target_count=12)
+    ev = _abi.GcEvent(kind=_abi.GC_EV_NO_PAIRS)
+    full = "[sgmc] no valid pairs to flip; stop."
+    assert lib.phmc_gc_event_format(ev, res, None, 0) == len(full)  # length only
+    buf = ctypes.create_string_buffer(8)
+    assert lib.phmc_gc_event_format(ev, res, buf, 8) == len(full) and buf.value.decode() == full[:7]
+    assert lib.phmc_gc_event_format(None, res, buf, 8) == -1
+    ev2 = _abi.Phase2Event(kind=_abi.P2_EV_NONE)
+    assert lib.phmc_phase2_event_format(ev2, buf, 8) == len("[phase2] no valid proposals; Stop.")
+    assert lib.phmc_phase2_event_format(None, buf, 8) == -1
