@@ -408,3 +408,11 @@ def test_report_formatters_truncate_and_refuse_nulls():
     ev2 = _abi.Phase2Event(kind=_abi.P2_EV_NONE)
     assert lib.phmc_phase2_event_format(ev2, buf, 8) == len("[phase2] no valid proposals; Stop.")
     assert lib.phmc_phase2_event_format(None, buf, 8) == -1
+
+
+def test_phase_entry_points_refuse_bad_arguments_before_any_device_call():
+    lib = _abi.lib()
+    job, res, ev = _abi.GcJob(), _abi.GcResult(), _abi.GcEvent()
+    assert lib.phmc_gc_phase(None, 1, job, res, ev, 1) == 1  # PHMC_ERR_ARG
+    j2, r2, e2 = _abi.Phase2Job(), _abi.Phase2Result(), _abi.Phase2Event()
+    assert lib.phmc_phase2(None, 1, j2, r2, e2, 1) == 1
