@@ -233,6 +233,14 @@ int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_
  * resident at once.  Decisions do not depend on it except through FP32 rounding
  * of the reciprocal-space dE. */
 int phmc_set_quorum(phmc_engine* e, double quorum);
+/* Bound on the MC kernel launches one call of phmc_run (phmc_run_timed, the
+ * autotuner's runs), phmc_gc_phase or phmc_phase2 may make; 0 (the default)
+ * leaves only the guard against a loop that makes no progress.  A call that
+ * reaches the bound with work left returns PHMC_ERR_BUDGET between launches:
+ * every replica's state is consistent and a later call continues from it (a
+ * device phase's results and events of that call are not written).  No
+ * counterpart in the reference, whose loops are unbounded host loops. */
+int phmc_set_launch_budget(phmc_engine* e, int64_t max_launches);
 
 /* ---- input files of the reference's driver (host side, no device use) ----
  * LAMMPS "full" data files: phmc_lammps_header reads the header (counts, box
@@ -327,16 +335,21 @@ int phmc_capacity(phmc_engine* e, int replica);
 
 /* ---- allocation-free reciprocal energy ----
  * No counterpart in the reference.  SPME reciprocal-space energy of n point
- * charges (host arrays), for callers that cannot call cudaMalloc: code running
- * while a stream is being captured into a CUDA graph, hosts whose device memory
- * is budgeted by another allocator, or per-trial loops that must not stall on an
- * allocation's implicit synchronisation.  It uses one file-scope device array
- * (about 3 MB, held by every GPU that loads the library until exit) and never
- * allocates.  Limits: n <= PHMC_STATIC_MAX_PARTICLES, nx*ny*nz <=
+ * charges (host arrays), for callers that cannot call cudaMalloc: a host
+ * program whose device memory is all handed out by its own allocator (a
+ * framework's caching pool, a fixed per-process budget), a plugin called back
+ * from such a program, or a per-trial loop that must not stall on an
+ * allocation's implicit device synchronisation.  It uses one file-scope device
+ * array (about 3 MB, held by every GPU that loads the library until exit) and
+ * never allocates.  Limits: n <= PHMC_STATIC_MAX_PARTICLES, nx*ny*nz <=
  * PHMC_STATIC_MAX_MESH, each side 2^a 3^b 5^c in [order, 512]; larger inputs
- * return PHMC_ERR_CAPACITY.  Works on the current device; that device's first
- * call looks up the array's device address (make it before any stream
- * capture).  Calls share the array: calls that overlap on the GPU race. */
+ * return PHMC_ERR_CAPACITY.  Works on the current device, on the legacy default
+ * stream, and synchronises before it returns.  That device's first call looks
+ * up the array's device address, so make it before any stream capture; after a
+ * cudaDeviceReset of the device do not call it again in the process.  Calls
+ * share the array (and host staging tables): a process-wide lock serialises
+ * them, so calls through this function never overlap, but any other work that
+ * overlaps a call on the GPU and touches the array races with it. */
 #define PHMC_STATIC_MAX_PARTICLES 32768
 #define PHMC_STATIC_MAX_MESH 131072
 int phmc_recip_energy_static(const float* x, const float* y, const float* z, const float* q, int n,

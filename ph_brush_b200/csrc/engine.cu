@@ -61,6 +61,8 @@ struct phmc_engine {
     GcDev* d_gc = nullptr;
     int* d_gc_pool = nullptr;
     unsigned char* d_gc_ev = nullptr;
+    // MC launches one run / phase call may make (0: only the no-progress guard)
+    long long launch_budget = 0;
 };
 
 static void drop_graph(phmc_engine* h) {
@@ -848,6 +850,8 @@ int phmc_run_loop(phmc_engine* h, int64_t n_trials, int check_every) {
         }
         if (*E.h_active == 0) break;
         if (iter > max_iter) return fail(PHMC_ERR_BUDGET, "trial loop made no progress");
+        if (h->launch_budget > 0 && iter >= h->launch_budget)
+            return fail(PHMC_ERR_BUDGET, "launch budget reached before every replica reached its target");
     }
     if (h->profiling) {
         std::vector<RepState> st1((size_t)E.R);
@@ -1204,6 +1208,8 @@ static int gc_run(phmc_engine* h, std::vector<GcDev>& G, const std::vector<const
         }
         if (all) break;
         if (it > max_launches) return fail(PHMC_ERR_BUDGET, "device phase made no progress");
+        if (h->launch_budget > 0 && it + 1 >= h->launch_budget)
+            return fail(PHMC_ERR_BUDGET, "launch budget reached before every job stopped");
     }
     return PHMC_OK;
 }
@@ -1593,6 +1599,13 @@ extern "C" int phmc_set_quorum(phmc_engine* h, double quorum) {
     CU(cudaStreamSynchronize(h->E.stream));
     h->E.quorum = (float)quorum;
     drop_graph(h);  // the quorum is a launch parameter of the captured MC launches
+    return PHMC_OK;
+}
+
+extern "C" int phmc_set_launch_budget(phmc_engine* h, int64_t max_launches) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    if (max_launches < 0) return fail(PHMC_ERR_ARG, "launch budget must be >= 0");
+    h->launch_budget = max_launches;
     return PHMC_OK;
 }
 

@@ -5,6 +5,7 @@
 // k_recip_energy_and_apply of the reference (MC/src/pme.cu:140-249,384-422).
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include "common.cuh"
 #include "engine.h"
@@ -265,13 +266,12 @@ cudaError_t mesh_set_smem_limits(Engine& E) {
 // ---------------------------------------------------------------------------
 // Reciprocal-space energy with no device allocation.
 //
-// For callers that must not allocate device memory: code that evaluates the
-// SPME energy inside a region where cudaMalloc is forbidden or unwanted (a
-// stream being captured into a CUDA graph, a host with a fixed device-memory
-// budget handed out by another allocator, a per-trial loop where an
-// allocation's implicit device synchronisation would stall the pipeline).
-// The reference itself allocates a device scalar on every energy call
-// (MC/src/energy_gpu.cu:55, MC/src/pme.cu:363).
+// For callers that must not allocate device memory: a host program whose
+// device memory is all handed out by its own allocator (a framework's caching
+// pool, a fixed per-process budget), a plugin called back from such a program,
+// or a per-trial loop where an allocation's implicit device synchronisation
+// would stall the pipeline.  The reference itself allocates a device scalar on
+// every energy call (MC/src/energy_gpu.cu:55, MC/src/pme.cu:363).
 //
 // All scratch lives in one file-scope __device__ array (every GPU that loads
 // the library holds it until the process exits): particle staging, the
@@ -279,8 +279,15 @@ cudaError_t mesh_set_smem_limits(Engine& E) {
 // twiddles and the energy partials.  Limits: n <= PHMC_STATIC_MAX_PARTICLES,
 // nx*ny*nz <= PHMC_STATIC_MAX_MESH, each mesh side <= 512.
 // Every call shares the array and leaves its contents behind; the call clears
-// what must start at zero.  Calls that overlap on the GPU (other host threads,
-// other streams) race on the array.
+// what must start at zero.  The small host tables are staged in file-scope host
+// arrays, shared by every host thread as well.  A process-wide lock serialises
+// the calls and each call waits for its own GPU work before it returns, so
+// calls made through this function never overlap; work that the caller queues
+// on other streams in the same interval and that touches the array would race
+// with it.  The array's device address is looked up once per device, on the
+// first call made with that device current; it belongs to the device's primary
+// context, so after a cudaDeviceReset of that device the entry point must not
+// be called again in the process.
 // ---------------------------------------------------------------------------
 #define ST_MAX_N PHMC_STATIC_MAX_PARTICLES
 #define ST_MAX_M PHMC_STATIC_MAX_MESH
@@ -309,6 +316,10 @@ static __device__ __align__(256) unsigned char g_recip_scratch[ST_BYTES];
 // Device address of g_recip_scratch per device, looked up on the first call made
 // with that device current.
 static unsigned char* g_recip_scratch_addr[64];
+
+// Serialises the calls: the host staging tables below and the device array are
+// shared by every host thread.
+static std::mutex g_recip_static_lock;
 
 // Host staging of the small tables (the same process-wide sharing rules apply).
 static float4 h_st_posq[ST_MAX_N];
@@ -386,6 +397,7 @@ extern "C" int phmc_recip_energy_static(const float* x, const float* y, const fl
         phmc_set_error(PHMC_ERR_CAPACITY, "phmc_recip_energy_static: mesh larger than PHMC_STATIC_MAX_MESH points");
         return PHMC_ERR_CAPACITY;
     }
+    std::lock_guard<std::mutex> serial(g_recip_static_lock);
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess || dev < 0 || dev >= 64) {

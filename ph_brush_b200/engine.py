@@ -121,6 +121,11 @@ class Engine:
         """MC launch quorum (0, 1]: a launch ends once that fraction of its running replicas is blocked."""
         _abi.check(self._lib.phmc_set_quorum(self._h, float(quorum)))
 
+    def set_launch_budget(self, max_launches):
+        """Bound on the MC launches of one run / device-phase call (0: unbounded);
+        a call that reaches it raises PhmcError(PHMC_ERR_BUDGET) with the state consistent."""
+        _abi.check(self._lib.phmc_set_launch_budget(self._h, int(max_launches)))
+
     def tuning(self):
         t = _abi.Tuning()
         _abi.check(self._lib.phmc_get_tuning(self._h, C.byref(t)))

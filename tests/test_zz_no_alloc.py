@@ -1,19 +1,20 @@
 """The allocation-free reciprocal-energy entry point (phmc_recip_energy_static).
 
-It serves callers that cannot call cudaMalloc (work recorded while a stream is
-captured into a CUDA graph, hosts whose device memory is handed out by another
-allocator, per-trial loops that must not stall on an allocation) and keeps its
-scratch in one file-scope device array.  Checked through the C ABI against the
-engine's own reciprocal energy (phmc_create + phmc_energy, which allocates),
-with the tolerance of the other energy tests, on two calls in a row so that a
-leftover from the first call (the array keeps its contents) would show up.
-The file name makes pytest collect it last.
+It serves callers that cannot call cudaMalloc (a process whose device memory
+is all handed out by its own allocator, a plugin called back from one, a
+per-trial loop that must not stall on an allocation) and keeps its scratch in
+one file-scope device array.  Checked through the C ABI against the engine's
+own reciprocal energy (phmc_create + phmc_energy, which allocates) and against
+the FP64 oracle's, with the tolerance of the other energy tests, on two calls
+in a row so that a leftover from the first call (the array keeps its contents)
+would show up.  The file name makes pytest collect it last.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
 
+from oracle import pyoracle as O
 from ph_brush_b200 import Engine, _abi, configs
 
 RTOL, ATOL = 1e-6, 1e-4
@@ -58,7 +59,9 @@ def test_static_recip_energy_matches_engine(case):
         assert p.mesh[0] % 2 == 1
     with Engine(s, p) as e:
         ref = e.energy()[0]["coul_recip"]
+    orc = O.energy(s, p)["coul_recip"]
     for _ in range(2):
         rc, got = call_static(s, p)
         assert rc == 0, _abi.lib().phmc_last_error()
         assert abs(got - ref) <= RTOL * abs(ref) + ATOL, (got, ref)
+        assert abs(got - orc) <= RTOL * abs(orc) + ATOL, (got, orc)
