@@ -19,15 +19,22 @@ of delayed acceptance against the plain engine, and the plain engine on config 2
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With N > 1 (torchrun, one process per GPU) every rank runs its own replica set
-(replicas only, weak scaling); the timed region is bracketed by barriers and
-the max device time over ranks is reported.  `--impl reference` runs the
-reference's own CUDA build (compiled from its sources into oracle/_ref) one
-replica at a time on sampled config-5 replicas in the reference's model, and on
-config 2, and prints the same metric.
+With N > 1 (torchrun, one process per GPU) the replica set holds 256 N
+replicas, split over the ranks by estimated cost (ph_brush_b200.replicas;
+replicas only, weak scaling); the timed region is bracketed by barriers and
+the max device time over ranks is reported.
+
+`--impl reference` runs the reference's own CUDA build (compiled from its
+sources into oracle/_ref; this process loads no library of this repository) on
+the same replica set: the systems are written in the reference's input format
+by oracle/_build/ref_inputs (the same generator, so the same particles), and
+the reference's per-trial loop -- its full energy per trial, one replica after
+the other -- runs a bounded sample of every replica's trials in the same move
+mix; value in the same unit.  Its line also carries the reference on config 2.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -46,6 +53,64 @@ WORKLOAD = ("config 5: 256 diblock brush replicas (20 permanent +1 + 30 titratab
             "delayed acceptance with the GPU-trained surrogate; 90% displacement / 10% protonation")
 CFG2 = ("config 2: plain constant-pH MC, 10x10 chains x 50 titratable beads, 40x40x100 box padded to 300, "
         "0.1 M salt, ~12k particles, SPME 64x64x384 order 5, rc 3, 90% displacement / 10% protonation")
+MOVE_MIX = "90% displacement (max 0.3 sigma) / 10% protonation"
+REF_INPUTS = os.path.join(ROOT, "oracle", "_build", "ref_inputs")
+REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+
+def workload_config(n_rep, ns):
+    """The `config` both arms print (the same dict for the same workload)."""
+    return {"workload": WORKLOAD, "replicas": int(n_rep), "particles_min_max": [int(min(ns)), int(max(ns))],
+            "move_mix": MOVE_MIX, "parallelism": "replicas only"}
+
+
+# ---------------------------------------------------------------------------
+# the workloads as brush specs for oracle/_build/ref_inputs: the values
+# ph_brush_b200.configs draws (config5, config2), restated here so that the
+# reference arm imports nothing of the package (tests/test_bench_inputs.py
+# checks the files against the package's systems)
+# ---------------------------------------------------------------------------
+def _molar(c):
+    return c * 0.6022 * 0.5 ** 3
+
+
+def _ideal(pH, pKa):
+    return 1.0 / (1.0 + 10.0 ** (pH - pKa))
+
+
+def config5_spec_lines(seed=2029, n_rep=256, pme_spacing=0.75):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    H = 60.0
+    out = []
+    for k in range(n_rep):
+        side = int(rng.integers(8, 13))
+        pH = float(rng.uniform(5.0, 9.0))
+        salt = float(math.exp(rng.uniform(math.log(0.001), math.log(0.3))))
+        out.append(f"c5_{k:04d} {side} {side} 4.0 50 50 20 0 {H!r} {3 * H!r} {_ideal(pH, 7.3)!r} {_molar(salt)!r} "
+                   f"0.97 0.9 {seed + 1000 + k} -1 {seed + 5000 + k} {pme_spacing!r} {pH!r} 7.3")
+    return out
+
+
+def config2_spec_line(pme_spacing=0.7):
+    return (f"c2 10 10 4.0 50 50 0 1 100.0 300.0 {_ideal(6.5, 7.5)!r} {_molar(0.1)!r} 0.97 0.9 2026 -1 5 "
+            f"{pme_spacing!r} 6.5 7.5")
+
+
+def write_ref_inputs(lines, out_dir):
+    """Run oracle/_build/ref_inputs on spec lines; returns {name: (natoms, n_native, n_sites)}."""
+    spec = os.path.join(out_dir, "spec.txt")
+    with open(spec, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    r = subprocess.run([REF_INPUTS, spec, out_dir], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("ref_inputs failed: " + r.stderr.strip()[-300:])
+    out = {}
+    for ln in r.stdout.split("\n"):
+        f = ln.split()
+        if len(f) == 4:
+            out[f[0]] = tuple(int(v) for v in f[1:])
+    return out
 
 
 def parse():
@@ -68,6 +133,8 @@ def parse():
                     help="only the plain engine on config 2 (one JSON line of its figures; for profiling)")
     ap.add_argument("--alpha-eq", type=int, default=1200, help="sweeps of equilibration in the alpha(pH) check")
     ap.add_argument("--alpha-sample", type=int, default=600, help="sweeps sampled in the alpha(pH) check")
+    ap.add_argument("--ref-trials", type=int, default=4,
+                    help="reference arm: trials per replica per step (its bounded sample of the step)")
     return ap.parse_args()
 
 
@@ -148,6 +215,16 @@ def reduce_max(val, world, dev):
     return float(t.item())
 
 
+def reduce_sum(val, world, dev):
+    if world == 1:
+        return val
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([val], dtype=torch.float64, device=f"cuda:{dev}")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -170,11 +247,21 @@ def sums(stats, keys=("evaluated", "passed", "accepted")):
 # ---------------------------------------------------------------------------
 # headline: batched + delayed acceptance on config 5
 # ---------------------------------------------------------------------------
-def build_headline(args, local, rank):
+def headline_replicas(args, rank, world):
+    """This rank's share of the config-5 replica set (256 per GPU), split by estimated
+    cost with the library's partitioner."""
+    from ph_brush_b200 import configs
+    from ph_brush_b200.replicas import partition, replica_cost
+    allr = configs.config5(seed=2029, n_rep=args.replicas * world)
+    a, b = partition([replica_cost(s.n, p.mesh) for s, p in allr], world)[rank]
+    return allr[a:b], [s.n for s, _ in allr]
+
+
+def build_headline(args, local, rank, world):
     """Config-5 engine, autotuned, with a surrogate trained on the GPU on exact dE
     harvested from its own replicas (all of this is set-up, outside the timed region)."""
-    from ph_brush_b200 import Engine, Surrogate, configs
-    reps = configs.config5(seed=2029 + 7919 * rank, n_rep=args.replicas)
+    from ph_brush_b200 import Engine, Surrogate
+    reps, n_all = headline_replicas(args, rank, world)
     eng = Engine([s for s, _ in reps], [p for _, p in reps], device=local)
     p0 = reps[0][1]
     sur = Surrogate(seed=2029)
@@ -195,7 +282,7 @@ def build_headline(args, local, rank):
     train = {"samples": n_samples, "epochs": args.epochs, "batch": 4096, "lr": 1e-3, "final_loss": loss,
              "seconds": t_fit, "samples_per_s": steps * 4096 / t_fit,
              "tflops": steps * 4096 * 4 * 3 * fl_row / t_fit / 1e12}
-    return reps, eng, sur, tune, train
+    return reps, n_all, eng, sur, tune, train
 
 
 def plain_aggregate(args, reps, local, trials, samples=3):
@@ -319,16 +406,15 @@ def plain_config2(args, local):
     return out, (s, p)
 
 
-def reference_phase2_on_device(local, attempts=2000, spacing=0.7, seed=5):
-    """The reference's phase 2 (MC/src/mc.cu:159-318) run on the device (phmc_phase2) on the
-    system and settings the reference arm's harness times it on (config 2 in the reference's
-    model, mesh from pme_spacing 0.7, pools by type, W and Cl below z_cut): attempts/s of the
-    same loop, the same draws and the same acceptance rule, device loop against host loop."""
+def reference_phase2_on_device(local, ref_dir, attempts=2000):
+    """The reference's phase 2 (MC/src/mc.cu:159-318) run on the device (phmc_phase2) on
+    the files the reference arm's harness times it on (config 2 in the reference's model,
+    written by oracle/_build/ref_inputs, read through the library's readers), with the
+    same settings and generator seed (std::mt19937(2025)): attempts/s of the same loop,
+    the same draws and acceptance rule, device loop against the reference's host loop."""
     import numpy as np
-    from ph_brush_b200 import Engine, configs
-    s2, _ = configs.config2()
-    n_sites = int(((s2.flags & 2) != 0).sum())
-    s, p = configs.to_reference_semantics(s2, n_w=n_sites, spacing=spacing, seed=seed)
+    from ph_brush_b200 import Engine, files
+    s, p = files.reference_model(os.path.join(ref_dir, "c2.data"), os.path.join(ref_dir, "c2.params"))
     t = s.type
     nhn, nhp, w, cl = 3, 4, 6, 7  # the reference's types 4, 5, 7, 8, 0-based
     sites = np.where((t == nhn) | (t == nhp))[0]
@@ -355,25 +441,37 @@ def reference_phase2_on_device(local, attempts=2000, spacing=0.7, seed=5):
             "timing": "host wall clock around the synchronous call (launches, rebuilds, event copies)"}
 
 
-def cpu_baseline(s, p, seconds, what):
-    """The FP64 oracle's Monte Carlo (same move set, energy from scratch per trial) on the host cores."""
+def cpu_baseline(ref_dir, name, seconds):
+    """The reference's per-trial loop restated in FP64 on the host cores (oracle.pyoracle.
+    RefTrialLoop: half list built once, LJ + cubic SPME recomputed every trial, OpenMP)
+    on one config-5 replica in the reference's model, in the benchmark's move mix."""
+    import numpy as np
     from oracle import pyoracle as O
-    mc = O.MC(s, p)
+    from ph_brush_b200 import files
+    base = os.path.join(ref_dir, name)
+    s, p = files.reference_model(base + ".data", base + ".params")
+    ex = open(base + ".extra").read().split()
+    kv = {ex[k]: ex[k + 1] for k in range(0, ex.index("mobile"), 2)}
+    nmob = int(ex[ex.index("mobile") + 1])
+    mobile = np.array([int(v) for v in ex[ex.index("mobile") + 2:ex.index("mobile") + 2 + nmob]])
+    loop = O.RefTrialLoop(s, p, mobile, float(kv["height"]), float(kv["pH"]), float(kv["pKa"]), seed=5)
     n = 0
     t0 = time.perf_counter()
     while True:
-        mc.step()
+        loop.trial(0.9)
         n += 1
         el = time.perf_counter() - t0
         if el > seconds and n >= 2:
             break
-    mc.close()
     tps = n / el
+    n_native = int(kv["n_native"])
     cores = os.cpu_count()
-    return {"value": tps / s.n, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} trials of {what} ({s.n} particles) in {el:.1f} s (FP64, O(N^2) pairs + FP64 FFT per "
-                      f"trial, {cores} OpenMP threads); sweeps/s = trials/s / {s.n}: one replica's rate, the "
-                      f"host's aggregate over a replica set run one at a time",
+    return {"value": tps / n_native, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} trials of config-5 replica {name} ({n_native} particles, {s.n} atoms in the reference's "
+                      f"model, mesh {list(p.mesh)}) in {el:.1f} s: the reference's per-trial loop restated in FP64 "
+                      f"(half list built once, LJ + cubic SPME per trial) on {cores} OpenMP threads; sweeps/s = "
+                      f"trials/s / {n_native}: one replica's rate, the host's aggregate over a replica set run one "
+                      f"at a time",
             "trials_per_s": tps}
 
 
@@ -387,10 +485,11 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     import numpy as np
 
-    reps, eng, sur, tune, train = build_headline(args, local, rank)
+    reps, n_all, eng, sur, tune, train = build_headline(args, local, rank, world)
     ns = np.array([s.n for s, _ in reps], np.float64)
     T = args.trials
-    sweeps_per_step = float((T / ns).sum())
+    sweeps_per_step = float((T / ns).sum())  # this rank's replicas
+    total_sweeps_per_step = reduce_sum(sweeps_per_step, world, local)  # all ranks
     for _ in range(args.warmup):
         eng.run(T)
     # ---- device-timed region: inputs resident, L2 flushed between steps ----
@@ -409,7 +508,7 @@ def run_ours(args):
     eng.set_profiling(False)
     da1 = sums(eng.da_stats())
     max_ms = reduce_max(dev_ms, world, local)
-    value = world * args.steps * sweeps_per_step / (max_ms / 1e3)
+    value = args.steps * total_sweeps_per_step / (max_ms / 1e3)
 
     # ---- end to end through the public API: pinned host state of every replica in,
     #      state and energies out, every step ----
@@ -432,7 +531,7 @@ def run_ours(args):
     e2e_s = time.perf_counter() - t0
     barrier(world)
     e2e_s = reduce_max(e2e_s, world, local)
-    e2e = {"value": world * args.steps * sweeps_per_step / e2e_s, "unit": UNIT,
+    e2e = {"value": args.steps * total_sweeps_per_step / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": slots * (16 + 4 + 4), "d2h_bytes_per_step": slots * (16 + 4 + 4) + 8 * len(reps),
            "timing": "host wall clock around phmc_set_state(all replicas, from pinned host arrays) + phmc_run + "
                      "phmc_get_state(all replicas, into pinned host arrays), synchronous calls"}
@@ -463,12 +562,11 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 pair/mesh/FFT, f64 accumulation and Metropolis, bf16 surrogate",
-            "data": "synthetic (seeded brush generator, config-5 seed 2029 + 7919 * rank)",
-            "config": {"workload": WORKLOAD, "replicas": len(reps), "particles_min_max": [int(ns.min()), int(ns.max())],
-                       "trials_per_replica_per_step": T, "sweeps_per_step": sweeps_per_step,
-                       "tuning": eng.tuning(), "autotune": tune, "da_threshold": args.da_threshold,
-                       "l2": "flushed between steps (256 MiB write on the engine stream)",
-                       "parallelism": f"replicas only x{world}"},
+            "data": "synthetic (seeded brush generator, config-5 seed 2029; 256 replicas per GPU split by cost)",
+            "config": workload_config(len(n_all), n_all),
+            "step": {"trials_per_replica": T, "sweeps": total_sweeps_per_step, "replicas_this_rank": len(reps),
+                     "l2": "flushed between steps (256 MiB write on the engine stream)"},
+            "tuning": {"chosen": eng.tuning(), "autotune": tune, "da_threshold": args.da_threshold},
             "roofline": dict(rl[dominant], kernel=dominant) if dominant else None,
             "roofline_other": {k: v for k, v in rl.items() if k != dominant},
             "e2e": e2e, "gpu_launches": int(prof["kernel_launches"]),
@@ -490,17 +588,20 @@ def run_ours(args):
         line["batched_exact_sweeps_per_s"] = sweeps_per_step / (ms_ex / 1e3)
         line["titration_phase"] = titration_phase(eng, sur, [int(s.meta["n_sites"]) for s, _ in reps], args.da_threshold)
     eng.close()
+    ref_dir = tempfile.mkdtemp(prefix="phmc_ref_")
+    if rank == 0 and world == 1 and (not args.no_extras or not args.no_cpu_baseline):
+        k_small = int(np.argmin(n_all))
+        write_ref_inputs([config2_spec_line(), config5_spec_lines(2029, len(n_all))[k_small]], ref_dir)
     if rank == 0 and world == 1 and not args.no_extras:
         line["plain_config2"], c2 = plain_config2(args, local)
         try:
-            line["reference_phase2_on_device"] = reference_phase2_on_device(local)
+            line["reference_phase2_on_device"] = reference_phase2_on_device(local, ref_dir)
         except Exception as e:  # an extra: the headline line is printed regardless
             line["reference_phase2_on_device"] = {"error": str(e)[:300]}
         if not args.no_alpha:
             line["alpha_check"] = alpha_check(local, args.alpha_eq, args.alpha_sample)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        small = min(reps, key=lambda sp: sp[0].n)
-        line["cpu_baseline"] = cpu_baseline(small[0], small[1], args.cpu_seconds, "the smallest config-5 replica")
+        line["cpu_baseline"] = cpu_baseline(ref_dir, f"c5_{k_small:04d}", args.cpu_seconds)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -511,21 +612,10 @@ def run_ours(args):
 # ---------------------------------------------------------------------------
 # reference arm: the reference's CUDA build, one replica at a time
 # ---------------------------------------------------------------------------
-def ref_time(harness, sn, spacing, per_step, steps, warmup, seed):
-    """Trials/s of the reference's phase-2 identity-swap loop (MC/src/mc.cu:159-318, total
-    energy recomputed per trial) on `sn` in the reference's model."""
-    from ph_brush_b200 import configs
-    n_sites = int(((sn.flags & 2) != 0).sum())
-    n_charged = int((((sn.flags & 2) != 0) & (sn.q != 0)).sum())
-    s, p = configs.to_reference_semantics(sn, n_w=n_sites, spacing=spacing, seed=seed)
-    d = tempfile.mkdtemp()
-    configs.write_lammps_data(os.path.join(d, "in.data"), s)
-    pct = 100.0 * (n_charged + 0.5) / max(n_sites, 1)  # floor(pct/100 * sites) == current count
-    configs.write_params_in(os.path.join(d, "params.in"), p, spacing, extra={"target_pct": f"{pct:.8f}"})
-    r = subprocess.run([harness, "time", os.path.join(d, "in.data"), os.path.join(d, "params.in"),
-                        str(per_step * steps), str(per_step * warmup)], capture_output=True, text=True)
+def run_harness(args_):
+    r = subprocess.run([REF_HARNESS] + [str(a) for a in args_], capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("reference harness failed: " + r.stderr.strip()[-200:])
+        raise RuntimeError("reference harness failed: " + (r.stderr.strip() or r.stdout.strip())[-300:])
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
@@ -533,44 +623,66 @@ def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
         return
-    from ph_brush_b200 import configs
-    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
-    if not os.path.exists(harness):
-        print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build missing: run `make -C oracle ref`"}))
+    n_gpus = max(world, args.gpus)
+    if not (os.path.exists(REF_HARNESS) and os.path.exists(REF_INPUTS)):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build or input writer missing: run "
+                                                              "`make -C oracle ref inputs`"}))
         return
-    reps = configs.config5(seed=2029, n_rep=args.replicas)
-    ns = [s.n for s, _ in reps]
-    idx = sorted(range(len(reps)), key=lambda r: ns[r])
-    pick = sorted({idx[0], idx[len(idx) // 2], idx[-1]})
-    per_step = 10
+    if local:
+        os.environ.setdefault("CUDA_VISIBLE_DEVICES", str(local))
+    d = tempfile.mkdtemp(prefix="phmc_ref_")
+    n_rep = args.replicas * n_gpus
     try:
-        runs = [ref_time(harness, reps[r][0], 0.7, per_step, args.steps, args.warmup, 5 + r) for r in pick]
-        s2, _ = configs.config2()
-        run2 = ref_time(harness, s2, 0.7, 20, args.steps, args.warmup, 5)
+        t0 = time.perf_counter()
+        info = write_ref_inputs(config5_spec_lines(2029, n_rep) + [config2_spec_line()], d)
+        t_inputs = time.perf_counter() - t0
+        names = [f"c5_{k:04d}" for k in range(n_rep)]
+        with open(os.path.join(d, "list.txt"), "w") as fh:
+            fh.write("\n".join(os.path.join(d, nm) for nm in names) + "\n")
+        mix = run_harness(["mix", os.path.join(d, "list.txt"), args.steps, args.warmup, args.ref_trials, 0.9, 0.3, 2025])
+        with open(os.path.join(d, "list2.txt"), "w") as fh:
+            fh.write(os.path.join(d, "c2") + "\n")
+        mix2 = run_harness(["mix", os.path.join(d, "list2.txt"), 3, 1, 400, 0.9, 0.3, 2025])
+        p2 = run_harness(["time", os.path.join(d, "c2.data"), os.path.join(d, "c2.params"), 2000, 50])
     except RuntimeError as e:
-        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        print(json.dumps({"impl": "reference", "unavailable": str(e)[:300]}))
         return
-    # aggregate over the replica set run one at a time: R sweeps / sum_r N_r t_r, from the samples
-    per_sweep = [ns[r] / o["trials_per_s"] for r, o in zip(pick, runs)]
-    value = 1.0 / (sum(per_sweep) / len(per_sweep))
-    secs = sum(o["seconds"] for o in runs)
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brush generator)",
-            "config": {"workload": WORKLOAD + " -- reference: no batching and no surrogate, so the replicas run one at "
-                                  "a time in its model (LJ cut at 3 sigma, 1-2 exclusions, cubic SPME, mesh from "
-                                  "pme_spacing 0.7, its phase-2 identity swaps with a full energy per trial); "
-                                  "aggregate from the smallest, median and largest replica",
-                       "sampled_replicas": pick, "particles": [ns[r] for r in pick],
-                       "reference_atoms": [o["natoms"] for o in runs], "meshes": [o["mesh"] for o in runs],
-                       "trials_per_s": [o["trials_per_s"] for o in runs], "trials_per_step": per_step},
+    n_native = mix["n_native"]
+    assert n_native == [info[nm][1] for nm in names]
+    sweeps_per_step = sum(args.ref_trials / n for n in n_native)
+    secs = mix["seconds"]
+    value = args.steps * sweeps_per_step / secs
+    n2 = info["c2"][1]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n_gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (the same seeded brush generator: oracle/_build/ref_inputs)",
+            "config": workload_config(n_rep, n_native),
+            "step": {"trials_per_replica": args.ref_trials, "sweeps": sweeps_per_step,
+                     "note": "a bounded sample of the step: every replica, a few trials each"},
+            "reference_path": "the reference's CUDA build (oracle/_ref/ref_harness linked with MC/src/*.o, sm_100a): "
+                              "per trial its device writes (set_atom_identity), its total energy (LJ over the half "
+                              "list + pmeEnergy: memset, cubic spread, cuFFT R2C, influence, Thrust reductions; "
+                              "MC/src/mc.cu:43-60), its acceptance (GC pair flips, MC/src/mc.cu:379-440, mu = kT "
+                              "ln10 (pKa - pH); displacements: Metropolis on its float energies), writes back on "
+                              "rejection; replicas one after the other",
+            "model_differences": "in its own model: LJ cut and shifted at 3 sigma (no WCA / FENE), cubic SPME (the "
+                                 "reference has no other order), mesh from pme_spacing 0.75 (" +
+                                 str(sorted({tuple(m) for m in mix["meshes"]})) + "), a W-bead identity pool per "
+                                 "titratable site, the half list built once (not rebuilt after displacements); each "
+                                 "of these makes its trial cheaper, not dearer",
+            "attempted": mix["attempted"], "accepted": mix["accepted"], "setup_seconds": mix["setup_seconds"],
+            "inputs_seconds": t_inputs,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                             "sample": f"{per_step * args.steps} timed trials per sampled replica of "
-                                       "phase2_swap_jitter (MC/src/mc.cu:159-318) in the reference's CUDA build on "
-                                       "this B200 (one host thread), CUDA-event timed"},
+                             "sample": f"{args.ref_trials * args.steps} timed trials per replica of all {n_rep} "
+                                       "replicas in the reference's CUDA build on this B200 (one host thread drives "
+                                       "it), CUDA-event timed per step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "config2": {"workload": CFG2, "trials_per_s": run2["trials_per_s"],
-                        "sweeps_per_s": run2["trials_per_s"] / configs.config2()[0].n, "mesh": run2["mesh"]}}
+            "config2": {"workload": CFG2 + " -- in the reference's model (" + str(info["c2"][0]) + " atoms, mesh " +
+                                    str(mix2["meshes"][0]) + ")",
+                        "mix_sweeps_per_s": 3 * 400 / n2 / mix2["seconds"], "mix_trials_per_s": 3 * 400 / mix2["seconds"],
+                        "phase2_attempts_per_s": p2["trials_per_s"], "phase2_wall_attempts_per_s":
+                            p2["trials"] / p2["wall_seconds"], "phase2_attempts": p2["trials"]}}
     print(json.dumps(line))
 
 

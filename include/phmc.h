@@ -507,6 +507,12 @@ typedef struct phmc_gc_job {
     const int* w; int n_w;
     const int* cl; int n_cl;
     uint32_t* mt_state;                        /* in / out: the caller's generator, 625 words */
+    /* Fixed-mu sampling (no counterpart in the reference, whose loop always steers mu
+     * to its target): with fixed_mu != 0, mu stays at mu_kT / beta (e.g. kT ln10
+     * (pKa - pH) for constant-pH sampling of a weak base), there is no mu feedback
+     * and no target stop; the call ends after max_trials attempts. */
+    int fixed_mu;
+    double mu_kT;
 } phmc_gc_job;
 typedef struct phmc_gc_result {
     int attempted, accepted, accepted_forward, accepted_backward, blocks_done;

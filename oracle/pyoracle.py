@@ -152,6 +152,91 @@ def direct_ewald(x, y, z, q, box, alpha, epsilon_r, slab, tol=1e-12):
     return dict(zip(["real", "recip", "self", "qcorr", "slab", "total"], out))
 
 
+class RefTrialLoop:
+    """The reference's per-trial loop restated in FP64 on the host cores (the CPU
+    baseline): its total energy recomputed for every trial (MC/src/mc.cu:43-60) -- LJ
+    over the half list built once at set-up (MC/src/main.cu:127,
+    MC/src/energy_gpu.cu:14-75) plus SPME with its cubic spreading, moduli and
+    influence function (MC/src/pme.cu:132-457), OpenMP-parallel in the oracle library
+    -- in the benchmark's move mix: displacements of mobile atoms within the slab
+    (the reference has none; the half list is not rebuilt, as in the reference
+    harness) and the reference's grand-canonical pair flips (MC/src/mc.cu:379-440)
+    with mu held at kT ln10 (pKa - pH).  Works on a system in the reference's model
+    (reference types, as ph_brush_b200.files.reference_model returns it)."""
+
+    def __init__(self, sysa, prm, mobile, height, pH, pKa, seed=1, disp_max=0.3, nh=(3, 4), w_cl=(6, 7)):
+        self.s, self.p = sysa, prm
+        self.x, self.y, self.z, self.q = (np.array(getattr(sysa, k), np.float64) for k in "xyzq")
+        self.t = np.ascontiguousarray(sysa.type, np.int32)
+        self.box = np.asarray(sysa.box, np.float64)
+        bh, bl = bond_csr(sysa.n, sysa.bond_i, sysa.bond_j)
+        self.head, self.lst = half_list(self.x, self.y, self.z, self.box, prm.rc_coul, bh, bl)
+        if not len(self.lst):
+            self.lst = np.zeros(1, np.int32)
+        T = prm.n_types
+        self.eps = np.ascontiguousarray(prm.lj_eps, np.float64).ravel()
+        self.sig = np.ascontiguousarray(prm.lj_sig, np.float64).ravel()
+        self.sh = np.zeros(T * T)
+        L.orc_ref_lj_shift(T, self.eps.ctypes.data_as(_dp), self.sig.ctypes.data_as(_dp), prm.rc_lj,
+                           self.sh.ctypes.data_as(_dp))
+        self.mobile = np.asarray(mobile, np.int64)
+        self.height, self.dmax = float(height), float(disp_max)
+        self.mu = math.log(10.0) * (pKa - pH)  # kT units, beta = 1
+        self.nhn, self.nhp = nh
+        self.wt, self.clt = w_cl
+        self.rng = np.random.default_rng(seed)
+        self.E = self.energy()
+
+    def energy(self):
+        s, p = self.s, self.p
+        pl = lambda a: a.ctypes.data_as(_dp)
+        elj = L.orc_ref_lj(s.n, pl(self.x), pl(self.y), pl(self.z), self.t.ctypes.data_as(_ip),
+                           self.head.ctypes.data_as(_ip), self.lst.ctypes.data_as(_ip), p.n_types, pl(self.box),
+                           pl(self.eps), pl(self.sig), pl(self.sh), p.lj_shift)
+        out = np.zeros(4)
+        ec = L.orc_ref_pme(s.n, pl(self.x), pl(self.y), pl(self.z), pl(self.q), self.head.ctypes.data_as(_ip),
+                           self.lst.ctypes.data_as(_ip), pl(self.box), p.ewald_alpha, p.epsilon_r, p.mesh[0], p.mesh[1],
+                           p.mesh[2], p.order, p.slab, pl(out))
+        return elj + ec
+
+    def trial(self, p_disp=0.9):
+        r = self.rng
+        if r.random() < p_disp:
+            i = int(self.mobile[r.integers(len(self.mobile))])
+            old = (self.x[i], self.y[i], self.z[i])
+            nz = old[2] + self.dmax * (2 * r.random() - 1)
+            nx = (old[0] + self.dmax * (2 * r.random() - 1)) % self.box[0]
+            ny = (old[1] + self.dmax * (2 * r.random() - 1)) % self.box[1]
+            if not 0.0 <= nz < self.height:
+                return
+            self.x[i], self.y[i], self.z[i] = nx, ny, nz
+            Et = self.energy()
+            if Et - self.E <= 0 or math.exp(max(-40.0, -(Et - self.E))) > r.random():
+                self.E = Et
+            else:
+                self.x[i], self.y[i], self.z[i] = old
+            return
+        pools = [np.flatnonzero(self.t == k) for k in (self.nhn, self.nhp, self.wt, self.clt)]
+        a, b, c, d = (len(v) for v in pools)
+        wf, wb = a * c, b * d
+        if wf + wb == 0:
+            return
+        fwd = r.random() < wf / (wf + wb)
+        i = int(pools[0 if fwd else 1][r.integers(a if fwd else b)])
+        j = int(pools[2 if fwd else 3][r.integers(c if fwd else d)])
+        old = (self.t[i], self.q[i], self.t[j], self.q[j])
+        self.t[i], self.q[i] = (self.nhp, 1.0) if fwd else (self.nhn, 0.0)
+        self.t[j], self.q[j] = (self.clt, -1.0) if fwd else (self.wt, 0.0)
+        Et = self.energy()
+        s_after = (a - 1) * (c - 1) + (b + 1) * (d + 1) if fwd else (a + 1) * (c + 1) + (b - 1) * (d - 1)
+        logH = math.log(wf + wb) - math.log(s_after) if s_after > 0 else 0.0
+        expo = min(40.0, max(-40.0, -(Et - self.E - (1 if fwd else -1) * self.mu) + logH))
+        if expo >= 0 or math.exp(expo) > r.random():
+            self.E = Et
+        else:
+            self.t[i], self.q[i], self.t[j], self.q[j] = old
+
+
 def philox(key, ctr):
     k = np.ascontiguousarray(key, np.uint32)
     c = np.ascontiguousarray(ctr, np.uint32)

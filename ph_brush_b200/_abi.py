@@ -146,7 +146,7 @@ class GcJob(C.Structure):
                 ("gc_block", C.c_int), ("epoch_attempt_max", C.c_int), ("max_trials", C.c_int64),
                 ("nh_n", _ip), ("n_nh_n", C.c_int), ("nh_p", _ip), ("n_nh_p", C.c_int),
                 ("w", _ip), ("n_w", C.c_int), ("cl", _ip), ("n_cl", C.c_int),
-                ("mt_state", C.POINTER(C.c_uint32))]
+                ("mt_state", C.POINTER(C.c_uint32)), ("fixed_mu", C.c_int), ("mu_kT", C.c_double)]
 
 
 class GcResult(C.Structure):

@@ -46,6 +46,7 @@ struct GcDev {
     int o_type[2];           // identities of iP, iN before the attempt
     float o_q[2];
     int stop_after_restore;  // phase ends once the NH half is restored
+    int fixed;               // mu held fixed: no feedback, no target stop
 };
 
 // Per-replica constant description (the ragged descriptor table).

@@ -1274,7 +1274,9 @@ extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs
         g.eta = J.mu_eta > 0.0 ? (float)J.mu_eta : 0.3f;
         g.E = gc_energy_real(st[(size_t)J.replica], E.desc[J.replica].coulomb);
         g.max_trials = (int)std::min<int64_t>(J.max_trials > 0 ? J.max_trials : 1000000000, 1000000000);
-        if (g.Nprot == g.target) {
+        g.fixed = J.fixed_mu ? 1 : 0;
+        if (g.fixed) g.mu = (float)(J.mu_kT / J.beta);
+        if (!g.fixed && g.Nprot == g.target) {
             g.stop = PHMC_GC_STOP_ALREADY;
             phmc_gc_event ev;
             std::memset(&ev, 0, sizeof ev);
@@ -1296,7 +1298,7 @@ extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs
         R.attempted = g.attempted; R.accepted = g.accepted;
         R.accepted_forward = g.fwd; R.accepted_backward = g.bwd; R.blocks_done = g.blocks_done;
         R.Nh = g.Nh; R.Nprot = g.Nprot; R.target_count = g.target;
-        R.reached_target = (g.stop == PHMC_GC_STOP_REACHED || g.stop == PHMC_GC_STOP_ALREADY) ? 1 : 0;
+        R.reached_target = (g.stop == PHMC_GC_STOP_REACHED || g.stop == PHMC_GC_STOP_ALREADY) ? 1 : 0;  // never when fixed
         R.stop = g.stop;
         R.E = g.E; R.mu_eff = g.mu;
         const auto ke = gc_events_out(evs[k], events ? events + (size_t)k * event_cap : nullptr, event_cap);

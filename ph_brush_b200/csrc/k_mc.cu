@@ -507,7 +507,7 @@ __device__ int gc_decide(GcDev& G, const RepDesc& D, const RepState& S, const De
         if (G.dir > 0) G.fwd++; else G.bwd++;
         G.E = Et;
         G.Nprot += G.dir;
-        if (G.Nprot == G.target) {
+        if (!G.fixed && G.Nprot == G.target) {
             phmc_gc_event ev = gc_event_base(G, PHMC_GC_EV_REACHED);
             ev.step_in_block = G.block_t + 1;
             gc_event(G, d, ev);
@@ -520,7 +520,7 @@ __device__ int gc_decide(GcDev& G, const RepDesc& D, const RepState& S, const De
         ev.acc_rate = __fdiv_rn((float)G.block_acc, (float)G.block_att);
         gc_event(G, d, ev);
         G.block_t = 0; G.block_att = 0; G.block_acc = 0;
-        if (!(G.acc_mu < G.nacc_target && G.att_mu < G.amax)) {  // the epoch ends: mu update
+        if (!G.fixed && !(G.acc_mu < G.nacc_target && G.att_mu < G.amax)) {  // the epoch ends: mu update
             const float f = G.Nh > 0 ? __fdiv_rn((float)G.Nprot, (float)G.Nh) : 0.0f;
             const float lo = (float)1e-6, hi = (float)(1.0 - 1e-6);
             const float f1 = gc_clamp(f, lo, hi);

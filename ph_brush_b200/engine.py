@@ -163,6 +163,7 @@ class Engine:
         device, one job per replica.  Each job is a dict with the keys of phmc_gc_job:
         replica, nh_n_type, nh_p_type, w_type, cl_type (engine types), q_nh_p, q_cl, beta,
         target_pct, optional mu_eta, nacc_frac, gc_block, epoch_attempt_max, max_trials,
+        fixed_mu and mu_kT (mu held at mu_kT / beta: no feedback, no target stop),
         the pools nh_n, nh_p, w, cl (slot indices in the reference's order) and mt_state
         (uint32[625], updated in place).  Returns [(result dict, [event dicts])]."""
         n = len(jobs)
@@ -183,6 +184,8 @@ class Engine:
             J[k].gc_block = j.get("gc_block", 0)
             J[k].epoch_attempt_max = j.get("epoch_attempt_max", 0)
             J[k].max_trials = j.get("max_trials", 0)
+            J[k].fixed_mu = 1 if j.get("fixed_mu") else 0
+            J[k].mu_kT = j.get("mu_kT", 0.0)
             for key in ("nh_n", "nh_p", "w", "cl"):
                 a = _abi.as_i32(j[key])
                 keep.append(a)

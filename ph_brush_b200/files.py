@@ -51,3 +51,32 @@ def read_params(path, ntypes, strict=False):
     vals["mesh"] = tuple(fp.mesh)
     unknown = [u for u in unk.value.decode().split(",") if u]
     return vals, eps.reshape(ntypes, ntypes), sig.reshape(ntypes, ntypes), sh.reshape(ntypes, ntypes), unknown
+
+
+def reference_model(data_path, params_path):
+    """A system in the reference's model from its input files, as its driver sets it up
+    (MC/src/main.cu:102-139: positions wrapped, Lz padded by pme_3dc's factor, 0-based
+    types, 1-2 pairs excluded from LJ and real-space Coulomb, cubic SPME with the
+    reference's moduli, mesh from pme_spacing, slab correction with pme_3dc):
+    returns (SystemArrays, ModelParams) for an Engine."""
+    from .configs import ref_mesh
+    from .model import ModelParams, SystemArrays
+    d = read_lammps(data_path, wrap=True)
+    T = int(d["ntypes"])
+    v, eps, sig, sh, _ = read_params(params_path, T)
+    box = np.array(d["box"], np.float64)
+    slab = bool(v["pme_3dc"])
+    if slab:
+        box[2] *= max(2.0, v["pme_3dc_zfac"])
+    n = int(d["natoms"])
+    s = SystemArrays(d["x"].copy(), d["y"].copy(), d["z"].copy(), d["q"].copy(), (d["type"] - 1).astype(np.int32),
+                     np.zeros(n, np.int32), d["bond_i"].astype(np.int32), d["bond_j"].astype(np.int32), box, capacity=n,
+                     meta={"height": float(d["box"][2]), "zfac": float(box[2] / d["box"][2])})
+    order = int(v["pme_order"]) if v["pme_order"] > 0 else 4
+    coul = _abi.COUL_EWALD if v["coulomb"] == _abi.COUL_EWALD else v["coulomb"]
+    p = ModelParams(n_types=T, lj_eps=eps, lj_sig=sig, lj_rc=None, rc_lj=v["rc"], lj_shift=int(v["lj_shift"]),
+                    coulomb=coul, rc_coul=v["rc"], epsilon_r=v["epsilon_r"], ewald_alpha=v["ewald_alpha"],
+                    mesh=ref_mesh(box, v["pme_spacing"], order), order=order, ref_moduli=1, slab=1 if slab else 0,
+                    excl_bonded_lj=1, excl_bonded_coul=1, fene_k=0.0, wall_lo=0.0, wall_hi=0.0, beta=v["beta"],
+                    p_disp=0.0, p_titr=0.0, p_swap=0.0)
+    return s, p
