@@ -219,10 +219,29 @@ int phmc_set_move_mix(phmc_engine* e, int replica, double p_disp, double p_titr,
 typedef struct phmc_tuning {
     int pending_max;
     int threads;
-    double us_per_trial;  /* device time per trial (all replicas), autotune only */
+    double us_per_trial;  /* autotune only: device time per trial (all replicas) of a trial-run candidate */
+    /* tile shapes (phmc_set_tile_shapes) */
+    int zpass;            /* z pass of the potential-mesh rebuild: 0 the shared-memory Stockham pass, k > 0 a
+                             register-resident two-stage split nz = zpass_n1 x zpass_n2 (when every replica
+                             has the same nz and a split for it exists) */
+    int zpass_n1, zpass_n2;
+    int cand_round;       /* pair pass: candidate particles per thread and round (2, 4 or 8 at order 5; 4
+                             otherwise); a round's neighbour tile is cand_round x threads candidates */
+    int energy_block;     /* full recompute: particles per block of the pair / FENE pass (64, 128, 256) */
+    double rebuild_us;    /* autotune only: device time of one rebuild of every replica's potential mesh */
+    double recompute_us;  /* autotune only: device time of one full pair / FENE recompute of every replica */
 } phmc_tuning;
 int phmc_set_tuning(phmc_engine* e, int pending_max, int threads);
+/* The tile shapes above; -1 leaves a field as it is.  Decisions do not depend on them
+ * except through FP32 / FP64 rounding of summation orders. */
+int phmc_set_tile_shapes(phmc_engine* e, int zpass, int cand_round, int energy_block);
 int phmc_get_tuning(phmc_engine* e, phmc_tuning* out);
+/* Autotuner: first the z pass (the Stockham pass and every register split of the
+ * replicas' nz, timed as whole rebuilds), then the full recompute's block size,
+ * then pending_max x threads by trial runs of `trials` trials per replica (two
+ * interleaved passes, each candidate's faster time kept), then the pair pass's
+ * round width at the best pending_max x threads; keeps the fastest of each stage.
+ * results[] gets one entry per candidate timed, with that stage's time set. */
 int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_results, int* n_results);
 /* Launch quorum, 0 < quorum <= 1: an MC launch of a batched engine ends once that
  * fraction of the replicas still running at its start have filled their pending
@@ -241,6 +260,19 @@ int phmc_set_quorum(phmc_engine* e, double quorum);
  * device phase's results and events of that call are not written).  No
  * counterpart in the reference, whose loops are unbounded host loops. */
 int phmc_set_launch_budget(phmc_engine* e, int64_t max_launches);
+/* z-density profiles of the constant-pH runs (no counterpart in the reference,
+ * whose driver writes configurations only): with nbins in 1..PHMC_ZHIST_MAX_BINS,
+ * each replica's MC kernel adds, whenever its trial count reaches a multiple of
+ * `every` during phmc_run, the histogram over z of its charged titratable sites,
+ * anions and cations (nbins equal bins between the walls; [0, Lz) without walls)
+ * to a device accumulator and counts the sample; nbins = 0 switches it off.  The
+ * call clears the accumulators.  phmc_get_zhist gives one replica's sums,
+ * counts[3 * nbins] (sites, anions, cations), and its number of samples: the mean
+ * profile is counts / n_samples, the mean degree of ionisation the site counts'
+ * sum / (n_samples * titratable sites). */
+#define PHMC_ZHIST_MAX_BINS 64
+int phmc_set_zhist(phmc_engine* e, int nbins, int64_t every);
+int phmc_get_zhist(phmc_engine* e, int replica, double* counts, int64_t* n_samples);
 
 /* ---- input files of the reference's driver (host side, no device use) ----
  * LAMMPS "full" data files: phmc_lammps_header reads the header (counts, box

@@ -187,6 +187,13 @@ struct DevPtrs {
     int* gc_pool;
     int gc_pool_stride;
     unsigned char* gc_ev;  // event records of either phase (phmc_gc_event / phmc_phase2_event)
+    // z-density profiles (phmc_set_zhist): after every zh_every trials each replica's MC
+    // block adds its histogram over z (zh_bins bins between the walls) of charged sites,
+    // anions and cations to zhist[r][3][zh_bins] and counts the sample in zh_samples[r]
+    int zh_bins;
+    long long zh_every;
+    unsigned long long* zhist;
+    long long* zh_samples;
 };
 
 #define DSC_STRIDE (SUR_ROWS * SUR_K + 2 * SUR_ROWS + 4)

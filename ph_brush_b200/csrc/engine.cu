@@ -73,6 +73,15 @@ static void drop_graph(phmc_engine* h) {
 
 static int flush_dirty(phmc_engine* h);
 
+// Make z-pass variant `id` the active one (0: the shared-memory Stockham pass; else a
+// register split of the engines' common nz): job table, its per-replica offsets and the
+// shared memory the kernel needs.  The caller raises the kernel's shared-memory cap.
+static void select_zpass(Engine& E, int id) {
+    E.zreg = id;
+    if (id) { E.d_zjobs = E.d_zj_reg; E.n_zjobs = E.n_zj_reg; E.d_zjob_off = E.d_zoff_reg; E.zpass_smem = E.zpass_smem_reg; }
+    else { E.d_zjobs = E.d_zj_stk; E.n_zjobs = E.n_zj_stk; E.d_zjob_off = E.d_zoff_stk; E.zpass_smem = E.zpass_smem_stk; }
+}
+
 // Capture `chunks` x (MC launch + potential-mesh rebuild) on the engine stream.
 static int build_chunk_graph(phmc_engine* h, int chunks) {
     Engine& E = h->E;
@@ -418,8 +427,9 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     DALLOC(E.d_cell_rep, E.total_cells);
     int maxcap = 0;
     for (int r = 0; r < R; ++r) maxcap = std::max(maxcap, E.desc[r].cap);
-    E.energy_blocks = std::max(1, std::min(64, (maxcap + 127) / 128));
-    DALLOC(d.partials, (size_t)R * E.energy_blocks * 8);
+    E.energy_blocks = std::max(1, std::min(PHMC_FULL_MAX_BPR, (maxcap + 127) / 128));
+    E.max_cap = maxcap;
+    DALLOC(d.partials, (size_t)R * PHMC_FULL_MAX_BPR * 8);  // any energy_block's blocks per replica
     DALLOC(E.d_active, 1);
     CU(cudaMallocHost((void**)&E.h_active, sizeof(int)));
 
@@ -474,33 +484,34 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
         CU(cudaMemcpy(d.twiddle, h_tw.data(), sizeof(float2) * h_tw.size(), cudaMemcpyHostToDevice));
         if (!E.use_r2c) CU(cudaMemset(d.qfix, 0, sizeof(unsigned long long) * E.total_mesh));
         std::vector<int2> pj, pjb;  // all planes; the wall band's planes
-        std::vector<int4> zj;
-        std::vector<int> zoff;
-        // register z pass when every replica has the same supported nz
-        E.zreg = E.use_r2c ? zreg_variant(E.desc[0].mesh[2]) : 0;
+        std::vector<int4> zj, zjr;  // z-pass jobs: shared-memory (Stockham) pass; register pass
+        std::vector<int> zoff, zoffr;
+        // register z pass possible when every replica has the same nz with a register variant
+        E.zreg_default = E.use_r2c ? zreg_variant(E.desc[0].mesh[2]) : 0;
         E.plane_reg = E.use_r2c;
         for (int r = 0; r < R && E.plane_reg; ++r)
             if (!plane_reg_supported(E.desc[r].mesh[0], E.desc[r].mesh[1])) E.plane_reg = false;
-        for (int r = 1; r < R && E.zreg; ++r)
-            if (E.desc[r].mesh[2] != E.desc[0].mesh[2]) E.zreg = 0;
+        for (int r = 1; r < R && E.zreg_default; ++r)
+            if (E.desc[r].mesh[2] != E.desc[0].mesh[2]) E.zreg_default = 0;
         for (int r = 0; r < R; ++r) {
             const RepDesc& D = E.desc[r];
             for (int z = 0; z < D.mesh[2]; ++z) pj.push_back(make_int2(r, z));
             for (int i = 0; i < D.zb_n; ++i) pjb.push_back(make_int2(r, (D.zb_lo + i) % D.mesh[2]));
             zoff.push_back((int)zj.size());
+            zoffr.push_back((int)zjr.size());
             if (E.use_r2c) {
                 // column tiles of near-equal width <= ZPASS_TX over the nx/2+1 half-spectrum columns
                 const int nxh = D.mesh[0] / 2 + 1;
-                if (E.zreg) {
+                if (E.zreg_default) {
                     // ZREG_TX consecutive columns of the flattened ny x nxh plane per job
                     const int ncol = nxh * D.mesh[1];
-                    for (int c0 = 0; c0 < ncol; c0 += ZREG_TX) zj.push_back(make_int4(r, c0, std::min(ZREG_TX, ncol - c0), 0));
-                } else {
-                    const int nt = (nxh + ZPASS_TX - 1) / ZPASS_TX;
-                    const int w = (nxh + nt - 1) / nt;
-                    for (int y = 0; y < D.mesh[1]; ++y)
-                        for (int x0 = 0; x0 < nxh; x0 += w) zj.push_back(make_int4(r, y, x0, std::min(w, nxh - x0)));
+                    for (int c0 = 0; c0 < ncol; c0 += ZREG_TX) zjr.push_back(make_int4(r, c0, std::min(ZREG_TX, ncol - c0), 0));
+                    E.zpass_smem_reg = std::max(E.zpass_smem_reg, zreg_smem(D.mesh[2]));
                 }
+                const int nt = (nxh + ZPASS_TX - 1) / ZPASS_TX;
+                const int w = (nxh + nt - 1) / nt;
+                for (int y = 0; y < D.mesh[1]; ++y)
+                    for (int x0 = 0; x0 < nxh; x0 += w) zj.push_back(make_int4(r, y, x0, std::min(w, nxh - x0)));
                 // + cell counts / ids of the cell layers a plane's stencils reach (<= order + 5 layers)
                 const size_t ncell = (size_t)std::min(D.ncell[2], E.order + 5) * D.ncell[0] * D.ncell[1];
                 // band spread: the 64-bit charge plane + cell counts; first pass: two complex buffers
@@ -514,17 +525,25 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
                     for (int x0 = 0; x0 < D.mesh[0]; x0 += ZPASS_TX) zj.push_back(make_int4(r, y, x0, 0));
                 E.plane_smem = std::max(E.plane_smem, (size_t)2 * D.mesh[0] * D.mesh[1] * sizeof(float2));
             }
-            E.zpass_smem = std::max(E.zpass_smem, E.zreg ? zreg_smem(D.mesh[2]) : (size_t)2 * ZPASS_TX * D.mesh[2] * sizeof(float2));
+            E.zpass_smem_stk = std::max(E.zpass_smem_stk, (size_t)2 * ZPASS_TX * D.mesh[2] * sizeof(float2));
         }
         zoff.push_back((int)zj.size());
-        E.n_plane_jobs = (int)pj.size(); E.n_zjobs = (int)zj.size(); E.n_band_jobs = (int)pjb.size();
-        DALLOC(E.d_plane_jobs, pj.size()); DALLOC(E.d_zjobs, zj.size()); DALLOC(E.d_zjob_off, zoff.size());
+        zoffr.push_back((int)zjr.size());
+        E.n_plane_jobs = (int)pj.size(); E.n_band_jobs = (int)pjb.size();
+        E.n_zj_stk = (int)zj.size(); E.n_zj_reg = (int)zjr.size();
+        DALLOC(E.d_plane_jobs, pj.size()); DALLOC(E.d_zj_stk, zj.size()); DALLOC(E.d_zoff_stk, zoff.size());
         DALLOC(E.d_band_jobs, pjb.size());
         CU(cudaMemcpy(E.d_band_jobs, pjb.data(), sizeof(int2) * pjb.size(), cudaMemcpyHostToDevice));
-        DALLOC(E.d_epart, zj.size());
+        DALLOC(E.d_epart, std::max(zj.size(), zjr.size()));
         CU(cudaMemcpy(E.d_plane_jobs, pj.data(), sizeof(int2) * pj.size(), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(E.d_zjobs, zj.data(), sizeof(int4) * zj.size(), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(E.d_zjob_off, zoff.data(), sizeof(int) * zoff.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(E.d_zj_stk, zj.data(), sizeof(int4) * zj.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(E.d_zoff_stk, zoff.data(), sizeof(int) * zoff.size(), cudaMemcpyHostToDevice));
+        if (!zjr.empty()) {
+            DALLOC(E.d_zj_reg, zjr.size()); DALLOC(E.d_zoff_reg, zoffr.size());
+            CU(cudaMemcpy(E.d_zj_reg, zjr.data(), sizeof(int4) * zjr.size(), cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(E.d_zoff_reg, zoffr.data(), sizeof(int) * zoffr.size(), cudaMemcpyHostToDevice));
+        }
+        select_zpass(E, E.zreg_default);
         if (E.use_r2c) CU(rebuild_set_smem_limits(E));
         else CU(mesh_set_smem_limits(E));
     }
@@ -605,6 +624,8 @@ extern "C" int phmc_destroy(phmc_engine* h) {
     if (h->d_dE) cudaFree(h->d_dE);
     if (E.d.log_move) { cudaFree(E.d.log_move); cudaFree(E.d.log_dE); cudaFree(E.d.log_acc); }
     if (E.d.log_stage) { cudaFree(E.d.log_stage); cudaFree(E.d.log_dEs); }
+    if (E.d.zhist) cudaFree(E.d.zhist);
+    if (E.d.zh_samples) cudaFree(E.d.zh_samples);
     if (E.d.hv_cap > 0) { cudaFree(E.d.hv_rows); cudaFree(E.d.hv_sign); cudaFree(E.d.hv_target); cudaFree(E.d.hv_count); }
     for (void* p : {(void*)h->st_x, (void*)h->st_y, (void*)h->st_z, (void*)h->st_q, (void*)h->st_t, (void*)h->st_f,
                     (void*)h->st_err, (void*)h->st_cnt, (void*)h->d_charged, (void*)h->d_gc, (void*)h->d_gc_pool,
@@ -1604,6 +1625,46 @@ extern "C" int phmc_set_quorum(phmc_engine* h, double quorum) {
     return PHMC_OK;
 }
 
+extern "C" int phmc_set_zhist(phmc_engine* h, int nbins, int64_t every) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    if (nbins < 0 || nbins > PHMC_ZHIST_MAX_BINS) return fail(PHMC_ERR_ARG, "nbins must be in 0..PHMC_ZHIST_MAX_BINS");
+    if (nbins > 0 && every < 1) return fail(PHMC_ERR_ARG, "every must be >= 1");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    if (E.d.zhist) { cudaFree(E.d.zhist); E.d.zhist = nullptr; }
+    if (E.d.zh_samples) { cudaFree(E.d.zh_samples); E.d.zh_samples = nullptr; }
+    E.d.zh_bins = 0;
+    E.d.zh_every = 1;
+    if (nbins > 0) {
+        CU(cudaMalloc(&E.d.zhist, sizeof(unsigned long long) * 3 * nbins * (size_t)E.R));
+        CU(cudaMalloc(&E.d.zh_samples, sizeof(long long) * (size_t)E.R));
+        CU(cudaMemset(E.d.zhist, 0, sizeof(unsigned long long) * 3 * nbins * (size_t)E.R));
+        CU(cudaMemset(E.d.zh_samples, 0, sizeof(long long) * (size_t)E.R));
+        E.d.zh_bins = nbins;
+        E.d.zh_every = every;
+    }
+    drop_graph(h);  // the captured MC launches hold the device pointers by value
+    return PHMC_OK;
+}
+
+extern "C" int phmc_get_zhist(phmc_engine* h, int replica, double* counts, int64_t* n_samples) {
+    if (!h || !counts || !n_samples) return fail(PHMC_ERR_ARG, "null argument");
+    Engine& E = h->E;
+    if (replica < 0 || replica >= E.R) return fail(PHMC_ERR_ARG, "replica index out of range");
+    if (E.d.zh_bins <= 0) return fail(PHMC_ERR_STATE, "z-density profiles are off (phmc_set_zhist)");
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    const int nb = E.d.zh_bins;
+    std::vector<unsigned long long> c((size_t)3 * nb);
+    long long ns = 0;
+    CU(cudaMemcpy(c.data(), E.d.zhist + (size_t)replica * 3 * nb, sizeof(unsigned long long) * 3 * nb, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&ns, E.d.zh_samples + replica, sizeof(long long), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 3 * nb; ++k) counts[k] = (double)c[k];
+    *n_samples = ns;
+    return PHMC_OK;
+}
+
 extern "C" int phmc_set_launch_budget(phmc_engine* h, int64_t max_launches) {
     if (!h) return fail(PHMC_ERR_ARG, "null engine");
     if (max_launches < 0) return fail(PHMC_ERR_ARG, "launch budget must be >= 0");
@@ -1611,11 +1672,82 @@ extern "C" int phmc_set_launch_budget(phmc_engine* h, int64_t max_launches) {
     return PHMC_OK;
 }
 
+static void fill_tuning(const Engine& E, phmc_tuning* out) {
+    std::memset(out, 0, sizeof *out);
+    out->pending_max = E.pend_max;
+    out->threads = E.threads;
+    out->zpass = E.zreg;
+    zreg_split(E.zreg, &out->zpass_n1, &out->zpass_n2);
+    out->cand_round = E.cand_round;
+    out->energy_block = E.energy_block;
+}
+
 extern "C" int phmc_get_tuning(phmc_engine* h, phmc_tuning* out) {
     if (!h || !out) return fail(PHMC_ERR_ARG, "null argument");
-    out->pending_max = h->E.pend_max;
-    out->threads = h->E.threads;
-    out->us_per_trial = 0.0;
+    fill_tuning(h->E, out);
+    return PHMC_OK;
+}
+
+// Apply tile shapes (-1: unchanged) after checking them; the previous ones stay on failure.
+static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_block) {
+    Engine& E = h->E;
+    if (zpass >= 0 && zpass != E.zreg) {
+        int ids[8];
+        const int n = E.zreg_default ? zreg_variants(E.desc[0].mesh[2], ids, 8) : 0;
+        bool ok = zpass == 0;
+        for (int k = 0; k < n; ++k) ok = ok || ids[k] == zpass;
+        if (!ok || !E.use_r2c) return fail(PHMC_ERR_UNSUPPORTED, "z pass not available for these replicas' meshes");
+        const int old = E.zreg;
+        select_zpass(E, zpass);
+        cudaError_t e = rebuild_set_smem_limits(E);
+        if (e != cudaSuccess) {
+            select_zpass(E, old);
+            return fail(PHMC_ERR_UNSUPPORTED, std::string("z pass does not fit the device: ") + cudaGetErrorString(e));
+        }
+    }
+    if (cand_round >= 0 && cand_round != E.cand_round) {
+        if (cand_round != 2 && cand_round != 4 && cand_round != 8) return fail(PHMC_ERR_ARG, "cand_round must be 2, 4 or 8");
+        const int old = E.cand_round;
+        E.cand_round = cand_round;
+        cudaError_t e = prepare_mc(E);
+        if (e != cudaSuccess) {
+            E.cand_round = old;
+            return fail(PHMC_ERR_UNSUPPORTED, "cand_round other than 4 needs SPME order 5");
+        }
+    }
+    if (energy_block >= 0) {
+        if (energy_block != 64 && energy_block != 128 && energy_block != 256)
+            return fail(PHMC_ERR_ARG, "energy_block must be 64, 128 or 256");
+        E.energy_block = energy_block;
+    }
+    drop_graph(h);  // captured launches hold the old shapes
+    return PHMC_OK;
+}
+
+extern "C" int phmc_set_tile_shapes(phmc_engine* h, int zpass, int cand_round, int energy_block) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    CU(cudaSetDevice(h->E.device));
+    CU(cudaStreamSynchronize(h->E.stream));
+    return apply_tiles(h, zpass, cand_round, energy_block);
+}
+
+// Device time (ms) of `reps` launches of f on the engine stream, after one untimed launch.
+template <class F>
+static int time_launches(Engine& E, int reps, F f, double* ms_out) {
+    f();
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    CU(cudaEventRecord(a, E.stream));
+    for (int k = 0; k < reps; ++k) f();
+    CU(cudaEventRecord(b, E.stream));
+    CU(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CU(cudaGetLastError());
+    *ms_out = ms / reps;
     return PHMC_OK;
 }
 
@@ -1624,40 +1756,123 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     Engine& E = h->E;
     CU(cudaSetDevice(E.device));
     CU(cudaStreamSynchronize(E.stream));
+    int n = 0;
+    auto emit = [&](double us_trial, double us_rebuild, double us_recompute) {
+        if (results && n < max_results) {
+            fill_tuning(E, &results[n]);
+            results[n].us_per_trial = us_trial; results[n].rebuild_us = us_rebuild; results[n].recompute_us = us_recompute;
+        }
+        ++n;
+    };
+    // 1. z pass: whole rebuilds of every replica's potential from its current charge mesh
+    //    (the potential is a function of that mesh, so the timing leaves the state as it is)
+    if (E.coulomb == PHMC_COUL_EWALD && E.use_r2c && E.zreg_default) {
+        int ids[9] = {0};
+        const int nv = zreg_variants(E.desc[0].mesh[2], ids + 1, 8) + 1;
+        int best_id = E.zreg;
+        double best = 1e300;
+        for (int k = 0; k < nv; ++k) {
+            if (apply_tiles(h, ids[k], -1, -1) != PHMC_OK) continue;
+            double ms = 0.0;
+            int s = time_launches(E, 10, [&]() { launch_rebuild_r2c(E, nullptr, 0, E.stream); }, &ms);
+            if (s) return s;
+            emit(0.0, ms * 1e3, 0.0);
+            if (ms < best) { best = ms; best_id = ids[k]; }
+        }
+        int s = apply_tiles(h, best_id, -1, -1);
+        if (s) return s;
+    }
+    // 2. full recompute's block size (pair / FENE pass and its reduction; the tracked
+    //    pair energies it rewrites are those of the current state)
+    {
+        const int blocks[3] = {64, 128, 256};
+        int best_b = E.energy_block;
+        double best = 1e300;
+        for (int b : blocks) {
+            apply_tiles(h, -1, -1, b);
+            double ms = 0.0;
+            int s = time_launches(E, 5, [&]() { launch_full_energy(E, E.stream); }, &ms);
+            if (s) return s;
+            emit(0.0, 0.0, ms * 1e3);
+            if (ms < best) { best = ms; best_b = b; }
+        }
+        apply_tiles(h, -1, -1, best_b);
+    }
+    // 3. pending capacity x block size by trial runs; two passes over the candidates, each
+    //    candidate's faster one kept: the chains move on while the tuner runs, and
+    //    interleaving keeps that drift from favouring one candidate
     const int pends[] = {8, 16, 24, 32, 48, 64, 96, 128};
     const int ths[] = {128, 256};
-    // two passes over the candidates, each candidate's faster one kept: the chains move on
-    // while the tuner runs, and interleaving keeps that drift from favouring one candidate
     std::vector<double> best_us(16, 1e300);
     std::vector<char> fits(16, 0);
+    auto time_run = [&](double* us) -> int {
+        int s = phmc_run_loop(h, std::max<int64_t>(trials / 4, 4), 4);  // warm-up (captures the graph)
+        if (s) return s;
+        double ms = 0.0;
+        s = phmc_run_timed(h, trials, &ms);
+        if (s) return s;
+        *us = ms * 1e3 / (double)trials;
+        return PHMC_OK;
+    };
     for (int pass = 0; pass < 2; ++pass) {
         int c = 0;
-        for (int t : ths)
+        for (int th : ths)
             for (int pm : pends) {
                 const int k = c++;
                 if (pm > PHMC_MAX_PEND || (pass == 1 && !fits[k])) continue;
-                if (apply_tuning(h, pm, t) != PHMC_OK) continue;  // does not fit: skip
+                if (apply_tuning(h, pm, th) != PHMC_OK) continue;  // does not fit: skip
                 fits[k] = 1;
-                int s = phmc_run_loop(h, std::max<int64_t>(trials / 4, 4), 4);  // warm-up (captures the graph)
+                double us = 0.0;
+                int s = time_run(&us);
                 if (s) return s;
-                double ms = 0.0;
-                s = phmc_run_timed(h, trials, &ms);
-                if (s) return s;
-                best_us[k] = std::min(best_us[k], ms * 1e3 / (double)trials);
+                best_us[k] = std::min(best_us[k], us);
             }
     }
-    int best_p = E.pend_max, best_t = E.threads, n = 0, c = 0;
+    int best_p = E.pend_max, best_t = E.threads, c = 0;
     double best = 1e300;
-    for (int t : ths)
+    for (int th : ths)
         for (int pm : pends) {
             const int k = c++;
             if (!fits[k]) continue;
-            if (results && n < max_results) { results[n].pending_max = pm; results[n].threads = t; results[n].us_per_trial = best_us[k]; }
-            ++n;
-            if (best_us[k] < best) { best = best_us[k]; best_p = pm; best_t = t; }
+            if (best_us[k] < best) { best = best_us[k]; best_p = pm; best_t = th; }
         }
+    c = 0;
+    for (int th : ths)
+        for (int pm : pends) {
+            const int k = c++;
+            if (!fits[k]) continue;
+            if (results && n < max_results) {
+                fill_tuning(E, &results[n]);
+                results[n].pending_max = pm; results[n].threads = th; results[n].us_per_trial = best_us[k];
+            }
+            ++n;
+        }
+    int s = apply_tuning(h, best_p, best_t);
+    if (s) return s;
+    // 4. the pair pass's round width at that pending capacity and block size (order 5)
+    if (E.order == 5) {
+        const int rounds[3] = {4, 2, 8};
+        double rbest[3] = {best, 1e300, 1e300};
+        for (int pass = 0; pass < 2; ++pass)
+            for (int k = 1; k < 3; ++k) {
+                if (apply_tiles(h, -1, rounds[k], -1) != PHMC_OK) continue;
+                double us = 0.0;
+                s = time_run(&us);
+                if (s) return s;
+                rbest[k] = std::min(rbest[k], us);
+            }
+        int bk = 0;
+        for (int k = 1; k < 3; ++k) {
+            if (rbest[k] >= 1e300) continue;
+            apply_tiles(h, -1, rounds[k], -1);
+            emit(rbest[k], 0.0, 0.0);
+            if (rbest[k] < rbest[bk]) bk = k;
+        }
+        s = apply_tiles(h, -1, rounds[bk], -1);
+        if (s) return s;
+    }
     if (n_results) *n_results = n;
-    return apply_tuning(h, best_p, best_t);
+    return PHMC_OK;
 }
 
 extern "C" int phmc_delta_energy_components(phmc_engine* h, int rep, const phmc_trial* trials, int n,
@@ -1726,9 +1941,13 @@ extern "C" int phmc_checkpoint_save(phmc_engine* h, const char* path) {
     if (!f) return fail(PHMC_ERR_IO, std::string("cannot write ") + path);
     const DevPtrs& d = E.d;
     const size_t N = (size_t)E.total_slots, C = (size_t)E.total_cells;
-    const int hdr[7] = {1, E.R, E.total_slots, E.total_cells, E.cell_cap, (int)sizeof(RepState), E.pend_max};
+    // version 2: the tile shapes follow the quorum (they fix summation orders, so an exact
+    // resume needs them)
+    const int hdr[7] = {2, E.R, E.total_slots, E.total_cells, E.cell_cap, (int)sizeof(RepState), E.pend_max};
+    const int tiles[3] = {E.zreg, E.cand_round, E.energy_block};
     bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(hdr, sizeof(int), 7, f) == 7 &&
-              fwrite(&E.threads, sizeof(int), 1, f) == 1 && fwrite(&E.quorum, sizeof(float), 1, f) == 1;
+              fwrite(&E.threads, sizeof(int), 1, f) == 1 && fwrite(&E.quorum, sizeof(float), 1, f) == 1 &&
+              fwrite(tiles, sizeof(int), 3, f) == 3;
     for (int r = 0; r < E.R && ok; ++r) {
         const RepDesc& D = E.desc[r];
         const CkptRep cr = {D.cap, D.slot_off, {D.ncell[0], D.ncell[1], D.ncell[2]}, {D.mesh[0], D.mesh[1], D.mesh[2]},
@@ -1764,9 +1983,11 @@ extern "C" int phmc_checkpoint_load(phmc_engine* h, const char* path) {
     if (fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return bad("not a checkpoint");
     if (fread(hdr, sizeof(int), 7, f) != 7 || fread(&threads, sizeof(int), 1, f) != 1 || fread(&quorum, sizeof(float), 1, f) != 1)
         return bad("truncated header");
-    if (hdr[0] != 1 || hdr[1] != E.R || hdr[2] != E.total_slots || hdr[3] != E.total_cells || hdr[4] != E.cell_cap ||
-        hdr[5] != (int)sizeof(RepState))
+    if ((hdr[0] != 1 && hdr[0] != 2) || hdr[1] != E.R || hdr[2] != E.total_slots || hdr[3] != E.total_cells ||
+        hdr[4] != E.cell_cap || hdr[5] != (int)sizeof(RepState))
         return bad("written by an engine with other replicas, capacities or cells");
+    int tiles[3] = {E.zreg, E.cand_round, E.energy_block};
+    if (hdr[0] == 2 && fread(tiles, sizeof(int), 3, f) != 3) return bad("truncated header");
     std::vector<CkptRep> reps((size_t)E.R);
     for (int r = 0; r < E.R; ++r) {
         if (fread(&reps[r], sizeof(CkptRep), 1, f) != 1) return bad("truncated replica table");
@@ -1797,6 +2018,10 @@ extern "C" int phmc_checkpoint_load(phmc_engine* h, const char* path) {
     CU(cudaMemcpy(E.d.desc, E.desc.data(), sizeof(RepDesc) * E.R, cudaMemcpyHostToDevice));
     if (hdr[6] != E.pend_max || threads != E.threads) {
         const int s = apply_tuning(h, hdr[6], threads);
+        if (s) return s;
+    }
+    {
+        const int s = apply_tiles(h, tiles[0], tiles[1], tiles[2]);
         if (s) return s;
     }
     E.quorum = quorum;

@@ -20,6 +20,8 @@ struct Engine {
     long long total_oct = 0;
     int threads = 256;
     int pend_max = 16;
+    int cand_round = 4;          // pair pass: candidates per thread per round (2, 4, 8 at order 5)
+    int energy_block = 128;      // full recompute: particles per block of the pair / FENE pass
     float quorum = 0.2f;         // MC launch quorum of blocked replicas (1: every replica runs until it stops)
     cudaStream_t stream = nullptr;
     DevPtrs d{};
@@ -29,14 +31,18 @@ struct Engine {
     int2* d_plane_jobs = nullptr;
     int n_band_jobs = 0;
     int2* d_band_jobs = nullptr;  // (replica, z) of the planes in each replica's wall band
-    int4* d_zjobs = nullptr;
+    int4* d_zjobs = nullptr;     // the active z pass's jobs and per-replica job offsets
     int* d_zjob_off = nullptr;
+    int4* d_zj_stk = nullptr; int* d_zoff_stk = nullptr; int n_zj_stk = 0;  // shared-memory (Stockham) z pass
+    int4* d_zj_reg = nullptr; int* d_zoff_reg = nullptr; int n_zj_reg = 0;  // register z pass
+    size_t zpass_smem_stk = 0, zpass_smem_reg = 0;
     double* d_epart = nullptr;
     size_t plane_smem = 0, zpass_smem = 0;
     bool use_r2c = false;        // every replica has even nx: band charge mesh + real-to-complex rebuild
     size_t rb_fwd_smem = 0, rb_inv_smem = 0, band_spread_smem = 0;
     long long total_qband = 0;   // points of the wall bands' fixed-point charge meshes
-    int zreg = 0;                // register z-pass variant for the shared nz (0: shared-memory z pass)
+    int zreg = 0;                // active register z-pass variant for the shared nz (0: shared-memory z pass)
+    int zreg_default = 0;        // the default register variant of that nz (0: none; the Stockham pass only)
     bool plane_reg = false;      // register first / last passes (every replica's lateral mesh square and supported)
     int flush_kernels = 0;       // kernels per potential-mesh rebuild
     bool unit_pending = false;   // next rebuild places a unit charge instead of the particles
@@ -49,11 +55,14 @@ struct Engine {
     // full-energy scratch
     double* d_epair = nullptr;   // per (replica, block) partial components
     int energy_blocks = 0;
+    int max_cap = 0;             // largest replica capacity (slots)
     // host copies for trial logs
     std::vector<int> bonds_host;
     std::vector<void*> allocs;
     bool has_G = false;
 };
+
+#define PHMC_FULL_MAX_BPR 64  // blocks per replica of the full-recompute pass at most
 
 // engine.cu: records the thread's last error message
 void phmc_set_error(int code, const std::string& msg);
@@ -69,7 +78,9 @@ cudaError_t mesh_set_smem_limits(Engine& E);
 void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st);
 cudaError_t rebuild_set_smem_limits(Engine& E);
 void launch_band_spread(Engine& E, cudaStream_t st);
-int zreg_variant(int nz);      // register z-pass variant for nz, 0 if none
+int zreg_variant(int nz);      // default register z-pass variant for nz, 0 if none
+int zreg_variants(int nz, int* ids, int max_ids);  // every register variant for nz
+void zreg_split(int id, int* n1, int* n2);         // its two stages nz = n1 x n2
 size_t zreg_smem(int nz);
 bool plane_reg_supported(int nx, int ny);
 size_t plane_reg_smem(int n);

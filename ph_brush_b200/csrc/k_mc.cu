@@ -716,7 +716,9 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
     a = red[96]; b = red[97]; c = red[98];
 }
 
-template <int P, int NT, bool GC>
+// RC: candidate particles per thread and round of the pair pass (the neighbour tile of a
+// round is RC x NT candidates), a tuning parameter
+template <int P, int NT, bool GC, int RC = 4>
 __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
     constexpr int W = 2 * P - 1;
@@ -759,6 +761,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     // grand-canonical mu-control phase: the job's state (block blockIdx.x runs job blockIdx.x)
     __shared__ __align__(16) typename std::conditional<GC, GcDev, int>::type sG;
     __shared__ int s_gc_ops, s_gc_find, s_gc_lt;
+    __shared__ unsigned int s_zh[3 * PHMC_ZHIST_MAX_BINS];
 
     const int r = GC ? d.gc[blockIdx.x].replica : ((mode == MC_RUN) ? blockIdx.x : ext_rep);
     const int tid = threadIdx.x;
@@ -913,14 +916,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             // pass; outer cells -> class counts binned by the distance of the cell centre
             const int nk0 = D.dnk[0], nk1 = D.dnk[1], nk2 = D.dnk[2];
             const int nc3 = nk0 * nk1 * nk2;
-            constexpr int RC = 3;
+            constexpr int DRC = 3;
             const FastDiv f3(nc3), f2(nk0 * nk1), f1(nk0);
-            for (int e0 = tid; e0 < T.nch * nc3; e0 += RC * NT) {
-                int cell_u[RC], k_u[RC], sl_u[RC];
-                int4 cc_u[RC];
-                int3 c3_u[RC];
+            for (int e0 = tid; e0 < T.nch * nc3; e0 += DRC * NT) {
+                int cell_u[DRC], k_u[DRC], sl_u[DRC];
+                int4 cc_u[DRC];
+                int3 c3_u[DRC];
 #pragma unroll
-                for (int u = 0; u < RC; ++u) {  // all loads of the batch first
+                for (int u = 0; u < DRC; ++u) {  // all loads of the batch first
                     const int e = e0 + u * NT;
                     cell_u[u] = -1;
                     if (e >= T.nch * nc3) continue;
@@ -943,7 +946,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < RC; ++u) {
+                for (int u = 0; u < DRC; ++u) {
                     const int cell = cell_u[u];
                     if (cell < 0) continue;
                     if (sl_u[u] >= 0) {  // inner cell: count for the particle pass
@@ -1262,7 +1265,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const int so = D.slot_off;
             // RC candidates per thread and round: all list loads, then all particle loads, then
             // the pair terms (each thread still adds its candidates in increasing order)
-            constexpr int RC = 4;
             for (int it0 = tid; it0 < total; it0 += RC * NT) {
                 int j_u[RC], p_u[RC];
 #pragma unroll
@@ -1526,6 +1528,32 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 __syncthreads();
             }
         }
+        // z-density sample after every zh_every trials of the run (S.trial was advanced by
+        // this trial's proposal before the barriers above, so every thread sees one value)
+        if (!GC && mode == MC_RUN && d.zh_bins > 0 && S.trial % d.zh_every == 0) {
+            const int nb = d.zh_bins;
+            for (int k = tid; k < 3 * nb; k += NT) s_zh[k] = 0u;
+            __syncthreads();
+            const float z0 = D.walls ? D.wall_lo : 0.0f;
+            const float inv = (float)nb / (D.walls ? (D.wall_hi - D.wall_lo) : D.L[2]);
+            for (int i = tid; i < D.cap; i += NT) {
+                const int fl = d.flags[D.slot_off + i];
+                if (fl & PHMC_F_GHOST) continue;
+                const float4 pq = d.posq[D.slot_off + i];
+                int cls = -1;
+                if (fl & PHMC_F_TITRATABLE) cls = pq.w != 0.0f ? 0 : -1;
+                else if (fl & PHMC_F_ANION) cls = 1;
+                else if (fl & PHMC_F_CATION) cls = 2;
+                if (cls < 0) continue;
+                const int b = min(max((int)((pq.z - z0) * inv), 0), nb - 1);
+                atomicAdd(&s_zh[cls * nb + b], 1u);
+            }
+            __syncthreads();
+            unsigned long long* h = d.zhist + (size_t)r * 3 * nb;  // this replica's row: one block, no race
+            for (int k = tid; k < 3 * nb; k += NT) h[k] += s_zh[k];
+            if (tid == 0) d.zh_samples[r] += 1;
+            __syncthreads();
+        }
     }
     if constexpr (GC) {
         const int* src = reinterpret_cast<const int*>(&sG);
@@ -1543,7 +1571,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     }
 }
 
-template <int P, int NT>
+template <int P, int NT, int RC>
 static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
     DevPtrs dd = E.d;
     size_t smem = mc_smem_bytes(P, E.pend_max, false);
@@ -1551,7 +1579,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     if (E.d.sur.H > 0) {
         // three staged layers when two blocks per SM still fit, else two buffers
         cudaFuncAttributes fa;
-        cudaFuncGetAttributes(&fa, k_mc<P, NT, false>);
+        cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC>);
         int per_sm = 0;
         cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, E.device);
         const size_t three = mc_smem_bytes(P, E.pend_max, true);
@@ -1565,7 +1593,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     dd.quorum = 1.0f;
     if (mode == MC_RUN && E.quorum < 1.0f) {
         int per_sm = 0, nsm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT, false>, NT, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT, false, RC>, NT, smem);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
         if ((long long)per_sm * nsm >= E.R) {
             dd.quorum = E.quorum;
@@ -1573,7 +1601,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
             if (e != cudaSuccess) return e;
         }
     }
-    k_mc<P, NT, false><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
+    k_mc<P, NT, false, RC><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
 }
 
@@ -1611,25 +1639,33 @@ cudaError_t launch_mc_gc(Engine& E, int n_jobs, cudaStream_t st) {
 
 // Raise the dynamic shared-memory cap of the engine's MC kernel instance to the
 // device maximum (minus its static shared memory), once, outside any capture.
-template <int P, int NT>
+template <int P, int NT, int RC>
 static cudaError_t prepare_mc_t(Engine& E) {
     int optin = 0;
     cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
     if (e != cudaSuccess) return e;
     cudaFuncAttributes fa;
-    e = cudaFuncGetAttributes(&fa, k_mc<P, NT, false>);
+    e = cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC>);
     if (e != cudaSuccess) return e;
     const int cap = optin - (int)fa.sharedSizeBytes;
     if ((size_t)cap < mc_smem_bytes(P, E.pend_max, true)) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(k_mc<P, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+    return cudaFuncSetAttribute(k_mc<P, NT, false, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
 }
 
 cudaError_t prepare_mc(Engine& E) {
     const int NTh = E.threads;
+    // the pair pass's round width is tunable at order 5 (the configurations' order); 4 elsewhere
+    if (E.cand_round != 4 && E.order != 5) return cudaErrorInvalidValue;
     switch (E.order) {
-        case 4: return NTh == 128 ? prepare_mc_t<4, 128>(E) : prepare_mc_t<4, 256>(E);
-        case 5: return NTh == 128 ? prepare_mc_t<5, 128>(E) : prepare_mc_t<5, 256>(E);
-        default: return NTh == 128 ? prepare_mc_t<6, 128>(E) : prepare_mc_t<6, 256>(E);
+        case 4: return NTh == 128 ? prepare_mc_t<4, 128, 4>(E) : prepare_mc_t<4, 256, 4>(E);
+        case 5:
+            switch (E.cand_round) {
+                case 2: return NTh == 128 ? prepare_mc_t<5, 128, 2>(E) : prepare_mc_t<5, 256, 2>(E);
+                case 8: return NTh == 128 ? prepare_mc_t<5, 128, 8>(E) : prepare_mc_t<5, 256, 8>(E);
+                case 4: return NTh == 128 ? prepare_mc_t<5, 128, 4>(E) : prepare_mc_t<5, 256, 4>(E);
+                default: return cudaErrorInvalidValue;
+            }
+        default: return NTh == 128 ? prepare_mc_t<6, 128, 4>(E) : prepare_mc_t<6, 256, 4>(E);
     }
 }
 
@@ -1651,8 +1687,13 @@ size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate, bool two_bu
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
     const int NTh = E.threads;
     switch (E.order) {
-        case 4: return NTh == 128 ? launch_mc_t<4, 128>(E, mode, rep, t, n, dE, st) : launch_mc_t<4, 256>(E, mode, rep, t, n, dE, st);
-        case 5: return NTh == 128 ? launch_mc_t<5, 128>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256>(E, mode, rep, t, n, dE, st);
-        default: return NTh == 128 ? launch_mc_t<6, 128>(E, mode, rep, t, n, dE, st) : launch_mc_t<6, 256>(E, mode, rep, t, n, dE, st);
+        case 4: return NTh == 128 ? launch_mc_t<4, 128, 4>(E, mode, rep, t, n, dE, st) : launch_mc_t<4, 256, 4>(E, mode, rep, t, n, dE, st);
+        case 5:
+            switch (E.cand_round) {
+                case 2: return NTh == 128 ? launch_mc_t<5, 128, 2>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256, 2>(E, mode, rep, t, n, dE, st);
+                case 8: return NTh == 128 ? launch_mc_t<5, 128, 8>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256, 8>(E, mode, rep, t, n, dE, st);
+                default: return NTh == 128 ? launch_mc_t<5, 128, 4>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256, 4>(E, mode, rep, t, n, dE, st);
+            }
+        default: return NTh == 128 ? launch_mc_t<6, 128, 4>(E, mode, rep, t, n, dE, st) : launch_mc_t<6, 256, 4>(E, mode, rep, t, n, dE, st);
     }
 }

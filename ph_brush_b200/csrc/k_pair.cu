@@ -4,6 +4,7 @@
 // Replaces build_half_neighbors_gpu (O(N^2), MC/src/neighbor.cu:21-125) and
 // k_lj_energy / k_coul_energy / k_real_ewald_energy plus the Thrust
 // reductions of pmeEnergy (MC/src/energy_gpu.cu:14-135, MC/src/pme.cu:252-288,425-447).
+#include <algorithm>
 #include "common.cuh"
 #include "engine.h"
 
@@ -136,8 +137,14 @@ __global__ void k_full_reduce(DevPtrs d, int R, int bpr) {
     S.E = S.E_pair_lj + S.E_pair_c + S.E_fene + S.E_rec + S.E_self + S.E_qcorr + S.E_slab;
 }
 
+// Particles per block (E.energy_block: 64, 128 or 256) is a tuning parameter; blocks per
+// replica cover the largest replica, at most PHMC_FULL_MAX_BPR (the partials' size).
 void launch_full_energy(Engine& E, cudaStream_t st) {
-    dim3 grid(E.energy_blocks, E.R);
-    k_full_energy<128><<<grid, 128, 0, st>>>(E.d, E.energy_blocks);
-    k_full_reduce<<<(E.R + 127) / 128, 128, 0, st>>>(E.d, E.R, E.energy_blocks);
+    const int nt = E.energy_block;
+    const int bpr = std::max(1, std::min(PHMC_FULL_MAX_BPR, (E.max_cap + nt - 1) / nt));
+    dim3 grid(bpr, E.R);
+    if (nt == 64) k_full_energy<64><<<grid, 64, 0, st>>>(E.d, bpr);
+    else if (nt == 256) k_full_energy<256><<<grid, 256, 0, st>>>(E.d, bpr);
+    else k_full_energy<128><<<grid, 128, 0, st>>>(E.d, bpr);
+    k_full_reduce<<<(E.R + 127) / 128, 128, 0, st>>>(E.d, E.R, bpr);
 }

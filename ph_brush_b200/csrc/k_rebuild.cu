@@ -333,9 +333,13 @@ __global__ void __launch_bounds__(NT) k_rb_zreg(DevPtrs d, const int4* __restric
     if (threadIdx.x == 0) epart[blockIdx.x] = 0.5 * es;
 }
 
-// nz -> (N1, N2) of the register z pass; 0 = shared-memory z pass
+// (id, nz, N1, N2) of the register z passes; id 0 = shared-memory z pass.  The first entry
+// of an nz is its default; the others are the splits the autotuner also tries.
 #define ZREG_LIST(X) X(1, 48, 8, 6) X(2, 128, 16, 8) X(3, 162, 18, 9) X(4, 192, 16, 12) X(5, 216, 24, 9) \
-                     X(6, 243, 27, 9) X(7, 256, 16, 16) X(8, 288, 32, 9) X(9, 384, 32, 12)
+                     X(6, 243, 27, 9) X(7, 256, 16, 16) X(8, 288, 32, 9) X(9, 384, 32, 12)            \
+                     X(10, 48, 6, 8) X(11, 128, 8, 16) X(12, 162, 9, 18) X(13, 192, 12, 16)           \
+                     X(14, 216, 9, 24) X(15, 243, 9, 27) X(16, 288, 9, 32) X(17, 384, 24, 16)         \
+                     X(18, 384, 12, 32)
 constexpr int ZREG_NT(int n2) { return (n2 * ZREG_TX + 31) / 32 * 32 > 256 ? 256 : (n2 * ZREG_TX + 31) / 32 * 32; }
 
 int zreg_variant(int nz) {
@@ -343,6 +347,19 @@ int zreg_variant(int nz) {
     ZREG_LIST(ZREG_CASE)
 #undef ZREG_CASE
     return 0;
+}
+int zreg_variants(int nz, int* ids, int max_ids) {
+    int n = 0;
+#define ZREG_ALL(id, nn, a, b) if (nz == nn && n < max_ids) ids[n++] = id;
+    ZREG_LIST(ZREG_ALL)
+#undef ZREG_ALL
+    return n;
+}
+void zreg_split(int id, int* n1, int* n2) {
+    *n1 = 0; *n2 = 0;
+#define ZREG_SPLIT(i, nn, a, b) if (id == i) { *n1 = a; *n2 = b; }
+    ZREG_LIST(ZREG_SPLIT)
+#undef ZREG_SPLIT
 }
 size_t zreg_smem(int nz) { return (size_t)(ZREG_TX + 2) * nz * sizeof(float2); }
 

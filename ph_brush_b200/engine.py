@@ -121,10 +121,29 @@ class Engine:
         """MC launch quorum (0, 1]: a launch ends once that fraction of its running replicas is blocked."""
         _abi.check(self._lib.phmc_set_quorum(self._h, float(quorum)))
 
+    def set_tile_shapes(self, zpass=-1, cand_round=-1, energy_block=-1):
+        """z pass of the rebuild (0 Stockham, k > 0 a register split), pair-pass round width,
+        full-recompute block size; -1 keeps a field."""
+        _abi.check(self._lib.phmc_set_tile_shapes(self._h, int(zpass), int(cand_round), int(energy_block)))
+
     def set_launch_budget(self, max_launches):
         """Bound on the MC launches of one run / device-phase call (0: unbounded);
         a call that reaches it raises PhmcError(PHMC_ERR_BUDGET) with the state consistent."""
         _abi.check(self._lib.phmc_set_launch_budget(self._h, int(max_launches)))
+
+    def set_zhist(self, nbins, every=1000):
+        """z-density profiles: every `every` trials each replica's MC kernel adds its histogram
+        (nbins bins between the walls) of charged sites, anions and cations; 0 bins: off."""
+        _abi.check(self._lib.phmc_set_zhist(self._h, int(nbins), int(every)))
+        self._zh_bins = int(nbins)
+
+    def zhist(self, replica=0):
+        """(counts[3, nbins] summed over samples: sites, anions, cations; number of samples)."""
+        nb = self._zh_bins
+        c = np.zeros(3 * nb, np.float64)
+        n = C.c_int64()
+        _abi.check(self._lib.phmc_get_zhist(self._h, int(replica), _abi.dptr(c), C.byref(n)))
+        return c.reshape(3, nb), n.value
 
     def tuning(self):
         t = _abi.Tuning()
@@ -132,10 +151,12 @@ class Engine:
         return t.asdict()
 
     def autotune(self, trials):
-        res = (_abi.Tuning * 32)()
+        """Every candidate timed (z pass: rebuild_us; full-recompute block: recompute_us; pending
+        capacity x threads and pair-pass round width: us_per_trial); the engine keeps the best."""
+        res = (_abi.Tuning * 64)()
         n = C.c_int()
-        _abi.check(self._lib.phmc_autotune(self._h, int(trials), res, 32, C.byref(n)))
-        return [res[k].asdict() for k in range(min(n.value, 32))]
+        _abi.check(self._lib.phmc_autotune(self._h, int(trials), res, 64, C.byref(n)))
+        return [res[k].asdict() for k in range(min(n.value, 64))]
 
     def set_move_mix(self, p_disp, p_titr, p_swap=0.0, replica=-1):
         _abi.check(self._lib.phmc_set_move_mix(self._h, int(replica), float(p_disp), float(p_titr), float(p_swap)))
