@@ -230,17 +230,24 @@ typedef struct phmc_tuning {
     int energy_block;     /* full recompute: particles per block of the pair / FENE pass (64, 128, 256) */
     double rebuild_us;    /* autotune only: device time of one rebuild of every replica's potential mesh */
     double recompute_us;  /* autotune only: device time of one full pair / FENE recompute of every replica */
+    int first_stage;      /* 1: the attached surrogate judges titration / swap trials first (delayed
+                             acceptance); 0: no surrogate, or bypassed because exact trials ran faster */
 } phmc_tuning;
 int phmc_set_tuning(phmc_engine* e, int pending_max, int threads);
 /* The tile shapes above; -1 leaves a field as it is.  Decisions do not depend on them
  * except through FP32 / FP64 rounding of summation orders. */
 int phmc_set_tile_shapes(phmc_engine* e, int zpass, int cand_round, int energy_block);
 int phmc_get_tuning(phmc_engine* e, phmc_tuning* out);
+/* Cost-based fallback of delayed acceptance: on = 0 bypasses the attached surrogate's
+ * first stage (every trial plain Metropolis on the exact dE, as with no surrogate)
+ * without detaching it; on = 1 restores it.  The autotuner sets it by timing both. */
+int phmc_set_first_stage(phmc_engine* e, int on);
 /* Autotuner: first the z pass (the Stockham pass and every register split of the
  * replicas' nz, timed as whole rebuilds), then the full recompute's block size,
  * then pending_max x threads by trial runs of `trials` trials per replica (two
  * interleaved passes, each candidate's faster time kept), then the pair pass's
- * round width at the best pending_max x threads; keeps the fastest of each stage.
+ * round width at the best pending_max x threads, then, with a surrogate attached,
+ * its first stage on against bypassed; keeps the fastest of each stage.
  * results[] gets one entry per candidate timed, with that stage's time set. */
 int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_results, int* n_results);
 /* Launch quorum, 0 < quorum <= 1: an MC launch of a batched engine ends once that

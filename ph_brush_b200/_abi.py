@@ -110,7 +110,8 @@ class DAStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("pending_max", C.c_int), ("threads", C.c_int), ("us_per_trial", C.c_double),
                 ("zpass", C.c_int), ("zpass_n1", C.c_int), ("zpass_n2", C.c_int), ("cand_round", C.c_int),
-                ("energy_block", C.c_int), ("rebuild_us", C.c_double), ("recompute_us", C.c_double)]
+                ("energy_block", C.c_int), ("rebuild_us", C.c_double), ("recompute_us", C.c_double),
+                ("first_stage", C.c_int)]
 
     def asdict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -197,7 +198,7 @@ class Phase2Result(C.Structure):
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
-           "phmc_set_state", "phmc_set_quorum", "phmc_set_launch_budget", "phmc_set_tile_shapes", "phmc_set_zhist", "phmc_get_zhist", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
+           "phmc_set_state", "phmc_set_quorum", "phmc_set_launch_budget", "phmc_set_tile_shapes", "phmc_set_first_stage", "phmc_set_zhist", "phmc_get_zhist", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
            "phmc_recip_energy_static",
            "phmc_surrogate_create", "phmc_surrogate_destroy", "phmc_surrogate_num_params",
            "phmc_surrogate_get_params", "phmc_surrogate_set_params", "phmc_surrogate_set_scaling",
@@ -242,6 +243,7 @@ def load_library(path=LIB_PATH):
         "phmc_set_quorum": ([eng, C.c_double], C.c_int),
         "phmc_set_launch_budget": ([eng, C.c_int64], C.c_int),
         "phmc_set_tile_shapes": ([eng, C.c_int, C.c_int, C.c_int], C.c_int),
+        "phmc_set_first_stage": ([eng, C.c_int], C.c_int),
         "phmc_set_zhist": ([eng, C.c_int, C.c_int64], C.c_int),
         "phmc_get_zhist": ([eng, C.c_int, _dp, C.POINTER(C.c_int64)], C.c_int),
         "phmc_get_profile": ([eng, C.POINTER(Profile), C.c_int], C.c_int),

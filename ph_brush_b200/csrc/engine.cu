@@ -1506,6 +1506,7 @@ extern "C" int phmc_surrogate_attach(phmc_engine* h, phmc_surrogate* sur, double
     }
     drop_graph(h);  // captured launches hold the old kernel parameters
     E.d.sur = v;
+    E.first_stage_off = false;
     E.d.da_threshold = (float)threshold;
     E.d.da_window = window;
     std::vector<RepState> st((size_t)E.R);
@@ -1680,6 +1681,16 @@ static void fill_tuning(const Engine& E, phmc_tuning* out) {
     zreg_split(E.zreg, &out->zpass_n1, &out->zpass_n2);
     out->cand_round = E.cand_round;
     out->energy_block = E.energy_block;
+    out->first_stage = (E.d.sur.H > 0 && !E.first_stage_off) ? 1 : 0;
+}
+
+extern "C" int phmc_set_first_stage(phmc_engine* h, int on) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    CU(cudaSetDevice(h->E.device));
+    CU(cudaStreamSynchronize(h->E.stream));
+    h->E.first_stage_off = !on;
+    drop_graph(h);
+    return PHMC_OK;
 }
 
 extern "C" int phmc_get_tuning(phmc_engine* h, phmc_tuning* out) {
@@ -1870,6 +1881,26 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
         }
         s = apply_tiles(h, -1, rounds[bk], -1);
         if (s) return s;
+    }
+    // 5. cost-based fallback of delayed acceptance: the attached surrogate's first stage
+    //    against exact trials, both timed at the chosen shapes (two passes each)
+    if (E.d.sur.H > 0) {
+        double us_on = 1e300, us_off = 1e300;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int off = 0; off < 2; ++off) {
+                E.first_stage_off = off != 0;
+                drop_graph(h);
+                double us = 0.0;
+                s = time_run(&us);
+                if (s) { E.first_stage_off = false; return s; }
+                (off ? us_off : us_on) = std::min(off ? us_off : us_on, us);
+            }
+        E.first_stage_off = false;
+        emit(us_on, 0.0, 0.0);
+        E.first_stage_off = true;
+        emit(us_off, 0.0, 0.0);
+        E.first_stage_off = us_off < us_on;
+        drop_graph(h);
     }
     if (n_results) *n_results = n;
     return PHMC_OK;

@@ -1576,7 +1576,8 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     DevPtrs dd = E.d;
     size_t smem = mc_smem_bytes(P, E.pend_max, false);
     dd.sur_late_l3 = 0;
-    if (E.d.sur.H > 0) {
+    if (E.first_stage_off) dd.sur.H = 0;  // surrogate attached but bypassed: every trial exact
+    if (dd.sur.H > 0) {
         // three staged layers when two blocks per SM still fit, else two buffers
         cudaFuncAttributes fa;
         cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC>);

@@ -126,6 +126,10 @@ class Engine:
         full-recompute block size; -1 keeps a field."""
         _abi.check(self._lib.phmc_set_tile_shapes(self._h, int(zpass), int(cand_round), int(energy_block)))
 
+    def set_first_stage(self, on):
+        """Delayed acceptance's first stage on (1) or bypassed (0) with the surrogate still attached."""
+        _abi.check(self._lib.phmc_set_first_stage(self._h, int(on)))
+
     def set_launch_budget(self, max_launches):
         """Bound on the MC launches of one run / device-phase call (0: unbounded);
         a call that reaches it raises PhmcError(PHMC_ERR_BUDGET) with the state consistent."""
