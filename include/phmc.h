@@ -564,6 +564,18 @@ typedef struct phmc_gc_result {
 /* events: n_jobs x event_cap records (job k at k * event_cap), or null. */
 int phmc_gc_phase(phmc_engine* e, int n_jobs, const phmc_gc_job* jobs, phmc_gc_result* results,
                   phmc_gc_event* events, int event_cap);
+/* Streaming of the phases' event records (no counterpart in the reference, whose
+ * loops write their report lines as they go): after each MC launch of
+ * phmc_gc_phase / phmc_phase2 (and for the records made before the first one)
+ * the engine calls fn(user, job, phase, record) for every new record of every
+ * job, in order, before the call returns, so a phase that runs long or never
+ * reaches its target still reports as it runs.  phase 1: record is a
+ * phmc_gc_event, and results[job] of the running call already holds the set-up
+ * fields Nh, target_count, R0, Nacc_target, epoch_attempt_max and gc_block;
+ * phase 2: a phmc_phase2_event.  Records are also stored in the call's event
+ * arrays as before.  fn = NULL switches streaming off. */
+typedef void (*phmc_event_fn)(void* user, int job, int phase, const void* record);
+int phmc_set_event_callback(phmc_engine* e, phmc_event_fn fn, void* user);
 
 /* ---- the reference's phase 2 (swap / jitter with patience) on the device ----
  * Replaces phase2_swap_jitter (MC/include/mc.hpp:62-71, MC/src/mc.cu:159-318):

@@ -63,6 +63,10 @@ FILE_PARAMS_D2 = ("pH", "pKa", "salt_conc", "wall_lo", "wall_hi", "fene_k", "fen
                   "disp_max")
 
 
+# phmc_event_fn: (user, job, phase, record)
+EventFn = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int, C.c_void_p)
+
+
 class FileParams(C.Structure):
     _fields_ = ([(k, C.c_double) for k in FILE_PARAMS_D1] + [(k, C.c_int) for k in FILE_PARAMS_I] +
                 [(k, C.c_double) for k in FILE_PARAMS_D2] + [("mesh", C.c_int * 3)])
@@ -198,7 +202,7 @@ class Phase2Result(C.Structure):
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
-           "phmc_set_state", "phmc_set_quorum", "phmc_set_launch_budget", "phmc_set_tile_shapes", "phmc_set_first_stage", "phmc_set_zhist", "phmc_get_zhist", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
+           "phmc_set_state", "phmc_set_quorum", "phmc_set_launch_budget", "phmc_set_tile_shapes", "phmc_set_event_callback", "phmc_set_first_stage", "phmc_set_zhist", "phmc_get_zhist", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
            "phmc_recip_energy_static",
            "phmc_surrogate_create", "phmc_surrogate_destroy", "phmc_surrogate_num_params",
            "phmc_surrogate_get_params", "phmc_surrogate_set_params", "phmc_surrogate_set_scaling",
@@ -244,6 +248,7 @@ def load_library(path=LIB_PATH):
         "phmc_set_launch_budget": ([eng, C.c_int64], C.c_int),
         "phmc_set_tile_shapes": ([eng, C.c_int, C.c_int, C.c_int], C.c_int),
         "phmc_set_first_stage": ([eng, C.c_int], C.c_int),
+        "phmc_set_event_callback": ([eng, EventFn, C.c_void_p], C.c_int),
         "phmc_set_zhist": ([eng, C.c_int, C.c_int64], C.c_int),
         "phmc_get_zhist": ([eng, C.c_int, _dp, C.POINTER(C.c_int64)], C.c_int),
         "phmc_get_profile": ([eng, C.POINTER(Profile), C.c_int], C.c_int),

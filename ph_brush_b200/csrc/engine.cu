@@ -63,6 +63,9 @@ struct phmc_engine {
     unsigned char* d_gc_ev = nullptr;
     // MC launches one run / phase call may make (0: only the no-progress guard)
     long long launch_budget = 0;
+    // streaming of the device phases' event records
+    phmc_event_fn ev_fn = nullptr;
+    void* ev_user = nullptr;
 };
 
 static void drop_graph(phmc_engine* h) {
@@ -1191,9 +1194,19 @@ static int gc_job_common(phmc_engine* h, int replica, std::vector<int>& seen, co
 // rebuild of its replicas) until every job has stopped, collect the event records
 // (ev_size bytes each) and return the final job states in G.
 static int gc_run(phmc_engine* h, std::vector<GcDev>& G, const std::vector<const int* const*>& pools,
-                  const std::vector<const int*>& npools, size_t ev_size, std::vector<std::vector<unsigned char>>& evs) {
+                  const std::vector<const int*>& npools, size_t ev_size, std::vector<std::vector<unsigned char>>& evs,
+                  int phase) {
     Engine& E = h->E;
     const int n_jobs = (int)G.size();
+    // records not yet handed to the caller's stream callback
+    std::vector<size_t> streamed((size_t)n_jobs, 0);
+    auto stream_new = [&]() {
+        if (!h->ev_fn) return;
+        for (int k = 0; k < n_jobs; ++k)
+            for (; streamed[k] + ev_size <= evs[k].size(); streamed[k] += ev_size)
+                h->ev_fn(h->ev_user, k, phase, evs[k].data() + streamed[k]);
+    };
+    stream_new();  // records made before the first launch
     if (!h->d_gc) {
         CU(cudaMalloc((void**)&h->d_gc, sizeof(GcDev) * E.R));
         CU(cudaMalloc((void**)&h->d_gc_pool, sizeof(int) * 4 * (size_t)E.total_slots));
@@ -1227,6 +1240,7 @@ static int gc_run(phmc_engine* h, std::vector<GcDev>& G, const std::vector<const
             }
             all = all && G[k].stop != 0;
         }
+        stream_new();
         if (all) break;
         if (it > max_launches) return fail(PHMC_ERR_BUDGET, "device phase made no progress");
         if (h->launch_budget > 0 && it + 1 >= h->launch_budget)
@@ -1308,7 +1322,8 @@ extern "C" int phmc_gc_phase(phmc_engine* h, int n_jobs, const phmc_gc_job* jobs
         std::memset(&R, 0, sizeof R);
         R.R0 = R0; R.Nacc_target = g.nacc_target; R.epoch_attempt_max = g.amax; R.gc_block = g.gc_block;
     }
-    int s = gc_run(h, G, pools, npools, sizeof(phmc_gc_event), evs);
+    for (int k = 0; k < n_jobs; ++k) { results[k].Nh = G[k].Nh; results[k].target_count = G[k].target; }
+    int s = gc_run(h, G, pools, npools, sizeof(phmc_gc_event), evs, 1);
     if (s) return s;
     for (int k = 0; k < n_jobs; ++k) {
         const GcDev& g = G[k];
@@ -1382,7 +1397,7 @@ extern "C" int phmc_phase2(phmc_engine* h, int n_jobs, const phmc_phase2_job* jo
             g.stop = PHMC_P2_STOP_NO_PROPOSALS;
         }
     }
-    int s = gc_run(h, G, pools, npools, sizeof(phmc_phase2_event), evs);
+    int s = gc_run(h, G, pools, npools, sizeof(phmc_phase2_event), evs, 2);
     if (s) return s;
     for (int k = 0; k < n_jobs; ++k) {
         const GcDev& g = G[k];
@@ -1663,6 +1678,13 @@ extern "C" int phmc_get_zhist(phmc_engine* h, int replica, double* counts, int64
     CU(cudaMemcpy(&ns, E.d.zh_samples + replica, sizeof(long long), cudaMemcpyDeviceToHost));
     for (int k = 0; k < 3 * nb; ++k) counts[k] = (double)c[k];
     *n_samples = ns;
+    return PHMC_OK;
+}
+
+extern "C" int phmc_set_event_callback(phmc_engine* h, phmc_event_fn fn, void* user) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    h->ev_fn = fn;
+    h->ev_user = user;
     return PHMC_OK;
 }
 

@@ -519,11 +519,17 @@ PhaseGCResult phmc_ref_phase_gc_mu_control(System& sys, DeviceAtoms& d_atoms, co
     J.cl = cl.data(); J.n_cl = (int)cl.size();
     J.mt_state = mt.data();
     phmc_gc_result R;
-    std::vector<phmc_gc_event> ev((size_t)1 << 16);
-    ck(phmc_gc_phase(g.eng, 1, &J, &R, ev.data(), (int)ev.size()), "phmc_gc_phase");
+    std::vector<phmc_gc_event> ev((size_t)1 << 10);
+    // report lines written as the device phase runs (the reference writes them as it goes):
+    // each record goes to the report stream from the engine's event callback
+    struct Ctx { const phmc_gc_result* R; } ctx{&R};
+    ck(phmc_set_event_callback(g.eng, [](void* u, int, int, const void* rec) {
+           phmc_gc_write_event(mc_report(), *static_cast<const phmc_gc_event*>(rec), *static_cast<Ctx*>(u)->R);
+       }, &ctx), "phmc_set_event_callback");
+    const int rc = phmc_gc_phase(g.eng, 1, &J, &R, ev.data(), (int)ev.size());
+    phmc_set_event_callback(g.eng, nullptr, nullptr);
+    ck(rc, "phmc_gc_phase");
     rng_set(rng, mt);
-    for (int i = 0; i < R.n_events; ++i) phmc_gc_write_event(mc_report(), ev[(size_t)i], R);
-    if (R.events_dropped > 0) mc_report() << "[sgmc] " << R.events_dropped << " further report lines not kept" << std::endl;
     take_identities(sys, d_atoms);
     PhaseGCResult out;
     out.attempted = R.attempted; out.accepted = R.accepted;
@@ -581,11 +587,14 @@ Phase2Result phmc_ref_phase2_swap_jitter(System& sys, DeviceAtoms& d_atoms, cons
     J.cl = cl.data(); J.n_cl = (int)cl.size();
     J.mt_state = mt.data();
     phmc_phase2_result R;
-    std::vector<phmc_phase2_event> ev((size_t)1 << 16);
-    ck(phmc_phase2(g.eng, 1, &J, &R, ev.data(), (int)ev.size()), "phmc_phase2");
+    std::vector<phmc_phase2_event> ev((size_t)1 << 10);
+    ck(phmc_set_event_callback(g.eng, [](void*, int, int, const void* rec) {
+           phmc_p2_write_event(mc_report(), *static_cast<const phmc_phase2_event*>(rec));
+       }, nullptr), "phmc_set_event_callback");
+    const int rc = phmc_phase2(g.eng, 1, &J, &R, ev.data(), (int)ev.size());
+    phmc_set_event_callback(g.eng, nullptr, nullptr);
+    ck(rc, "phmc_phase2");
     rng_set(rng, mt);
-    for (int i = 0; i < R.n_events; ++i) phmc_p2_write_event(mc_report(), ev[(size_t)i]);
-    if (R.events_dropped > 0) mc_report() << "[phase2] " << R.events_dropped << " further report lines not kept\n";
     take_identities(sys, d_atoms);
     Phase2Result out;
     out.attempted = R.attempted;

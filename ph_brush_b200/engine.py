@@ -183,6 +183,16 @@ class Engine:
                                             _abi.fptr(q), _abi.iptr(t), _abi.iptr(f)))
         return {"x": x, "y": y, "z": z, "q": q, "type": t, "flags": f}
 
+    def set_event_callback(self, fn):
+        """fn(job, phase, record_address) after each launch of a device phase for every new
+        event record (phase 1: phmc_gc_event, 2: phmc_phase2_event); None switches it off."""
+        if fn is None:
+            self._ev_cb = None
+            _abi.check(self._lib.phmc_set_event_callback(self._h, _abi.EventFn(), None))
+            return
+        self._ev_cb = _abi.EventFn(lambda user, job, phase, rec: fn(job, phase, rec))
+        _abi.check(self._lib.phmc_set_event_callback(self._h, self._ev_cb, None))
+
     def gc_phase(self, jobs, event_cap=1 << 14):
         """The reference's grand-canonical mu-control phase (MC/src/mc.cu:320-548) on the
         device, one job per replica.  Each job is a dict with the keys of phmc_gc_job:

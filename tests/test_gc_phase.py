@@ -416,3 +416,27 @@ def test_phase_entry_points_refuse_bad_arguments_before_any_device_call():
     assert lib.phmc_gc_phase(None, 1, job, res, ev, 1) == 1  # PHMC_ERR_ARG
     j2, r2, e2 = _abi.Phase2Job(), _abi.Phase2Result(), _abi.Phase2Event()
     assert lib.phmc_phase2(None, 1, j2, r2, e2, 1) == 1
+
+
+@pytest.mark.gpu
+def test_event_records_stream_while_the_phase_runs():
+    """With a stream callback every record reaches the caller during the call, in order,
+    launch by launch (a fixed-mu phase of many launches never reaches a target and would
+    otherwise report nothing until max_trials), also beyond the stored records' capacity;
+    the stored records are the stream's first ones."""
+    s, p, job = gc_setup()
+    streamed = []
+    with Engine(s, p) as e:
+        e.set_tuning(8, 128)  # short launches: many of them
+        e.set_event_callback(lambda j, ph, rec: streamed.append(
+            (j, ph, _abi.GcEvent.from_address(rec).asdict())))
+        (res, evs), = e.gc_phase([dict(job, mt_state=mt_seeded(7), fixed_mu=1, mu_kT=0.5, max_trials=1200)],
+                                 event_cap=3)
+        e.set_event_callback(None)
+        (res2, _), = e.gc_phase([dict(job, mt_state=mt_seeded(8), fixed_mu=1, mu_kT=0.5, max_trials=100)])
+    assert res["attempted"] == 1200 and res["stop"] == _abi.GC_STOP_MAX_TRIALS and res["reached_target"] == 0
+    assert len(streamed) == res["n_events"] + res["events_dropped"] == 1200 // 50
+    assert all(j == 0 and ph == 1 for j, ph, _ in streamed)
+    assert [r for _, _, r in streamed][:3] == evs
+    assert [r["kind"] for _, _, r in streamed] == [_abi.GC_EV_CHUNK] * 24
+    assert len(streamed) == 24 and res2["attempted"] == 100  # no callback after it was switched off
