@@ -412,6 +412,10 @@ int phmc_recip_energy_static(const float* x, const float* y, const float* z, con
 #define PHMC_SUR_DESC_STRIDE (PHMC_SUR_ROWS * PHMC_SUR_INPUTS + 2 * PHMC_SUR_ROWS + 4)
 typedef struct phmc_surrogate phmc_surrogate;
 int phmc_surrogate_create(int n_in, int hidden, uint64_t seed, phmc_surrogate** out);
+/* Training products (forward, input and weight gradients) on the fifth-generation
+ * tensor cores (tcgen05.mma, FP32 accumulator in tensor memory) when tcgen05 != 0
+ * (the default), else on the mma.sync path; process-wide, for comparisons. */
+int phmc_surrogate_set_gemm(int tcgen05);
 int phmc_surrogate_destroy(phmc_surrogate* s);
 int phmc_surrogate_num_params(phmc_surrogate* s);
 /* flat FP32 parameters: W1[n_in*H], b1[H], W2[H*H], b2[H], W3[H*H], b3[H], w4[H], b4;

@@ -204,7 +204,7 @@ EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
            "phmc_set_state", "phmc_set_quorum", "phmc_set_launch_budget", "phmc_set_tile_shapes", "phmc_set_event_callback", "phmc_set_first_stage", "phmc_set_zhist", "phmc_get_zhist", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
            "phmc_recip_energy_static",
-           "phmc_surrogate_create", "phmc_surrogate_destroy", "phmc_surrogate_num_params",
+           "phmc_surrogate_create", "phmc_surrogate_set_gemm", "phmc_surrogate_destroy", "phmc_surrogate_num_params",
            "phmc_surrogate_get_params", "phmc_surrogate_set_params", "phmc_surrogate_set_scaling",
            "phmc_surrogate_get_scaling", "phmc_surrogate_predict", "phmc_surrogate_gradient",
            "phmc_surrogate_train", "phmc_surrogate_save", "phmc_surrogate_load", "phmc_harvest",
@@ -257,6 +257,7 @@ def load_library(path=LIB_PATH):
         "phmc_recip_energy_static": ([_fp, _fp, _fp, _fp, C.c_int, _dp, _ip, C.c_int, C.c_double, C.c_double,
                                       C.c_int, _dp], C.c_int),
         "phmc_surrogate_create": ([C.c_int, C.c_int, C.c_uint64, C.POINTER(eng)], C.c_int),
+        "phmc_surrogate_set_gemm": ([C.c_int], C.c_int),
         "phmc_surrogate_destroy": ([eng], C.c_int),
         "phmc_surrogate_num_params": ([eng], C.c_int),
         "phmc_surrogate_get_params": ([eng, _fp, C.c_int], C.c_int),

@@ -63,6 +63,12 @@ struct Engine {
     bool has_G = false;
 };
 
+// k_umma.cu: tcgen05 GEMM for the surrogate's training (N <= 256)
+cudaError_t launch_umma_gemm(int M, int N, int K, const __nv_bfloat16* A, long sai, long sak, const __nv_bfloat16* B,
+                             long sbk, long sbj, int epi, float* Cf, const float* bias, const float* Zin,
+                             __nv_bfloat16* Hb, int kchunk, int splits, cudaStream_t st);
+int umma_take_error(cudaStream_t st);
+
 #define PHMC_FULL_MAX_BPR 64  // blocks per replica of the full-recompute pass at most
 
 // engine.cu: records the thread's last error message

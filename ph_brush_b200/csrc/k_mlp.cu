@@ -130,26 +130,43 @@ __global__ void k_sum_splits(const float* __restrict__ part, int splits, int n, 
 
 #define GEMM_MAX_SPLITS 64
 
+// The training products run on the fifth-generation tensor cores (k_umma.cu: tcgen05.mma,
+// accumulator in tensor memory) when N is at most 256; the mma.sync kernel above is the
+// other path, selectable for comparison (phmc_surrogate_set_gemm).
+static bool g_gemm_tcgen05 = true;
+
+extern "C" int phmc_surrogate_set_gemm(int tcgen05) {
+    g_gemm_tcgen05 = tcgen05 != 0;
+    return PHMC_OK;
+}
+
+// PHMC_OK, or the error a tensor-core GEMM recorded since the last check (a bounded wait
+// that ran out: its output is not written).
+static int gemm_status() {
+    const int e = umma_take_error(0);
+    if (e) phmc_set_error(e, "surrogate GEMM: a tensor-core wait ran out (results not written)");
+    return e;
+}
+
 static void gemm(int M, int N, int K, const __nv_bfloat16* A, long sai, long sak, const __nv_bfloat16* B, long sbk,
                  long sbj, int epi, float* Cf, const float* bias, const float* Zin, __nv_bfloat16* Hb, cudaStream_t st,
                  float* split_buf = nullptr) {
+    const bool umma = g_gemm_tcgen05 && N <= 256;
     dim3 grid((N + 63) / 64, (M + 63) / 64, 1);
     // long-K products with few output tiles (weight gradients): split K over enough blocks to fill the GPU
     int splits = 1;
     if (epi == EPI_STORE && split_buf) {
-        const int tiles = grid.x * grid.y;
-        splits = std::min(GEMM_MAX_SPLITS, std::max(1, 296 / tiles));
+        const int tiles = umma ? (M + 127) / 128 : (int)(grid.x * grid.y);
+        splits = std::min(GEMM_MAX_SPLITS, std::max(1, (umma ? 148 : 296) / tiles));
         splits = std::min(splits, std::max(1, K / 256));
     }
     const int kchunk = ((K + splits - 1) / splits + 15) / 16 * 16;
     splits = (K + kchunk - 1) / kchunk;
     grid.z = splits;
-    if (splits == 1) {
-        k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, A, sai, sak, B, sbk, sbj, epi, Cf, bias, Zin, Hb, kchunk);
-        return;
-    }
-    k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, A, sai, sak, B, sbk, sbj, epi, split_buf, bias, Zin, Hb, kchunk);
-    k_sum_splits<<<(M * N + 255) / 256, 256, 0, st>>>(split_buf, splits, M * N, Cf);
+    float* out = splits == 1 ? Cf : split_buf;
+    if (umma) launch_umma_gemm(M, N, K, A, sai, sak, B, sbk, sbj, epi, out, bias, Zin, Hb, kchunk, splits, st);
+    else k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, A, sai, sak, B, sbk, sbj, epi, out, bias, Zin, Hb, kchunk);
+    if (splits > 1) k_sum_splits<<<(M * N + 255) / 256, 256, 0, st>>>(split_buf, splits, M * N, Cf);
 }
 
 // ---------------------------------------------------------------------------
@@ -549,7 +566,7 @@ extern "C" int phmc_surrogate_predict(phmc_surrogate* h, const float* x, int n, 
     cudaError_t e = cudaMemcpy(y, h->y, sizeof(float) * n, cudaMemcpyDeviceToHost);
     cudaFree(dx);
     if (e != cudaSuccess) { phmc_set_error(PHMC_ERR_CUDA, cudaGetErrorString(e)); return PHMC_ERR_CUDA; }
-    return PHMC_OK;
+    return gemm_status();
 }
 
 // loss and gradient (w.r.t. the flat master parameters) of n host samples with the current scaling
@@ -577,7 +594,7 @@ extern "C" int phmc_surrogate_gradient(phmc_surrogate* h, const float* x, const 
     if (e == cudaSuccess) e = cudaMemcpy(loss, h->loss, sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(dx); cudaFree(ds); cudaFree(dt);
     if (e != cudaSuccess) { phmc_set_error(PHMC_ERR_CUDA, cudaGetErrorString(e)); return PHMC_ERR_CUDA; }
-    return PHMC_OK;
+    return gemm_status();
 }
 
 // Adam training on device-resident samples (rows [ns][SUR_ROWS][nin], signs, targets).
@@ -625,6 +642,8 @@ int sur_train_device(phmc_surrogate* h, const float* d_x, const float* d_sign, c
     cudaFree(d_perm);
     if (e != cudaSuccess) { phmc_set_error(PHMC_ERR_CUDA, cudaGetErrorString(e)); return PHMC_ERR_CUDA; }
     h->packed_ok = false;
+    s = gemm_status();
+    if (s) return s;
     if (last_loss) *last_loss = nb ? lsum / nb : 0.0;
     return PHMC_OK;
 }

@@ -1,0 +1,241 @@
+// Fifth-generation tensor-core GEMM (tcgen05 / UMMA, sm_100a) for the surrogate's
+// training products: C[M x N] = sum_k A(i, k) B(k, j), BF16 operands, FP32
+// accumulation in tensor memory.  Same operand strides, epilogues and split-K
+// contract as the mma.sync GEMM in k_mlp.cu (A(i,k) = A[i*sai + k*sak],
+// B(k,j) = B[k*sbk + j*sbj]); no counterpart in the reference.
+//
+// One CTA of 128 threads per 128-row tile of C and all N <= 256 columns:
+//  * K advances in chunks of 64 through two shared-memory stages; all threads
+//    stage a chunk of A (128 x 64) and B (N x 64) in the canonical K-major
+//    layout without swizzle (8-row x 16-byte core matrices, 128 bytes each,
+//    consecutive in the M / N direction, the next 8 columns of K one
+//    "leading byte offset" further);
+//  * one thread issues the chunk's four 128 x N x 16 MMAs (tcgen05.mma
+//    .cta_group::1.kind::f16, smem descriptors for A and B, accumulator in
+//    TMEM) and commits them to the stage's mbarrier, which frees the stage
+//    for the chunk after next;
+//  * the epilogue reads the accumulator with tcgen05.ld (each warp its 32
+//    TMEM lanes = rows), applies the GEMM's epilogue and stores C.
+// Every wait on an mbarrier is bounded; a wait that runs out records
+// PHMC_ERR_BUDGET in *err, the CTA then waits (bounded) for its MMAs in flight,
+// frees its tensor memory and returns.
+#include <cstdint>
+#include "engine.h"
+
+namespace {
+
+constexpr int UM_KC = 64;      // K per stage
+constexpr int UM_ROWS = 128;   // M per CTA (one TMEM lane per row)
+constexpr uint32_t UM_WAIT = 1u << 22;
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: start address, leading (K-direction) and stride
+// (M/N-direction) byte offsets in 16-byte units, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M x N.
+__device__ __forceinline__ uint32_t umma_idesc(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(b)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+    for (uint32_t it = 0; it < UM_WAIT; ++it) {
+        uint32_t ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(ok)
+                     : "r"(su32(b)), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void umma_issue(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n"
+        :
+        : "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* b) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(b)) : "memory");
+}
+
+__device__ __forceinline__ float gelu_dev(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752440f)); }
+__device__ __forceinline__ float gelu_grad_dev(float x) {
+    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752440f));
+    const float pdf = 0.39894228040143267794f * expf(-0.5f * x * x);
+    return cdf + x * pdf;
+}
+
+// Stage one K chunk of `rows` rows (element (r, k) = src[(row0 + r) * s_r + (k0 + k) * s_k], zero
+// outside [0, nrow) x [k0, kend)) into the canonical K-major layout at dst.
+__device__ __forceinline__ void stage_tile(unsigned char* dst, int rows, const __nv_bfloat16* __restrict__ src,
+                                           long s_r, long s_k, int row0, int nrow, int k0, int kend) {
+    const __nv_bfloat16 z = __float2bfloat16(0.0f);
+    const int groups = rows >> 3;
+    for (int e = threadIdx.x; e < rows * UM_KC; e += blockDim.x) {
+        int r, k;
+        if (s_k == 1) { r = e / UM_KC; k = e - r * UM_KC; }  // lanes along the contiguous axis
+        else { k = e / rows; r = e - k * rows; }
+        const int gr = row0 + r, gk = k0 + k;
+        const __nv_bfloat16 v = (gr < nrow && gk < kend) ? src[(long)gr * s_r + (long)gk * s_k] : z;
+        const int off = (((k >> 3) * groups + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1);
+        *reinterpret_cast<__nv_bfloat16*>(dst + off) = v;
+    }
+}
+
+}  // namespace
+
+// epi 0 store (split z writes Cf + z M N), 1 bias + GELU (Z -> Cf, gelu(Z) -> Hb), 2 dZ = acc gelu'(Zin) -> Hb
+__global__ void __launch_bounds__(128, 1) k_umma_gemm(int M, int N, int K, const __nv_bfloat16* __restrict__ A, long sai,
+                                                      long sak, const __nv_bfloat16* __restrict__ B, long sbk, long sbj,
+                                                      int epi, float* __restrict__ Cf, const float* __restrict__ bias,
+                                                      const float* __restrict__ Zin, __nv_bfloat16* __restrict__ Hb,
+                                                      int kchunk, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char um_smem[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int Np = (N + 15) & ~15;                       // N of the MMA (multiple of 16)
+    const uint32_t ncols = Np <= 32 ? 32u : (Np <= 64 ? 64u : (Np <= 128 ? 128u : 256u));
+    const int a_bytes = UM_ROWS * UM_KC * 2, b_bytes = Np * UM_KC * 2;
+    unsigned char* stA[2] = {um_smem, um_smem + a_bytes + b_bytes};
+    unsigned char* stB[2] = {um_smem + a_bytes, um_smem + 2 * a_bytes + b_bytes};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = blockIdx.y * UM_ROWS;
+    const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
+    if (threadIdx.x == 0) { mbar_init(&s_bar[0]); mbar_init(&s_bar[1]); s_fail = 0; }
+    if (warp == 0) {  // tensor memory for the accumulator: ncols FP32 columns x 128 lanes
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&s_tmem)), "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = umma_idesc(UM_ROWS, Np);
+    const int nchunks = (kend - kbeg + UM_KC - 1) / UM_KC;
+    int issued = 0;  // chunks whose MMAs were committed
+    for (int c = 0; c < nchunks; ++c) {
+        const int b = c & 1;
+        if (c >= 2) {  // the stage's previous MMAs (chunk c - 2) must have read it
+            if (threadIdx.x == 0 && !mbar_wait(&s_bar[b], (uint32_t)(((c >> 1) - 1) & 1))) s_fail = 1;
+            __syncthreads();
+            if (s_fail) break;
+        }
+        const int k0 = kbeg + c * UM_KC;
+        stage_tile(stA[b], UM_ROWS, A, sai, sak, i0, M, k0, kend);
+        stage_tile(stB[b], Np, B, sbj, sbk, 0, N, k0, kend);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = su32(stA[b]), b0 = su32(stB[b]);
+#pragma unroll
+            for (int s = 0; s < UM_KC / 16; ++s) {
+                // K step s: core-matrix columns 2s and 2s + 1
+                const uint64_t da = umma_sdesc(a0 + 2 * s * (UM_ROWS / 8) * 128, (UM_ROWS / 8) * 128, 128);
+                const uint64_t db = umma_sdesc(b0 + 2 * s * (Np / 8) * 128, (Np / 8) * 128, 128);
+                umma_issue(tmem, da, db, idesc, (c > 0 || s > 0) ? 1u : 0u);
+            }
+            umma_commit(&s_bar[b]);
+        }
+        issued = c + 1;
+    }
+    // completion of every MMA issued: the last commit's phase (bounded); after a failed
+    // wait above, the chunks in flight are waited for the same way
+    if (threadIdx.x == 0 && issued > 0) {
+        const int cl = issued - 1;
+        if (!mbar_wait(&s_bar[cl & 1], (uint32_t)((cl >> 1) & 1))) s_fail = 1;
+        if (issued > 1 && s_fail) mbar_wait(&s_bar[(cl - 1) & 1], (uint32_t)(((cl - 1) >> 1) & 1));
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool ok = !s_fail;
+    if (ok && nchunks > 0) {
+        const int row = i0 + warp * 32 + lane;
+        if (epi == 0) Cf += (size_t)blockIdx.z * M * N;
+        for (int c0 = 0; c0 < Np; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int j = c0 + q;
+                    if (j >= N) break;
+                    const float acc = __uint_as_float(v[q]);
+                    const long o = (long)row * N + j;
+                    if (epi == 0) Cf[o] = acc;
+                    else if (epi == 1) {
+                        const float zz = acc + bias[j];
+                        Cf[o] = zz;
+                        Hb[o] = __float2bfloat16(gelu_dev(zz));
+                    } else {
+                        Hb[o] = __float2bfloat16(acc * gelu_grad_dev(Zin[o]));
+                    }
+                }
+            }
+        }
+    } else if (!ok && threadIdx.x == 0 && err) {
+        atomicExch(err, PHMC_ERR_BUDGET);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// Shared memory of one launch: two stages of A (128 x 64) and B (Np x 64) BF16.
+static size_t umma_gemm_smem(int N) {
+    const int Np = (N + 15) & ~15;
+    return (size_t)2 * (UM_ROWS * UM_KC * 2 + Np * UM_KC * 2);
+}
+
+// A failed bounded wait of any launch on this device (PHMC_ERR_BUDGET), cleared when read.
+static __device__ int g_umma_err;
+
+// Launch: grid (1, ceil(M / 128), splits); each split covers kchunk of K.
+cudaError_t launch_umma_gemm(int M, int N, int K, const __nv_bfloat16* A, long sai, long sak, const __nv_bfloat16* B,
+                             long sbk, long sbj, int epi, float* Cf, const float* bias, const float* Zin,
+                             __nv_bfloat16* Hb, int kchunk, int splits, cudaStream_t st) {
+    if (N < 1 || N > 256) return cudaErrorInvalidValue;
+    const size_t smem = umma_gemm_smem(N);
+    cudaError_t e = cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int* err = nullptr;
+    e = cudaGetSymbolAddress((void**)&err, g_umma_err);
+    if (e != cudaSuccess) return e;
+    dim3 grid(1, (M + UM_ROWS - 1) / UM_ROWS, splits);
+    k_umma_gemm<<<grid, 128, smem, st>>>(M, N, K, A, sai, sak, B, sbk, sbj, epi, Cf, bias, Zin, Hb, kchunk, err);
+    return cudaGetLastError();
+}
+
+// The recorded error of this device's launches (0 none), cleared; synchronises the stream.
+int umma_take_error(cudaStream_t st) {
+    int v = 0;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return PHMC_ERR_CUDA;
+    if (cudaMemcpyFromSymbol(&v, g_umma_err, sizeof(int)) != cudaSuccess) return PHMC_ERR_CUDA;
+    if (v) {
+        const int z = 0;
+        if (cudaMemcpyToSymbol(g_umma_err, &z, sizeof(int)) != cudaSuccess) return PHMC_ERR_CUDA;
+    }
+    return v;
+}

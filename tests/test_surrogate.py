@@ -123,8 +123,18 @@ def test_descriptor_rows_flip_sign_under_reversal():
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
+@pytest.fixture(params=[1, 0], ids=["tcgen05", "mma_sync"])
+def gemm_path(request):
+    """The training products on the fifth-generation tensor cores (tcgen05.mma, TMEM
+    accumulator) and on the mma.sync path; the process-wide switch is restored after."""
+    lib = _abi.lib()
+    assert lib.phmc_surrogate_set_gemm(request.param) == 0
+    yield request.param
+    lib.phmc_surrogate_set_gemm(1)
+
+
 @pytest.mark.gpu
-def test_forward_matches_oracle():
+def test_forward_matches_oracle(gemm_path):
     rng = np.random.default_rng(10)
     sur = Surrogate(seed=3)
     x = rng.normal(0, 1, (300, K)).astype(np.float32)
@@ -138,7 +148,7 @@ def test_forward_matches_oracle():
 
 
 @pytest.mark.gpu
-def test_gradient_matches_oracle():
+def test_gradient_matches_oracle(gemm_path):
     rng = np.random.default_rng(11)
     sur = Surrogate(seed=4)
     x, sign, t = random_samples(rng, 256)
@@ -153,6 +163,29 @@ def test_gradient_matches_oracle():
     assert rel < 1e-2, rel
     cos = g @ gx / (np.linalg.norm(g) * np.linalg.norm(gx))
     assert cos > 0.99, cos
+
+
+@pytest.mark.gpu
+def test_tcgen05_and_mma_sync_gradients_agree_at_batch_4096():
+    """A training batch's products (M = 16384 rows, weight gradients split over K) on both
+    tensor-core paths: the same FP32 sums in other orders, so the same gradient to FP32
+    rounding of the BF16 products' sums."""
+    rng = np.random.default_rng(14)
+    x, sign, t = random_samples(rng, 4096)
+    mu, sd = x.reshape(-1, K).mean(0), x.reshape(-1, K).std(0) + 0.5
+    out = []
+    lib = _abi.lib()
+    try:
+        for path in (1, 0):
+            lib.phmc_surrogate_set_gemm(path)
+            sur = Surrogate(seed=15)
+            sur.set_scaling(mu, sd, 3.0)
+            out.append(sur.gradient(x, sign, t, clip=25.0))
+    finally:
+        lib.phmc_surrogate_set_gemm(1)
+    (l1, g1), (l0, g0) = out
+    assert abs(l1 - l0) <= 1e-4 * abs(l0), (l1, l0)
+    assert np.linalg.norm(g1 - g0) <= 2e-3 * np.linalg.norm(g0), np.linalg.norm(g1 - g0) / np.linalg.norm(g0)
 
 
 @pytest.mark.gpu
