@@ -129,11 +129,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline only (plain comparison, phases, alpha skipped)")
     ap.add_argument("--no-alpha", action="store_true")
+    ap.add_argument("--no-config1", action="store_true")
+    ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--plain-config2-only", action="store_true",
                     help="only the plain engine on config 2 (one JSON line of its figures; for profiling)")
-    ap.add_argument("--alpha-eq", type=int, default=1200, help="sweeps of equilibration in the alpha(pH) check")
-    ap.add_argument("--alpha-sample", type=int, default=600, help="sweeps sampled in the alpha(pH) check")
+    ap.add_argument("--alpha-eq", type=int, default=400, help="sweeps of equilibration in the alpha(pH) check")
+    ap.add_argument("--alpha-sample", type=int, default=300, help="sweeps sampled in the alpha(pH) check")
     ap.add_argument("--ref-trials", type=int, default=4,
                     help="reference arm: trials per replica per step (its bounded sample of the step)")
     return ap.parse_args()
@@ -325,6 +327,62 @@ def titration_phase(eng, sur, n_sites, threshold):
             "gain": ms_p / ms_d, "exact_dE_skipped": 1.0 - ps / max(ev, 1), "second_stage_agreement": ac / max(ps, 1)}
 
 
+def engine_rate(eng, ns, trials, steps=3):
+    """Aggregate sweeps/s and trials/s of `steps` timed runs of `trials` trials per replica
+    (L2 flushed before each), with each kernel family's share and algorithmic bandwidth."""
+    eng.set_profiling(True)
+    eng.profile(reset=True)
+    ms = 0.0
+    for _ in range(steps):
+        eng.flush_l2(256 << 20)
+        ms += eng.run_timed(trials)
+    prof = eng.profile(reset=True)
+    eng.set_profiling(False)
+    sweeps = steps * sum(trials / n for n in ns)
+    out = {"sweeps_per_s": sweeps / (ms / 1e3), "trials_per_s": steps * trials * len(ns) / (ms / 1e3),
+           "ms_per_run": ms / steps, "tuning": eng.tuning()}
+    peak, kind = measured_peak()
+    for name, t_ms, by, nl in (("k_mc", prof["mc_ms"], prof["mc_alg_bytes"], prof["mc_launches"]),
+                               ("mesh_rebuild", prof["flush_ms"], prof["flush_alg_bytes"], prof["flush_launches"])):
+        if nl:
+            gbs = by / (t_ms / 1e3) / 1e9
+            out[name] = {"share": t_ms / ms, "alg_gbs": gbs, "frac": gbs / peak, "peak_source": kind,
+                         "launches": nl, "avg_launch_ms": t_ms / nl}
+    return out
+
+
+def config1_run(local, trials=20000):
+    """Config 1: one small brush (16 chains x 20 beads, 4x4 lattice, 16x16x40 padded to 120,
+    mesh 32x32x128, order 5), the plain engine (exact dE), autotuned."""
+    from ph_brush_b200 import Engine, configs
+    s, p = configs.config1()
+    with Engine(s, p, device=local) as eng:
+        tune = eng.autotune(4000)
+        eng.run(trials)
+        out = engine_rate(eng, [s.n], trials)
+    out.update(workload="config 1: 16 chains x 20 titratable beads (pKa 7.5, pH 7.5), 16x16x40 padded to 120, "
+                        "mesh 32x32x128, order 5, 90% displacement / 10% protonation, plain engine",
+               particles=s.n, autotune_candidates=len(tune))
+    return out
+
+
+def config3_run(local, trials=1000):
+    """Config 3: 96 replicas, pH 4.0-9.75 x salt 0.001-0.5 M, grafting density 0.05/0.1/0.2,
+    chain length 30-60: uneven particle counts and meshes in one engine (one MC launch per
+    chunk for all replicas, the Stockham z pass for the differing nz), exact dE, autotuned."""
+    from ph_brush_b200 import Engine, configs
+    reps = configs.config3()
+    ns = [s.n for s, _ in reps]
+    with Engine([s for s, _ in reps], [p for _, p in reps], device=local) as eng:
+        tune = eng.autotune(trials)
+        eng.run(trials)
+        out = engine_rate(eng, ns, trials)
+    out.update(workload="config 3: 96 replicas, pH 4.0-9.75 x salt {0.001, 0.01, 0.1, 0.5} M, grafting density "
+                        "0.05/0.1/0.2, chains of 30-60 beads, meshes 32-36 x 162-288, batched exact",
+               replicas=len(reps), particles_min_max=[min(ns), max(ns)], autotune_candidates=len(tune))
+    return out
+
+
 def config4_run(local, samples=2_000_000, epochs=4, trials=4000):
     """Config 4: the config-2 system (10x10 chains x 50 titratable beads, 0.1 M salt) with
     reservoir Na+/Cl- pair swaps (85 % displacement / 10 % protonation / 5 % swaps), at 8 pH
@@ -400,59 +458,86 @@ def _alpha(stats, n_sites):
     return [st["n_charged_sites"] / n for st, n in zip(stats, n_sites)]
 
 
-def alpha_check(local, sweeps_eq, sweeps_sample, snaps=20):
-    """alpha(pH) of delayed acceptance against the plain engine on config-5 chemistry (small
-    diblock replicas that equilibrate within the run).  The plain engine equilibrates, its
-    exact dE of the last part of the equilibration train the surrogate, a second engine takes
-    over the equilibrated states with delayed acceptance, and both engines then sample."""
+def alpha_check(local, sur, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins=16, max_rounds=3):
+    """alpha(pH) and z-profiles of delayed acceptance against the plain engine on real config-5
+    replicas (the 24 smallest of the headline set, its move mix; batched exact is the plain
+    engine): the plain engine equilibrates until the drift of its degree of ionisation
+    between the two halves of a sample is below 0.002 (at most max_rounds rounds), a second
+    engine takes over the equilibrated states with the headline's surrogate as first stage,
+    and both sample `sweeps_sample` sweeps; every 250 trials each replica's MC kernel adds
+    its z-histogram (phmc_set_zhist), read back per block."""
     import numpy as np
-    from ph_brush_b200 import Engine, Surrogate, configs
-    reps = configs.diblock_small()
-    S, P = [a for a, _ in reps], [b for _, b in reps]
-    for p in P:
-        p.p_disp, p.p_titr = 0.5, 0.5  # titration-heavy: alpha relaxes within the run
-    ns = [a.meta["n_sites"] for a in S]
-    nmax = max(a.n for a in S)
+    from ph_brush_b200 import Engine, configs
+    allr = configs.config5(seed=2029, n_rep=256)
+    idx = sorted(range(len(allr)), key=lambda k: allr[k][0].n)[:n_rep]
+    S, P = [allr[k][0] for k in idx], [allr[k][1] for k in idx]
+    ns_site = np.array([s.meta["n_sites"] for s in S], np.float64)
+    nmax = max(s.n for s in S)
+    per_block = max(1, sweeps_sample * nmax // blocks)
+
+    def sample(eng):
+        """per-block alpha [blocks, R] and mean profiles [R, 3, nbins] over the sample"""
+        eng.set_zhist(nbins, every=250)
+        prev = [(np.zeros((3, nbins)), 0)] * len(S)
+        a = []
+        for _ in range(blocks):
+            eng.run(per_block)
+            cur = [eng.zhist(r) for r in range(len(S))]
+            a.append([(c[0][0].sum() - p_[0][0].sum()) / max(c[1] - p_[1], 1) / ns_site[r]
+                      for r, (c, p_) in enumerate(zip(cur, prev))])
+            prev = cur
+        prof = np.array([c[0] / max(c[1], 1) for c in prev])
+        eng.set_zhist(0)
+        return np.array(a), prof
+
     A = Engine(S, P, device=local)
     A.autotune(2000)
     A.run(sweeps_eq * nmax)
-    A.harvest(131072)
-    A.run(max(nmax * 10, 2 * 131072 // len(S)))
-    sur = Surrogate(seed=31)
-    loss = A.surrogate_fit(sur, epochs=12, batch=2048, lr=1e-3, clip=25.0, seed=3)
-    A.harvest(0)
+    rounds, drift = 0, 1.0
+    while True:
+        rounds += 1
+        a_p, prof_p = sample(A)
+        half = blocks // 2
+        drift = float(np.abs(a_p[half:].mean(0) - a_p[:half].mean(0)).mean())
+        if drift < 0.002 or rounds >= max_rounds:
+            break
     B = Engine(S, P, device=local)
     tn = A.tuning()
     B.set_tuning(tn["pending_max"], tn["threads"])
     B.set_state(A.state(-1), -1)
     B.attach_surrogate(sur, threshold=0.0, window=0)
-    per = max(1, sweeps_sample * nmax // snaps)
-    a_p, a_d = [], []
-    for _ in range(snaps):
-        a_p.append(_alpha(A.run(per), ns))
-        a_d.append(_alpha(B.run(per), ns))
+    a_d, prof_d = sample(B)
     ev, ps, ac = sums(B.da_stats())
     A.close()
     B.close()
-    a_p, a_d = np.array(a_p), np.array(a_d)
     mp, md = a_p.mean(0), a_d.mean(0)
-    half = snaps // 2
-    drift = float(np.abs(a_p[half:].mean(0) - a_p[:half].mean(0)).mean())
-    se = np.sqrt(a_p.var(0, ddof=1) / snaps + a_d.var(0, ddof=1) / snaps)
+    se = np.sqrt(a_p.var(0, ddof=1) / blocks + a_d.var(0, ddof=1) / blocks)
     pH = np.array([p.pH for p in P])
     curve = []
     for lo in (5.0, 6.0, 7.0, 8.0):
         m = (pH >= lo) & (pH < lo + 1.0 + (1e-9 if lo == 8.0 else 0.0))
+        if not m.any():
+            continue
+        se_b = float(np.sqrt((se[m] ** 2).sum()) / m.sum())
+        diff = float(md[m].mean() - mp[m].mean())
         curve.append({"pH": [lo, lo + 1.0], "replicas": int(m.sum()), "alpha_plain": float(mp[m].mean()),
-                      "alpha_da": float(md[m].mean()), "diff": float(md[m].mean() - mp[m].mean()),
-                      "stderr": float(np.sqrt((se[m] ** 2).sum()) / m.sum())})
-    return {"workload": "config-5 chemistry, 24 replicas of 4x4 diblock chains (20 permanent +1 + 30 titratable, "
-                        "pKa 7.3), pH 5-9, salt 0.01-0.1 M, 50% displacement / 50% protonation",
-            "sweeps_equilibrate": sweeps_eq, "sweeps_sample": sweeps_sample, "snapshots": snaps,
-            "fit_loss": loss, "exact_dE_skipped": 1.0 - ps / max(ev, 1), "second_stage_agreement": ac / max(ps, 1),
-            "pH_curve": curve, "max_curve_diff": float(max(abs(c["diff"]) for c in curve)),
-            "mean_abs_diff_per_replica": float(np.abs(md - mp).mean()), "median_stderr_per_replica": float(np.median(se)),
-            "plain_drift_between_halves": drift}
+                      "alpha_da": float(md[m].mean()), "diff": diff, "stderr": se_b,
+                      "within_2se": abs(diff) <= 2 * se_b})
+    # z-profiles: per bin, the replica-mean profile difference against its spread over replicas
+    dprof = prof_d - prof_p
+    zscore = np.abs(dprof.mean(0)) / (dprof.std(0, ddof=1) / np.sqrt(len(S)) + 1e-12)
+    return {"workload": f"the {n_rep} smallest config-5 replicas ({min(s.n for s in S)}-{nmax} particles), "
+                        "90% displacement / 10% protonation, batched exact as the plain engine",
+            "sweeps_equilibrate": sweeps_eq + (rounds - 1) * sweeps_sample, "sweeps_sample": sweeps_sample,
+            "blocks": blocks, "rounds": rounds, "exact_dE_skipped": 1.0 - ps / max(ev, 1),
+            "second_stage_agreement": ac / max(ps, 1), "pH_curve": curve,
+            "max_curve_diff": float(max(abs(c["diff"]) for c in curve)),
+            "all_within_2se": bool(all(c["within_2se"] for c in curve)),
+            "mean_abs_diff_per_replica": float(np.abs(md - mp).mean()),
+            "median_stderr_per_replica": float(np.median(se)), "plain_drift_between_halves": drift,
+            "z_profile_bins": nbins,
+            "z_profile_max_zscore": {"sites": float(zscore[0].max()), "anions": float(zscore[1].max()),
+                                     "cations": float(zscore[2].max())}}
 
 
 def plain_config2(args, local):
@@ -671,12 +756,15 @@ def run_ours(args):
         except Exception as e:  # an extra: the headline line is printed regardless
             line["reference_phase2_on_device"] = {"error": str(e)[:300]}
         if not args.no_alpha:
-            line["alpha_check"] = alpha_check(local, args.alpha_eq, args.alpha_sample)
-        if not args.no_config4:
+            line["alpha_check"] = alpha_check(local, sur, args.alpha_eq, args.alpha_sample)
+        for key, fn, off in (("config1", config1_run, args.no_config1), ("config3", config3_run, args.no_config3),
+                             ("config4", config4_run, args.no_config4)):
+            if off:
+                continue
             try:
-                line["config4"] = config4_run(local)
+                line[key] = fn(local)
             except Exception as e:  # an extra: the headline line is printed regardless
-                line["config4"] = {"error": str(e)[:300]}
+                line[key] = {"error": str(e)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ref_dir, f"c5_{k_small:04d}", args.cpu_seconds)
     if world > 1:
