@@ -227,6 +227,8 @@ typedef struct phmc_tuning {
     int zpass_n1, zpass_n2;
     int cand_round;       /* pair pass: candidate particles per thread and round (2, 4 or 8 at order 5; 4
                              otherwise); a round's neighbour tile is cand_round x threads candidates */
+    int g_rows;           /* pending-correction sum: rows of the influence kernel G in flight per thread
+                             (2; 3 or 4 with cand_round 2 at order 5) */
     int energy_block;     /* full recompute: particles per block of the pair / FENE pass (64, 128, 256) */
     double rebuild_us;    /* autotune only: device time of one rebuild of every replica's potential mesh */
     double recompute_us;  /* autotune only: device time of one full pair / FENE recompute of every replica */
@@ -236,7 +238,7 @@ typedef struct phmc_tuning {
 int phmc_set_tuning(phmc_engine* e, int pending_max, int threads);
 /* The tile shapes above; -1 leaves a field as it is.  Decisions do not depend on them
  * except through FP32 / FP64 rounding of summation orders. */
-int phmc_set_tile_shapes(phmc_engine* e, int zpass, int cand_round, int energy_block);
+int phmc_set_tile_shapes(phmc_engine* e, int zpass, int cand_round, int g_rows, int energy_block);
 int phmc_get_tuning(phmc_engine* e, phmc_tuning* out);
 /* Cost-based fallback of delayed acceptance: on = 0 bypasses the attached surrogate's
  * first stage (every trial plain Metropolis on the exact dE, as with no surrogate)
@@ -246,7 +248,7 @@ int phmc_set_first_stage(phmc_engine* e, int on);
  * replicas' nz, timed as whole rebuilds), then the full recompute's block size,
  * then pending_max x threads by trial runs of `trials` trials per replica (two
  * interleaved passes, each candidate's faster time kept), then the pair pass's
- * round width at the best pending_max x threads, then, with a surrogate attached,
+ * shape (round width x G rows) at the best pending_max x threads, then, with a surrogate attached,
  * its first stage on against bypassed; keeps the fastest of each stage.
  * results[] gets one entry per candidate timed, with that stage's time set. */
 int phmc_autotune(phmc_engine* e, int64_t trials, phmc_tuning* results, int max_results, int* n_results);

@@ -1702,6 +1702,7 @@ static void fill_tuning(const Engine& E, phmc_tuning* out) {
     out->zpass = E.zreg;
     zreg_split(E.zreg, &out->zpass_n1, &out->zpass_n2);
     out->cand_round = E.cand_round;
+    out->g_rows = E.g_rows;
     out->energy_block = E.energy_block;
     out->first_stage = (E.d.sur.H > 0 && !E.first_stage_off) ? 1 : 0;
 }
@@ -1722,7 +1723,7 @@ extern "C" int phmc_get_tuning(phmc_engine* h, phmc_tuning* out) {
 }
 
 // Apply tile shapes (-1: unchanged) after checking them; the previous ones stay on failure.
-static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_block) {
+static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_block, int g_rows = -1) {
     Engine& E = h->E;
     if (zpass >= 0 && zpass != E.zreg) {
         int ids[8];
@@ -1738,14 +1739,18 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
             return fail(PHMC_ERR_UNSUPPORTED, std::string("z pass does not fit the device: ") + cudaGetErrorString(e));
         }
     }
-    if (cand_round >= 0 && cand_round != E.cand_round) {
-        if (cand_round != 2 && cand_round != 4 && cand_round != 8) return fail(PHMC_ERR_ARG, "cand_round must be 2, 4 or 8");
-        const int old = E.cand_round;
-        E.cand_round = cand_round;
+    if ((cand_round >= 0 && cand_round != E.cand_round) || (g_rows >= 0 && g_rows != E.g_rows)) {
+        if (cand_round >= 0 && cand_round != 2 && cand_round != 4 && cand_round != 8)
+            return fail(PHMC_ERR_ARG, "cand_round must be 2, 4 or 8");
+        if (g_rows >= 0 && (g_rows < 2 || g_rows > 4)) return fail(PHMC_ERR_ARG, "g_rows must be 2, 3 or 4");
+        const int old_c = E.cand_round, old_g = E.g_rows;
+        if (cand_round >= 0) E.cand_round = cand_round;
+        if (g_rows >= 0) E.g_rows = g_rows;
         cudaError_t e = prepare_mc(E);
         if (e != cudaSuccess) {
-            E.cand_round = old;
-            return fail(PHMC_ERR_UNSUPPORTED, "cand_round other than 4 needs SPME order 5");
+            E.cand_round = old_c; E.g_rows = old_g;
+            return fail(PHMC_ERR_UNSUPPORTED, "pair-pass shape not compiled: at order 5 (cand_round, g_rows) is one of "
+                                              "(4, 2), (2, 2), (8, 2), (2, 3), (2, 4); (4, 2) at other orders");
         }
     }
     if (energy_block >= 0) {
@@ -1757,11 +1762,11 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
     return PHMC_OK;
 }
 
-extern "C" int phmc_set_tile_shapes(phmc_engine* h, int zpass, int cand_round, int energy_block) {
+extern "C" int phmc_set_tile_shapes(phmc_engine* h, int zpass, int cand_round, int g_rows, int energy_block) {
     if (!h) return fail(PHMC_ERR_ARG, "null engine");
     CU(cudaSetDevice(h->E.device));
     CU(cudaStreamSynchronize(h->E.stream));
-    return apply_tiles(h, zpass, cand_round, energy_block);
+    return apply_tiles(h, zpass, cand_round, energy_block, g_rows);
 }
 
 // Device time (ms) of `reps` launches of f on the engine stream, after one untimed launch.
@@ -1882,26 +1887,27 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
         }
     int s = apply_tuning(h, best_p, best_t);
     if (s) return s;
-    // 4. the pair pass's round width at that pending capacity and block size (order 5)
+    // 4. the pair pass's shape at that pending capacity and block size (order 5): round width
+    //    (candidates per thread per round) x G rows in flight in the correction sum
     if (E.order == 5) {
-        const int rounds[3] = {4, 2, 8};
-        double rbest[3] = {best, 1e300, 1e300};
+        const int shapes[5][2] = {{4, 2}, {2, 2}, {8, 2}, {2, 3}, {2, 4}};
+        double sbest[5] = {best, 1e300, 1e300, 1e300, 1e300};
         for (int pass = 0; pass < 2; ++pass)
-            for (int k = 1; k < 3; ++k) {
-                if (apply_tiles(h, -1, rounds[k], -1) != PHMC_OK) continue;
+            for (int k = 1; k < 5; ++k) {
+                if (apply_tiles(h, -1, shapes[k][0], -1, shapes[k][1]) != PHMC_OK) continue;
                 double us = 0.0;
                 s = time_run(&us);
                 if (s) return s;
-                rbest[k] = std::min(rbest[k], us);
+                sbest[k] = std::min(sbest[k], us);
             }
         int bk = 0;
-        for (int k = 1; k < 3; ++k) {
-            if (rbest[k] >= 1e300) continue;
-            apply_tiles(h, -1, rounds[k], -1);
-            emit(rbest[k], 0.0, 0.0);
-            if (rbest[k] < rbest[bk]) bk = k;
+        for (int k = 1; k < 5; ++k) {
+            if (sbest[k] >= 1e300) continue;
+            apply_tiles(h, -1, shapes[k][0], -1, shapes[k][1]);
+            emit(sbest[k], 0.0, 0.0);
+            if (sbest[k] < sbest[bk]) bk = k;
         }
-        s = apply_tiles(h, -1, rounds[bk], -1);
+        s = apply_tiles(h, -1, shapes[bk][0], -1, shapes[bk][1]);
         if (s) return s;
     }
     // 5. cost-based fallback of delayed acceptance: the attached surrogate's first stage
@@ -1997,10 +2003,10 @@ extern "C" int phmc_checkpoint_save(phmc_engine* h, const char* path) {
     // version 2: the tile shapes follow the quorum (they fix summation orders, so an exact
     // resume needs them)
     const int hdr[7] = {2, E.R, E.total_slots, E.total_cells, E.cell_cap, (int)sizeof(RepState), E.pend_max};
-    const int tiles[3] = {E.zreg, E.cand_round, E.energy_block};
+    const int tiles[4] = {E.zreg, E.cand_round, E.energy_block, E.g_rows};
     bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(hdr, sizeof(int), 7, f) == 7 &&
               fwrite(&E.threads, sizeof(int), 1, f) == 1 && fwrite(&E.quorum, sizeof(float), 1, f) == 1 &&
-              fwrite(tiles, sizeof(int), 3, f) == 3;
+              fwrite(tiles, sizeof(int), 4, f) == 4;
     for (int r = 0; r < E.R && ok; ++r) {
         const RepDesc& D = E.desc[r];
         const CkptRep cr = {D.cap, D.slot_off, {D.ncell[0], D.ncell[1], D.ncell[2]}, {D.mesh[0], D.mesh[1], D.mesh[2]},
@@ -2039,8 +2045,8 @@ extern "C" int phmc_checkpoint_load(phmc_engine* h, const char* path) {
     if ((hdr[0] != 1 && hdr[0] != 2) || hdr[1] != E.R || hdr[2] != E.total_slots || hdr[3] != E.total_cells ||
         hdr[4] != E.cell_cap || hdr[5] != (int)sizeof(RepState))
         return bad("written by an engine with other replicas, capacities or cells");
-    int tiles[3] = {E.zreg, E.cand_round, E.energy_block};
-    if (hdr[0] == 2 && fread(tiles, sizeof(int), 3, f) != 3) return bad("truncated header");
+    int tiles[4] = {E.zreg, E.cand_round, E.energy_block, E.g_rows};
+    if (hdr[0] == 2 && fread(tiles, sizeof(int), 4, f) != 4) return bad("truncated header");
     std::vector<CkptRep> reps((size_t)E.R);
     for (int r = 0; r < E.R; ++r) {
         if (fread(&reps[r], sizeof(CkptRep), 1, f) != 1) return bad("truncated replica table");
@@ -2074,7 +2080,7 @@ extern "C" int phmc_checkpoint_load(phmc_engine* h, const char* path) {
         if (s) return s;
     }
     {
-        const int s = apply_tiles(h, tiles[0], tiles[1], tiles[2]);
+        const int s = apply_tiles(h, tiles[0], tiles[1], tiles[2], tiles[3]);
         if (s) return s;
     }
     E.quorum = quorum;

@@ -21,6 +21,7 @@ struct Engine {
     int threads = 256;
     int pend_max = 16;
     int cand_round = 4;          // pair pass: candidates per thread per round (2, 4, 8 at order 5)
+    int g_rows = 2;              // pending-correction sum: G rows in flight per thread (2, 3, 4 with round 2)
     int energy_block = 128;      // full recompute: particles per block of the pair / FENE pass
     bool first_stage_off = false;  // the attached surrogate's first stage bypassed (cost-based fallback)
     float quorum = 0.2f;         // MC launch quorum of blocked replicas (1: every replica runs until it stops)

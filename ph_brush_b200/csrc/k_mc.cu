@@ -717,8 +717,9 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
 }
 
 // RC: candidate particles per thread and round of the pair pass (the neighbour tile of a
-// round is RC x NT candidates), a tuning parameter
-template <int P, int NT, bool GC, int RC = 4>
+// round is RC x NT candidates); RR: rows of the influence kernel G each thread has in
+// flight per step of the pending-correction sum; both tuning parameters
+template <int P, int NT, bool GC, int RC = 4, int RR = 2>
 __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
     constexpr int W = 2 * P - 1;
@@ -1325,7 +1326,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const int ox = D.oct[0], oy = D.oct[1];
             constexpr int WW = W * W;
             const int nrow = T.npairs * WW;
-            constexpr int RR = 2;
             for (int r0 = tid; r0 < nrow; r0 += RR * NT) {
                 float gv[RR][W];
                 int qv[RR], rv[RR];
@@ -1571,7 +1571,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     }
 }
 
-template <int P, int NT, int RC>
+template <int P, int NT, int RC, int RR>
 static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
     DevPtrs dd = E.d;
     size_t smem = mc_smem_bytes(P, E.pend_max, false);
@@ -1580,7 +1580,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     if (dd.sur.H > 0) {
         // three staged layers when two blocks per SM still fit, else two buffers
         cudaFuncAttributes fa;
-        cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC>);
+        cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC, RR>);
         int per_sm = 0;
         cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, E.device);
         const size_t three = mc_smem_bytes(P, E.pend_max, true);
@@ -1594,7 +1594,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     dd.quorum = 1.0f;
     if (mode == MC_RUN && E.quorum < 1.0f) {
         int per_sm = 0, nsm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT, false, RC>, NT, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT, false, RC, RR>, NT, smem);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
         if ((long long)per_sm * nsm >= E.R) {
             dd.quorum = E.quorum;
@@ -1602,7 +1602,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
             if (e != cudaSuccess) return e;
         }
     }
-    k_mc<P, NT, false, RC><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
+    k_mc<P, NT, false, RC, RR><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
 }
 
@@ -1640,34 +1640,43 @@ cudaError_t launch_mc_gc(Engine& E, int n_jobs, cudaStream_t st) {
 
 // Raise the dynamic shared-memory cap of the engine's MC kernel instance to the
 // device maximum (minus its static shared memory), once, outside any capture.
-template <int P, int NT, int RC>
+template <int P, int NT, int RC, int RR>
 static cudaError_t prepare_mc_t(Engine& E) {
     int optin = 0;
     cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
     if (e != cudaSuccess) return e;
     cudaFuncAttributes fa;
-    e = cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC>);
+    e = cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC, RR>);
     if (e != cudaSuccess) return e;
     const int cap = optin - (int)fa.sharedSizeBytes;
     if ((size_t)cap < mc_smem_bytes(P, E.pend_max, true)) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(k_mc<P, NT, false, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+    return cudaFuncSetAttribute(k_mc<P, NT, false, RC, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+}
+
+// The compiled (order, round width, G rows) variants: order 5 (the configurations' order)
+// has five pair-pass shapes, orders 4 and 6 the default one.  f gets the four template
+// values as integral constants; an unsupported combination gives cudaErrorInvalidValue.
+template <int V>
+using IC = std::integral_constant<int, V>;
+template <class F>
+static cudaError_t mc_dispatch(const Engine& E, F&& f) {
+    const bool t128 = E.threads == 128;
+    const int rc = E.cand_round, rr = E.g_rows;
+#define MC_VARIANT(p, c, g) \
+    if (rc == c && rr == g) return t128 ? f(IC<p>{}, IC<128>{}, IC<c>{}, IC<g>{}) : f(IC<p>{}, IC<256>{}, IC<c>{}, IC<g>{});
+    switch (E.order) {
+        case 4: MC_VARIANT(4, 4, 2) break;
+        case 5: MC_VARIANT(5, 4, 2) MC_VARIANT(5, 2, 2) MC_VARIANT(5, 8, 2) MC_VARIANT(5, 2, 3) MC_VARIANT(5, 2, 4) break;
+        default: MC_VARIANT(6, 4, 2) break;
+    }
+#undef MC_VARIANT
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t prepare_mc(Engine& E) {
-    const int NTh = E.threads;
-    // the pair pass's round width is tunable at order 5 (the configurations' order); 4 elsewhere
-    if (E.cand_round != 4 && E.order != 5) return cudaErrorInvalidValue;
-    switch (E.order) {
-        case 4: return NTh == 128 ? prepare_mc_t<4, 128, 4>(E) : prepare_mc_t<4, 256, 4>(E);
-        case 5:
-            switch (E.cand_round) {
-                case 2: return NTh == 128 ? prepare_mc_t<5, 128, 2>(E) : prepare_mc_t<5, 256, 2>(E);
-                case 8: return NTh == 128 ? prepare_mc_t<5, 128, 8>(E) : prepare_mc_t<5, 256, 8>(E);
-                case 4: return NTh == 128 ? prepare_mc_t<5, 128, 4>(E) : prepare_mc_t<5, 256, 4>(E);
-                default: return cudaErrorInvalidValue;
-            }
-        default: return NTh == 128 ? prepare_mc_t<6, 128, 4>(E) : prepare_mc_t<6, 256, 4>(E);
-    }
+    return mc_dispatch(E, [&](auto p, auto nt, auto rc, auto rr) {
+        return prepare_mc_t<decltype(p)::value, decltype(nt)::value, decltype(rc)::value, decltype(rr)::value>(E);
+    });
 }
 
 size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate, bool two_buffers) {
@@ -1686,15 +1695,8 @@ size_t mc_smem_bytes(int order, int pend_max, bool staged_surrogate, bool two_bu
 }
 
 cudaError_t launch_mc(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
-    const int NTh = E.threads;
-    switch (E.order) {
-        case 4: return NTh == 128 ? launch_mc_t<4, 128, 4>(E, mode, rep, t, n, dE, st) : launch_mc_t<4, 256, 4>(E, mode, rep, t, n, dE, st);
-        case 5:
-            switch (E.cand_round) {
-                case 2: return NTh == 128 ? launch_mc_t<5, 128, 2>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256, 2>(E, mode, rep, t, n, dE, st);
-                case 8: return NTh == 128 ? launch_mc_t<5, 128, 8>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256, 8>(E, mode, rep, t, n, dE, st);
-                default: return NTh == 128 ? launch_mc_t<5, 128, 4>(E, mode, rep, t, n, dE, st) : launch_mc_t<5, 256, 4>(E, mode, rep, t, n, dE, st);
-            }
-        default: return NTh == 128 ? launch_mc_t<6, 128, 4>(E, mode, rep, t, n, dE, st) : launch_mc_t<6, 256, 4>(E, mode, rep, t, n, dE, st);
-    }
+    return mc_dispatch(E, [&](auto p, auto nt, auto rc, auto rr) {
+        return launch_mc_t<decltype(p)::value, decltype(nt)::value, decltype(rc)::value, decltype(rr)::value>(
+            E, mode, rep, t, n, dE, st);
+    });
 }

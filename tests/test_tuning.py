@@ -21,11 +21,12 @@ def test_retuning_keeps_tracked_energy_consistent():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tiles", [(-1, -1, -1), (0, 2, 64), (-1, 8, 256)])
+@pytest.mark.parametrize("tiles", [(-1, -1, -1, -1), (0, 2, 64, -1), (-1, 8, 256, -1), (-1, 2, -1, 4),
+                                   (0, 2, 128, 3)])
 def test_tuning_leaves_the_trial_stream_unchanged_on_a_short_run(tiles):
     """Same seed, different tuning and tile shapes (config 1's nz = 128: the Stockham
-    z pass against the register split; pair-pass rounds of 2 and 8 candidates; full
-    recompute blocks of 64 and 256): the same proposals; decisions agree unless a dE
+    z pass against the register split; pair-pass rounds of 2 and 8 candidates; 3 and 4 G
+    rows in flight; full recompute blocks of 64 and 256): the same proposals; decisions agree unless a dE
     sits within FP32 rounding of its acceptance threshold (none on a short run)."""
     s, p = configs.config1(seed=52)
     logs = []
@@ -33,10 +34,11 @@ def test_tuning_leaves_the_trial_stream_unchanged_on_a_short_run(tiles):
         with Engine(s, p) as e:
             e.set_tuning(pend, th)
             if k == 1:
-                e.set_tile_shapes(*tiles)
+                e.set_tile_shapes(zpass=tiles[0], cand_round=tiles[1], energy_block=tiles[2], g_rows=tiles[3])
                 t = e.tuning()
                 assert tiles[1] < 0 or t["cand_round"] == tiles[1]
                 assert tiles[0] < 0 or t["zpass"] == tiles[0]
+                assert tiles[3] < 0 or t["g_rows"] == tiles[3]
             log = e.set_trial_log(4000)
             e.run(4000)
             logs.append((log[0].copy(), log[1].copy(), log[2].copy()))
@@ -63,11 +65,13 @@ def test_autotune_keeps_the_fastest_candidate():
         assert len(zp) >= 2 and {r["zpass"] for r in zp} >= {0, 2}  # Stockham and nz = 128's default split
         assert {r["energy_block"] for r in eb} == {64, 128, 256}
         assert len(grid) >= 10 and {r["cand_round"] for r in runs} == {2, 4, 8}
+        assert {(r["cand_round"], r["g_rows"]) for r in runs} >= {(2, 2), (8, 2), (2, 3), (2, 4)}
         t = e.tuning()
         best = min(grid, key=lambda r: r["us_per_trial"])
         assert (t["pending_max"], t["threads"]) == (best["pending_max"], best["threads"])
-        rounds = [best] + [r for r in runs if r["cand_round"] != 4]
-        assert t["cand_round"] == min(rounds, key=lambda r: r["us_per_trial"])["cand_round"]
+        shapes = [best] + [r for r in runs if (r["cand_round"], r["g_rows"]) != (4, 2)]
+        fastest = min(shapes, key=lambda r: r["us_per_trial"])
+        assert (t["cand_round"], t["g_rows"]) == (fastest["cand_round"], fastest["g_rows"])
         assert t["zpass"] == min(zp, key=lambda r: r["rebuild_us"])["zpass"]
         assert t["energy_block"] == min(eb, key=lambda r: r["recompute_us"])["energy_block"]
         st = e.run(2000)
@@ -107,7 +111,7 @@ def test_launch_quorum_keeps_the_chains_and_energies():
 
 def test_tuning_arguments_are_checked_without_a_gpu():
     lib = _abi.lib()
-    assert lib.phmc_set_tile_shapes(None, 0, 4, 128) != 0
+    assert lib.phmc_set_tile_shapes(None, 0, 4, 2, 128) != 0
     assert lib.phmc_set_tuning(None, 16, 256) != 0
     assert lib.phmc_autotune(None, 100, None, 0, None) != 0
     assert lib.phmc_set_quorum(None, 0.5) != 0
