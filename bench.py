@@ -124,7 +124,8 @@ def parse():
     ap.add_argument("--harvest", type=int, default=262144, help="surrogate training samples harvested")
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--da-threshold", type=float, default=0.3)
-    ap.add_argument("--tuning", default=None, help="pending_max,threads instead of the autotuner (for profiling)")
+    ap.add_argument("--tuning", default=None, help="pending_max,threads[,cand_round,g_rows,zpass,plane_pipe,first_stage] "
+                                                    "instead of the autotuner (for profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline only (plain comparison, phases, alpha skipped)")
@@ -235,10 +236,16 @@ def barrier(world):
 
 
 def tune_engine(eng, args, trials):
-    """Autotune (pending capacity x block size), or apply --tuning."""
+    """Autotune, or apply --tuning pending_max,threads[,cand_round,g_rows,zpass,plane_pipe,first_stage]
+    (fixed shapes for profiling commands; -1 keeps a field)."""
     if args.tuning:
-        pm, th = (int(v) for v in args.tuning.split(","))
-        eng.set_tuning(pm, th)
+        v = [int(x) for x in args.tuning.split(",")]
+        eng.set_tuning(v[0], v[1])
+        if len(v) > 2:
+            v += [-1] * (7 - len(v))
+            eng.set_tile_shapes(zpass=v[4], cand_round=v[2], g_rows=v[3], plane_pipe=v[5])
+            if v[6] >= 0:
+                eng.set_first_stage(v[6])
         return None
     return eng.autotune(trials)
 
@@ -728,8 +735,11 @@ def run_ours(args):
             "roofline_other": {k: v for k, v in rl.items() if k != dominant},
             "e2e": e2e, "gpu_launches": int(prof["kernel_launches"]),
             "trials_per_s": world * prof["trials"] / (max_ms / 1e3) if prof["trials"] else None,
-            "surrogate": {"training": train, "exact_dE_skipped": 1.0 - (da1[1] - da0[1]) / max(da1[0] - da0[0], 1),
-                          "second_stage_agreement": (da1[2] - da0[2]) / max(da1[1] - da0[1], 1),
+            "surrogate": {"training": train,
+                          "first_stage": bool(eng.tuning()["first_stage"]),
+                          "judged_trials": int(da1[0] - da0[0]),
+                          "exact_dE_skipped": (1.0 - (da1[1] - da0[1]) / (da1[0] - da0[0])) if da1[0] > da0[0] else None,
+                          "second_stage_agreement": ((da1[2] - da0[2]) / (da1[1] - da0[1])) if da1[1] > da0[1] else None,
                           "fallbacks": int(sum(d["fallback"] for d in eng.da_stats()))},
             "clocks": clk}
     if rank == 0 and world == 1 and not args.no_extras:

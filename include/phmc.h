@@ -229,6 +229,9 @@ typedef struct phmc_tuning {
                              otherwise); a round's neighbour tile is cand_round x threads candidates */
     int g_rows;           /* pending-correction sum: rows of the influence kernel G in flight per thread
                              (2; 3 or 4 with cand_round 2 at order 5) */
+    int plane_pipe;       /* rebuild's first pass: 1 persistent blocks that bulk-copy the next band plane's
+                             charges into shared memory while transforming the current one; 0 one block per
+                             plane (square lateral meshes of the register passes only) */
     int energy_block;     /* full recompute: particles per block of the pair / FENE pass (64, 128, 256) */
     double rebuild_us;    /* autotune only: device time of one rebuild of every replica's potential mesh */
     double recompute_us;  /* autotune only: device time of one full pair / FENE recompute of every replica */
@@ -238,14 +241,15 @@ typedef struct phmc_tuning {
 int phmc_set_tuning(phmc_engine* e, int pending_max, int threads);
 /* The tile shapes above; -1 leaves a field as it is.  Decisions do not depend on them
  * except through FP32 / FP64 rounding of summation orders. */
-int phmc_set_tile_shapes(phmc_engine* e, int zpass, int cand_round, int g_rows, int energy_block);
+int phmc_set_tile_shapes(phmc_engine* e, int zpass, int cand_round, int g_rows, int energy_block, int plane_pipe);
 int phmc_get_tuning(phmc_engine* e, phmc_tuning* out);
 /* Cost-based fallback of delayed acceptance: on = 0 bypasses the attached surrogate's
  * first stage (every trial plain Metropolis on the exact dE, as with no surrogate)
  * without detaching it; on = 1 restores it.  The autotuner sets it by timing both. */
 int phmc_set_first_stage(phmc_engine* e, int on);
 /* Autotuner: first the z pass (the Stockham pass and every register split of the
- * replicas' nz, timed as whole rebuilds), then the full recompute's block size,
+ * replicas' nz, timed as whole rebuilds), the first pass pipelined or not (the same
+ * rebuilds), then the full recompute's block size,
  * then pending_max x threads by trial runs of `trials` trials per replica (two
  * interleaved passes, each candidate's faster time kept), then the pair pass's
  * shape (round width x G rows) at the best pending_max x threads, then, with a surrogate attached,

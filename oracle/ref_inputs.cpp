@@ -83,8 +83,9 @@ int write_replica(const std::string& line, const std::string& dir) {
                          bj.data(), counts, box) != PHMC_OK)
         return 1;
     const int n = counts[0], nb = counts[1];
-    int n_sites = 0;
-    for (int i = 0; i < n; ++i) n_sites += (f[i] & PHMC_F_TITRATABLE) ? 1 : 0;
+    int n_sites = 0, n_charged = 0;
+    for (int i = 0; i < n; ++i)
+        if (f[i] & PHMC_F_TITRATABLE) { ++n_sites; n_charged += q[i] != 0.0f ? 1 : 0; }
     if (n_w < 0) n_w = n_sites;
     Xo rng(w_seed);
     std::vector<float> wx(n_w), wy(n_w), wz(n_w);
@@ -120,6 +121,9 @@ int write_replica(const std::string& line, const std::string& dir) {
     fprintf(fh, "cutoff_nm = 3\nlj_shift = yes\nepsilon_r = %.10g\ncoulombtype = pme\newald_rtol = 1e-5\n", KE / L_BJERRUM);
     fprintf(fh, "pme_spacing = %.10g\npme_order = 4\npme_3dc = yes %.10g\nbeta = 1.0\n", pme_spacing, zfac);
     fprintf(fh, "nh_n_type = 4\nnh_p_type = 5\nw_type = 7\ncl_type = 8\n");
+    // target = the current protonation (floor(pct / 100 sites) == charged sites): the reference's
+    // build_plan refuses a target below the current count (MC/src/mc.cu:88-91)
+    fprintf(fh, "target_protonation_pct = %.10f\n", n_sites > 0 ? 100.0 * (n_charged + 0.5) / n_sites : 10.0);
     for (int i = 1; i <= REF_NTYPES; ++i)
         for (int j = i; j <= REF_NTYPES; ++j) fprintf(fh, "lj %d %d %d 1\n", i, j, (i == REF_W || j == REF_W) ? 0 : 1);
     fclose(fh);

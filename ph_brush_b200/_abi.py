@@ -114,7 +114,7 @@ class DAStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("pending_max", C.c_int), ("threads", C.c_int), ("us_per_trial", C.c_double),
                 ("zpass", C.c_int), ("zpass_n1", C.c_int), ("zpass_n2", C.c_int), ("cand_round", C.c_int),
-                ("g_rows", C.c_int),
+                ("g_rows", C.c_int), ("plane_pipe", C.c_int),
                 ("energy_block", C.c_int), ("rebuild_us", C.c_double), ("recompute_us", C.c_double),
                 ("first_stage", C.c_int)]
 
@@ -247,7 +247,7 @@ def load_library(path=LIB_PATH):
         "phmc_checkpoint_load": ([eng, C.c_char_p], C.c_int),
         "phmc_set_quorum": ([eng, C.c_double], C.c_int),
         "phmc_set_launch_budget": ([eng, C.c_int64], C.c_int),
-        "phmc_set_tile_shapes": ([eng, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "phmc_set_tile_shapes": ([eng, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "phmc_set_first_stage": ([eng, C.c_int], C.c_int),
         "phmc_set_event_callback": ([eng, EventFn, C.c_void_p], C.c_int),
         "phmc_set_zhist": ([eng, C.c_int, C.c_int64], C.c_int),

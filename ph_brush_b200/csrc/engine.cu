@@ -1703,6 +1703,7 @@ static void fill_tuning(const Engine& E, phmc_tuning* out) {
     zreg_split(E.zreg, &out->zpass_n1, &out->zpass_n2);
     out->cand_round = E.cand_round;
     out->g_rows = E.g_rows;
+    out->plane_pipe = E.fwd_pipe ? 1 : 0;
     out->energy_block = E.energy_block;
     out->first_stage = (E.d.sur.H > 0 && !E.first_stage_off) ? 1 : 0;
 }
@@ -1723,8 +1724,13 @@ extern "C" int phmc_get_tuning(phmc_engine* h, phmc_tuning* out) {
 }
 
 // Apply tile shapes (-1: unchanged) after checking them; the previous ones stay on failure.
-static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_block, int g_rows = -1) {
+static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_block, int g_rows = -1,
+                       int plane_pipe = -1) {
     Engine& E = h->E;
+    if (plane_pipe >= 0) {
+        if (plane_pipe > 1) return fail(PHMC_ERR_ARG, "plane_pipe must be 0 or 1");
+        E.fwd_pipe = plane_pipe == 1 && E.plane_reg;
+    }
     if (zpass >= 0 && zpass != E.zreg) {
         int ids[8];
         const int n = E.zreg_default ? zreg_variants(E.desc[0].mesh[2], ids, 8) : 0;
@@ -1762,11 +1768,12 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
     return PHMC_OK;
 }
 
-extern "C" int phmc_set_tile_shapes(phmc_engine* h, int zpass, int cand_round, int g_rows, int energy_block) {
+extern "C" int phmc_set_tile_shapes(phmc_engine* h, int zpass, int cand_round, int g_rows, int energy_block,
+                                    int plane_pipe) {
     if (!h) return fail(PHMC_ERR_ARG, "null engine");
     CU(cudaSetDevice(h->E.device));
     CU(cudaStreamSynchronize(h->E.stream));
-    return apply_tiles(h, zpass, cand_round, energy_block, g_rows);
+    return apply_tiles(h, zpass, cand_round, energy_block, g_rows, plane_pipe);
 }
 
 // Device time (ms) of `reps` launches of f on the engine stream, after one untimed launch.
@@ -1818,6 +1825,20 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
             if (ms < best) { best = ms; best_id = ids[k]; }
         }
         int s = apply_tiles(h, best_id, -1, -1);
+        if (s) return s;
+    }
+    // 1b. the first pass pipelined or not, with that z pass (the same whole rebuilds)
+    if (E.coulomb == PHMC_COUL_EWALD && E.use_r2c && E.plane_reg) {
+        double ms_pipe[2] = {1e300, 1e300};
+        for (int pp = 0; pp < 2; ++pp) {
+            if (apply_tiles(h, -1, -1, -1, -1, pp) != PHMC_OK) continue;
+            int s = time_launches(E, 10, [&]() { launch_rebuild_r2c(E, nullptr, 0, E.stream); }, &ms_pipe[pp]);
+            if (s) return s;
+            int s2 = check_kernel_errors(h);
+            if (s2) return s2;
+            emit(0.0, ms_pipe[pp] * 1e3, 0.0);
+        }
+        int s = apply_tiles(h, -1, -1, -1, -1, ms_pipe[1] < ms_pipe[0] ? 1 : 0);
         if (s) return s;
     }
     // 2. full recompute's block size (pair / FENE pass and its reduction; the tracked
@@ -2003,10 +2024,10 @@ extern "C" int phmc_checkpoint_save(phmc_engine* h, const char* path) {
     // version 2: the tile shapes follow the quorum (they fix summation orders, so an exact
     // resume needs them)
     const int hdr[7] = {2, E.R, E.total_slots, E.total_cells, E.cell_cap, (int)sizeof(RepState), E.pend_max};
-    const int tiles[4] = {E.zreg, E.cand_round, E.energy_block, E.g_rows};
+    const int tiles[5] = {E.zreg, E.cand_round, E.energy_block, E.g_rows, E.fwd_pipe ? 1 : 0};
     bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(hdr, sizeof(int), 7, f) == 7 &&
               fwrite(&E.threads, sizeof(int), 1, f) == 1 && fwrite(&E.quorum, sizeof(float), 1, f) == 1 &&
-              fwrite(tiles, sizeof(int), 4, f) == 4;
+              fwrite(tiles, sizeof(int), 5, f) == 5;
     for (int r = 0; r < E.R && ok; ++r) {
         const RepDesc& D = E.desc[r];
         const CkptRep cr = {D.cap, D.slot_off, {D.ncell[0], D.ncell[1], D.ncell[2]}, {D.mesh[0], D.mesh[1], D.mesh[2]},
@@ -2045,8 +2066,8 @@ extern "C" int phmc_checkpoint_load(phmc_engine* h, const char* path) {
     if ((hdr[0] != 1 && hdr[0] != 2) || hdr[1] != E.R || hdr[2] != E.total_slots || hdr[3] != E.total_cells ||
         hdr[4] != E.cell_cap || hdr[5] != (int)sizeof(RepState))
         return bad("written by an engine with other replicas, capacities or cells");
-    int tiles[4] = {E.zreg, E.cand_round, E.energy_block, E.g_rows};
-    if (hdr[0] == 2 && fread(tiles, sizeof(int), 4, f) != 4) return bad("truncated header");
+    int tiles[5] = {E.zreg, E.cand_round, E.energy_block, E.g_rows, E.fwd_pipe ? 1 : 0};
+    if (hdr[0] == 2 && fread(tiles, sizeof(int), 5, f) != 5) return bad("truncated header");
     std::vector<CkptRep> reps((size_t)E.R);
     for (int r = 0; r < E.R; ++r) {
         if (fread(&reps[r], sizeof(CkptRep), 1, f) != 1) return bad("truncated replica table");
@@ -2080,7 +2101,7 @@ extern "C" int phmc_checkpoint_load(phmc_engine* h, const char* path) {
         if (s) return s;
     }
     {
-        const int s = apply_tiles(h, tiles[0], tiles[1], tiles[2], tiles[3]);
+        const int s = apply_tiles(h, tiles[0], tiles[1], tiles[2], tiles[3], tiles[4]);
         if (s) return s;
     }
     E.quorum = quorum;

@@ -24,6 +24,8 @@ struct Engine {
     int g_rows = 2;              // pending-correction sum: G rows in flight per thread (2, 3, 4 with round 2)
     int energy_block = 128;      // full recompute: particles per block of the pair / FENE pass
     bool first_stage_off = false;  // the attached surrogate's first stage bypassed (cost-based fallback)
+    bool fwd_pipe = false;       // the rebuild's first pass pipelined (persistent blocks, bulk-copied planes)
+    int nsm = 0;                 // the device's SM count
     float quorum = 0.2f;         // MC launch quorum of blocked replicas (1: every replica runs until it stops)
     cudaStream_t stream = nullptr;
     DevPtrs d{};

@@ -24,6 +24,7 @@
 // zero).  The unit-charge rebuild of the influence kernel computes every plane.
 // Replaces the memset + k_spread_cubic + cuFFT R2C + influence kernel chain of
 // the reference (MC/src/pme.cu:140-249,362,384-422).
+#include <algorithm>
 #include "common.cuh"
 #include "engine.h"
 #include "fft.cuh"
@@ -415,9 +416,13 @@ __global__ void __launch_bounds__(NT) k_rb_inv(DevPtrs d, const int2* __restrict
 #define PLANE_LIST(X) X(16, 4, 4) X(32, 8, 4) X(36, 6, 6) X(48, 8, 6) X(54, 9, 6) X(64, 8, 8)
 constexpr int plane_ms(int m) { return (m % 2 == 0) ? m + 1 : m + 2; }  // odd row stride (float2)
 constexpr int PLANE_NT = 128;
+constexpr int PLANE_STAGE_BYTES = 64 * 64 * 8;  // one staged plane of the largest listed lateral mesh
 
+// qs: the plane's fixed-point charges already staged in shared memory (the pipelined
+// pass), or null to read them from global memory.
 template <int N, int N1, int N2, int NT>
-__device__ void plane_fwd(const DevPtrs& d, const RepDesc& D, int z, int unit_charge, float2* sa, float2* sb) {
+__device__ void plane_fwd(const DevPtrs& d, const RepDesc& D, int z, int unit_charge, float2* sa, float2* sb,
+                          const ulonglong2* qs = nullptr) {
     constexpr int M = N / 2, NXH = M + 1, MS = plane_ms(M);
     static_assert(N1 * N2 == N, "y split");
     const int tid = threadIdx.x;
@@ -431,7 +436,7 @@ __device__ void plane_fwd(const DevPtrs& d, const RepDesc& D, int z, int unit_ch
     } else {
         int zrel = z - D.zb_lo;
         zrel += (zrel < 0) ? D.mesh[2] : 0;
-        const ulonglong2* q = reinterpret_cast<const ulonglong2*>(d.qband + D.qb_off + (size_t)zrel * N * N);
+        const ulonglong2* q = qs ? qs : reinterpret_cast<const ulonglong2*>(d.qband + D.qb_off + (size_t)zrel * N * N);
         for (int i = tid; i < N * M; i += NT) {
             const int y = i / M, j = i - y * M;
             const ulonglong2 v = q[i];
@@ -568,6 +573,64 @@ __global__ void __launch_bounds__(NT) k_rb_fwd_reg(DevPtrs d, const int2* __rest
     }
 }
 
+// Pipelined first pass: persistent blocks walk the band-plane jobs with a stride of the
+// grid; while a block transforms one plane, the next plane's fixed-point charges (N^2
+// 8-byte values, contiguous) arrive in the other half of a two-stage shared-memory
+// buffer by a bulk asynchronous copy (this GPU's own memory, no multicast), so the
+// loads of the planes overlap the FFT work instead of opening every block.  Waits are
+// bounded: a copy that does not arrive records PHMC_ERR_BUDGET in the replica's state
+// and the block stops (the rebuild is then reported as failed).
+template <int NT>
+__global__ void __launch_bounds__(NT) k_rb_fwd_pipe(DevPtrs d, const int2* __restrict__ jobs, int njobs,
+                                                    const int* __restrict__ dirty, int stage_off) {
+    extern __shared__ __align__(16) float2 psm[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ int s_fail;
+    unsigned char* stage[2] = {reinterpret_cast<unsigned char*>(psm) + stage_off,
+                               reinterpret_cast<unsigned char*>(psm) + stage_off + PLANE_STAGE_BYTES};
+    if (threadIdx.x == 0) { sur_mbar_init(&s_bar[0]); sur_mbar_init(&s_bar[1]); s_fail = 0; }
+    __syncthreads();
+    auto wanted = [&](int j) { return j < njobs && (!dirty || dirty[jobs[j].x]); };
+    auto issue = [&](int j, int s) {  // thread 0: the plane of job j into stage s
+        const int2 job = jobs[j];
+        const RepDesc& D = d.desc[job.x];
+        const int n = D.mesh[0];
+        int zrel = job.y - D.zb_lo;
+        zrel += (zrel < 0) ? D.mesh[2] : 0;
+        sur_bulk_load(stage[s], d.qband + D.qb_off + (size_t)zrel * n * n, (uint32_t)(n * n * 8), &s_bar[s]);
+    };
+    int uses[2] = {0, 0};  // copies issued into each stage (every thread counts alike)
+    int j = blockIdx.x, it = 0;
+    if (wanted(j)) { if (threadIdx.x == 0) issue(j, 0); uses[0]++; }
+    for (; j < njobs; j += gridDim.x, ++it) {
+        const int s = it & 1, jn = j + gridDim.x;
+        if (wanted(jn)) { if (threadIdx.x == 0) issue(jn, s ^ 1); uses[s ^ 1]++; }  // its stage was read last step
+        if (!wanted(j)) continue;
+        if (threadIdx.x == 0 && !sur_mbar_wait(&s_bar[s], (uint32_t)((uses[s] - 1) & 1))) s_fail = 1;
+        __syncthreads();
+        if (s_fail) {
+            if (threadIdx.x == 0) {
+                atomicExch(&d.state[jobs[j].x].error, PHMC_ERR_BUDGET);
+                sur_mbar_wait(&s_bar[s ^ 1], (uint32_t)((uses[s ^ 1] - 1) & 1));  // the copy in flight, bounded
+            }
+            return;
+        }
+        const int2 job = jobs[j];
+        const RepDesc& D = d.desc[job.x];
+        const int n = D.mesh[0];
+        float2* sa = psm;
+        float2* sb = psm + n * plane_ms(n / 2);
+        const ulonglong2* qs = reinterpret_cast<const ulonglong2*>(stage[s]);
+        switch (n) {
+#define PLANE_FWD(nn, a, b) case nn: plane_fwd<nn, a, b, NT>(d, D, job.y, 0, sa, sb, qs); break;
+            PLANE_LIST(PLANE_FWD)
+#undef PLANE_FWD
+            default: break;
+        }
+        __syncthreads();  // every thread is done with stage s and the plane buffers
+    }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT) k_rb_inv_reg(DevPtrs d, const int2* __restrict__ jobs, const int* __restrict__ dirty) {
     extern __shared__ __align__(16) float2 psm[];
@@ -600,7 +663,11 @@ size_t plane_reg_smem(int n) { return ((size_t)n * plane_ms(n / 2) + (size_t)n *
 void launch_rebuild_r2c(Engine& E, const int* dirty, int unit_charge, cudaStream_t st) {
     const int2* pj = unit_charge ? E.d_plane_jobs : E.d_band_jobs;
     const int npj = unit_charge ? E.n_plane_jobs : E.n_band_jobs;
-    if (E.plane_reg) k_rb_fwd_reg<PLANE_NT><<<npj, PLANE_NT, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty);
+    if (E.plane_reg && E.fwd_pipe && !unit_charge && E.nsm > 0) {
+        const int off = (int)((E.rb_fwd_smem + 127) / 128 * 128);
+        const int grid = std::min(npj, 2 * E.nsm);
+        k_rb_fwd_pipe<PLANE_NT><<<grid, PLANE_NT, off + 2 * PLANE_STAGE_BYTES, st>>>(E.d, pj, npj, dirty, off);
+    } else if (E.plane_reg) k_rb_fwd_reg<PLANE_NT><<<npj, PLANE_NT, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty);
     else k_rb_fwd<256><<<npj, 256, E.rb_fwd_smem, st>>>(E.d, pj, unit_charge, dirty);
     switch (E.zreg) {
 #define ZREG_LAUNCH(id, n, a, b) \
@@ -644,6 +711,12 @@ cudaError_t rebuild_set_smem_limits(Engine& E) {
     }
     if (e != cudaSuccess) return e;
     e = E.plane_reg ? raise_cap(k_rb_fwd_reg<PLANE_NT>, E.device, E.rb_fwd_smem) : raise_cap(k_rb_fwd<256>, E.device, E.rb_fwd_smem);
+    if (e != cudaSuccess) return e;
+    if (E.nsm == 0) {
+        e = cudaDeviceGetAttribute(&E.nsm, cudaDevAttrMultiProcessorCount, E.device);
+        if (e != cudaSuccess) return e;
+    }
+    if (E.plane_reg) e = raise_cap(k_rb_fwd_pipe<PLANE_NT>, E.device, (E.rb_fwd_smem + 127) / 128 * 128 + 2 * PLANE_STAGE_BYTES);
     if (e != cudaSuccess) return e;
     switch (E.zreg) {
 #define ZREG_CAP(id, n, a, b) case id: e = raise_cap(k_rb_zreg<a, b, ZREG_NT(b), ZREG_TX>, E.device, E.zpass_smem); break;

@@ -121,11 +121,12 @@ class Engine:
         """MC launch quorum (0, 1]: a launch ends once that fraction of its running replicas is blocked."""
         _abi.check(self._lib.phmc_set_quorum(self._h, float(quorum)))
 
-    def set_tile_shapes(self, zpass=-1, cand_round=-1, energy_block=-1, g_rows=-1):
+    def set_tile_shapes(self, zpass=-1, cand_round=-1, energy_block=-1, g_rows=-1, plane_pipe=-1):
         """z pass of the rebuild (0 Stockham, k > 0 a register split), pair-pass round width,
-        full-recompute block size, G rows in flight per thread; -1 keeps a field."""
+        full-recompute block size, G rows in flight per thread, pipelined first pass; -1 keeps
+        a field."""
         _abi.check(self._lib.phmc_set_tile_shapes(self._h, int(zpass), int(cand_round), int(g_rows),
-                                                  int(energy_block)))
+                                                  int(energy_block), int(plane_pipe)))
 
     def set_first_stage(self, on):
         """Delayed acceptance's first stage on (1) or bypassed (0) with the surrogate still attached."""
