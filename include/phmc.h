@@ -232,7 +232,8 @@ typedef struct phmc_tuning {
     int plane_pipe;       /* rebuild's first pass: 1 persistent blocks that bulk-copy the next band plane's
                              charges into shared memory while transforming the current one; 0 one block per
                              plane (square lateral meshes of the register passes only) */
-    int energy_block;     /* full recompute: particles per block of the pair / FENE pass (64, 128, 256) */
+    int energy_block;     /* full recompute: particles per block of the pair / FENE pass (64, 128, 256), or 0
+                             for the cell-ordered pass (one warp per cell, partners read by broadcast) */
     double rebuild_us;    /* autotune only: device time of one rebuild of every replica's potential mesh */
     double recompute_us;  /* autotune only: device time of one full pair / FENE recompute of every replica */
     int first_stage;      /* 1: the attached surrogate judges titration / swap trials first (delayed

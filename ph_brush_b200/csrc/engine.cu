@@ -432,6 +432,7 @@ static int build(phmc_engine* h, int R, const phmc_system* sys, const phmc_param
     for (int r = 0; r < R; ++r) maxcap = std::max(maxcap, E.desc[r].cap);
     E.energy_blocks = std::max(1, std::min(PHMC_FULL_MAX_BPR, (maxcap + 127) / 128));
     E.max_cap = maxcap;
+    for (const RepDesc& D : E.desc) E.max_cells = std::max(E.max_cells, D.ncell[0] * D.ncell[1] * D.ncell[2]);
     DALLOC(d.partials, (size_t)R * PHMC_FULL_MAX_BPR * 8);  // any energy_block's blocks per replica
     DALLOC(E.d_active, 1);
     CU(cudaMallocHost((void**)&E.h_active, sizeof(int)));
@@ -1760,8 +1761,8 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
         }
     }
     if (energy_block >= 0) {
-        if (energy_block != 64 && energy_block != 128 && energy_block != 256)
-            return fail(PHMC_ERR_ARG, "energy_block must be 64, 128 or 256");
+        if (energy_block != 0 && energy_block != 64 && energy_block != 128 && energy_block != 256)
+            return fail(PHMC_ERR_ARG, "energy_block must be 0 (cell order), 64, 128 or 256");
         E.energy_block = energy_block;
     }
     drop_graph(h);  // captured launches hold the old shapes
@@ -1844,7 +1845,7 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     // 2. full recompute's block size (pair / FENE pass and its reduction; the tracked
     //    pair energies it rewrites are those of the current state)
     {
-        const int blocks[3] = {64, 128, 256};
+        const int blocks[4] = {0, 64, 128, 256};
         int best_b = E.energy_block;
         double best = 1e300;
         for (int b : blocks) {

@@ -60,6 +60,7 @@ struct Engine {
     double* d_epair = nullptr;   // per (replica, block) partial components
     int energy_blocks = 0;
     int max_cap = 0;             // largest replica capacity (slots)
+    int max_cells = 0;           // largest replica's cell count
     // host copies for trial logs
     std::vector<int> bonds_host;
     std::vector<void*> allocs;

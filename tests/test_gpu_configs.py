@@ -237,3 +237,16 @@ def test_batched_config5_replicas_match_the_oracle_replica_for_replica():
         ref = O.energy(fin[r], P[r])
         assert_components(fresh[r], ref, what=f"replica {pick[r]} after the run")
         assert abs(sts[r]["energy"] - ref["total"]) <= 1e-6 * abs(ref["total"]) + 1e-3, (pick[r], sts[r]["energy"])
+
+
+@pytest.mark.gpu
+def test_cell_ordered_full_recompute_matches_the_oracle():
+    """The full recompute in cell order (energy_block 0: one warp per cell) on config 2 and
+    a config-5 replica: every component against the oracle, as the particle-ordered pass."""
+    k, s5, p5 = config5_by_lateral_mesh()[-1]
+    for s, p in (configs.config2(), (s5, p5)):
+        ref = O.energy(s, p)
+        with Engine(s, p) as e:
+            e.set_tile_shapes(energy_block=0)
+            assert e.tuning()["energy_block"] == 0
+            assert_components(e.energy()[0], ref, what="cell order", overlaps=True)
