@@ -130,6 +130,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline only (plain comparison, phases, alpha skipped)")
     ap.add_argument("--no-alpha", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true", help="no surrogate (profiling the exact path)")
     ap.add_argument("--no-config1", action="store_true")
     ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--no-config4", action="store_true")
@@ -273,6 +274,8 @@ def build_headline(args, local, rank, world):
     from ph_brush_b200 import Engine, Surrogate
     reps, n_all = headline_replicas(args, rank, world)
     eng = Engine([s for s, _ in reps], [p for _, p in reps], device=local)
+    if args.no_surrogate:  # profiling the exact path: no harvest, training or first stage
+        return reps, n_all, eng, None, tune_engine(eng, args, args.trials), {}
     p0 = reps[0][1]
     sur = Surrogate(seed=2029)
     eng.set_move_mix(0.5, 0.5, 0.0)  # titration-heavy harvest
@@ -465,16 +468,16 @@ def _alpha(stats, n_sites):
     return [st["n_charged_sites"] / n for st, n in zip(stats, n_sites)]
 
 
-def alpha_check(local, sur, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins=16, max_rounds=3):
+def alpha_check(local, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins=16, max_rounds=3):
     """alpha(pH) and z-profiles of delayed acceptance against the plain engine on real config-5
     replicas (the 24 smallest of the headline set, its move mix; batched exact is the plain
     engine): the plain engine equilibrates until the drift of its degree of ionisation
     between the two halves of a sample is below 0.002 (at most max_rounds rounds), a second
-    engine takes over the equilibrated states with the headline's surrogate as first stage,
-    and both sample `sweeps_sample` sweeps; every 250 trials each replica's MC kernel adds
+    engine takes over the equilibrated states with a surrogate trained on exact dE harvested
+    from them as first stage, and both sample `sweeps_sample` sweeps; every 250 trials each replica's MC kernel adds
     its z-histogram (phmc_set_zhist), read back per block."""
     import numpy as np
-    from ph_brush_b200 import Engine, configs
+    from ph_brush_b200 import Engine, Surrogate, configs
     allr = configs.config5(seed=2029, n_rep=256)
     idx = sorted(range(len(allr)), key=lambda k: allr[k][0].n)[:n_rep]
     S, P = [allr[k][0] for k in idx], [allr[k][1] for k in idx]
@@ -500,6 +503,14 @@ def alpha_check(local, sur, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins
     A = Engine(S, P, device=local)
     A.autotune(2000)
     A.run(sweeps_eq * nmax)
+    # the first stage's network, trained on exact dE harvested from these equilibrated replicas
+    # (the headline's network saw the generated, unrelaxed brushes only)
+    A.harvest(131072)
+    while A.harvest_count() < 131072:
+        A.run(20000)
+    sur = Surrogate(seed=31)
+    fit_loss = A.surrogate_fit(sur, epochs=12, batch=2048, lr=1e-3, clip=25.0, seed=3)
+    A.harvest(0)
     rounds, drift = 0, 1.0
     while True:
         rounds += 1
@@ -536,7 +547,7 @@ def alpha_check(local, sur, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins
     return {"workload": f"the {n_rep} smallest config-5 replicas ({min(s.n for s in S)}-{nmax} particles), "
                         "90% displacement / 10% protonation, batched exact as the plain engine",
             "sweeps_equilibrate": sweeps_eq + (rounds - 1) * sweeps_sample, "sweeps_sample": sweeps_sample,
-            "blocks": blocks, "rounds": rounds, "exact_dE_skipped": 1.0 - ps / max(ev, 1),
+            "blocks": blocks, "rounds": rounds, "fit_loss": fit_loss, "exact_dE_skipped": 1.0 - ps / max(ev, 1),
             "second_stage_agreement": ac / max(ps, 1), "pH_curve": curve,
             "max_curve_diff": float(max(abs(c["diff"]) for c in curve)),
             "all_within_2se": bool(all(c["within_2se"] for c in curve)),
@@ -753,7 +764,9 @@ def run_ours(args):
         eng.flush_l2(256 << 20)
         ms_ex = eng.run_timed(T)
         line["batched_exact_sweeps_per_s"] = sweeps_per_step / (ms_ex / 1e3)
-        line["titration_phase"] = titration_phase(eng, sur, [int(s.meta["n_sites"]) for s, _ in reps], args.da_threshold)
+        if sur is not None:
+            line["titration_phase"] = titration_phase(eng, sur, [int(s.meta["n_sites"]) for s, _ in reps],
+                                                      args.da_threshold)
     eng.close()
     ref_dir = tempfile.mkdtemp(prefix="phmc_ref_")
     if rank == 0 and world == 1 and (not args.no_extras or not args.no_cpu_baseline):
@@ -766,7 +779,7 @@ def run_ours(args):
         except Exception as e:  # an extra: the headline line is printed regardless
             line["reference_phase2_on_device"] = {"error": str(e)[:300]}
         if not args.no_alpha:
-            line["alpha_check"] = alpha_check(local, sur, args.alpha_eq, args.alpha_sample)
+            line["alpha_check"] = alpha_check(local, args.alpha_eq, args.alpha_sample)
         for key, fn, off in (("config1", config1_run, args.no_config1), ("config3", config3_run, args.no_config3),
                              ("config4", config4_run, args.no_config4)):
             if off:

@@ -437,10 +437,24 @@ __device__ void plane_fwd(const DevPtrs& d, const RepDesc& D, int z, int unit_ch
         int zrel = z - D.zb_lo;
         zrel += (zrel < 0) ? D.mesh[2] : 0;
         const ulonglong2* q = qs ? qs : reinterpret_cast<const ulonglong2*>(d.qband + D.qb_off + (size_t)zrel * N * N);
-        for (int i = tid; i < N * M; i += NT) {
-            const int y = i / M, j = i - y * M;
-            const ulonglong2 v = q[i];
-            xa[y * MS + j] = make_float2((float)((double)(long long)v.x * PHMC_FIX_INV), (float)((double)(long long)v.y * PHMC_FIX_INV));
+        // batches of LB loads issued back to back before their shared-memory stores (the stores
+        // could alias the loads as far as the compiler knows, so it would not hoist them)
+        constexpr int LB = 8;
+        for (int i0 = tid; i0 < N * M; i0 += LB * NT) {
+            ulonglong2 v[LB];
+#pragma unroll
+            for (int u = 0; u < LB; ++u) {
+                const int i = i0 + u * NT;
+                if (i < N * M) v[u] = q[i];
+            }
+#pragma unroll
+            for (int u = 0; u < LB; ++u) {
+                const int i = i0 + u * NT;
+                if (i >= N * M) break;
+                const int y = i / M, j = i - y * M;
+                xa[y * MS + j] = make_float2((float)((double)(long long)v[u].x * PHMC_FIX_INV),
+                                             (float)((double)(long long)v[u].y * PHMC_FIX_INV));
+            }
         }
     }
     __syncthreads();

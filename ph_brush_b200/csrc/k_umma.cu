@@ -78,19 +78,55 @@ __device__ __forceinline__ float gelu_grad_dev(float x) {
 }
 
 // Stage one K chunk of `rows` rows (element (r, k) = src[(row0 + r) * s_r + (k0 + k) * s_k], zero
-// outside [0, nrow) x [k0, kend)) into the canonical K-major layout at dst.
+// outside [0, nrow) x [k0, kend)) into the canonical K-major layout at dst.  Groups of 8
+// elements along the contiguous axis move as one 16-byte load when aligned: along K
+// (s_k == 1) a group is one 16-byte row of a core matrix; along the rows (s_r == 1) it
+// is one element of 8 consecutive core-matrix rows.  Other strides, and groups that
+// straddle the edge, go element by element.
 __device__ __forceinline__ void stage_tile(unsigned char* dst, int rows, const __nv_bfloat16* __restrict__ src,
                                            long s_r, long s_k, int row0, int nrow, int k0, int kend) {
     const __nv_bfloat16 z = __float2bfloat16(0.0f);
     const int groups = rows >> 3;
-    for (int e = threadIdx.x; e < rows * UM_KC; e += blockDim.x) {
-        int r, k;
-        if (s_k == 1) { r = e / UM_KC; k = e - r * UM_KC; }  // lanes along the contiguous axis
-        else { k = e / rows; r = e - k * rows; }
+    auto put = [&](int r, int k, __nv_bfloat16 v) {
+        *reinterpret_cast<__nv_bfloat16*>(dst + ((((k >> 3) * groups + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1))) = v;
+    };
+    auto get = [&](int r, int k) {
         const int gr = row0 + r, gk = k0 + k;
-        const __nv_bfloat16 v = (gr < nrow && gk < kend) ? src[(long)gr * s_r + (long)gk * s_k] : z;
-        const int off = (((k >> 3) * groups + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1);
-        *reinterpret_cast<__nv_bfloat16*>(dst + off) = v;
+        return (gr < nrow && gk < kend) ? src[(long)gr * s_r + (long)gk * s_k] : z;
+    };
+    const bool base16 = ((uintptr_t)src & 15) == 0;
+    if (s_k == 1 && base16 && (s_r & 7) == 0) {
+        for (int g = threadIdx.x; g < rows * (UM_KC / 8); g += blockDim.x) {
+            const int r = g / (UM_KC / 8), kq = (g - r * (UM_KC / 8)) * 8;
+            const int gr = row0 + r, gk = k0 + kq;
+            union { uint4 u; __nv_bfloat16 h[8]; } v;  // 16-byte aligned either way
+            v.u = make_uint4(0u, 0u, 0u, 0u);
+            if (gr < nrow && gk + 8 <= kend) v.u = *reinterpret_cast<const uint4*>(src + (long)gr * s_r + gk);
+            else if (gr < nrow && gk < kend) {
+                for (int q = 0; q < 8; ++q) v.h[q] = get(r, kq + q);
+            }
+            *reinterpret_cast<uint4*>(dst + ((((kq >> 3) * groups + (r >> 3)) << 7) + ((r & 7) << 4))) = v.u;
+        }
+    } else if (s_r == 1 && base16 && (s_k & 7) == 0 && (row0 & 7) == 0) {
+        for (int g = threadIdx.x; g < groups * UM_KC; g += blockDim.x) {
+            const int k = g / groups, r8 = (g - k * groups) * 8;
+            const int gr = row0 + r8, gk = k0 + k;
+            union { uint4 u; __nv_bfloat16 h[8]; } e;
+            if (gk < kend && gr + 8 <= nrow) {
+                e.u = *reinterpret_cast<const uint4*>(src + gr + (long)gk * s_k);
+            } else {
+                for (int q = 0; q < 8; ++q) e.h[q] = get(r8 + q, k);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) put(r8 + q, k, e.h[q]);
+        }
+    } else {
+        for (int e = threadIdx.x; e < rows * UM_KC; e += blockDim.x) {
+            int r, k;
+            if (s_k == 1) { r = e / UM_KC; k = e - r * UM_KC; }  // lanes along the contiguous axis
+            else { k = e / rows; r = e - k * rows; }
+            put(r, k, get(r, k));
+        }
     }
 }
 
