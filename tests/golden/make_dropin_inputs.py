@@ -3,7 +3,10 @@
 pool, and phase settings short enough for a test, so that the reference's own
 driver (MC/src/main.cu: protonation phase and phase-2 swaps) can run it both in
 its own build and linked against the engine's reference-API shim.
-dropin_gc.params runs the same system through a longer protonation phase.
+dropin_gc.params runs the same system through a longer protonation phase;
+dropin_already.params sets the target to the current protonation (29 of 108
+sites), so the protonation phase reports "already at target" in the stream
+state the plan summary left behind.
 With --large DIR it writes instead the timing input of the drop-in builds: the
 config-2 system (10x10 chains of 50, ~17k atoms with the W pool) in the
 reference's model, target 95 % (the direct protonation phase) and 3000
@@ -22,6 +25,8 @@ PHASES = {"target_pct": "30", "rng_seed": "2025", "max_attempts": "1500", "patie
           "energy_interval": "100", "gc_block_fixed": "300", "sgmc_epoch_attempt_max": "1500", "phase2_wc": "yes"}
 # the same system with a protonation phase of many blocks and mu updates (dropin_gc.params)
 PHASES_GC = dict(PHASES, target_pct="35", gc_block_fixed="10", sgmc_epoch_attempt_max="40")
+# target = the current protonation: floor(27.32 / 100 * 108) = 29 (dropin_already.params)
+PHASES_ALREADY = dict(PHASES, target_pct="27.32")
 
 
 LARGE = {"target_pct": "95", "rng_seed": "2025", "max_attempts": "3000", "patience": "100000",
@@ -46,6 +51,7 @@ def main():
     configs.write_lammps_data(os.path.join(HERE, "inputs", "dropin_small.data"), s)
     configs.write_params_in(os.path.join(HERE, "inputs", "dropin_small.params"), p, 0.5, extra=PHASES)
     configs.write_params_in(os.path.join(HERE, "inputs", "dropin_gc.params"), p, 0.5, extra=PHASES_GC)
+    configs.write_params_in(os.path.join(HERE, "inputs", "dropin_already.params"), p, 0.5, extra=PHASES_ALREADY)
 
 
 if __name__ == "__main__":
