@@ -468,18 +468,40 @@ def _alpha(stats, n_sites):
     return [st["n_charged_sites"] / n for st, n in zip(stats, n_sites)]
 
 
-def alpha_check(local, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins=16, max_rounds=3):
+def blocking_se(x):
+    """Standard error of the mean of a correlated series (axis 0: consecutive samples): the
+    largest naive error of the series averaged in blocks of 1, 2, 4, ... samples while at least
+    five blocks remain (the blocking method, Flyvbjerg & Petersen 1989)."""
+    import numpy as np
+    x = np.asarray(x, np.float64)
+    best = np.zeros(x.shape[1:])
+    while x.shape[0] >= 5:
+        best = np.maximum(best, np.sqrt(x.var(0, ddof=1) / x.shape[0]))
+        m = x.shape[0] // 2
+        x = 0.5 * (x[0:2 * m:2] + x[1:2 * m:2])
+    return best
+
+
+def alpha_check(local, sweeps_eq, sweeps_sample, per_bin=6, blocks=20, nbins=16, max_rounds=3):
     """alpha(pH) and z-profiles of delayed acceptance against the plain engine on real config-5
-    replicas (the 24 smallest of the headline set, its move mix; batched exact is the plain
-    engine): the plain engine equilibrates until the drift of its degree of ionisation
-    between the two halves of a sample is below 0.002 (at most max_rounds rounds), a second
-    engine takes over the equilibrated states with a surrogate trained on exact dE harvested
-    from them as first stage, and both sample `sweeps_sample` sweeps; every 250 trials each replica's MC kernel adds
-    its z-histogram (phmc_set_zhist), read back per block."""
+    replicas (in each pH bin 5-6, 6-7, 7-8, 8-9 the `per_bin` smallest of the headline set; its
+    move mix; batched exact is the plain engine): the plain engine equilibrates until the drift
+    of its degree of ionisation between the two halves of a sample is below 0.002 (at most
+    max_rounds rounds); a second engine, with a surrogate trained on exact dE harvested from
+    the equilibrated replicas as first stage, starts from the state the plain engine's last
+    sample started from, so both sample the same `sweeps_sample` sweeps after the same state.
+    Every 250 trials each replica's MC kernel adds its z-histogram (phmc_set_zhist), read
+    back per block; the error of each replica's alpha difference is the blocking-method error
+    of its per-block difference series."""
     import numpy as np
     from ph_brush_b200 import Engine, Surrogate, configs
+    t0 = time.perf_counter()
     allr = configs.config5(seed=2029, n_rep=256)
-    idx = sorted(range(len(allr)), key=lambda k: allr[k][0].n)[:n_rep]
+    pH_all = np.array([p.pH for _, p in allr])
+    idx = []
+    for lo in (5.0, 6.0, 7.0, 8.0):
+        m = [k for k in range(len(allr)) if lo <= pH_all[k] < lo + 1.0 + (1e-9 if lo == 8.0 else 0.0)]
+        idx += sorted(m, key=lambda k: allr[k][0].n)[:per_bin]
     S, P = [allr[k][0] for k in idx], [allr[k][1] for k in idx]
     ns_site = np.array([s.meta["n_sites"] for s in S], np.float64)
     nmax = max(s.n for s in S)
@@ -514,6 +536,7 @@ def alpha_check(local, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins=16, 
     rounds, drift = 0, 1.0
     while True:
         rounds += 1
+        start = A.state(-1)
         a_p, prof_p = sample(A)
         half = blocks // 2
         drift = float(np.abs(a_p[half:].mean(0) - a_p[:half].mean(0)).mean())
@@ -522,14 +545,15 @@ def alpha_check(local, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins=16, 
     B = Engine(S, P, device=local)
     tn = A.tuning()
     B.set_tuning(tn["pending_max"], tn["threads"])
-    B.set_state(A.state(-1), -1)
+    B.set_state(start, -1)
     B.attach_surrogate(sur, threshold=0.0, window=0)
     a_d, prof_d = sample(B)
     ev, ps, ac = sums(B.da_stats())
     A.close()
     B.close()
     mp, md = a_p.mean(0), a_d.mean(0)
-    se = np.sqrt(a_p.var(0, ddof=1) / blocks + a_d.var(0, ddof=1) / blocks)
+    se = blocking_se(a_d - a_p)  # per replica: both chains' blocks cover the same trials after one state
+    se_unpaired = np.sqrt(blocking_se(a_p) ** 2 + blocking_se(a_d) ** 2)
     pH = np.array([p.pH for p in P])
     curve = []
     for lo in (5.0, 6.0, 7.0, 8.0):
@@ -540,22 +564,28 @@ def alpha_check(local, sweeps_eq, sweeps_sample, n_rep=24, blocks=20, nbins=16, 
         diff = float(md[m].mean() - mp[m].mean())
         curve.append({"pH": [lo, lo + 1.0], "replicas": int(m.sum()), "alpha_plain": float(mp[m].mean()),
                       "alpha_da": float(md[m].mean()), "diff": diff, "stderr": se_b,
+                      "stderr_unpaired": float(np.sqrt((se_unpaired[m] ** 2).sum()) / m.sum()),
                       "within_2se": abs(diff) <= 2 * se_b})
     # z-profiles: per bin, the replica-mean profile difference against its spread over replicas
     dprof = prof_d - prof_p
     zscore = np.abs(dprof.mean(0)) / (dprof.std(0, ddof=1) / np.sqrt(len(S)) + 1e-12)
-    return {"workload": f"the {n_rep} smallest config-5 replicas ({min(s.n for s in S)}-{nmax} particles), "
-                        "90% displacement / 10% protonation, batched exact as the plain engine",
+    max_diff = float(max(abs(c["diff"]) for c in curve))
+    return {"workload": f"config-5 replicas, the {per_bin} smallest in each pH bin 5-6, 6-7, 7-8, 8-9 "
+                        f"({min(s.n for s in S)}-{nmax} particles), 90% displacement / 10% protonation, "
+                        "batched exact as the plain engine",
             "sweeps_equilibrate": sweeps_eq + (rounds - 1) * sweeps_sample, "sweeps_sample": sweeps_sample,
             "blocks": blocks, "rounds": rounds, "fit_loss": fit_loss, "exact_dE_skipped": 1.0 - ps / max(ev, 1),
             "second_stage_agreement": ac / max(ps, 1), "pH_curve": curve,
-            "max_curve_diff": float(max(abs(c["diff"]) for c in curve)),
+            "stderr_method": "blocking method on each replica's per-block difference series; both chains "
+                             "start from the same state and sample the same number of trials",
+            "max_curve_diff": max_diff, "within_0_005": max_diff <= 0.005,
             "all_within_2se": bool(all(c["within_2se"] for c in curve)),
             "mean_abs_diff_per_replica": float(np.abs(md - mp).mean()),
             "median_stderr_per_replica": float(np.median(se)), "plain_drift_between_halves": drift,
             "z_profile_bins": nbins,
             "z_profile_max_zscore": {"sites": float(zscore[0].max()), "anions": float(zscore[1].max()),
-                                     "cations": float(zscore[2].max())}}
+                                     "cations": float(zscore[2].max())},
+            "seconds": time.perf_counter() - t0}
 
 
 def plain_config2(args, local):

@@ -9,13 +9,16 @@
 //    stage a chunk of A (128 x 64) and B (N x 64) in the canonical K-major
 //    layout without swizzle (8-row x 16-byte core matrices, 128 bytes each,
 //    consecutive in the M / N direction, the next 8 columns of K one
-//    "leading byte offset" further);
+//    "leading byte offset" further): 16-byte cp.async where the operand is
+//    contiguous along K, a warp-wide movmatrix transpose of 8 x 8 blocks
+//    where it is contiguous along M / N;
 //  * one thread issues the chunk's four 128 x N x 16 MMAs (tcgen05.mma
 //    .cta_group::1.kind::f16, smem descriptors for A and B, accumulator in
 //    TMEM) and commits them to the stage's mbarrier, which frees the stage
 //    for the chunk after next;
 //  * the epilogue reads the accumulator with tcgen05.ld (each warp its 32
-//    TMEM lanes = rows), applies the GEMM's epilogue and stores C.
+//    TMEM lanes = rows) into a shared-memory tile, then applies the GEMM's
+//    epilogue and stores C along the rows.
 // Every wait on an mbarrier is bounded; a wait that runs out records
 // PHMC_ERR_BUDGET in *err, the CTA then waits (bounded) for its MMAs in flight,
 // frees its tensor memory and returns.
@@ -78,11 +81,29 @@ __device__ __forceinline__ float gelu_grad_dev(float x) {
 }
 
 // Stage one K chunk of `rows` rows (element (r, k) = src[(row0 + r) * s_r + (k0 + k) * s_k], zero
-// outside [0, nrow) x [k0, kend)) into the canonical K-major layout at dst.  Groups of 8
-// elements along the contiguous axis move as one 16-byte load when aligned: along K
-// (s_k == 1) a group is one 16-byte row of a core matrix; along the rows (s_r == 1) it
-// is one element of 8 consecutive core-matrix rows.  Other strides, and groups that
-// straddle the edge, go element by element.
+// outside [0, nrow) x [k0, kend)) into the canonical K-major layout at dst: 8-row x 16-byte core
+// matrices of 128 bytes, consecutive along the rows, the next 8 columns of K one
+// (rows / 8) x 128 bytes further.  Every load of a chunk is in flight before the chunk is
+// waited for:
+//  * contiguous along K (s_k == 1, 16-byte aligned rows): one 16-byte cp.async per core-matrix
+//    row (zero-filled outside the tile); groups that straddle kend go element by element;
+//  * contiguous along the rows (s_r == 1): each warp moves whole core matrices — lane i loads
+//    the two elements (rows 2(i%4), 2(i%4)+1) of K column i/4 as one 4-byte word (the 8 x 8
+//    block in movmatrix's fragment layout, K along its rows), movmatrix.trans hands lane i
+//    K columns 2(i%4), 2(i%4)+1 of row i/4, which is the 4-byte word at byte 4i of the core
+//    matrix; eight blocks' loads are issued before the first transpose;
+//  * anything else element by element.
+// The caller completes the cp.asyncs (cp.async.wait_all) before the tensor cores read.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(su32(sdst)), "l"(gsrc), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ uint32_t movmatrix_t(uint32_t a) {
+    uint32_t d;
+    asm volatile("movmatrix.sync.aligned.m8n8.trans.b16 %0, %1;" : "=r"(d) : "r"(a));
+    return d;
+}
+
 __device__ __forceinline__ void stage_tile(unsigned char* dst, int rows, const __nv_bfloat16* __restrict__ src,
                                            long s_r, long s_k, int row0, int nrow, int k0, int kend) {
     const __nv_bfloat16 z = __float2bfloat16(0.0f);
@@ -94,31 +115,44 @@ __device__ __forceinline__ void stage_tile(unsigned char* dst, int rows, const _
         const int gr = row0 + r, gk = k0 + k;
         return (gr < nrow && gk < kend) ? src[(long)gr * s_r + (long)gk * s_k] : z;
     };
-    const bool base16 = ((uintptr_t)src & 15) == 0;
-    if (s_k == 1 && base16 && (s_r & 7) == 0) {
+    if (s_k == 1 && ((uintptr_t)src & 15) == 0 && (s_r & 7) == 0) {
         for (int g = threadIdx.x; g < rows * (UM_KC / 8); g += blockDim.x) {
             const int r = g / (UM_KC / 8), kq = (g - r * (UM_KC / 8)) * 8;
             const int gr = row0 + r, gk = k0 + kq;
-            union { uint4 u; __nv_bfloat16 h[8]; } v;  // 16-byte aligned either way
-            v.u = make_uint4(0u, 0u, 0u, 0u);
-            if (gr < nrow && gk + 8 <= kend) v.u = *reinterpret_cast<const uint4*>(src + (long)gr * s_r + gk);
-            else if (gr < nrow && gk < kend) {
+            unsigned char* d = dst + ((((kq >> 3) * groups + (r >> 3)) << 7) + ((r & 7) << 4));
+            if (gr < nrow && gk < kend && gk + 8 > kend) {
+                union { uint4 u; __nv_bfloat16 h[8]; } v;  // 16-byte aligned either way
                 for (int q = 0; q < 8; ++q) v.h[q] = get(r, kq + q);
-            }
-            *reinterpret_cast<uint4*>(dst + ((((kq >> 3) * groups + (r >> 3)) << 7) + ((r & 7) << 4))) = v.u;
-        }
-    } else if (s_r == 1 && base16 && (s_k & 7) == 0 && (row0 & 7) == 0) {
-        for (int g = threadIdx.x; g < groups * UM_KC; g += blockDim.x) {
-            const int k = g / groups, r8 = (g - k * groups) * 8;
-            const int gr = row0 + r8, gk = k0 + k;
-            union { uint4 u; __nv_bfloat16 h[8]; } e;
-            if (gk < kend && gr + 8 <= nrow) {
-                e.u = *reinterpret_cast<const uint4*>(src + gr + (long)gk * s_k);
+                *reinterpret_cast<uint4*>(d) = v.u;
             } else {
-                for (int q = 0; q < 8; ++q) e.h[q] = get(r8 + q, k);
+                const bool ok = gr < nrow && gk + 8 <= kend;
+                cp_async16(d, ok ? (const void*)(src + (long)gr * s_r + gk) : (const void*)src, ok);
+            }
+        }
+    } else if (s_r == 1 && ((uintptr_t)src & 3) == 0 && (s_k & 1) == 0 && (row0 & 1) == 0) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        const int ncm = groups * (UM_KC / 8);  // core matrices of the tile: (row group, K group)
+        const int rl = 2 * (lane & 3), kl = lane >> 2;
+        for (int c0 = warp * 8; c0 < ncm; c0 += nw * 8) {
+            uint32_t w[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int cm = c0 + j;
+                const int kg = cm / groups, rg = cm - kg * groups;
+                const int gr = row0 + rg * 8 + rl, gk = k0 + kg * 8 + kl;
+                w[j] = 0u;
+                if (cm < ncm && gk < kend && gr < nrow) {
+                    const __nv_bfloat16* p = src + gr + (long)gk * s_k;
+                    if (gr + 1 < nrow) w[j] = *reinterpret_cast<const uint32_t*>(p);
+                    else w[j] = (uint32_t)__bfloat16_as_ushort(p[0]);
+                }
             }
 #pragma unroll
-            for (int q = 0; q < 8; ++q) put(r8 + q, k, e.h[q]);
+            for (int j = 0; j < 8; ++j) {
+                const int cm = c0 + j;
+                const uint32_t t = movmatrix_t(w[j]);  // every lane takes part (cm is warp-uniform)
+                if (cm < ncm) *reinterpret_cast<uint32_t*>(dst + (cm << 7) + 4 * lane) = t;
+            }
         }
     } else {
         for (int e = threadIdx.x; e < rows * UM_KC; e += blockDim.x) {
@@ -173,6 +207,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(int M, int N, int K, const
         const int k0 = kbeg + c * UM_KC;
         stage_tile(stA[b], UM_ROWS, A, sai, sak, i0, M, k0, kend);
         stage_tile(stB[b], Np, B, sbj, sbk, 0, N, k0, kend);
+        asm volatile("cp.async.wait_all;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -200,24 +235,35 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(int M, int N, int K, const
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const bool ok = !s_fail;
     if (ok && nchunks > 0) {
-        const int row = i0 + warp * 32 + lane;
+        // each warp moves its 32 TMEM lanes (rows) through shared memory, 64 columns at a
+        // time (32 x 65 floats per warp: the stages are free once every MMA has completed),
+        // so that the epilogue's loads and stores run along the rows
+        float* tile = reinterpret_cast<float*>(um_smem) + warp * (32 * 65);
         if (epi == 0) Cf += (size_t)blockIdx.z * M * N;
-        for (int c0 = 0; c0 < Np; c0 += 16) {
-            uint32_t v[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15}, [%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
+        for (int cb = 0; cb < Np; cb += 64) {
+            const int cw = min(64, Np - cb);
+            for (int c0 = 0; c0 < cw; c0 += 16) {
+                uint32_t v[16];
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int j = c0 + q;
-                    if (j >= N) break;
-                    const float acc = __uint_as_float(v[q]);
+                for (int q = 0; q < 16; ++q) tile[lane * 65 + c0 + q] = __uint_as_float(v[q]);
+            }
+            __syncwarp();
+            for (int rr = 0; rr < 32; ++rr) {
+                const int row = i0 + warp * 32 + rr;
+                if (row >= M) break;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int jj = lane + 32 * h, j = cb + jj;
+                    if (jj >= cw || j >= N) continue;
+                    const float acc = tile[rr * 65 + jj];
                     const long o = (long)row * N + j;
                     if (epi == 0) Cf[o] = acc;
                     else if (epi == 1) {
@@ -229,6 +275,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(int M, int N, int K, const
                     }
                 }
             }
+            __syncwarp();
         }
     } else if (!ok && threadIdx.x == 0 && err) {
         atomicExch(err, PHMC_ERR_BUDGET);
@@ -239,10 +286,13 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(int M, int N, int K, const
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
-// Shared memory of one launch: two stages of A (128 x 64) and B (Np x 64) BF16.
+// Shared memory of one launch: two stages of A (128 x 64) and B (Np x 64) BF16, at least the
+// epilogue's four 32 x 65 float tiles.
 static size_t umma_gemm_smem(int N) {
     const int Np = (N + 15) & ~15;
-    return (size_t)2 * (UM_ROWS * UM_KC * 2 + Np * UM_KC * 2);
+    const size_t stages = (size_t)2 * (UM_ROWS * UM_KC * 2 + Np * UM_KC * 2);
+    const size_t epilogue = (size_t)4 * 32 * 65 * sizeof(float);  // the epilogue's row tiles (reuse the stages)
+    return stages > epilogue ? stages : epilogue;
 }
 
 // A failed bounded wait of any launch on this device (PHMC_ERR_BUDGET), cleared when read.
