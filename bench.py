@@ -783,6 +783,16 @@ def run_ours(args):
                           "second_stage_agreement": ((da1[2] - da0[2]) / (da1[1] - da0[1])) if da1[1] > da0[1] else None,
                           "fallbacks": int(sum(d["fallback"] for d in eng.da_stats()))},
             "clocks": clk}
+    if rank == 0 and world == 1:
+        # where a trial's time goes (after the timed region): SM cycles per trial of each MC-kernel
+        # phase, summed over the replicas' blocks (one extra barrier per trial while measured)
+        eng.set_phase_clock(True)
+        eng.phase_cycles(reset=True)
+        eng.run(max(T // 4, 1))
+        pc = eng.phase_cycles(reset=True)
+        eng.set_phase_clock(False)
+        if pc["trials"]:
+            line["k_mc_phase_cycles_per_trial"] = {k: v / pc["trials"] for k, v in pc.items() if k != "trials"}
     if rank == 0 and world == 1 and not args.no_extras:
         plain, pick = plain_aggregate(args, reps, local, 400)
         line["plain_aggregate_sweeps_per_s"] = plain

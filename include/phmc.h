@@ -228,7 +228,9 @@ typedef struct phmc_tuning {
     int cand_round;       /* pair pass: candidate particles per thread and round (2, 4 or 8 at order 5; 4
                              otherwise); a round's neighbour tile is cand_round x threads candidates */
     int g_rows;           /* pending-correction sum: rows of the influence kernel G in flight per thread
-                             (2; 3 or 4 with cand_round 2 at order 5) */
+                             (2; 3 or 4 with cand_round 2 at order 5, one row per work item); 12 or 13 with
+                             cand_round 2 at order 5: work items of 2 or 3 rows of one (pair, z) plane, the
+                             pair's x tables held in registers */
     int plane_pipe;       /* rebuild's first pass: 1 persistent blocks that bulk-copy the next band plane's
                              charges into shared memory while transforming the current one; 0 one block per
                              plane (square lateral meshes of the register passes only) */
@@ -371,6 +373,19 @@ typedef struct phmc_profile {
 /* Profiling on: per-launch CUDA events around the MC kernel and the rebuilds. */
 int phmc_set_profiling(phmc_engine* e, int on);
 int phmc_get_profile(phmc_engine* e, phmc_profile* out, int reset);
+/* Phase clocks of the MC kernel: with `on`, each replica's block adds the SM cycles of
+ * its trial phases (read with clock64 by the block's first thread at the barrier that
+ * ends each phase; one extra barrier per trial separates phases 4 and 5):
+ *   0 proposal (and the charge-mesh updates of the last accepted change),
+ *   1 surrogate first stage, 2 cell counts + stencils + direct and bonded terms,
+ *   3 candidate offsets + stencil-pair tables, 4 candidate pair terms,
+ *   5 stencil . phi + pending-stencil corrections + block reduction,
+ *   6 decision + commit, 7 trials that end before phase 2.
+ * phmc_get_phase_cycles sums them over replicas (and the trials run, when `trials` is
+ * not NULL); `reset` zeroes them.  No counterpart in the reference. */
+#define PHMC_PHASES 8
+int phmc_set_phase_clock(phmc_engine* e, int on);
+int phmc_get_phase_cycles(phmc_engine* e, int64_t cycles[PHMC_PHASES], int64_t* trials, int reset);
 /* phmc_run with its device time (CUDA events on the engine stream) in *device_ms. */
 int phmc_run_timed(phmc_engine* e, int64_t n_trials, double* device_ms);
 /* Write `bytes` of scratch on the engine stream (evicts L2 between timed steps). */

@@ -200,10 +200,13 @@ class Phase2Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+PHASES = ("proposal", "first_stage", "cells_stencils_direct", "offsets_pair_tables", "candidate_pairs",
+          "phi_pending_reduce", "decision_commit", "ended_early")
+
 EXPORTS = ["phmc_abi_version", "phmc_last_error", "phmc_create", "phmc_destroy", "phmc_energy",
            "phmc_delta_energy", "phmc_commit", "phmc_set_identity", "phmc_run", "phmc_set_trial_log",
            "phmc_set_replay", "phmc_get_state", "phmc_get_cells", "phmc_capacity", "phmc_build_brush",
-           "phmc_set_state", "phmc_set_quorum", "phmc_set_launch_budget", "phmc_set_tile_shapes", "phmc_set_event_callback", "phmc_set_first_stage", "phmc_set_zhist", "phmc_get_zhist", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_run_timed", "phmc_flush_l2",
+           "phmc_set_state", "phmc_set_quorum", "phmc_set_launch_budget", "phmc_set_tile_shapes", "phmc_set_event_callback", "phmc_set_first_stage", "phmc_set_zhist", "phmc_get_zhist", "phmc_checkpoint_save", "phmc_checkpoint_load", "phmc_lammps_header", "phmc_lammps_read", "phmc_lammps_write", "phmc_params_read", "phmc_set_profiling", "phmc_get_profile", "phmc_set_phase_clock", "phmc_get_phase_cycles", "phmc_run_timed", "phmc_flush_l2",
            "phmc_recip_energy_static",
            "phmc_surrogate_create", "phmc_surrogate_set_gemm", "phmc_surrogate_destroy", "phmc_surrogate_num_params",
            "phmc_surrogate_get_params", "phmc_surrogate_set_params", "phmc_surrogate_set_scaling",
@@ -253,6 +256,8 @@ def load_library(path=LIB_PATH):
         "phmc_set_zhist": ([eng, C.c_int, C.c_int64], C.c_int),
         "phmc_get_zhist": ([eng, C.c_int, _dp, C.POINTER(C.c_int64)], C.c_int),
         "phmc_get_profile": ([eng, C.POINTER(Profile), C.c_int], C.c_int),
+        "phmc_set_phase_clock": ([eng, C.c_int], C.c_int),
+        "phmc_get_phase_cycles": ([eng, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int], C.c_int),
         "phmc_run_timed": ([eng, C.c_int64, _dp], C.c_int),
         "phmc_flush_l2": ([eng, C.c_int64], C.c_int),
         "phmc_recip_energy_static": ([_fp, _fp, _fp, _fp, C.c_int, _dp, _ip, C.c_int, C.c_double, C.c_double,

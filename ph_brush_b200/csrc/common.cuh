@@ -133,6 +133,9 @@ struct RepState {
     int da_off;         // agreement fell below the threshold: plain Metropolis from then on
     int da_pad;
     long long busy_ns;  // summed run time of this replica's MC blocks (globaltimer)
+    // with phase clocks on (phmc_set_phase_clock): SM cycles of the MC kernel's phases,
+    // measured by the block's thread 0 at the block barriers that end them (PHMC_PHASES)
+    long long clk[8];
 };
 
 // Device pointers of the whole engine (all replicas concatenated).
@@ -190,6 +193,7 @@ struct DevPtrs {
     // z-density profiles (phmc_set_zhist): after every zh_every trials each replica's MC
     // block adds its histogram over z (zh_bins bins between the walls) of charged sites,
     // anions and cations to zhist[r][3][zh_bins] and counts the sample in zh_samples[r]
+    int phase_clk;      // MC kernel: accumulate RepState::clk (one extra barrier per trial)
     int zh_bins;
     long long zh_every;
     unsigned long long* zhist;

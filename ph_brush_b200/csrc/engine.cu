@@ -910,6 +910,34 @@ extern "C" int phmc_get_profile(phmc_engine* h, phmc_profile* out, int reset) {
     return PHMC_OK;
 }
 
+extern "C" int phmc_set_phase_clock(phmc_engine* h, int on) {
+    if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    h->E.d.phase_clk = on != 0;
+    drop_graph(h);  // captured launches hold the old flag
+    return PHMC_OK;
+}
+
+extern "C" int phmc_get_phase_cycles(phmc_engine* h, int64_t cycles[PHMC_PHASES], int64_t* trials, int reset) {
+    if (!h || !cycles) return fail(PHMC_ERR_ARG, "null argument");
+    Engine& E = h->E;
+    CU(cudaSetDevice(E.device));
+    CU(cudaStreamSynchronize(E.stream));
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    int64_t t = 0;
+    for (int k = 0; k < PHMC_PHASES; ++k) cycles[k] = 0;
+    for (const RepState& r : st) {
+        for (int k = 0; k < PHMC_PHASES; ++k) cycles[k] += r.clk[k];
+        t += r.trials_run;
+    }
+    if (trials) *trials = t;
+    if (reset) {
+        for (RepState& r : st) std::memset(r.clk, 0, sizeof(r.clk));
+        CU(cudaMemcpy(E.d.state, st.data(), sizeof(RepState) * E.R, cudaMemcpyHostToDevice));
+    }
+    return PHMC_OK;
+}
+
 extern "C" int phmc_run_timed(phmc_engine* h, int64_t n_trials, double* device_ms) {
     if (!h || n_trials < 0 || !device_ms) return fail(PHMC_ERR_ARG, "invalid argument");
     Engine& E = h->E;
@@ -1749,7 +1777,8 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
     if ((cand_round >= 0 && cand_round != E.cand_round) || (g_rows >= 0 && g_rows != E.g_rows)) {
         if (cand_round >= 0 && cand_round != 2 && cand_round != 4 && cand_round != 8)
             return fail(PHMC_ERR_ARG, "cand_round must be 2, 4 or 8");
-        if (g_rows >= 0 && (g_rows < 2 || g_rows > 4)) return fail(PHMC_ERR_ARG, "g_rows must be 2, 3 or 4");
+        if (g_rows >= 0 && !(g_rows >= 2 && g_rows <= 4) && g_rows != 12 && g_rows != 13)
+            return fail(PHMC_ERR_ARG, "g_rows must be 2, 3, 4, 12 or 13");
         const int old_c = E.cand_round, old_g = E.g_rows;
         if (cand_round >= 0) E.cand_round = cand_round;
         if (g_rows >= 0) E.g_rows = g_rows;
@@ -1757,7 +1786,7 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
         if (e != cudaSuccess) {
             E.cand_round = old_c; E.g_rows = old_g;
             return fail(PHMC_ERR_UNSUPPORTED, "pair-pass shape not compiled: at order 5 (cand_round, g_rows) is one of "
-                                              "(4, 2), (2, 2), (8, 2), (2, 3), (2, 4); (4, 2) at other orders");
+                                              "(4, 2), (2, 2), (8, 2), (2, 3), (2, 4), (2, 12), (2, 13); (4, 2) at other orders");
         }
     }
     if (energy_block >= 0) {
@@ -1912,10 +1941,11 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     // 4. the pair pass's shape at that pending capacity and block size (order 5): round width
     //    (candidates per thread per round) x G rows in flight in the correction sum
     if (E.order == 5) {
-        const int shapes[5][2] = {{4, 2}, {2, 2}, {8, 2}, {2, 3}, {2, 4}};
-        double sbest[5] = {best, 1e300, 1e300, 1e300, 1e300};
+        const int shapes[7][2] = {{4, 2}, {2, 2}, {8, 2}, {2, 3}, {2, 4}, {2, 12}, {2, 13}};
+        constexpr int NSH = 7;
+        double sbest[NSH] = {best, 1e300, 1e300, 1e300, 1e300, 1e300, 1e300};
         for (int pass = 0; pass < 2; ++pass)
-            for (int k = 1; k < 5; ++k) {
+            for (int k = 1; k < NSH; ++k) {
                 if (apply_tiles(h, -1, shapes[k][0], -1, shapes[k][1]) != PHMC_OK) continue;
                 double us = 0.0;
                 s = time_run(&us);
@@ -1923,7 +1953,7 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
                 sbest[k] = std::min(sbest[k], us);
             }
         int bk = 0;
-        for (int k = 1; k < 5; ++k) {
+        for (int k = 1; k < NSH; ++k) {
             if (sbest[k] >= 1e300) continue;
             apply_tiles(h, -1, shapes[k][0], -1, shapes[k][1]);
             emit(sbest[k], 0.0, 0.0);

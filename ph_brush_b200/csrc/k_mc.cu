@@ -718,7 +718,9 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
 
 // RC: candidate particles per thread and round of the pair pass (the neighbour tile of a
 // round is RC x NT candidates); RR: rows of the influence kernel G each thread has in
-// flight per step of the pending-correction sum; both tuning parameters
+// flight per step of the pending-correction sum (2-4: one row per work item, strided over
+// the block; 10 + g: work items of g rows of one (pair, dz) plane, the pair's x tables in
+// registers); both tuning parameters
 template <int P, int NT, bool GC, int RC = 4, int RR = 2>
 __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
@@ -805,6 +807,18 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     }
     unsigned long long t_start = 0;
     if (tid == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
+    // phase clocks (thread 0, after the barrier that ends each phase): 0 proposal, 1 first
+    // stage, 2 cell counts + stencils + direct terms, 3 offsets + pair tables, 4 candidate pair
+    // terms, 5 phi gather + pending corrections + reduction, 6 decision + commit, 7 trials
+    // ended before phase 2 (first-stage rejections, invalid proposals)
+    long long clk_last = clock64();
+    auto mark = [&](int ph) {
+        if (tid == 0 && d.phase_clk) {
+            const long long now = clock64();
+            S.clk[ph] += now - clk_last;
+            clk_last = now;
+        }
+    };
     __syncthreads();
 
     for (;;) {
@@ -904,6 +918,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         }
         __syncthreads();
         if (T.stop) break;
+        mark(0);
         if (tid == 0) { s_hv_slot = -1; s_nqjob = 0; }
         // ---------------- surrogate first stage ----------------
         if (T.desc) {
@@ -1098,6 +1113,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             }
             __syncthreads();
         }
+        mark(1);
         if (T.skip) {
             if (tid == 0) {
                 if (mode == MC_RUN && T.move < 3) S.att[T.move]++;
@@ -1116,6 +1132,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 }
             }
             __syncthreads();
+            mark(7);
             continue;
         }
         // ---------------- phase 2: cell counts, stencils, direct & bonded terms ----------------
@@ -1180,6 +1197,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             T.d_fene = df;
         }
         __syncthreads();
+        mark(2);
         // ---------------- phase 3: candidate offsets, stencil pair kernels ----------------
         if (tid < 32) {
             int carry = 0;
@@ -1240,6 +1258,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             if (tid == 32) T.npairs = npairs;
         }
         __syncthreads();
+        mark(3);
         // ---------------- phase 4: all pair / mesh work items ----------------
         // helper loads off the critical path: the next trial's primary particle,
         // and the cell bookkeeping a commit of this trial would need
@@ -1305,6 +1324,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 }
             }
         }
+        if (d.phase_clk) {  // uniform over the block
+            __syncthreads();
+            mark(4);
+        }
         if (D.coulomb == PHMC_COUL_EWALD) {
             // W_t . phi: element (stencil, c, b, a), a fastest (lanes read consecutive x)
             const float* phi = d.phi + D.mesh_off;
@@ -1325,6 +1348,41 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const float* G = d.goct + D.oct_off;
             const int ox = D.oct[0], oy = D.oct[1];
             constexpr int WW = W * W;
+            if constexpr (RR > 10) {
+                // work items of GR rows of one (pair, dz) plane: the pair's x tables (folded
+                // coordinates and Kx) are read from shared memory once per item and kept in
+                // registers; the item's GR x W loads of G are in flight together
+                constexpr int GR = RR - 10;
+                constexpr int NG = (W + GR - 1) / GR;  // row groups per plane
+                const int nitem = T.npairs * W * NG;
+                for (int it = tid; it < nitem; it += NT) {
+                    const int q = it / (W * NG), rw = it - q * (W * NG);
+                    const int dz = rw / NG, dy0 = (rw - dz * NG) * GR;
+                    const PairK<P>& pk = s_pair[q];
+                    int fx[W];
+                    float kx[W];
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) { fx[dx] = pk.f[0][dx]; kx[dx] = pk.K[0][dx]; }
+                    const float* Gz = G + (size_t)pk.f[2][dz] * oy * ox;
+                    float gv[GR][W];
+#pragma unroll
+                    for (int u = 0; u < GR; ++u) {
+                        const int dy = min(dy0 + u, W - 1);
+                        const float* Grow = Gz + pk.f[1][dy] * ox;
+#pragma unroll
+                        for (int dx = 0; dx < W; ++dx) gv[u][dx] = __ldg(&Grow[fx[dx]]);
+                    }
+                    const float cz = pk.coef * pk.K[2][dz];
+#pragma unroll
+                    for (int u = 0; u < GR; ++u) {
+                        if (dy0 + u >= W) continue;
+                        float s = 0.0f;
+#pragma unroll
+                        for (int dx = 0; dx < W; ++dx) s = fmaf(kx[dx], gv[u][dx], s);
+                        acc_rec += (double)(cz * pk.K[1][dy0 + u] * s);
+                    }
+                }
+            } else {
             const int nrow = T.npairs * WW;
             for (int r0 = tid; r0 < nrow; r0 += RR * NT) {
                 float gv[RR][W];
@@ -1351,8 +1409,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                     acc_rec += (double)(pk.coef * pk.K[1][dy] * pk.K[2][dz] * s);
                 }
             }
+            }
         }
         block_sum3<NT>(acc_lj, acc_c, acc_rec, red);
+        mark(5);
         // ---------------- phase 5: decision and update ----------------
         if (tid == 0) {
             Moments mo;
@@ -1554,6 +1614,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             if (tid == 0) d.zh_samples[r] += 1;
             __syncthreads();
         }
+        mark(6);
     }
     if constexpr (GC) {
         const int* src = reinterpret_cast<const int*>(&sG);
@@ -1654,7 +1715,7 @@ static cudaError_t prepare_mc_t(Engine& E) {
 }
 
 // The compiled (order, round width, G rows) variants: order 5 (the configurations' order)
-// has five pair-pass shapes, orders 4 and 6 the default one.  f gets the four template
+// has seven pair-pass shapes, orders 4 and 6 the default one.  f gets the four template
 // values as integral constants; an unsupported combination gives cudaErrorInvalidValue.
 template <int V>
 using IC = std::integral_constant<int, V>;
@@ -1666,7 +1727,9 @@ static cudaError_t mc_dispatch(const Engine& E, F&& f) {
     if (rc == c && rr == g) return t128 ? f(IC<p>{}, IC<128>{}, IC<c>{}, IC<g>{}) : f(IC<p>{}, IC<256>{}, IC<c>{}, IC<g>{});
     switch (E.order) {
         case 4: MC_VARIANT(4, 4, 2) break;
-        case 5: MC_VARIANT(5, 4, 2) MC_VARIANT(5, 2, 2) MC_VARIANT(5, 8, 2) MC_VARIANT(5, 2, 3) MC_VARIANT(5, 2, 4) break;
+        case 5:
+            MC_VARIANT(5, 4, 2) MC_VARIANT(5, 2, 2) MC_VARIANT(5, 8, 2) MC_VARIANT(5, 2, 3) MC_VARIANT(5, 2, 4)
+            MC_VARIANT(5, 2, 12) MC_VARIANT(5, 2, 13) break;
         default: MC_VARIANT(6, 4, 2) break;
     }
 #undef MC_VARIANT

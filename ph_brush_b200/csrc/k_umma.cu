@@ -91,7 +91,7 @@ __device__ __forceinline__ float gelu_grad_dev(float x) {
 //    the two elements (rows 2(i%4), 2(i%4)+1) of K column i/4 as one 4-byte word (the 8 x 8
 //    block in movmatrix's fragment layout, K along its rows), movmatrix.trans hands lane i
 //    K columns 2(i%4), 2(i%4)+1 of row i/4, which is the 4-byte word at byte 4i of the core
-//    matrix; eight blocks' loads are issued before the first transpose;
+//    matrix; 32 blocks' loads are issued before the first transpose;
 //  * anything else element by element.
 // The caller completes the cp.asyncs (cp.async.wait_all) before the tensor cores read.
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
@@ -133,10 +133,10 @@ __device__ __forceinline__ void stage_tile(unsigned char* dst, int rows, const _
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
         const int ncm = groups * (UM_KC / 8);  // core matrices of the tile: (row group, K group)
         const int rl = 2 * (lane & 3), kl = lane >> 2;
-        for (int c0 = warp * 8; c0 < ncm; c0 += nw * 8) {
-            uint32_t w[8];
+        for (int c0 = warp * 32; c0 < ncm; c0 += nw * 32) {
+            uint32_t w[32];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < 32; ++j) {
                 const int cm = c0 + j;
                 const int kg = cm / groups, rg = cm - kg * groups;
                 const int gr = row0 + rg * 8 + rl, gk = k0 + kg * 8 + kl;
@@ -148,7 +148,7 @@ __device__ __forceinline__ void stage_tile(unsigned char* dst, int rows, const _
                 }
             }
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < 32; ++j) {
                 const int cm = c0 + j;
                 const uint32_t t = movmatrix_t(w[j]);  // every lane takes part (cm is warp-uniform)
                 if (cm < ncm) *reinterpret_cast<uint32_t*>(dst + (cm << 7) + 4 * lane) = t;
@@ -256,22 +256,46 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(int M, int N, int K, const
                 for (int q = 0; q < 16; ++q) tile[lane * 65 + c0 + q] = __uint_as_float(v[q]);
             }
             __syncwarp();
-            for (int rr = 0; rr < 32; ++rr) {
-                const int row = i0 + warp * 32 + rr;
-                if (row >= M) break;
+            // eight rows at a time: their inputs (the tile, and Zin for the GELU gradient) are
+            // loaded before any of them is computed and stored
+            float bj[2] = {0.0f, 0.0f};
+            if (epi == 1) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const int jj = lane + 32 * h, j = cb + jj;
-                    if (jj >= cw || j >= N) continue;
-                    const float acc = tile[rr * 65 + jj];
-                    const long o = (long)row * N + j;
-                    if (epi == 0) Cf[o] = acc;
-                    else if (epi == 1) {
-                        const float zz = acc + bias[j];
-                        Cf[o] = zz;
-                        Hb[o] = __float2bfloat16(gelu_dev(zz));
-                    } else {
-                        Hb[o] = __float2bfloat16(acc * gelu_grad_dev(Zin[o]));
+                    if (jj < cw && j < N) bj[h] = bias[j];
+                }
+            }
+            for (int r0 = 0; r0 < 32; r0 += 8) {
+                float av[8][2], zv[8][2];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int row = i0 + warp * 32 + r0 + u;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int jj = lane + 32 * h, j = cb + jj;
+                        av[u][h] = tile[(r0 + u) * 65 + jj];
+                        zv[u][h] = (epi == 2 && row < M && jj < cw && j < N) ? Zin[(long)row * N + j] : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int row = i0 + warp * 32 + r0 + u;
+                    if (row >= M) continue;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int jj = lane + 32 * h, j = cb + jj;
+                        if (jj >= cw || j >= N) continue;
+                        const float acc = av[u][h];
+                        const long o = (long)row * N + j;
+                        if (epi == 0) Cf[o] = acc;
+                        else if (epi == 1) {
+                            const float zz = acc + bj[h];
+                            Cf[o] = zz;
+                            Hb[o] = __float2bfloat16(gelu_dev(zz));
+                        } else {
+                            Hb[o] = __float2bfloat16(acc * gelu_grad_dev(zv[u][h]));
+                        }
                     }
                 }
             }

@@ -279,6 +279,19 @@ class Engine:
         _abi.check(self._lib.phmc_get_profile(self._h, C.byref(p), int(reset)))
         return p.asdict()
 
+    def set_phase_clock(self, on=True):
+        """Per-phase SM cycle counters of the MC kernel (phmc_set_phase_clock)."""
+        _abi.check(self._lib.phmc_set_phase_clock(self._h, int(on)))
+
+    def phase_cycles(self, reset=False):
+        """{phase name: SM cycles summed over replicas, "trials": trials run}."""
+        c = (C.c_int64 * 8)()
+        t = C.c_int64()
+        _abi.check(self._lib.phmc_get_phase_cycles(self._h, c, C.byref(t), int(reset)))
+        out = {k: int(v) for k, v in zip(_abi.PHASES, c)}
+        out["trials"] = int(t.value)
+        return out
+
     def run_timed(self, n_trials):
         ms = C.c_double()
         _abi.check(self._lib.phmc_run_timed(self._h, int(n_trials), C.byref(ms)))
