@@ -228,9 +228,9 @@ typedef struct phmc_tuning {
     int cand_round;       /* pair pass: candidate particles per thread and round (2, 4 or 8 at order 5; 4
                              otherwise); a round's neighbour tile is cand_round x threads candidates */
     int g_rows;           /* pending-correction sum: rows of the influence kernel G in flight per thread
-                             (2; 3 or 4 with cand_round 2 at order 5, one row per work item); 12 or 13 with
-                             cand_round 2 at order 5: work items of 2 or 3 rows of one (pair, z) plane, the
-                             pair's x tables held in registers */
+                             (2; 3 or 4 with cand_round 2 at order 5, one row per work item); 21 or 22 with
+                             cand_round 2 at order 5: one stencil pair per warp (1 or 2 pairs in flight), the
+                             lanes over the pair's (y, x) window plane, every z plane's loads in flight */
     int plane_pipe;       /* rebuild's first pass: 1 persistent blocks that bulk-copy the next band plane's
                              charges into shared memory while transforming the current one; 0 one block per
                              plane (square lateral meshes of the register passes only) */
@@ -381,8 +381,9 @@ int phmc_get_profile(phmc_engine* e, phmc_profile* out, int reset);
  *   3 candidate offsets + stencil-pair tables, 4 candidate pair terms,
  *   5 stencil . phi + pending-stencil corrections + block reduction,
  *   6 decision + commit, 7 trials that end before phase 2.
- * phmc_get_phase_cycles sums them over replicas (and the trials run, when `trials` is
- * not NULL); `reset` zeroes them.  No counterpart in the reference. */
+ * phmc_get_phase_cycles sums them over replicas, with the trials the replicas ran
+ * since the clocks were last switched or reset in *trials (when not NULL); `reset`
+ * zeroes them.  No counterpart in the reference. */
 #define PHMC_PHASES 8
 int phmc_set_phase_clock(phmc_engine* e, int on);
 int phmc_get_phase_cycles(phmc_engine* e, int64_t cycles[PHMC_PHASES], int64_t* trials, int reset);

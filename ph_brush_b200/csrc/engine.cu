@@ -39,6 +39,7 @@ struct phmc_engine {
     std::vector<int> caps;
     // measurement
     bool profiling = false;
+    int64_t clk_trials0 = 0;  // trials run by all replicas when the phase clocks were last switched or reset
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<std::pair<size_t, size_t>> ev_mc, ev_flush;  // (start, end) indices into ev_pool
@@ -910,8 +911,22 @@ extern "C" int phmc_get_profile(phmc_engine* h, phmc_profile* out, int reset) {
     return PHMC_OK;
 }
 
+// trials run by all replicas so far (the phase clocks' trial count is taken against it)
+static int trials_run_total(Engine& E, int64_t* out) {
+    std::vector<RepState> st((size_t)E.R);
+    CU(cudaStreamSynchronize(E.stream));
+    CU(cudaMemcpy(st.data(), E.d.state, sizeof(RepState) * E.R, cudaMemcpyDeviceToHost));
+    int64_t t = 0;
+    for (const RepState& r : st) t += r.trials_run;
+    *out = t;
+    return PHMC_OK;
+}
+
 extern "C" int phmc_set_phase_clock(phmc_engine* h, int on) {
     if (!h) return fail(PHMC_ERR_ARG, "null engine");
+    CU(cudaSetDevice(h->E.device));
+    const int s = trials_run_total(h->E, &h->clk_trials0);
+    if (s) return s;
     h->E.d.phase_clk = on != 0;
     drop_graph(h);  // captured launches hold the old flag
     return PHMC_OK;
@@ -930,10 +945,11 @@ extern "C" int phmc_get_phase_cycles(phmc_engine* h, int64_t cycles[PHMC_PHASES]
         for (int k = 0; k < PHMC_PHASES; ++k) cycles[k] += r.clk[k];
         t += r.trials_run;
     }
-    if (trials) *trials = t;
+    if (trials) *trials = t - h->clk_trials0;  // since the clocks were last switched or reset
     if (reset) {
         for (RepState& r : st) std::memset(r.clk, 0, sizeof(r.clk));
         CU(cudaMemcpy(E.d.state, st.data(), sizeof(RepState) * E.R, cudaMemcpyHostToDevice));
+        h->clk_trials0 = t;
     }
     return PHMC_OK;
 }
@@ -1777,8 +1793,8 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
     if ((cand_round >= 0 && cand_round != E.cand_round) || (g_rows >= 0 && g_rows != E.g_rows)) {
         if (cand_round >= 0 && cand_round != 2 && cand_round != 4 && cand_round != 8)
             return fail(PHMC_ERR_ARG, "cand_round must be 2, 4 or 8");
-        if (g_rows >= 0 && !(g_rows >= 2 && g_rows <= 4) && g_rows != 12 && g_rows != 13)
-            return fail(PHMC_ERR_ARG, "g_rows must be 2, 3, 4, 12 or 13");
+        if (g_rows >= 0 && !(g_rows >= 2 && g_rows <= 4) && g_rows != 21 && g_rows != 22)
+            return fail(PHMC_ERR_ARG, "g_rows must be 2, 3, 4, 21 or 22");
         const int old_c = E.cand_round, old_g = E.g_rows;
         if (cand_round >= 0) E.cand_round = cand_round;
         if (g_rows >= 0) E.g_rows = g_rows;
@@ -1786,7 +1802,7 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
         if (e != cudaSuccess) {
             E.cand_round = old_c; E.g_rows = old_g;
             return fail(PHMC_ERR_UNSUPPORTED, "pair-pass shape not compiled: at order 5 (cand_round, g_rows) is one of "
-                                              "(4, 2), (2, 2), (8, 2), (2, 3), (2, 4), (2, 12), (2, 13); (4, 2) at other orders");
+                                              "(4, 2), (2, 2), (8, 2), (2, 3), (2, 4), (2, 21), (2, 22); (4, 2) at other orders");
         }
     }
     if (energy_block >= 0) {
@@ -1941,7 +1957,7 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     // 4. the pair pass's shape at that pending capacity and block size (order 5): round width
     //    (candidates per thread per round) x G rows in flight in the correction sum
     if (E.order == 5) {
-        const int shapes[7][2] = {{4, 2}, {2, 2}, {8, 2}, {2, 3}, {2, 4}, {2, 12}, {2, 13}};
+        const int shapes[7][2] = {{4, 2}, {2, 2}, {8, 2}, {2, 3}, {2, 4}, {2, 21}, {2, 22}};
         constexpr int NSH = 7;
         double sbest[NSH] = {best, 1e300, 1e300, 1e300, 1e300, 1e300, 1e300};
         for (int pass = 0; pass < 2; ++pass)

@@ -719,8 +719,8 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
 // RC: candidate particles per thread and round of the pair pass (the neighbour tile of a
 // round is RC x NT candidates); RR: rows of the influence kernel G each thread has in
 // flight per step of the pending-correction sum (2-4: one row per work item, strided over
-// the block; 10 + g: work items of g rows of one (pair, dz) plane, the pair's x tables in
-// registers); both tuning parameters
+// the block; 20 + w: one pair per warp, w pairs in flight, lanes over the pair's (dy, dx)
+// plane); both tuning parameters
 template <int P, int NT, bool GC, int RC = 4, int RR = 2>
 __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
@@ -1348,38 +1348,50 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const float* G = d.goct + D.oct_off;
             const int ox = D.oct[0], oy = D.oct[1];
             constexpr int WW = W * W;
-            if constexpr (RR > 10) {
-                // work items of GR rows of one (pair, dz) plane: the pair's x tables (folded
-                // coordinates and Kx) are read from shared memory once per item and kept in
-                // registers; the item's GR x W loads of G are in flight together
-                constexpr int GR = RR - 10;
-                constexpr int NG = (W + GR - 1) / GR;  // row groups per plane
-                const int nitem = T.npairs * W * NG;
-                for (int it = tid; it < nitem; it += NT) {
-                    const int q = it / (W * NG), rw = it - q * (W * NG);
-                    const int dz = rw / NG, dy0 = (rw - dz * NG) * GR;
-                    const PairK<P>& pk = s_pair[q];
-                    int fx[W];
-                    float kx[W];
+            if constexpr (RR > 20) {
+                // one pair per warp and step (RR - 20 pairs in flight per warp): each lane takes
+                // EL elements (dy, dx) of the pair's W x W plane, so a load instruction reads
+                // about 32 / W consecutive rows of G; the lane's loads of all W z planes are in
+                // flight together; FP32 sums over the lane's EL elements, FP64 over planes
+                constexpr int PW = RR - 20;
+                constexpr int EL = (WW + 31) / 32;
+                const int warp = tid >> 5, lane = tid & 31;
+                for (int q0 = warp * PW; q0 < T.npairs; q0 += (NT / 32) * PW) {
+                    int off[PW][EL];
+                    float kk[PW][EL];
+                    float g[PW][W][EL];
 #pragma unroll
-                    for (int dx = 0; dx < W; ++dx) { fx[dx] = pk.f[0][dx]; kx[dx] = pk.K[0][dx]; }
-                    const float* Gz = G + (size_t)pk.f[2][dz] * oy * ox;
-                    float gv[GR][W];
+                    for (int v = 0; v < PW; ++v) {
+                        const int q = min(q0 + v, T.npairs - 1);
+                        const PairK<P>& pk = s_pair[q];
 #pragma unroll
-                    for (int u = 0; u < GR; ++u) {
-                        const int dy = min(dy0 + u, W - 1);
-                        const float* Grow = Gz + pk.f[1][dy] * ox;
+                        for (int k = 0; k < EL; ++k) {
+                            const int e = min(lane + 32 * k, WW - 1);
+                            const int dy = e / W, dx = e - dy * W;
+                            off[v][k] = pk.f[1][dy] * ox + pk.f[0][dx];
+                            kk[v][k] = (lane + 32 * k < WW && q0 + v < T.npairs) ? pk.K[1][dy] * pk.K[0][dx] : 0.0f;
+                        }
+                        int zoff[W];  // uniform over the warp
 #pragma unroll
-                        for (int dx = 0; dx < W; ++dx) gv[u][dx] = __ldg(&Grow[fx[dx]]);
+                        for (int dz = 0; dz < W; ++dz) zoff[dz] = pk.f[2][dz] * oy * ox;
+#pragma unroll
+                        for (int k = 0; k < EL; ++k) {
+                            const float* Gk = G + off[v][k];
+#pragma unroll
+                            for (int dz = 0; dz < W; ++dz) g[v][dz][k] = __ldg(Gk + zoff[dz]);
+                        }
                     }
-                    const float cz = pk.coef * pk.K[2][dz];
 #pragma unroll
-                    for (int u = 0; u < GR; ++u) {
-                        if (dy0 + u >= W) continue;
-                        float s = 0.0f;
+                    for (int v = 0; v < PW; ++v) {
+                        if (q0 + v >= T.npairs) continue;
+                        const PairK<P>& pk = s_pair[q0 + v];
 #pragma unroll
-                        for (int dx = 0; dx < W; ++dx) s = fmaf(kx[dx], gv[u][dx], s);
-                        acc_rec += (double)(cz * pk.K[1][dy0 + u] * s);
+                        for (int dz = 0; dz < W; ++dz) {
+                            float t = 0.0f;
+#pragma unroll
+                            for (int k = 0; k < EL; ++k) t = fmaf(kk[v][k], g[v][dz][k], t);
+                            acc_rec += (double)(pk.coef * pk.K[2][dz] * t);
+                        }
                     }
                 }
             } else {
@@ -1729,7 +1741,7 @@ static cudaError_t mc_dispatch(const Engine& E, F&& f) {
         case 4: MC_VARIANT(4, 4, 2) break;
         case 5:
             MC_VARIANT(5, 4, 2) MC_VARIANT(5, 2, 2) MC_VARIANT(5, 8, 2) MC_VARIANT(5, 2, 3) MC_VARIANT(5, 2, 4)
-            MC_VARIANT(5, 2, 12) MC_VARIANT(5, 2, 13) break;
+            MC_VARIANT(5, 2, 21) MC_VARIANT(5, 2, 22) break;
         default: MC_VARIANT(6, 4, 2) break;
     }
 #undef MC_VARIANT

@@ -22,12 +22,14 @@ def test_phase_clocks_leave_the_chain_unchanged_and_count_every_trial():
             states.append([e.state(r) for r in range(len(reps))])
             if on:
                 assert pc["trials"] == 3 * 1500
+                e.run(100)
+                assert e.phase_cycles()["trials"] == 3 * 100
                 for k in ("proposal", "cells_stencils_direct", "offsets_pair_tables", "candidate_pairs",
                           "phi_pending_reduce", "decision_commit"):
                     assert pc[k] > 0, k
                 assert pc["first_stage"] >= 0 and pc["ended_early"] >= 0
-                again = e.phase_cycles()
-                assert all(again[k] == 0 for k in _abi.PHASES)
+                again = e.phase_cycles(reset=True)
+                assert all(again[k] > 0 for k in ("proposal", "decision_commit"))
             else:
                 assert all(pc[k] == 0 for k in _abi.PHASES)
     for a, b in zip(*states):
