@@ -228,9 +228,9 @@ typedef struct phmc_tuning {
     int cand_round;       /* pair pass: candidate particles per thread and round (2, 4 or 8 at order 5; 4
                              otherwise); a round's neighbour tile is cand_round x threads candidates */
     int g_rows;           /* pending-correction sum: rows of the influence kernel G in flight per thread
-                             (2; 3 or 4 with cand_round 2 at order 5, one row per work item); 21 or 22 with
-                             cand_round 2 at order 5: one stencil pair per warp (1 or 2 pairs in flight), the
-                             lanes over the pair's (y, x) window plane, every z plane's loads in flight */
+                             (2; 3 or 4 with cand_round 2 at order 5, one row per work item); 21 with
+                             cand_round 2 or 4 at order 5: one stencil pair per warp, the lanes over its
+                             (y, x) window plane, every z plane's loads in flight */
     int plane_pipe;       /* rebuild's first pass: 1 persistent blocks that bulk-copy the next band plane's
                              charges into shared memory while transforming the current one; 0 one block per
                              plane (square lateral meshes of the register passes only) */

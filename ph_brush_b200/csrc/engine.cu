@@ -587,6 +587,43 @@ static int full_recompute(phmc_engine* h) {
     return check_kernel_errors(h);
 }
 
+// Replicas with the same box, mesh, order and Ewald parameters have bit-identical influence
+// kernels G: point every replica at the first copy of its octant, so that the MC kernel's G
+// reads of all such replicas share one table in L2 (config 5: 256 replicas, five distinct
+// boxes).  Octants are compared byte for byte on the host; the duplicates' storage is left
+// allocated and unused.
+static int share_octants(phmc_engine* h) {
+    Engine& E = h->E;
+    if (E.total_oct <= 0) return PHMC_OK;
+    std::vector<float> g((size_t)E.total_oct);
+    CU(cudaStreamSynchronize(E.stream));
+    CU(cudaMemcpy(g.data(), E.d.goct, sizeof(float) * (size_t)E.total_oct, cudaMemcpyDeviceToHost));
+    std::map<unsigned long long, std::vector<int>> by_hash;
+    bool changed = false;
+    for (int r = 0; r < E.R; ++r) {
+        RepDesc& D = E.desc[r];
+        const size_t n = (size_t)D.oct[0] * D.oct[1] * D.oct[2];
+        const float* p = g.data() + D.oct_off;
+        unsigned long long hs = 1469598103934665603ull ^ n;  // FNV-1a over the 32-bit words
+        for (size_t i = 0; i < n; ++i) {
+            uint32_t w;
+            std::memcpy(&w, p + i, 4);
+            hs = (hs ^ w) * 1099511628211ull;
+        }
+        std::vector<int>& seen = by_hash[hs];
+        int same = -1;
+        for (int c : seen) {
+            const RepDesc& C = E.desc[c];
+            if (C.oct[0] == D.oct[0] && C.oct[1] == D.oct[1] && C.oct[2] == D.oct[2] &&
+                std::memcmp(g.data() + C.oct_off, p, n * sizeof(float)) == 0) { same = c; break; }
+        }
+        if (same >= 0) { D.oct_off = E.desc[same].oct_off; changed = true; }
+        else seen.push_back(r);
+    }
+    if (changed) CU(cudaMemcpy(E.d.desc, E.desc.data(), sizeof(RepDesc) * E.R, cudaMemcpyHostToDevice));
+    return PHMC_OK;
+}
+
 extern "C" int phmc_create(int n_replicas, const phmc_system* systems, const phmc_params* params, int device,
                            phmc_engine** out) {
     if (!out) return fail(PHMC_ERR_ARG, "out is null");
@@ -606,6 +643,8 @@ extern "C" int phmc_create(int n_replicas, const phmc_system* systems, const phm
         for (int r = 0; r < E.R; ++r) launch_extract_octant(E, r, E.stream);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { phmc_destroy(h); return fail(PHMC_ERR_CUDA, std::string("G build: ") + cudaGetErrorString(e)); }
+        s = share_octants(h);
+        if (s) { std::string m = g_err; phmc_destroy(h); g_err = m; return s; }
     }
     s = full_recompute(h);
     if (s) { std::string m = g_err; phmc_destroy(h); g_err = m; return s; }
@@ -1793,8 +1832,8 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
     if ((cand_round >= 0 && cand_round != E.cand_round) || (g_rows >= 0 && g_rows != E.g_rows)) {
         if (cand_round >= 0 && cand_round != 2 && cand_round != 4 && cand_round != 8)
             return fail(PHMC_ERR_ARG, "cand_round must be 2, 4 or 8");
-        if (g_rows >= 0 && !(g_rows >= 2 && g_rows <= 4) && g_rows != 21 && g_rows != 22)
-            return fail(PHMC_ERR_ARG, "g_rows must be 2, 3, 4, 21 or 22");
+        if (g_rows >= 0 && !(g_rows >= 2 && g_rows <= 4) && g_rows != 21)
+            return fail(PHMC_ERR_ARG, "g_rows must be 2, 3, 4 or 21");
         const int old_c = E.cand_round, old_g = E.g_rows;
         if (cand_round >= 0) E.cand_round = cand_round;
         if (g_rows >= 0) E.g_rows = g_rows;
@@ -1802,7 +1841,7 @@ static int apply_tiles(phmc_engine* h, int zpass, int cand_round, int energy_blo
         if (e != cudaSuccess) {
             E.cand_round = old_c; E.g_rows = old_g;
             return fail(PHMC_ERR_UNSUPPORTED, "pair-pass shape not compiled: at order 5 (cand_round, g_rows) is one of "
-                                              "(4, 2), (2, 2), (8, 2), (2, 3), (2, 4), (2, 21), (2, 22); (4, 2) at other orders");
+                                              "(4, 2), (2, 2), (8, 2), (2, 3), (2, 4), (2, 21), (4, 21); (4, 2) at other orders");
         }
     }
     if (energy_block >= 0) {
@@ -1957,7 +1996,7 @@ extern "C" int phmc_autotune(phmc_engine* h, int64_t trials, phmc_tuning* result
     // 4. the pair pass's shape at that pending capacity and block size (order 5): round width
     //    (candidates per thread per round) x G rows in flight in the correction sum
     if (E.order == 5) {
-        const int shapes[7][2] = {{4, 2}, {2, 2}, {8, 2}, {2, 3}, {2, 4}, {2, 21}, {2, 22}};
+        const int shapes[7][2] = {{4, 2}, {2, 2}, {8, 2}, {2, 3}, {2, 4}, {2, 21}, {4, 21}};
         constexpr int NSH = 7;
         double sbest[NSH] = {best, 1e300, 1e300, 1e300, 1e300, 1e300, 1e300};
         for (int pass = 0; pass < 2; ++pass)

@@ -24,6 +24,8 @@
 
 #define NST_MAX 4    // stencils per trial
 #define NPROBE_MAX 4 // (old, new) states of up to two particles
+#define LIST_PF 16   // leading cell-list entries of each probe cell loaded with its count
+#define CAND_MAP 4096 // candidates whose probe-cell entry is tabulated in phase 3
 
 template <int P>
 struct Stencil {
@@ -80,34 +82,41 @@ struct Prefetch {
     int4 bonds;
 };
 
-__device__ __forceinline__ void probe_add(TrialS& T, float4 p, int type, int owner, float sign, const RepDesc& D) {
-    const int k = T.nprobe++;
-    T.probe_p[k] = p; T.probe_t[k] = type; T.probe_owner[k] = owner; T.probe_sign[k] = sign;
-    T.probe_cell[k] = cell_index(D, p.x, p.y, p.z);
-}
-
-__device__ __forceinline__ void stencil_add(TrialS& T, float4 p, float c) {
-    if (c == 0.0f) return;
-    T.st_pos[T.nst] = p; T.st_coef[T.nst] = c; T.nst++;
-}
-
 // Fill probes and stencils from the changes in T (old -> new states).
+// (The trial's fields are read once into registers and the counters kept in registers:
+// one thread runs this while the block waits, so its shared-memory round trips count.)
 __device__ void trial_setup(TrialS& T, const RepDesc& D) {
-    T.nprobe = 0; T.nst = 0;
-    for (int k = 0; k < T.nch; ++k) {
-        if (T.pres_old[k]) probe_add(T, T.po[k], T.to[k], k, -1.0f, D);
-        if (T.pres_new[k]) probe_add(T, T.pn[k], T.tn[k], k, 1.0f, D);
-        if (D.coulomb == PHMC_COUL_EWALD) {
-            const bool same_pos = T.pres_old[k] && T.pres_new[k] && T.po[k].x == T.pn[k].x && T.po[k].y == T.pn[k].y &&
-                                  T.po[k].z == T.pn[k].z;
+    const int nch = T.nch;
+    const bool ewald = D.coulomb == PHMC_COUL_EWALD;
+    int np = 0, ns = 0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (k >= nch) break;
+        const bool pold = T.pres_old[k], pnew = T.pres_new[k];
+        const float4 o = T.po[k], n = T.pn[k];
+        const int to = T.to[k], tn = T.tn[k];
+        if (pold) {
+            T.probe_p[np] = o; T.probe_t[np] = to; T.probe_owner[np] = k; T.probe_sign[np] = -1.0f;
+            T.probe_cell[np] = cell_index(D, o.x, o.y, o.z);
+            ++np;
+        }
+        if (pnew) {
+            T.probe_p[np] = n; T.probe_t[np] = tn; T.probe_owner[np] = k; T.probe_sign[np] = 1.0f;
+            T.probe_cell[np] = cell_index(D, n.x, n.y, n.z);
+            ++np;
+        }
+        if (ewald) {
+            const bool same_pos = pold && pnew && o.x == n.x && o.y == n.y && o.z == n.z;
             if (same_pos) {
-                stencil_add(T, T.pn[k], T.pn[k].w - T.po[k].w);
+                const float c = n.w - o.w;
+                if (c != 0.0f) { T.st_pos[ns] = n; T.st_coef[ns] = c; ++ns; }
             } else {
-                if (T.pres_old[k]) stencil_add(T, T.po[k], -T.po[k].w);
-                if (T.pres_new[k]) stencil_add(T, T.pn[k], T.pn[k].w);
+                if (pold && o.w != 0.0f) { T.st_pos[ns] = o; T.st_coef[ns] = -o.w; ++ns; }
+                if (pnew && n.w != 0.0f) { T.st_pos[ns] = n; T.st_coef[ns] = n.w; ++ns; }
             }
         }
     }
+    T.nprobe = np; T.nst = ns;
 }
 
 __device__ __forceinline__ float4 rand_pos(const RepDesc& D, uint32_t a, uint32_t b, uint32_t c) {
@@ -181,18 +190,29 @@ __device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const De
     };
     if (move == PHMC_MOVE_DISP) {
         if (S.n_mobile == 0) { T.skip = 1; return; }
-        load_primary(use_pf ? -1 : d.mobile[so + pick_index(A[1], S.n_mobile)]);
+        float4 po;
+        int to;
+        if (use_pf) {  // the prefetched particle, kept in registers for the new position
+            po = pf.pq; to = pf.type;
+            T.idx[0] = pf.idx; T.fo[0] = pf.flags; T.pres_old[0] = !(pf.flags & PHMC_F_GHOST);
+            T.po[0] = po; T.to[0] = to; T.bonds[0] = pf.bonds;
+        } else {
+            load_old(0, d.mobile[so + pick_index(A[1], S.n_mobile)]);
+            po = T.po[0]; to = T.to[0];
+        }
         const float dm = D.disp_max;
         const float dx = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[2])), 1.0f));
         const float dy = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[3])), 1.0f));
         const float dz = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(B[0])), 1.0f));
-        float nx = __fadd_rn(T.po[0].x, dx), ny = __fadd_rn(T.po[0].y, dy), nz = __fadd_rn(T.po[0].z, dz);
-        if (nx < 0.0f) nx = __fadd_rn(nx, D.L[0]); else if (nx >= D.L[0]) nx = __fsub_rn(nx, D.L[0]);
-        if (ny < 0.0f) ny = __fadd_rn(ny, D.L[1]); else if (ny >= D.L[1]) ny = __fsub_rn(ny, D.L[1]);
-        if (!D.walls) { if (nz < 0.0f) nz = __fadd_rn(nz, D.L[2]); else if (nz >= D.L[2]) nz = __fsub_rn(nz, D.L[2]); }
-        T.pres_new[0] = 1; T.pn[0] = make_float4(nx, ny, nz, T.po[0].w); T.tn[0] = T.to[0];
+        const float Lx = D.L[0], Ly = D.L[1], Lz = D.L[2];
+        float nx = __fadd_rn(po.x, dx), ny = __fadd_rn(po.y, dy), nz = __fadd_rn(po.z, dz);
+        if (nx < 0.0f) nx = __fadd_rn(nx, Lx); else if (nx >= Lx) nx = __fsub_rn(nx, Lx);
+        if (ny < 0.0f) ny = __fadd_rn(ny, Ly); else if (ny >= Ly) ny = __fsub_rn(ny, Ly);
+        const int walls = D.walls;
+        if (!walls) { if (nz < 0.0f) nz = __fadd_rn(nz, Lz); else if (nz >= Lz) nz = __fsub_rn(nz, Lz); }
+        T.pres_new[0] = 1; T.pn[0] = make_float4(nx, ny, nz, po.w); T.tn[0] = to;
         T.nch = 1;
-        if (D.walls && (nz < D.wall_lo || nz >= D.wall_hi)) T.skip = 2;  // hard wall: infinite energy
+        if (walls && (nz < D.wall_lo || nz >= D.wall_hi)) T.skip = 2;  // hard wall: infinite energy
     } else if (move == PHMC_MOVE_TITR) {
         if (D.n_titr == 0) { T.skip = 1; return; }
         load_primary(use_pf ? -1 : d.titr[so + pick_index(A[1], D.n_titr)]);
@@ -257,24 +277,26 @@ __device__ void load_external(TrialS& T, const RepDesc& D, const DevPtrs& d, con
     if (T.nch == 1) T.move = PHMC_MOVE_DISP;
 }
 
+// Axis k of the stencil of a charge at p (weights, base, wrapped mesh indices).
 template <int P>
-__device__ __forceinline__ void make_stencil(Stencil<P>& s, const RepDesc& D, float4 p, float coef) {
-    const float g[3] = {p.x / D.L[0] * (float)D.mesh[0], p.y / D.L[1] * (float)D.mesh[1], p.z / D.L[2] * (float)D.mesh[2]};
+__device__ __forceinline__ void make_stencil_axis(Stencil<P>& s, const RepDesc& D, float4 p, int k) {
+    const float pk = (k == 0) ? p.x : (k == 1 ? p.y : p.z);
+    const float g = pk / D.L[k] * (float)D.mesh[k];
+    const float fl = floorf(g);
+    float w[P];
+    bspline_weights<P>(g - fl, w);
+    const int base = (int)fl + P / 2 - P + 1;
+    s.base[k] = base;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float fl = floorf(g[k]);
-        bspline_weights<P>(g[k] - fl, s.w[k]);
-        s.base[k] = (int)fl + P / 2 - P + 1;
-#pragma unroll
-        for (int j = 0; j < P; ++j) {  // base + j lies in [-P, n + P): one correction wraps it
-            int m = s.base[k] + j;
-            m += (m < 0) ? D.mesh[k] : 0;
-            m -= (m >= D.mesh[k]) ? D.mesh[k] : 0;
-            s.m[k][j] = m;
-        }
+    for (int j = 0; j < P; ++j) {  // base + j lies in [-P, n + P): one correction wraps it
+        int m = base + j;
+        m += (m < 0) ? D.mesh[k] : 0;
+        m -= (m >= D.mesh[k]) ? D.mesh[k] : 0;
+        s.m[k][j] = m;
+        s.w[k][j] = w[j];
     }
-    s.coef = coef;
 }
+
 
 __device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 // i mod n for |i| within a few periods (descriptor cell offsets)
@@ -734,7 +756,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     __shared__ TrialS T;
     __shared__ RepState S;
     __shared__ int s_cnt[NPROBE_MAX * 27], s_off[NPROBE_MAX * 27 + 1], s_cell[NPROBE_MAX * 27];
+    __shared__ __align__(16) int s_list[NPROBE_MAX * 27 * LIST_PF];  // phase 2: leading entries of the probe cells
+    __shared__ uint8_t s_cmap[CAND_MAP];  // phase 3: probe-cell entry of each candidate
     __shared__ double red[100];
+    __shared__ double s_fene[4];     // FENE dE per bond slot (phase 2), summed in phase 3
+    __shared__ Moments s_mo;         // the trial's charge-moment terms (phase 4)
     __shared__ int s_npend;
     __shared__ float4 s_qjob[4];     // charge-mesh updates of the last accepted change: (x, y, z, q) out / in
     __shared__ int s_qsgn[4], s_nqjob;
@@ -901,11 +927,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                         }
                     }
                 }
-            }
-            // quorum of the launch: read off the proposing warp's path, used from the next trial on
-            if (tid == 32 && s_qin) {
-                const int started = *(volatile int*)&d.quorum_ctl[0], blocked = *(volatile int*)&d.quorum_ctl[1];
-                if (blocked > 0 && (float)blocked >= d.quorum * (float)started) s_qstop = 1;
             }
             // idle threads: store the previous trial's harvested rows, clear the shell histogram
             if (s_hv_slot >= 0) {
@@ -1145,13 +1166,33 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const int nc = (wrap1(cz + nb / 9 - 1, D.ncell[2]) * D.ncell[1] + wrap1(cy + (nb / 3) % 3 - 1, D.ncell[1])) *
                                D.ncell[0] + wrap1(cx + nb % 3 - 1, D.ncell[0]);
             s_cell[tid] = nc;
-            s_cnt[tid] = min(d.cell_count[D.cell_off + nc], D.cell_cap);
+            // the count and the cell's leading list entries in one round trip (entries past the
+            // count are stale and never read)
+            const int* row = d.cell_list + ((size_t)D.cell_off + nc) * D.cell_cap;
+            int* dst = s_list + tid * LIST_PF;
+            if (D.cell_cap >= LIST_PF && (D.cell_cap & 3) == 0) {
+                int4 v[LIST_PF / 4];
+#pragma unroll
+                for (int q = 0; q < LIST_PF / 4; ++q) v[q] = reinterpret_cast<const int4*>(row)[q];
+                s_cnt[tid] = min(d.cell_count[D.cell_off + nc], D.cell_cap);
+#pragma unroll
+                for (int q = 0; q < LIST_PF / 4; ++q) reinterpret_cast<int4*>(dst)[q] = v[q];
+            } else {
+                const int m = min(D.cell_cap, LIST_PF);
+                for (int q = 0; q < m; ++q) dst[q] = row[q];
+                s_cnt[tid] = min(d.cell_count[D.cell_off + nc], D.cell_cap);
+            }
         }
-        if (tid >= 108 && tid < 108 + T.nst) {
-            const int k = tid - 108;
-            make_stencil<P>(s_tst[k], D, T.st_pos[k], T.st_coef[k]);
+        // roles after the cell counts (threads < 108): with 256 threads each in a warp of its
+        // own, so that the branches run side by side rather than one after another in one warp
+        constexpr int ST0 = NT >= 256 ? 128 : 108, DIR = NT >= 256 ? 160 : 120, FEN0 = NT >= 256 ? 192 : 121;
+        // the trial's stencils: one thread per (stencil, axis)
+        if (tid >= ST0 && tid < ST0 + 3 * T.nst) {
+            const int k = (tid - ST0) / 3, ax = tid - ST0 - 3 * k;
+            make_stencil_axis<P>(s_tst[k], D, T.st_pos[k], ax);
+            if (ax == 0) s_tst[k].coef = T.st_coef[k];
         }
-        if (tid == 112) {
+        if (tid == DIR) {
             double dl = 0.0, dc = 0.0;
             if (T.nch == 2) {
                 const bool bonded = in_bonds(T.bonds[0], T.idx[1]);
@@ -1169,32 +1210,38 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             }
             T.d_direct_lj = dl; T.d_direct_c = dc;
         }
-        if (tid == 113) {
+        // FENE: one thread per bond slot b, over the changed particles; the four partial sums
+        // are added in slot order in phase 3
+        if (tid >= FEN0 && tid < FEN0 + 4) {
+            const int b = tid - FEN0;
             double df = 0.0;
             if (D.fene_k > 0.0f) {
-                for (int k = 0; k < T.nch; ++k) {
-                    if (!(T.pres_old[k] && T.pres_new[k])) continue;
-                    const int bl[4] = {T.bonds[k].x, T.bonds[k].y, T.bonds[k].z, T.bonds[k].w};
-                    float4 pjs[4];
+                const int nch = T.nch;
+                int jb[2];
+                float4 pjs[2];
 #pragma unroll
-                    for (int b = 0; b < 4; ++b)  // independent loads, issued together
-                        pjs[b] = (bl[b] >= 0) ? d.posq[D.slot_off + bl[b]] : make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int k = 0; k < 2; ++k) {  // independent loads, issued together
+                    const int4 bk = T.bonds[k];
+                    const int j = (b == 0) ? bk.x : (b == 1 ? bk.y : (b == 2 ? bk.z : bk.w));
+                    jb[k] = (k < nch && T.pres_old[k] && T.pres_new[k]) ? j : -1;
+                    pjs[k] = (jb[k] >= 0) ? d.posq[D.slot_off + jb[k]] : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const int j = bl[b];
-                        if (j < 0 || (T.nch == 2 && (j == T.idx[0] || j == T.idx[1]))) continue;
-                        const float4 pj = pjs[b];
-                        float dx = min_image(T.pn[k].x - pj.x, D.L[0]), dy = min_image(T.pn[k].y - pj.y, D.L[1]),
-                              dz = min_image(T.pn[k].z - pj.z, D.L[2]);
-                        const float en = fene_energy(D, dx * dx + dy * dy + dz * dz);
-                        dx = min_image(T.po[k].x - pj.x, D.L[0]); dy = min_image(T.po[k].y - pj.y, D.L[1]);
-                        dz = min_image(T.po[k].z - pj.z, D.L[2]);
-                        const float eo = fene_energy(D, dx * dx + dy * dy + dz * dz);
-                        df += (double)en - (double)eo;
-                    }
+                for (int k = 0; k < 2; ++k) {
+                    const int j = jb[k];
+                    if (j < 0 || (nch == 2 && (j == T.idx[0] || j == T.idx[1]))) continue;
+                    const float4 pj = pjs[k];
+                    const float4 pn = T.pn[k], po = T.po[k];
+                    float dx = min_image(pn.x - pj.x, D.L[0]), dy = min_image(pn.y - pj.y, D.L[1]),
+                          dz = min_image(pn.z - pj.z, D.L[2]);
+                    const float en = fene_energy(D, dx * dx + dy * dy + dz * dz);
+                    dx = min_image(po.x - pj.x, D.L[0]); dy = min_image(po.y - pj.y, D.L[1]);
+                    dz = min_image(po.z - pj.z, D.L[2]);
+                    const float eo = fene_energy(D, dx * dx + dy * dy + dz * dz);
+                    df += (double)en - (double)eo;
                 }
             }
-            T.d_fene = df;
+            s_fene[b] = df;
         }
         __syncthreads();
         mark(2);
@@ -1213,7 +1260,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 if (e < nent) s_off[e] = carry + x - v;
                 carry += __shfl_sync(0xffffffffu, x, 31);
             }
-            if (tid == 0) { s_off[nent] = carry; T.total_cand = carry; }
+            if (tid == 0) {
+                s_off[nent] = carry; T.total_cand = carry;
+                T.d_fene = ((s_fene[0] + s_fene[1]) + s_fene[2]) + s_fene[3];
+            }
+            __syncwarp();
+            // candidate -> probe-cell entry table (the pair pass reads it instead of searching)
+            for (int e = tid; e < nent; e += 32) {
+                const int b = s_off[e], en = min(s_off[e + 1], CAND_MAP);
+                for (int c = b; c < en; ++c) s_cmap[c] = (uint8_t)e;
+            }
         } else if (D.coulomb == PHMC_COUL_EWALD) {
             const int nst = T.nst, np = s_npend;
             const int npairs = nst * np + nst * (nst + 1) / 2;
@@ -1267,6 +1323,13 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             if (tn - s_rng_base >= 0 && tn - s_rng_base < 32) prefetch_primary(pf, tn, s_rng[tn - s_rng_base], D, S, d);
             else pf.valid = 0;
         }
+        // the trial's charge-moment terms (self, charged-system and slab corrections) for the
+        // decision, off the decision thread's path
+        if (tid == NT - 4) {
+            Moments mo;
+            moment_terms(T, D, S, mo);
+            s_mo = mo;
+        }
         if (tid >= NT - 3 && tid < NT - 1) {
             const int k = NT - 2 - tid;
             if (k < T.nch && T.pres_old[k]) {
@@ -1280,6 +1343,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             }
         }
         double acc_lj = 0.0, acc_c = 0.0, acc_rec = 0.0;
+        // quorum of the launch: read here, compared after the pair work (the loads' latency
+        // hides behind it), used from the next trial's proposal on
+        const bool q_chk = tid == 32 && s_qin;
+        int q_started = 0, q_blocked = 0;
+        if (q_chk) { q_started = *(volatile int*)&d.quorum_ctl[0]; q_blocked = *(volatile int*)&d.quorum_ctl[1]; }
         {
             const int total = T.total_cand;
             const int so = D.slot_off;
@@ -1293,13 +1361,20 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                     j_u[u] = -1;
                     p_u[u] = 0;
                     if (it >= total) continue;
-                    int lo = 0, hi = nent - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+                    int lo;
+                    if (it < CAND_MAP) lo = s_cmap[it];
+                    else {
+                        lo = 0;
+                        int hi = nent - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+                        }
                     }
                     p_u[u] = lo / 27;
-                    j_u[u] = d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + (it - s_off[lo])];
+                    const int k = it - s_off[lo];
+                    j_u[u] = (k < LIST_PF) ? s_list[lo * LIST_PF + k]
+                                           : d.cell_list[((size_t)D.cell_off + s_cell[lo]) * D.cell_cap + k];
                 }
                 float4 pj_u[RC];
                 int tj_u[RC];
@@ -1356,34 +1431,32 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 constexpr int PW = RR - 20;
                 constexpr int EL = (WW + 31) / 32;
                 const int warp = tid >> 5, lane = tid & 31;
-                for (int q0 = warp * PW; q0 < T.npairs; q0 += (NT / 32) * PW) {
+                const int npairs = T.npairs;
+                const int oxy = oy * ox;
+                for (int q0 = warp * PW; q0 < npairs; q0 += (NT / 32) * PW) {
                     int off[PW][EL];
                     float kk[PW][EL];
                     float g[PW][W][EL];
 #pragma unroll
                     for (int v = 0; v < PW; ++v) {
-                        const int q = min(q0 + v, T.npairs - 1);
-                        const PairK<P>& pk = s_pair[q];
+                        const PairK<P>& pk = s_pair[min(q0 + v, npairs - 1)];
 #pragma unroll
                         for (int k = 0; k < EL; ++k) {
                             const int e = min(lane + 32 * k, WW - 1);
                             const int dy = e / W, dx = e - dy * W;
                             off[v][k] = pk.f[1][dy] * ox + pk.f[0][dx];
-                            kk[v][k] = (lane + 32 * k < WW && q0 + v < T.npairs) ? pk.K[1][dy] * pk.K[0][dx] : 0.0f;
+                            kk[v][k] = (lane + 32 * k < WW && q0 + v < npairs) ? pk.K[1][dy] * pk.K[0][dx] : 0.0f;
                         }
-                        int zoff[W];  // uniform over the warp
 #pragma unroll
-                        for (int dz = 0; dz < W; ++dz) zoff[dz] = pk.f[2][dz] * oy * ox;
+                        for (int dz = 0; dz < W; ++dz) {
+                            const int zo = pk.f[2][dz] * oxy;
 #pragma unroll
-                        for (int k = 0; k < EL; ++k) {
-                            const float* Gk = G + off[v][k];
-#pragma unroll
-                            for (int dz = 0; dz < W; ++dz) g[v][dz][k] = __ldg(Gk + zoff[dz]);
+                            for (int k = 0; k < EL; ++k) g[v][dz][k] = __ldg(G + off[v][k] + zo);
                         }
                     }
 #pragma unroll
                     for (int v = 0; v < PW; ++v) {
-                        if (q0 + v >= T.npairs) continue;
+                        if (q0 + v >= npairs) continue;
                         const PairK<P>& pk = s_pair[q0 + v];
 #pragma unroll
                         for (int dz = 0; dz < W; ++dz) {
@@ -1423,12 +1496,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             }
             }
         }
+        if (q_chk && q_blocked > 0 && (float)q_blocked >= d.quorum * (float)q_started) s_qstop = 1;
         block_sum3<NT>(acc_lj, acc_c, acc_rec, red);
         mark(5);
         // ---------------- phase 5: decision and update ----------------
         if (tid == 0) {
-            Moments mo;
-            moment_terms(T, D, S, mo);
+            const Moments mo = s_mo;
             const double dQ = mo.dQ, dQ2 = mo.dQ2, dMz = mo.dMz, dS2 = mo.dS2;
             const double dself = mo.dself, dqc = mo.dqc, dslab = mo.dslab;
             const double dlj = acc_lj + T.d_direct_lj, dc = acc_c + T.d_direct_c;
@@ -1741,7 +1814,7 @@ static cudaError_t mc_dispatch(const Engine& E, F&& f) {
         case 4: MC_VARIANT(4, 4, 2) break;
         case 5:
             MC_VARIANT(5, 4, 2) MC_VARIANT(5, 2, 2) MC_VARIANT(5, 8, 2) MC_VARIANT(5, 2, 3) MC_VARIANT(5, 2, 4)
-            MC_VARIANT(5, 2, 21) MC_VARIANT(5, 2, 22) break;
+            MC_VARIANT(5, 2, 21) MC_VARIANT(5, 4, 21) break;
         default: MC_VARIANT(6, 4, 2) break;
     }
 #undef MC_VARIANT

@@ -22,7 +22,7 @@ def test_retuning_keeps_tracked_energy_consistent():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("tiles", [(-1, -1, -1, -1), (0, 2, 64, -1), (-1, 8, 256, -1), (-1, 2, -1, 4),
-                                   (0, 2, 0, 3), (-1, 2, -1, 21), (-1, 2, -1, 22)])
+                                   (0, 2, 0, 3), (-1, 2, -1, 21), (-1, 4, -1, 21)])
 def test_tuning_leaves_the_trial_stream_unchanged_on_a_short_run(tiles):
     """Same seed, different tuning and tile shapes (config 1's nz = 128: the Stockham
     z pass against the register split; pair-pass rounds of 2 and 8 candidates; 3 and 4 G
@@ -66,7 +66,7 @@ def test_autotune_keeps_the_fastest_candidate():
         assert len(zp) >= 2 and {r["zpass"] for r in zp} >= {0, 2}  # Stockham and nz = 128's default split
         assert {r["energy_block"] for r in eb} == {0, 64, 128, 256}
         assert len(grid) >= 10 and {r["cand_round"] for r in runs} == {2, 4, 8}
-        assert {(r["cand_round"], r["g_rows"]) for r in runs} >= {(2, 2), (8, 2), (2, 3), (2, 4), (2, 21), (2, 22)}
+        assert {(r["cand_round"], r["g_rows"]) for r in runs} >= {(2, 2), (8, 2), (2, 3), (2, 4), (2, 21), (4, 21)}
         t = e.tuning()
         best = min(grid, key=lambda r: r["us_per_trial"])
         assert (t["pending_max"], t["threads"]) == (best["pending_max"], best["threads"])
@@ -150,7 +150,7 @@ def test_pair_shapes_agree_on_a_config5_replica():
     reps = configs.config5(seed=2029, n_rep=256)
     s, p = min(reps, key=lambda r: r[0].n)
     logs = []
-    for shape in ((4, 2), (2, 2), (8, 2), (2, 3), (2, 4), (2, 21), (2, 22)):
+    for shape in ((4, 2), (2, 2), (8, 2), (2, 3), (2, 4), (2, 21), (4, 21)):
         with Engine(s, p) as e:
             e.set_tuning(48, 256)
             e.set_tile_shapes(cand_round=shape[0], g_rows=shape[1])
