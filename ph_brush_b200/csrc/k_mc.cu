@@ -23,6 +23,7 @@
 #include "fft.cuh"
 
 #define NST_MAX 4    // stencils per trial
+static_assert(NST_MAX <= 4, "the pair tables count a pending pair's trial stencil by three comparisons");
 #define NPROBE_MAX 4 // (old, new) states of up to two particles
 #define LIST_PF 16   // leading cell-list entries of each probe cell loaded with its count
 #define CAND_MAP 4096 // candidates whose probe-cell entry is tabulated in phase 3
@@ -1282,7 +1283,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 const Stencil<P>* sb;
                 float c;
                 if (q < nst * np) {
-                    ta = q / np; tb = q - ta * np;
+                    ta = (q >= np) + (q >= 2 * np) + (q >= 3 * np);  // q / np for nst <= NST_MAX = 4
+                    tb = q - ta * np;
                     sb = &s_pend[tb];
                     c = s_tst[ta].coef * s_pend[tb].coef;
                 } else {

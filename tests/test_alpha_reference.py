@@ -11,8 +11,11 @@ from the same std::mt19937 seed (the phase draws the reference's own stream),
 in blocks whose ends are the sampling points (pools then rebuilt in index
 order on both sides).  Per pH, alpha and the z-profiles of the protonated
 sites and of the Cl ions, from block-end snapshots, must agree within two
-standard errors (combined, from the block-to-block spread); the profiles by
-their mean height and bin by bin.
+standard errors (combined; each from its chain's block-end series by the
+blocking method, since consecutive snapshots are correlated); the profiles by
+their mean height and bin by bin.  The reference adds float atomics (its charge
+spread, its energy reductions), so its chain differs from run to run: the comparison is
+statistical on both sides.
 """
 import os
 import subprocess
@@ -72,14 +75,18 @@ def device_blocks(s, p, mu_kT, seed, height):
 
 
 def stats(blocks, key):
+    """Mean over the block-end samples and its standard error.  Consecutive samples of one
+    chain are correlated, so the error is the blocking method's (the largest naive error of
+    the series averaged over 1, 2, 4, ... samples while five or more remain), not the
+    naive one, which would understate it."""
     a = np.array([b[key] for b in blocks], np.float64)
-    return a.mean(0), a.std(0, ddof=1) / np.sqrt(len(a))
+    return a.mean(0), bench.blocking_se(a)
 
 
 def mean_height(blocks, key, height):
     centres = (np.arange(NBINS) + 0.5) * height / NBINS
     m = np.array([np.dot(b[key], centres) / max(np.sum(b[key]), 1) for b in blocks])
-    return m.mean(), m.std(ddof=1) / np.sqrt(len(m))
+    return m.mean(), float(bench.blocking_se(m[:, None])[0])
 
 
 @pytest.fixture(scope="module")
