@@ -1162,8 +1162,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         Stencil<P>* s_tst = s_pend + s_npend;  // this trial's stencils
         if (tid < nent) {
             const int p = tid / 27, nb = tid % 27;
-            const int c = T.probe_cell[p];
-            const int cx = c % D.ncell[0], cy = (c / D.ncell[0]) % D.ncell[1], cz = c / (D.ncell[0] * D.ncell[1]);
+            // the probe's cell coordinates as cell_index computes them (no integer divisions)
+            const float4 pp = T.probe_p[p];
+            const int cx = min(D.ncell[0] - 1, max(0, (int)(pp.x * D.cell_scale[0])));
+            const int cy = min(D.ncell[1] - 1, max(0, (int)(pp.y * D.cell_scale[1])));
+            const int cz = min(D.ncell[2] - 1, max(0, (int)(pp.z * D.cell_scale[2])));
             const int nc = (wrap1(cz + nb / 9 - 1, D.ncell[2]) * D.ncell[1] + wrap1(cy + (nb / 3) % 3 - 1, D.ncell[1])) *
                                D.ncell[0] + wrap1(cx + nb % 3 - 1, D.ncell[0]);
             s_cell[tid] = nc;
@@ -1426,46 +1429,65 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
             const int ox = D.oct[0], oy = D.oct[1];
             constexpr int WW = W * W;
             if constexpr (RR > 20) {
-                // one pair per warp and step (RR - 20 pairs in flight per warp): each lane takes
-                // EL elements (dy, dx) of the pair's W x W plane, so a load instruction reads
-                // about 32 / W consecutive rows of G; the lane's loads of all W z planes are in
-                // flight together; FP32 sums over the lane's EL elements, FP64 over planes
-                constexpr int PW = RR - 20;
+                // one work unit per warp and step: each lane takes EL elements (dy, dx) of the
+                // unit's W x W window plane, so a load instruction reads about 32 / W consecutive
+                // rows of G; the lane's loads of all W z planes are in flight together; FP32 sums
+                // over the lane's EL elements, FP64 over planes.  A unit is one stencil pair, or,
+                // when the trial's two stencils (a displacement's old and new charge) have the
+                // same base, both of its pairs with one pending stencil: their windows are the
+                // same G values (equal folded coordinates), read once and weighted twice
+                static_assert(RR == 21, "one unit in flight per warp");
                 constexpr int EL = (WW + 31) / 32;
                 const int warp = tid >> 5, lane = tid & 31;
-                const int npairs = T.npairs;
+                const int npairs = T.npairs, np = s_npend;
+                const bool merge = T.nst == 2 && np > 0 && s_tst[0].base[0] == s_tst[1].base[0] &&
+                                   s_tst[0].base[1] == s_tst[1].base[1] && s_tst[0].base[2] == s_tst[1].base[2];
+                const int nunit = merge ? npairs - np : npairs;
                 const int oxy = oy * ox;
-                for (int q0 = warp * PW; q0 < npairs; q0 += (NT / 32) * PW) {
-                    int off[PW][EL];
-                    float kk[PW][EL];
-                    float g[PW][W][EL];
+                for (int u = warp; u < nunit; u += NT / 32) {
+                    // pairs (trial stencil 0, pending u) and (trial stencil 1, pending u) sit at u
+                    // and np + u of the tables; the trial stencils' own pairs follow at 2 np
+                    const int qa = (merge && u >= np) ? u + np : u;
+                    const int qb = (merge && u < np) ? np + u : -1;
+                    const PairK<P>& pa = s_pair[qa];
+                    const PairK<P>& pb = s_pair[qb < 0 ? qa : qb];
+                    int off[EL];
+                    float ka[EL];
 #pragma unroll
-                    for (int v = 0; v < PW; ++v) {
-                        const PairK<P>& pk = s_pair[min(q0 + v, npairs - 1)];
+                    for (int k = 0; k < EL; ++k) {
+                        const int e = min(lane + 32 * k, WW - 1);
+                        const int dy = e / W, dx = e - dy * W;
+                        off[k] = pa.f[1][dy] * ox + pa.f[0][dx];
+                        ka[k] = (lane + 32 * k < WW) ? pa.K[1][dy] * pa.K[0][dx] : 0.0f;
+                    }
+                    float g[W][EL];
+#pragma unroll
+                    for (int dz = 0; dz < W; ++dz) {
+                        const int zo = pa.f[2][dz] * oxy;
+#pragma unroll
+                        for (int k = 0; k < EL; ++k) g[dz][k] = __ldg(G + off[k] + zo);
+                    }
+#pragma unroll
+                    for (int dz = 0; dz < W; ++dz) {
+                        float t = 0.0f;
+#pragma unroll
+                        for (int k = 0; k < EL; ++k) t = fmaf(ka[k], g[dz][k], t);
+                        acc_rec += (double)(pa.coef * pa.K[2][dz] * t);
+                    }
+                    if (qb >= 0) {
+                        float kb[EL];
 #pragma unroll
                         for (int k = 0; k < EL; ++k) {
                             const int e = min(lane + 32 * k, WW - 1);
                             const int dy = e / W, dx = e - dy * W;
-                            off[v][k] = pk.f[1][dy] * ox + pk.f[0][dx];
-                            kk[v][k] = (lane + 32 * k < WW && q0 + v < npairs) ? pk.K[1][dy] * pk.K[0][dx] : 0.0f;
+                            kb[k] = (lane + 32 * k < WW) ? pb.K[1][dy] * pb.K[0][dx] : 0.0f;
                         }
-#pragma unroll
-                        for (int dz = 0; dz < W; ++dz) {
-                            const int zo = pk.f[2][dz] * oxy;
-#pragma unroll
-                            for (int k = 0; k < EL; ++k) g[v][dz][k] = __ldg(G + off[v][k] + zo);
-                        }
-                    }
-#pragma unroll
-                    for (int v = 0; v < PW; ++v) {
-                        if (q0 + v >= npairs) continue;
-                        const PairK<P>& pk = s_pair[q0 + v];
 #pragma unroll
                         for (int dz = 0; dz < W; ++dz) {
                             float t = 0.0f;
 #pragma unroll
-                            for (int k = 0; k < EL; ++k) t = fmaf(kk[v][k], g[v][dz][k], t);
-                            acc_rec += (double)(pk.coef * pk.K[2][dz] * t);
+                            for (int k = 0; k < EL; ++k) t = fmaf(kb[k], g[dz][k], t);
+                            acc_rec += (double)(pb.coef * pb.K[2][dz] * t);
                         }
                     }
                 }
