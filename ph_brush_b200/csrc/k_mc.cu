@@ -1330,13 +1330,13 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         }
         // the trial's charge-moment terms (self, charged-system and slab corrections) for the
         // decision, off the decision thread's path
-        if (tid == NT - 4) {
+        if (tid == NT - 97) {  // (helpers on warps of their own: a warp runs divergent branches one after another)
             Moments mo;
             moment_terms(T, D, S, mo);
             s_mo = mo;
         }
-        if (tid >= NT - 3 && tid < NT - 1) {
-            const int k = NT - 2 - tid;
+        if (tid == NT - 33 || tid == NT - 65) {
+            const int k = (tid == NT - 33) ? 0 : 1;
             if (k < T.nch && T.pres_old[k]) {
                 const int gi = D.slot_off + T.idx[k];
                 const int c = cell_index(D, T.po[k].x, T.po[k].y, T.po[k].z);
