@@ -260,6 +260,55 @@ __device__ void propose(TrialS& T, const RepDesc& D, const RepState& S, const De
     }
 }
 
+// Displacement of the prefetched particle: propose() and trial_setup() for that case,
+// computed in registers from the prefetch and the trial's words and stored to the trial
+// once (the general path reads back, through shared memory, fields it has just written;
+// one thread runs this while the block waits).  Same values, field for field.
+__device__ __forceinline__ void propose_disp_setup(TrialS& T, const RepDesc& D, const Prefetch& pf, const uint32_t* rw) {
+    const uint32_t* A = rw;
+    const uint32_t* B = rw + 4;
+    const float4 po = pf.pq;
+    const int to = pf.type, fl = pf.flags;
+    const bool pold = !(fl & PHMC_F_GHOST);
+    const float dm = D.disp_max;
+    const float Lx = D.L[0], Ly = D.L[1], Lz = D.L[2];
+    const int walls = D.walls;
+    const float dx = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[2])), 1.0f));
+    const float dy = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(A[3])), 1.0f));
+    const float dz = __fmul_rn(dm, __fsub_rn(__fmul_rn(2.0f, u24(B[0])), 1.0f));
+    float nx = __fadd_rn(po.x, dx), ny = __fadd_rn(po.y, dy), nz = __fadd_rn(po.z, dz);
+    if (nx < 0.0f) nx = __fadd_rn(nx, Lx); else if (nx >= Lx) nx = __fsub_rn(nx, Lx);
+    if (ny < 0.0f) ny = __fadd_rn(ny, Ly); else if (ny >= Ly) ny = __fsub_rn(ny, Ly);
+    if (!walls) { if (nz < 0.0f) nz = __fadd_rn(nz, Lz); else if (nz >= Lz) nz = __fsub_rn(nz, Lz); }
+    const float4 pn = make_float4(nx, ny, nz, po.w);
+    const int skip = (walls && (nz < D.wall_lo || nz >= D.wall_hi)) ? 2 : 0;  // hard wall: infinite energy
+    T.ua = B[2]; T.ub = B[3];
+    T.move = PHMC_MOVE_DISP; T.skip = skip; T.nch = 1; T.logf = 0.0;
+    T.idx[0] = pf.idx; T.fo[0] = fl; T.pres_old[0] = pold;
+    T.po[0] = po; T.to[0] = to; T.bonds[0] = pf.bonds;
+    T.pres_new[0] = 1; T.pn[0] = pn; T.tn[0] = to;
+    if (skip) return;
+    int np = 0, ns = 0;
+    if (pold) {
+        T.probe_p[np] = po; T.probe_t[np] = to; T.probe_owner[np] = 0; T.probe_sign[np] = -1.0f;
+        T.probe_cell[np] = cell_index(D, po.x, po.y, po.z);
+        ++np;
+    }
+    T.probe_p[np] = pn; T.probe_t[np] = to; T.probe_owner[np] = 0; T.probe_sign[np] = 1.0f;
+    T.probe_cell[np] = cell_index(D, pn.x, pn.y, pn.z);
+    ++np;
+    if (D.coulomb == PHMC_COUL_EWALD) {
+        if (pold && po.x == pn.x && po.y == pn.y && po.z == pn.z) {
+            const float c = pn.w - po.w;
+            if (c != 0.0f) { T.st_pos[ns] = pn; T.st_coef[ns] = c; ++ns; }
+        } else {
+            if (pold && po.w != 0.0f) { T.st_pos[ns] = po; T.st_coef[ns] = -po.w; ++ns; }
+            if (pn.w != 0.0f) { T.st_pos[ns] = pn; T.st_coef[ns] = pn.w; ++ns; }
+        }
+    }
+    T.nprobe = np; T.nst = ns;
+}
+
 // External trial (phmc_delta_energy / phmc_commit / phmc_set_identity).
 __device__ void load_external(TrialS& T, const RepDesc& D, const DevPtrs& d, const phmc_trial& e) {
     const int so = D.slot_off;
@@ -715,8 +764,9 @@ __device__ int p2_decide(GcDev& G, const RepDesc& D, const RepState& S, const De
     return accept;
 }
 
+// (an atomic add whose result is unused does not wait for the line: the commit thread goes on)
 __device__ __forceinline__ void cls_add(const DevPtrs& d, const RepDesc& D, int cell, int cls, int delta) {
-    if (cls >= 0 && cell >= 0) reinterpret_cast<int*>(d.cell_cls + D.cell_off + cell)[cls] += delta;
+    if (cls >= 0 && cell >= 0) atomicAdd(reinterpret_cast<int*>(d.cell_cls + D.cell_off + cell) + cls, delta);
 }
 
 template <int NT>
@@ -861,6 +911,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 }
             }
             if (tid == 0) {
+                bool set_up = false;
                 T.stop = 0; T.desc = 0; T.da = 0;
                 if (S.error) T.stop = 1;
                 else if (GC) {
@@ -874,13 +925,21 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                         T.stop = 1; S.stop_reason = 1;
                         if (s_qin) atomicAdd(&d.quorum_ctl[1], 1);
                     } else if (s_qstop) { T.stop = 1; S.stop_reason = 2; }
-                    else { T.tnum = S.trial; propose(T, D, S, d, s_rng[S.trial - s_rng_base], pf); S.trial++; }
+                    else {
+                        T.tnum = S.trial;
+                        const uint32_t* rw = s_rng[S.trial - s_rng_base];
+                        if (pf.valid && pf.t == S.trial && pf.move == PHMC_MOVE_DISP && S.n_mobile > 0) {
+                            propose_disp_setup(T, D, pf, rw);  // the common case, set up already
+                            set_up = true;
+                        } else propose(T, D, S, d, rw, pf);
+                        S.trial++;
+                    }
                 } else {
                     if (T.ext_k >= n_ext) T.stop = 1;
                     else { load_external(T, D, d, ext[T.ext_k]); T.tnum = T.ext_k; }
                 }
                 if (!T.stop && T.skip == 0) {
-                    trial_setup(T, D);
+                    if (!set_up) trial_setup(T, D);
                     if (mode == MC_DESCRIBE) {
                         T.desc = 1; T.da = d.sur.H > 0;
                     } else if (mode == MC_RUN && (T.move == PHMC_MOVE_TITR || T.move == PHMC_MOVE_SWAP)) {
@@ -980,7 +1039,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                         cc_u[u].x = d.cell_count[D.cell_off + cell];
                     } else {
                         sl_u[u] = -1;
-                        cc_u[u] = d.cell_cls[D.cell_off + cell];
+                        cc_u[u] = __ldcg(&d.cell_cls[D.cell_off + cell]);  // (updated by L2 atomics)
                     }
                 }
 #pragma unroll
