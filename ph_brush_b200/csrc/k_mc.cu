@@ -794,7 +794,10 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
 // flight per step of the pending-correction sum (2-4: one row per work item, strided over
 // the block; 20 + w: one pair per warp, w pairs in flight, lanes over the pair's (dy, dx)
 // plane); both tuning parameters
-template <int P, int NT, bool GC, int RC = 4, int RR = 2>
+// FS: the surrogate's first stage (descriptor, network, training-sample harvest) compiled in;
+// launches that use none of it (plain Monte Carlo) take the instance without its code, whose
+// hot loop is then smaller in the instruction caches
+template <int P, int NT, bool GC, int RC = 4, int RR = 2, bool FS = true>
 __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ext_rep, const phmc_trial* __restrict__ ext, int n_ext,
                                            double* __restrict__ ext_dE, int pend_max) {
     constexpr int W = 2 * P - 1;
@@ -940,14 +943,15 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                 }
                 if (!T.stop && T.skip == 0) {
                     if (!set_up) trial_setup(T, D);
-                    if (mode == MC_DESCRIBE) {
+                    if (!FS) {
+                    } else if (mode == MC_DESCRIBE) {
                         T.desc = 1; T.da = d.sur.H > 0;
                     } else if (mode == MC_RUN && (T.move == PHMC_MOVE_TITR || T.move == PHMC_MOVE_SWAP)) {
                         // delayed acceptance (not under replay, which dictates decisions)
                         T.da = d.sur.H > 0 && !S.da_off && !(r == 0 && d.replay);
                         T.desc = T.da || d.hv_cap > 0;
                     }
-                    if (T.desc) desc_setup(T, D);
+                    if (FS && T.desc) desc_setup(T, D);
                 }
             }
         } else {
@@ -1002,7 +1006,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
         mark(0);
         if (tid == 0) { s_hv_slot = -1; s_nqjob = 0; }
         // ---------------- surrogate first stage ----------------
-        if (T.desc) {
+        if (FS && T.desc) {
             if (T.da && tid == 0) {  // stage the three hidden layers while the descriptor is built
                 sur_bulk_load(wa, d.sur.w[0], sur_layer_bytes(SUR_K, d.sur.H), &s_mbar[0]);
                 sur_bulk_load(wb, d.sur.w[1], sur_layer_bytes(d.sur.H, d.sur.H), &s_mbar[1]);
@@ -1803,13 +1807,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
 template <int P, int NT, int RC, int RR>
 static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t, int n, double* dE, cudaStream_t st) {
     DevPtrs dd = E.d;
+    if (E.first_stage_off) dd.sur.H = 0;  // surrogate attached but bypassed: every trial exact
+    // plain Monte Carlo (no network, no harvest) takes the instance without the first stage
+    const bool fs = dd.sur.H > 0 || dd.hv_cap > 0 || mode != MC_RUN;
+    auto kern = fs ? k_mc<P, NT, false, RC, RR, true> : k_mc<P, NT, false, RC, RR, false>;
     size_t smem = mc_smem_bytes(P, E.pend_max, false);
     dd.sur_late_l3 = 0;
-    if (E.first_stage_off) dd.sur.H = 0;  // surrogate attached but bypassed: every trial exact
     if (dd.sur.H > 0) {
         // three staged layers when two blocks per SM still fit, else two buffers
         cudaFuncAttributes fa;
-        cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC, RR>);
+        cudaFuncGetAttributes(&fa, kern);
         int per_sm = 0;
         cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, E.device);
         const size_t three = mc_smem_bytes(P, E.pend_max, true);
@@ -1823,7 +1830,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
     dd.quorum = 1.0f;
     if (mode == MC_RUN && E.quorum < 1.0f) {
         int per_sm = 0, nsm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc<P, NT, false, RC, RR>, NT, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
         if ((long long)per_sm * nsm >= E.R) {
             dd.quorum = E.quorum;
@@ -1831,7 +1838,7 @@ static cudaError_t launch_mc_t(Engine& E, int mode, int rep, const phmc_trial* t
             if (e != cudaSuccess) return e;
         }
     }
-    k_mc<P, NT, false, RC, RR><<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
+    kern<<<grid, NT, smem, st>>>(dd, mode, rep, t, n, dE, E.pend_max);
     return cudaGetLastError();
 }
 
@@ -1847,15 +1854,15 @@ static cudaError_t launch_mc_gc_t(Engine& E, int n_jobs, cudaStream_t st) {
     dd.sur.H = 0;
     const size_t smem = mc_smem_bytes(P, E.pend_max, false);
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, k_mc<P, 128, true>);
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_mc<P, 128, true, 4, 2, false>);
     if (e != cudaSuccess) return e;
     int optin = 0;
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
     if (e != cudaSuccess) return e;
     if (smem + fa.sharedSizeBytes > (size_t)optin) return cudaErrorInvalidValue;
-    e = cudaFuncSetAttribute(k_mc<P, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(k_mc<P, 128, true, 4, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_mc<P, 128, true><<<n_jobs, 128, smem, st>>>(dd, MC_GC, 0, nullptr, 0, nullptr, E.pend_max);
+    k_mc<P, 128, true, 4, 2, false><<<n_jobs, 128, smem, st>>>(dd, MC_GC, 0, nullptr, 0, nullptr, E.pend_max);
     return cudaGetLastError();
 }
 
@@ -1874,12 +1881,17 @@ static cudaError_t prepare_mc_t(Engine& E) {
     int optin = 0;
     cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E.device);
     if (e != cudaSuccess) return e;
-    cudaFuncAttributes fa;
-    e = cudaFuncGetAttributes(&fa, k_mc<P, NT, false, RC, RR>);
-    if (e != cudaSuccess) return e;
-    const int cap = optin - (int)fa.sharedSizeBytes;
-    if ((size_t)cap < mc_smem_bytes(P, E.pend_max, true)) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(k_mc<P, NT, false, RC, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+    for (int fs = 0; fs < 2; ++fs) {  // with and without the first stage
+        auto kern = fs ? k_mc<P, NT, false, RC, RR, true> : k_mc<P, NT, false, RC, RR, false>;
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, kern);
+        if (e != cudaSuccess) return e;
+        const int cap = optin - (int)fa.sharedSizeBytes;
+        if ((size_t)cap < mc_smem_bytes(P, E.pend_max, true)) return cudaErrorInvalidValue;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // The compiled (order, round width, G rows) variants: order 5 (the configurations' order)
