@@ -846,6 +846,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
     __shared__ int s_gc_ops, s_gc_find, s_gc_lt;
     __shared__ unsigned int s_zh[3 * PHMC_ZHIST_MAX_BINS];
 
+    // the instance without the first stage runs Monte Carlo launches only: with the mode a
+    // constant the external-trial paths drop out of its code as well
+    if constexpr (!FS && !GC) mode = MC_RUN;
     const int r = GC ? d.gc[blockIdx.x].replica : ((mode == MC_RUN) ? blockIdx.x : ext_rep);
     const int tid = threadIdx.x;
     if constexpr (GC) {
@@ -1612,7 +1615,17 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_mc(DevPtrs d, int mode, int ex
                     // delayed acceptance, second stage: the exact dE judges the surrogate's
                     // estimate (Christen & Fox 2005; the log factor cancels)
                     const double expo = T.da ? -D.beta * (dE - T.dEs) : -D.beta * dE + T.logf;
-                    accept = (expo >= 0.0) || (u53(T.ua, T.ub) < exp(expo));
+                    if (expo >= 0.0) accept = 1;
+                    else {
+                        // the FP64 exp only when the uniform lies within 1e-3 (relative) of a
+                        // float estimate, whose error is below 1e-4 for every expo < 0: the
+                        // decision is the FP64 comparison's in every case
+                        const double u = u53(T.ua, T.ub);
+                        const double ef = (double)__expf((float)expo);
+                        if (u < ef * (1.0 - 1e-3)) accept = 1;
+                        else if (u > ef * (1.0 + 1e-3)) accept = 0;
+                        else accept = u < exp(expo);
+                    }
                 }
                 if (T.da) {
                     if (accept) { S.da_acc++; S.da_wacc++; }
