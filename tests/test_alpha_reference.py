@@ -10,12 +10,15 @@ engine's grand-canonical phase with fixed_mu set, on the same input files,
 from the same std::mt19937 seed (the phase draws the reference's own stream),
 in blocks whose ends are the sampling points (pools then rebuilt in index
 order on both sides).  Per pH, alpha and the z-profiles of the protonated
-sites and of the Cl ions, from block-end snapshots, must agree within two
-standard errors (combined; each from its chain's block-end series by the
-blocking method, since consecutive snapshots are correlated); the profiles by
-their mean height and bin by bin.  The reference adds float atomics (its charge
-spread, its energy reductions), so its chain differs from run to run: the comparison is
-statistical on both sides.
+sites and of the Cl ions come from block-end snapshots, each side's standard
+error from its block-end series by the blocking method (consecutive snapshots
+are correlated).  The two chains part ways trajectory by trajectory (their
+float energies differ in the last bits, so near-threshold decisions go either
+way), so the comparison is statistical: a single comparison at two standard
+errors fails by chance about one time in twenty, and the twelve below would
+fail a correct build about half the time.  So every difference must lie
+within three standard errors, alpha's over the four pH values must pass a
+chi-square test at the 1 % level, and at most one of them may lie beyond two.
 """
 import os
 import subprocess
@@ -113,30 +116,36 @@ def runs(tmp_path_factory):
     return out
 
 
+CHI2_4_1PCT = 13.277  # chi-square with 4 degrees of freedom, upper 1 % point
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("pH", PHS)
-def test_alpha_within_two_standard_errors_of_the_reference(runs, pH):
-    ref, dev, _ = runs[pH]
-    ma, sa = stats(ref, "alpha")
-    mb, sb = stats(dev, "alpha")
-    se = float(np.hypot(sa, sb))
-    assert abs(ma - mb) <= 2 * se + 1e-12, (pH, ma, mb, se)
+def test_alpha_agrees_with_the_reference(runs):
+    z = []
+    for pH in PHS:
+        ref, dev, _ = runs[pH]
+        ma, sa = stats(ref, "alpha")
+        mb, sb = stats(dev, "alpha")
+        z.append(float((ma - mb) / np.hypot(sa, sb)))
+    z = np.array(z)
+    assert np.all(np.abs(z) <= 3.0), dict(zip(PHS, z))
+    assert float(np.sum(z ** 2)) <= CHI2_4_1PCT, dict(zip(PHS, z))
+    assert int(np.sum(np.abs(z) > 2.0)) <= 1, dict(zip(PHS, z))
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("pH", PHS)
-def test_z_profiles_within_two_standard_errors_of_the_reference(runs, pH):
+def test_z_profiles_agree_with_the_reference(runs, pH):
     ref, dev, height = runs[pH]
     for key in ("sites", "cl"):
         ha, ea = mean_height(ref, key, height)
         hb, eb = mean_height(dev, key, height)
-        assert abs(ha - hb) <= 2 * np.hypot(ea, eb) + 1e-9, (pH, key, ha, hb)
+        assert abs(ha - hb) <= 3 * np.hypot(ea, eb) + 1e-9, (pH, key, ha, hb, ea, eb)
         ma, sa = stats(ref, key)
         mb, sb = stats(dev, key)
         se = np.hypot(sa, sb)
         occupied = (ma + mb) > 0
-        within = np.abs(ma - mb)[occupied] <= 2 * se[occupied] + 1e-9
-        assert within.mean() >= 0.85, (pH, key, ma, mb, se)
+        assert np.all(np.abs(ma - mb)[occupied] <= 3 * se[occupied] + 1e-9), (pH, key, ma, mb, se)
 
 
 @pytest.mark.gpu
