@@ -21,8 +21,9 @@ struct Engine {
     int threads = 256;
     int pend_max = 16;
     int cand_round = 4;          // pair pass: candidates per thread per round (2, 4, 8 at order 5)
-    int g_rows = 2;              // pending-correction sum: G rows in flight per thread (2, 3, 4 with round 2)
-    int energy_block = 128;      // full recompute: particles per block of the pair / FENE pass
+    int g_rows = 2;              // pending-correction sum: G rows in flight per thread (2; 3, 4 with round
+                                 // width 2), or 21: one unit of stencil pairs per warp (round width 2 or 4)
+    int energy_block = 128;      // full recompute: particles per block of the pair / FENE pass (0: cell order)
     bool first_stage_off = false;  // the attached surrogate's first stage bypassed (cost-based fallback)
     bool fwd_pipe = false;       // the rebuild's first pass pipelined (persistent blocks, bulk-copied planes)
     int nsm = 0;                 // the device's SM count
