@@ -126,6 +126,8 @@ def parse():
     ap.add_argument("--da-threshold", type=float, default=0.3)
     ap.add_argument("--tuning", default=None, help="pending_max,threads[,cand_round,g_rows,zpass,plane_pipe,first_stage] "
                                                     "instead of the autotuner (for profiling)")
+    ap.add_argument("--quorum", type=float, default=None,
+                    help="launch quorum of blocked replicas (default: the engine's, 0.2; for sweeps)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline only (plain comparison, phases, alpha skipped)")
@@ -239,6 +241,8 @@ def barrier(world):
 def tune_engine(eng, args, trials):
     """Autotune, or apply --tuning pending_max,threads[,cand_round,g_rows,zpass,plane_pipe,first_stage]
     (fixed shapes for profiling commands; -1 keeps a field)."""
+    if getattr(args, "quorum", None) is not None:
+        eng.set_quorum(args.quorum)
     if args.tuning:
         v = [int(x) for x in args.tuning.split(",")]
         eng.set_tuning(v[0], v[1])
